@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark: leaf-cell RK3 updates/s on the four-quadrant Riemann workload.
+
+One step = one solute iteration (step control + 3 SSP-RK3 stages + ghost
+fill) over every interior leaf.  Workload: four-quadrant Riemann problem on
+[0,1]^2, base grid 128^2 (134^2 with ghosts), 4 refinement levels, the cells
+within 0.2/0.15/0.1/0.05 of the quadrant split lines refined to levels
+1/2/3/4 (about 1.0M leaves); synthetic state (the config's initial
+condition).  The state (~1.1 GB with tables) is far larger than L2, and L2
+is also flushed before every timed step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): one independent instance per rank (weak scaling, no
+collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from fdm_cell_based_amr_cartesian_b200 import params as P  # noqa: E402
+
+METRIC = "leaf-cell RK3 updates/s"
+UNIT = "updates/s"
+BAND = [0.2, 0.15, 0.1, 0.05]
+FLOPS_PER_FACE = 1233          # IEEE FP64 ops of one face flux (add/mul/div/sqrt/min)
+FLOPS_PER_CELL = 150           # residual, conversions and RK blend per leaf and stage
+BYTES_PER_UPDATE = 256         # 8 x 32-byte (rho,u,v,p) transfers per leaf per RK3 step
+
+
+def workload():
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+    cfg = P.riemann4(base=128, lvl_amr=4)
+    keys = S.distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], BAND)
+    prim = S.initial_state(cfg, keys)
+    return cfg, keys, prim
+
+
+def workload_desc(n_leaves, n_interior):
+    return {"workload": "riemann4 four-quadrant, base 128x128, 4 levels, distance-refined bands "
+                        "0.2/0.15/0.1/0.05 around the split lines",
+            "leaves": int(n_leaves), "interior_leaves": int(n_interior),
+            "l2": "flushed before every timed step (256 MiB write); state > L2"}
+
+
+# ------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def profile_traffic():
+    """DRAM bytes per face-kernel launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "face_flux_riemann4.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------ CPU legs
+def cpu_sample(cfg, keys, prim, lam, tstep, steps):
+    """Time the oracle (the CPU restatement of the reference OpenMP path) on
+    the same mesh: `steps` RK3 steps, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    o = oracle.Oracle(cfg, initial=False)
+    o.set_leaves(keys, prim)
+    o.set_scalars(lam[0], lam[1], tstep, 0.0, 1)
+    n_int = o.num_interior()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.time_advance_rk()
+    dt = time.perf_counter() - t0
+    o.close()
+    return n_int, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg, keys, prim = workload()
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    # lambda of the initial state (the GPU arm's first step control gives the same)
+    r, u, v, p = prim[:, 0], prim[:, 1], prim[:, 2], prim[:, 3]
+    c = np.sqrt(cfg.params.gama * p / r)
+    lam = (float(np.max(np.abs(u) + c)), float(np.max(np.abs(v) + c)))
+    o = oracle.Oracle(cfg, initial=False, threads=threads)
+    o.set_leaves(keys, prim)
+    o.set_scalars(lam[0], lam[1], 1e-5, 0.0, 1)
+    n_int = o.num_interior()
+    per = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        o.time_advance_rk()
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            per.append(dt)
+        if sum(per) > 150:
+            break
+    o.close()
+    total = sum(per)
+    value = n_int * len(per) / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": len(per), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(per),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_desc(len(keys), n_int),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{len(per)} RK3 steps of the full mesh, OpenMP restatement of "
+                                       "Time_advance_RK (no Fortran compiler on the box)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    cfg, keys, prim = workload()
+    g = S.Solver(cfg)
+    g.upload(keys, prim)
+    g.body_boundary(1)
+    g.step_control()
+    cnt = g.counters()
+    NI = cnt["n_interior"]
+    stream_ptr, _, _ = g.device_state()
+    ext = torch.cuda.ExternalStream(stream_ptr)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # warm-up (also captures the step graph)
+    for _ in range(args.warmup):
+        g.advance(1)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(ext):
+            for k in range(args.steps):
+                flush.zero_()
+                ev[k][0].record(ext)
+                g.advance(1)
+                ev[k][1].record(ext)
+        torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = NI * world * args.steps / (ms / 1e3)
+    clocks = clk.summary()
+
+    # per-kernel times (CUDA events on the handle's stream) -> roofline
+    kt = g.time_kernels(reps=10)
+    nfaces = cnt["n_faces_x"] + cnt["n_faces_y"]
+    face_bytes = (cnt["n_leaves"] + cnt["n_wls_requests"] + cnt["n_restrict_requests"]) * 32 + nfaces * 32
+    face_gbs = face_bytes / (kt["faces"] * 1e-3) / 1e9
+    peaks = measured_peaks()
+    hbm_peak = peaks["hbm_gbs"] if peaks else 6650.0
+    fp64_peak = S.fp64_peak_tflops()
+    face_tflops = nfaces * FLOPS_PER_FACE / (kt["faces"] * 1e-3) / 1e12
+    step_bytes = NI * BYTES_PER_UPDATE
+    step_gbs = step_bytes / (ms / args.steps * 1e-3) / 1e9
+    traffic = profile_traffic()
+
+    # end-to-end through the public API with host buffers
+    e2e = None
+    if True:
+        host_in = torch.empty((len(keys), 4), dtype=torch.float64, pin_memory=True)
+        host_in.numpy()[:] = g.leaves()[1]
+        t0 = time.perf_counter()
+        n_e2e = max(3, min(args.steps, 10))
+        for _ in range(n_e2e):
+            g.set_values(host_in.numpy())
+            g.advance(1)
+            _, out = g.leaves()
+        e2e_s = time.perf_counter() - t0
+        e2e = {"value": NI * world * n_e2e / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(len(keys) * 32), "d2h_bytes_per_step": int(len(keys) * 40)}
+
+    launches_per_step = 1 + 1 + 1 + 3 * (2 + 2 + (1 if cnt["n_wls_requests"] + cnt["n_restrict_requests"] else 0)
+                                          + (1 if cnt["n_ghost"] else 0))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        sc = g.scalars()
+        n_int, dt = cpu_sample(cfg, keys, prim, (sc["lambda_x"], sc["lambda_y"]), sc["tstep"], args.cpu_steps)
+        cpu = {"value": n_int * args.cpu_steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_steps} RK3 step(s) of the same mesh, OpenMP restatement of Time_advance_RK"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_desc(len(keys), NI),
+                "roofline": {"bound": "hbm", "achieved": face_gbs, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": face_gbs / hbm_peak, "traffic": traffic,
+                             "kernel": "k_faces (x+y)", "ms_per_launch": kt["faces"],
+                             "peak_source": "measured" if peaks else "fallback"},
+                "roofline_fp64": {"achieved": face_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                                  "frac": face_tflops / fp64_peak, "flops_per_face": FLOPS_PER_FACE,
+                                  "peak_source": "measured DFMA probe"},
+                "step_hbm": {"algorithmic_bytes_per_update": BYTES_PER_UPDATE, "achieved_gbs": step_gbs,
+                             "frac": step_gbs / hbm_peak},
+                "kernel_ms": kt, "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+                "counters": cnt, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    g.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

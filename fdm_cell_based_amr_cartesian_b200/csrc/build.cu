@@ -1,0 +1,756 @@
+// build.cu — device construction of the leaf order, neighbour, stencil,
+// hanging-node and ghost tables of a leaf set.
+//
+// Replaces, for the GPU path, what the reference rebuilds after every
+// change of the tree: idneighbor (src/neighbor.F90:399-449), the leaf lists
+// of IDgrid (src/solution.F90:593-693), and the per-call stencil search of
+// parent_value_weno / child_value_weno / search_cell_5 / WLSI_US_WENO's
+// geometry (src/XuanGua.F90:45-356), which the reference redoes inside
+// every stage for every hanging face.
+#include <cub/cub.cuh>
+
+#include "handle.cuh"
+#include "topo.cuh"
+
+namespace fdm {
+
+#define FDM_ATAN_BIAS 1.000000013351432e-10   /* REAL(4) 1e-10, src/XuanGua.F90:40 */
+#define FDM_PI_REF 3.1415926535897932
+
+enum BuildErr { BE_PARTITION = 0, BE_NULLNB = 1, BE_OVERFLOW = 2, BE_ROOT = 3, BE_LEVEL = 4 };
+
+static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+// get_direction (src/XuanGua.F90:33-43): 45-degree sector 1..8 (1 = east,
+// counter-clockwise) of (xx,yy) seen from (x,y).
+__device__ __forceinline__ int get_direction(double xx, double yy, double x, double y) {
+    const double dx = xx - x;
+    const double dy = yy - y;
+    const double angle = (atan2(dy, dx) + FDM_ATAN_BIAS) * 180.0 / FDM_PI_REF;
+    const int f = (int)floor((angle + 22.5) / 45.0 + 8);
+    return ((f % 8) + 8) % 8 + 1;
+}
+
+// ------------------------------------------------------------ classify
+__global__ void k_classify(const uint64_t *__restrict__ lkey, int64_t NL, Geometry G,
+                           int32_t *fI, int32_t *fG, int32_t *fC, int8_t *cross, int32_t *err) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    const int64_t total = (int64_t)G.m * G.n;
+    const uint64_t key = lkey[k];
+    const int lvl = (int)(key & 15u);
+    const int64_t root = (int64_t)(key >> 34);
+    const uint64_t pos = key_pos(key);
+    if (root >= total) { atomicExch(err + BE_ROOT, 1); return; }
+    if (lvl >= MAXLVL_TAB - 1) atomicExch(err + BE_LEVEL, 1);
+    if (pos & (span_of_level(lvl) - 1)) atomicExch(err + BE_PARTITION, 1);
+    const uint64_t prev_end = k == 0 ? 0ull : key_pos(lkey[k - 1]) + span_of_level((int)(lkey[k - 1] & 15u));
+    if (pos != prev_end) atomicExch(err + BE_PARTITION, 1);
+    if (k == NL - 1 && pos + span_of_level(lvl) != ((uint64_t)total << 30)) atomicExch(err + BE_PARTITION, 1);
+    const int c = root_cross(G, root);
+    cross[k] = (int8_t)c;
+    fI[k] = c == 0;
+    fC[k] = c == -5;
+    fG[k] = (c != 0 && c != -5);
+}
+
+__global__ void k_slots(int64_t NL, int64_t NI, int64_t NG, const int32_t *fI, const int32_t *fG,
+                        const int32_t *sI, const int32_t *sG, const int32_t *sC, int32_t *lslot,
+                        int32_t *slot_leaf) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    const int32_t s = fI[k] ? sI[k] : fG[k] ? (int32_t)(NI + sG[k]) : (int32_t)(NI + NG + sC[k]);
+    lslot[k] = s;
+    slot_leaf[s] = (int32_t)k;
+}
+
+__global__ void k_scatter(int64_t NL, const int32_t *perm, const int32_t *lslot,
+                          const double *__restrict__ prim, double4 *B0) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    const int64_t src = perm[k];
+    B0[lslot[k]] = make_double4(prim[4 * src], prim[4 * src + 1], prim[4 * src + 2], prim[4 * src + 3]);
+}
+
+__global__ void k_centers(int64_t NL, const uint64_t *lkey, Geometry G, double *cx, double *cy) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    double x, y;
+    node_center(G, node_of_key(lkey[k]), x, y);
+    cx[k] = x;
+    cy[k] = y;
+}
+
+// ------------------------------------------------------- stencil resolve
+// Tip/Tim/Tjp/Tjm and Tipp/Timm/Tjpp/Tjmm (src/XuanGua.F90:401-590):
+// each of the 8 stencil entries of an interior leaf is either a same-level
+// leaf (its slot) or a request: parent_value_weno on a same-level internal
+// node, or child_value_weno on a coarser leaf at a target point.
+struct ResolveOut {
+    int32_t *slot;    // >= 0 direct slot, -1 request
+    int32_t *kind;    // 0 parent, 1 child
+    int64_t *ref;     // parent: node key; child: sorted leaf index
+    double *tx, *ty;  // target point
+};
+
+__device__ __forceinline__ void target_point(const Geometry &G, double cx, double cy, int lvl, int dir,
+                                             int k2, double &xx, double &yy) {
+    if (k2 == 1) {
+        switch (dir) {
+            case DIR_RIGHT: xx = cx + G.xf * G.h / ipow2d(lvl); yy = cy; break;
+            case DIR_LEFT: xx = cx - G.xf * G.h / ipow2d(lvl); yy = cy; break;
+            case DIR_UP: xx = cx; yy = cy + G.h / ipow2d(lvl); break;
+            default: xx = cx; yy = cy - G.h / ipow2d(lvl); break;
+        }
+    } else {
+        switch (dir) {
+            case DIR_RIGHT: xx = cx + 2.0 * G.xf * G.h / ipow2d(lvl); yy = cy; break;
+            case DIR_LEFT: xx = cx - 2.0 * G.xf * G.h / ipow2d(lvl); yy = cy; break;
+            case DIR_UP: xx = cx; yy = cy + 2.0 * G.h / ipow2d(lvl); break;
+            default: xx = cx; yy = cy - 2.0 * G.h / ipow2d(lvl); break;
+        }
+    }
+}
+
+__global__ void k_resolve(Tables T, Geometry G, ResolveOut O, uint8_t *ilvl, int32_t *err) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= T.NI) return;
+    const int32_t k = T.slot_leaf[i];
+    NodeRef c;
+    c.n = node_of_key(T.lkey[k]);
+    c.leaf = k;
+    c.valid = 1;
+    ilvl[i] = (uint8_t)c.n.lvl;
+    const double cx = T.lcx[k], cy = T.lcy[k];
+    const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
+    for (int q = 0; q < 4; ++q) {
+        const int d = dirs[q];
+        const NodeRef cn = face_nb(T, G, c, d);
+        if (!cn.valid) { atomicExch(err + BE_NULLNB, 1); return; }
+        // T1
+        int64_t e = i * 8 + q;
+        if (cn.n.lvl == c.n.lvl) {
+            if (cn.leaf >= 0) O.slot[e] = T.lslot[cn.leaf];
+            else { O.slot[e] = -1; O.kind[e] = 0; O.ref[e] = (int64_t)node_key(cn.n); }
+        } else {
+            O.slot[e] = -1; O.kind[e] = 1; O.ref[e] = cn.leaf;
+            target_point(G, cx, cy, c.n.lvl, d, 1, O.tx[e], O.ty[e]);
+        }
+        // T2
+        e = i * 8 + 4 + q;
+        if (cn.n.lvl == c.n.lvl) {
+            const NodeRef cnn = face_nb(T, G, cn, d);
+            if (!cnn.valid) { atomicExch(err + BE_NULLNB, 1); return; }
+            if (cnn.n.lvl == cn.n.lvl) {
+                if (cnn.leaf >= 0) O.slot[e] = T.lslot[cnn.leaf];
+                else { O.slot[e] = -1; O.kind[e] = 0; O.ref[e] = (int64_t)node_key(cnn.n); }
+            } else {
+                O.slot[e] = -1; O.kind[e] = 1; O.ref[e] = cnn.leaf;
+                target_point(G, cx, cy, c.n.lvl, d, 2, O.tx[e], O.ty[e]);
+            }
+        } else {
+            O.slot[e] = -1; O.kind[e] = 1; O.ref[e] = cn.leaf;
+            target_point(G, cx, cy, c.n.lvl, d, 2, O.tx[e], O.ty[e]);
+        }
+    }
+}
+
+__global__ void k_req_flags(int64_t n, const int32_t *slot, int32_t *flag) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    flag[e] = slot[e] < 0;
+}
+
+struct ReqDesc {
+    int32_t *kind;
+    int64_t *ref;
+    double *tx, *ty;
+};
+
+__global__ void k_emit(int64_t n, int64_t VS0, ResolveOut O, const int32_t *ridx, int32_t *ist, ReqDesc R) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int32_t s = O.slot[e];
+    if (s >= 0) { ist[e] = s; return; }
+    const int32_t r = ridx[e];
+    ist[e] = (int32_t)(VS0 + r);
+    R.kind[r] = O.kind[e];
+    R.ref[r] = O.ref[e];
+    R.tx[r] = O.tx[e];
+    R.ty[r] = O.ty[e];
+}
+
+// ---------------------------------------------------------- WLS gather
+struct Gather {
+    int32_t m1, m2;
+    int32_t n1[WLS_MAXM], n2[WLS_MAXM];  // sorted leaf indices
+    bool used[8];
+    int32_t overflow;
+};
+
+__device__ __forceinline__ void g_add(Gather &g, int32_t leaf, int dir) {
+    g.used[dir - 1] = true;
+    const bool axis = (dir == 1 || dir == 3 || dir == 5 || dir == 7);
+    if (axis) {
+        for (int t = 0; t < g.m1; ++t) if (g.n1[t] == leaf) return;
+        if (g.m1 >= WLS_MAXM) { g.overflow = 1; return; }
+        g.n1[g.m1++] = leaf;
+    } else {
+        for (int t = 0; t < g.m2; ++t) if (g.n2[t] == leaf) return;
+        if (g.m2 >= WLS_MAXM) { g.overflow = 1; return; }
+        g.n2[g.m2++] = leaf;
+    }
+}
+
+// search_cell_5 (src/XuanGua.F90:152-177) on a node: its leaves in DFS
+// order son1, son2, son3, son4; the first leaf of every still-unused
+// sector joins the stencil.  The DFS rank of a leaf is its Morton path with
+// each digit mapped 0,1,2,3 -> 0,1,3,2 (son1, son2, son4, son3).
+__device__ void g_search(const Tables &T, const NodeRef &X, double x, double y, Gather &g) {
+    if (!X.valid) return;
+    if (X.leaf >= 0) {
+        const int dir = get_direction(T.lcx[X.leaf], T.lcy[X.leaf], x, y);
+        if (!g.used[dir - 1]) g_add(g, X.leaf, dir);
+        return;
+    }
+    const uint64_t p0 = node_pos(X.n);
+    const int64_t lo = lower_bound_pos(T.lkey, T.NL, p0);
+    const int64_t hi = lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(X.n.lvl));
+    uint64_t best_rank[8];
+    int32_t best_leaf[8];
+    for (int s = 0; s < 8; ++s) { best_rank[s] = ~0ull; best_leaf[s] = -1; }
+    for (int64_t k = lo; k < hi; ++k) {
+        const int dir = get_direction(T.lcx[k], T.lcy[k], x, y);
+        if (g.used[dir - 1]) continue;
+        const uint64_t path = key_pos(T.lkey[k]) & ((1ull << 30) - 1ull);
+        const uint64_t rank = path ^ ((path & 0x2AAAAAAAull) >> 1);
+        if (rank < best_rank[dir - 1]) { best_rank[dir - 1] = rank; best_leaf[dir - 1] = (int32_t)k; }
+    }
+    for (;;) {
+        int bs = -1;
+        uint64_t br = ~0ull;
+        for (int s = 0; s < 8; ++s)
+            if (best_leaf[s] >= 0 && best_rank[s] < br) { br = best_rank[s]; bs = s; }
+        if (bs < 0) break;
+        g_add(g, best_leaf[bs], bs + 1);
+        best_leaf[bs] = -1;
+    }
+}
+
+// brinv (src/XuanGua.F90:593-660): full-pivot Gauss-Jordan in place;
+// returns false on the singular test (the partially reduced matrix stays).
+template <int N>
+__device__ bool brinv_dev(double *r) {
+    int is[N], js[N];
+    for (int k = 0; k < N; ++k) { is[k] = 0; js[k] = 0; }
+    for (int k = 0; k < N; ++k) {
+        double d = 0.0;
+        for (int i = k; i < N; ++i)
+            for (int j = k; j < N; ++j)
+                if (fabs(r[i * N + j]) > d) { d = fabs(r[i * N + j]); is[k] = i; js[k] = j; }
+        if (d + 1.0 == 1.0) return false;
+        for (int j = 0; j < N; ++j) { double t = r[k * N + j]; r[k * N + j] = r[is[k] * N + j]; r[is[k] * N + j] = t; }
+        for (int i = 0; i < N; ++i) { double t = r[i * N + k]; r[i * N + k] = r[i * N + js[k]]; r[i * N + js[k]] = t; }
+        r[k * N + k] = 1.0 / r[k * N + k];
+        for (int j = 0; j < N; ++j) if (j != k) r[k * N + j] = r[k * N + j] * r[k * N + k];
+        for (int i = 0; i < N; ++i)
+            if (i != k)
+                for (int j = 0; j < N; ++j)
+                    if (j != k) r[i * N + j] = r[i * N + j] - r[i * N + k] * r[k * N + j];
+        for (int i = 0; i < N; ++i) if (i != k) r[i * N + k] = -r[i * N + k] * r[k * N + k];
+    }
+    for (int k = N - 1; k >= 0; --k) {
+        for (int j = 0; j < N; ++j) { double t = r[k * N + j]; r[k * N + j] = r[js[k] * N + j]; r[js[k] * N + j] = t; }
+        for (int i = 0; i < N; ++i) { double t = r[i * N + k]; r[i * N + k] = r[i * N + is[k]]; r[i * N + is[k]] = t; }
+    }
+    return true;
+}
+
+struct ReqOut {
+    int32_t *kind;
+    int32_t *m;
+    int32_t *mem;
+    double *geo;
+    unsigned long long *counts;   // [0] singular, [1] wls, [2] restrict, [3] copy
+};
+
+// One hanging-node request: stencil gather of parent_value_weno /
+// child_value_weno (src/XuanGua.F90:45-150), then either the WLS geometry
+// (P^T W P and its three brinv inverses, src/XuanGua.F90:206-255) or the
+// reference's fallback when fewer than 7 points were found.
+__global__ void k_gather(Tables T, Geometry G, ReqDesc D, ReqOut O, int32_t *err) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= T.NR) return;
+    Gather g;
+    g.m1 = 0; g.m2 = 0; g.overflow = 0;
+    for (int s = 0; s < 8; ++s) g.used[s] = false;
+    NodeRef c;
+    double x, y, xx, yy;
+    int32_t *mem = O.mem + r * WLS_MAXM;
+    double *geo = O.geo + r * RQ_GEO;
+    if (D.kind[r] == 0) {
+        // parent_value_weno on the internal node
+        c.n = node_of_key((uint64_t)D.ref[r]);
+        c.leaf = -1;
+        c.valid = 1;
+        node_center(G, c.n, x, y);
+        xx = x; yy = y;
+        const int qs[4] = {0, 1, 3, 2};
+        for (int t = 0; t < 4; ++t) g_search(T, child_ref(T, c, qs[t]), x, y, g);
+        if (g.m1 + g.m2 < 8) {
+            g_search(T, face_nb(T, G, c, DIR_LEFT), x, y, g);
+            g_search(T, face_nb(T, G, c, DIR_RIGHT), x, y, g);
+            g_search(T, face_nb(T, G, c, DIR_DOWN), x, y, g);
+            g_search(T, face_nb(T, G, c, DIR_UP), x, y, g);
+        }
+        if (g.m1 + g.m2 < 7) {
+            const uint64_t p0 = node_pos(c.n);
+            O.kind[r] = RQ_RESTRICT;
+            O.m[2 * r] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0);
+            O.m[2 * r + 1] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(c.n.lvl));
+            geo[G_LVL] = (double)c.n.lvl;
+            atomicAdd(O.counts + 2, 1ull);
+            return;
+        }
+    } else {
+        // child_value_weno on the coarse leaf at the target point
+        const int32_t L = (int32_t)D.ref[r];
+        c.n = node_of_key(T.lkey[L]);
+        c.leaf = L;
+        c.valid = 1;
+        x = T.lcx[L]; y = T.lcy[L];
+        xx = D.tx[r]; yy = D.ty[r];
+        g.n1[g.m1++] = L;
+        const bool diag = root_cross(G, c.n.root) >= 0;
+        const NodeRef nul = null_ref();
+        g_search(T, diag ? downleft_nb(T, G, c) : nul, x, y, g);
+        g_search(T, face_nb(T, G, c, DIR_LEFT), x, y, g);
+        g_search(T, diag ? upleft_nb(T, G, c) : nul, x, y, g);
+        g_search(T, face_nb(T, G, c, DIR_DOWN), x, y, g);
+        g_search(T, face_nb(T, G, c, DIR_UP), x, y, g);
+        g_search(T, diag ? downright_nb(T, G, c) : nul, x, y, g);
+        g_search(T, face_nb(T, G, c, DIR_RIGHT), x, y, g);
+        g_search(T, diag ? upright_nb(T, G, c) : nul, x, y, g);
+        if (g.m1 + g.m2 < 7) {
+            O.kind[r] = RQ_COPY;
+            mem[0] = T.lslot[L];
+            O.m[2 * r] = 1;
+            O.m[2 * r + 1] = 0;
+            atomicAdd(O.counts + 3, 1ull);
+            return;
+        }
+    }
+    if (g.overflow) atomicExch(err + BE_OVERFLOW, 1);
+    // WLSI_US_WENO geometry
+    const int m1 = g.m1, m2 = g.m2, m = m1 + m2;
+    O.kind[r] = RQ_WLS;
+    O.m[2 * r] = m1;
+    O.m[2 * r + 1] = m2;
+    double *gx = geo + G_X, *gy = geo + G_Y, *gw = geo + G_W;
+    for (int i = 0; i < m; ++i) {
+        const int32_t leaf = i < m1 ? g.n1[i] : g.n2[i - m1];
+        mem[i] = T.lslot[leaf];
+        const double xi = T.lcx[leaf], yi = T.lcy[leaf];
+        gx[i] = xi;
+        gy[i] = yi;
+        const double d = sqrt((xi - xx) * (xi - xx) + (yi - yy) * (yi - yy));
+        gw[i] = 1.0 / (d + 1.e-6);
+    }
+    geo[G_XX] = xx;
+    geo[G_YY] = yy;
+    double P[WLS_MAXM][6];
+    for (int i = 0; i < m; ++i) {
+        P[i][0] = 1.0; P[i][1] = gx[i]; P[i][2] = gy[i];
+        P[i][3] = gx[i] * gy[i]; P[i][4] = gx[i] * gx[i]; P[i][5] = gy[i] * gy[i];
+    }
+    double *L = geo + G_L, *A = geo + G_A, *B = geo + G_B;
+    for (int a = 0; a < 6; ++a)
+        for (int b = 0; b < 6; ++b) {
+            double s = 0.0;
+            for (int i = 0; i < m; ++i) s = s + P[i][a] * (gw[i] * P[i][b]);
+            L[a * 6 + b] = s;
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double s = 0.0, t = 0.0;
+            for (int i = 0; i < m1; ++i) s = s + P[i][a] * (gw[i] * P[i][b]);
+            for (int i = m1; i < m; ++i) t = t + P[i][a] * (gw[i] * P[i][b]);
+            A[a * 3 + b] = s;
+            B[a * 3 + b] = t;
+        }
+    unsigned long long ns = 0;
+    if (!brinv_dev<6>(L)) ++ns;
+    if (!brinv_dev<3>(A)) ++ns;
+    if (!brinv_dev<3>(B)) ++ns;
+    if (ns) atomicAdd(O.counts + 0, ns);
+    atomicAdd(O.counts + 1, 1ull);
+    // smoothness box of the node (compute_smoothness, src/XuanGua.F90:318-323)
+    double ncx, ncy;
+    node_center(G, c.n, ncx, ncy);
+    if (c.leaf >= 0) { ncx = T.lcx[c.leaf]; ncy = T.lcy[c.leaf]; }
+    const double hx = G.xf * G.h / ipow2d(c.n.lvl + 1);
+    const double hy = G.h / ipow2d(c.n.lvl + 1);
+    geo[G_BOX + 0] = ncx - hx;
+    geo[G_BOX + 1] = ncx + hx;
+    geo[G_BOX + 2] = ncy - hy;
+    geo[G_BOX + 3] = ncy + hy;
+}
+
+// ------------------------------------------------------------- ghosts
+struct GhostOut {
+    int32_t *kind, *a, *b, *flip;
+    double *x, *y;
+};
+
+__device__ __forceinline__ void ghost_from_ref(const Tables &T, const NodeRef &img, GhostOut &O, int64_t g) {
+    if (img.leaf >= 0) {
+        O.kind[g] = GH_COPY;
+        O.a[g] = T.lslot[img.leaf];
+        O.b[g] = 0;
+    } else {
+        const uint64_t p0 = node_pos(img.n);
+        O.kind[g] = GH_RESTRICT;
+        O.a[g] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0);
+        O.b[g] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(img.n.lvl));
+    }
+}
+
+// image node for the extension kinds: root (row1, col1) 1-based, descent along
+// the ghost's path from the root with the quadrant bits transformed
+// (mode 0 keep, 1 force x, 2 force y, 3 mirror y, 4 mirror x)
+__device__ NodeRef ext_image(const Tables &T, const Geometry &G, const Node &gn, int row1, int col1,
+                             int mode, int bit) {
+    Node r0;
+    r0.root = (int64_t)(row1 - 1) * G.m + (col1 - 1);
+    r0.lvl = 0; r0.ix = 0; r0.iy = 0;
+    NodeRef cur = resolve(T, r0);
+    for (int j = 1; j <= gn.lvl; ++j) {
+        if (cur.leaf >= 0) break;
+        int q = (int)(((gn.ix >> (gn.lvl - j)) & 1u) | (((gn.iy >> (gn.lvl - j)) & 1u) << 1));
+        if (mode == 1) q = (q & 2) | bit;
+        else if (mode == 2) q = (q & 1) | (bit << 1);
+        else if (mode == 3) q ^= 2;
+        else if (mode == 4) q ^= 1;
+        cur = child_ref(T, cur, q);
+    }
+    return cur;
+}
+
+__global__ void k_ghosts(Tables T, Geometry G, fdm_params P, GhostOut O) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= T.NG) return;
+    const int32_t k = T.slot_leaf[T.NI + g];
+    const Node gn = node_of_key(T.lkey[k]);
+    const int a = root_cross(G, gn.root);
+    const int row = (int)(gn.root / G.m) + 1, col = (int)(gn.root % G.m) + 1;
+    const int m = G.m, n = G.n;
+    int kind;
+    if (a == -4) kind = P.kind_xmbc;
+    else if (a == -2) kind = P.kind_xpbc;
+    else if (a == -3) kind = P.kind_ypbc;
+    else kind = P.kind_ymbc;
+    O.flip[g] = 0;
+    O.x[g] = T.lcx[k];
+    O.y[g] = T.lcy[k];
+    if (kind == FDM_BC_PERIODIC) {
+        // BC_cyc (src/solution.F90:116-166): image root by index arithmetic,
+        // descent along the ghost's sp list taken deepest level first
+        const int num1 = row, num2 = col;
+        int i1;
+        if (a == -4) i1 = num1 * m + num2 - 6;
+        else if (a == -2) i1 = num1 * m + num2 - 2 * m + 6;
+        else if (a == -3) i1 = num1 * m + num2 - (n - 5) * m;
+        else i1 = num1 * m + num2 - (7 - n) * m;
+        Node r0;
+        r0.root = i1 - 1; r0.lvl = 0; r0.ix = 0; r0.iy = 0;
+        NodeRef cur = resolve(T, r0);
+        for (int j = 0; j < gn.lvl; ++j) {
+            if (cur.leaf >= 0) break;
+            // sp(j+1) = sp of the ancestor j levels above the ghost
+            const int l = gn.lvl - j;
+            const int q = (int)(((gn.ix >> (gn.lvl - l)) & 1u) | (((gn.iy >> (gn.lvl - l)) & 1u) << 1));
+            cur = child_ref(T, cur, q);
+        }
+        ghost_from_ref(T, cur, O, g);
+        return;
+    }
+    if (kind == FDM_BC_TRANSMISSIVE) {
+        NodeRef img;
+        if (a == -4) img = ext_image(T, G, gn, row, 4, 1, 0);
+        else if (a == -2) img = ext_image(T, G, gn, row, m - 3, 1, 1);
+        else if (a == -1) img = ext_image(T, G, gn, 4, col, 2, 0);
+        else img = ext_image(T, G, gn, n - 3, col, 2, 1);
+        ghost_from_ref(T, img, O, g);
+        return;
+    }
+    if (kind == FDM_BC_WALL || kind == FDM_BC_DMR_BOTTOM) {
+        if (kind == FDM_BC_DMR_BOTTOM && T.lcx[k] <= P.dmr_x0) {
+            O.kind[g] = GH_STATE; O.a[g] = 4; O.b[g] = 0;
+            return;
+        }
+        NodeRef img;
+        if (a == -1) img = ext_image(T, G, gn, 7 - row, col, 3, 0);
+        else if (a == -3) img = ext_image(T, G, gn, 2 * n - 5 - row, col, 3, 0);
+        else if (a == -4) img = ext_image(T, G, gn, row, 7 - col, 4, 0);
+        else img = ext_image(T, G, gn, row, 2 * m - 5 - col, 4, 0);
+        ghost_from_ref(T, img, O, g);
+        O.flip[g] = (a == -1 || a == -3) ? 2 : 1;
+        return;
+    }
+    if (kind == FDM_BC_INFLOW) {
+        O.kind[g] = GH_STATE;
+        O.a[g] = a == -4 ? 0 : a == -2 ? 1 : a == -1 ? 2 : 3;
+        O.b[g] = 0;
+        return;
+    }
+    if (kind == FDM_BC_DMR_TOP) {
+        O.kind[g] = GH_DMR_TOP; O.a[g] = 0; O.b[g] = 0;
+        return;
+    }
+    O.kind[g] = GH_NONE; O.a[g] = 0; O.b[g] = 0;
+}
+
+// --------------------------------------------------------------- faces
+// The right (top) face of every interior leaf is face i.  Its left (bottom)
+// face is the right face of the left neighbour j when j is an interior
+// same-level leaf whose 4-point face stencil is slot-for-slot the same;
+// otherwise the leaf owns a separate left face.
+__global__ void k_face_flags(Tables T, int32_t *ux, int32_t *uy) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= T.NI) return;
+    const int32_t *s = T.ist + i * 8;
+    int shared = 0;
+    const int32_t j = s[1];
+    if (j >= 0 && j < T.NI) {
+        const int32_t *t = T.ist + (int64_t)j * 8;
+        shared = (t[1] == s[5]) && (t[0] == (int32_t)i) && (t[4] == s[0]);
+    }
+    ux[i] = !shared;
+    int shy = 0;
+    const int32_t jy = s[3];
+    if (jy >= 0 && jy < T.NI) {
+        const int32_t *t = T.ist + (int64_t)jy * 8;
+        shy = (t[3] == s[7]) && (t[2] == (int32_t)i) && (t[6] == s[2]);
+    }
+    uy[i] = !shy;
+}
+__global__ void k_face_assign(Tables T, const int32_t *ux, const int32_t *uy, const int32_t *sx,
+                              const int32_t *sy, int32_t *ifxl, int32_t *ifyl, int32_t *uxl, int32_t *uyl) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= T.NI) return;
+    const int32_t *s = T.ist + i * 8;
+    if (ux[i]) { ifxl[i] = (int32_t)(T.NI + sx[i]); uxl[sx[i]] = (int32_t)i; }
+    else ifxl[i] = s[1];
+    if (uy[i]) { ifyl[i] = (int32_t)(T.NI + sy[i]); uyl[sy[i]] = (int32_t)i; }
+    else ifyl[i] = s[3];
+}
+
+__global__ void k_lmax(int64_t NI, const uint8_t *ilvl, int32_t *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int v = i < NI ? (int)ilvl[i] : 0;
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, v);
+}
+
+// ------------------------------------------------------------ host side
+static int scan_i32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n) {
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceScan::ExclusiveSum(h->cub_tmp.p, bytes, in, out, (int)n, h->s));
+    return FDM_OK;
+}
+// total of an exclusive scan: last scan value + last flag
+static int scan_total(fdm_handle *h, const int32_t *flags, const int32_t *scan, int64_t n, int64_t &total) {
+    if (n == 0) { total = 0; return FDM_OK; }
+    int32_t a = 0, b = 0;
+    FDM_CK(h, cudaMemcpyAsync(&a, flags + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(&b, scan + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    total = (int64_t)a + b;
+    return FDM_OK;
+}
+
+#define FDM_RC(x)                 \
+    do {                          \
+        int rc_ = (x);            \
+        if (rc_) return rc_;      \
+    } while (0)
+
+int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double *prim_in) {
+    const int TB = 256;
+    cudaStream_t s = h->s;
+    if (n <= 0 || n >= (1ll << 31) - 1) return arg_fail(h, "leaf count out of range");
+    h->NL = n;
+    int32_t *err = h->flag.as<int32_t>();
+    FDM_CK(h, cudaMemsetAsync(err, 0, 8 * sizeof(int32_t), s));
+    // 1. sort keys, carrying the input index
+    FDM_CK(h, h->lkey.ensure(n * 8));
+    FDM_CK(h, h->tmp[0].ensure(n * 4));   // iota
+    FDM_CK(h, h->tmp[1].ensure(n * 4));   // perm
+    {
+        int32_t *iota = h->tmp[0].as<int32_t>();
+        std::vector<int32_t> hi((size_t)n);
+        for (int64_t k = 0; k < n; ++k) hi[(size_t)k] = (int32_t)k;
+        FDM_CK(h, cudaMemcpyAsync(iota, hi.data(), n * 4, cudaMemcpyHostToDevice, s));
+        size_t bytes = 0;
+        FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
+                                                  h->tmp[1].as<int32_t>(), (int)n, 0, 64, s));
+        FDM_CK(h, h->cub_tmp.ensure(bytes));
+        FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
+                                                  h->tmp[1].as<int32_t>(), (int)n, 0, 64, s));
+        FDM_CK(h, cudaStreamSynchronize(s));   // host iota buffer
+    }
+    const uint64_t *lkey = h->lkey.as<uint64_t>();
+    const int32_t *perm = h->tmp[1].as<int32_t>();
+    // 2. classify + partition check
+    FDM_CK(h, h->tmp[2].ensure(n * 4 * 6));
+    int32_t *fI = h->tmp[2].as<int32_t>(), *fG = fI + n, *fC = fG + n;
+    int32_t *sI = fC + n, *sG = sI + n, *sC = sG + n;
+    FDM_CK(h, h->lcross.ensure(n));
+    k_classify<<<nblk(n, TB), TB, 0, s>>>(lkey, n, h->G, fI, fG, fC, h->lcross.as<int8_t>(), err);
+    FDM_RC(scan_i32(h, fI, sI, n));
+    FDM_RC(scan_i32(h, fG, sG, n));
+    FDM_RC(scan_i32(h, fC, sC, n));
+    int64_t NI, NG, NC;
+    FDM_RC(scan_total(h, fI, sI, n, NI));
+    FDM_RC(scan_total(h, fG, sG, n, NG));
+    FDM_RC(scan_total(h, fC, sC, n, NC));
+    {
+        int32_t he[8];
+        FDM_CK(h, cudaMemcpy(he, err, sizeof(he), cudaMemcpyDeviceToHost));
+        if (he[BE_ROOT]) return arg_fail(h, "leaf key names a background cell outside the m x n grid");
+        if (he[BE_PARTITION]) return arg_fail(h, "leaf set does not partition the background grid (gap, overlap or duplicate)");
+        if (he[BE_LEVEL]) return arg_fail(h, "leaf level above the supported maximum (14)");
+    }
+    if (NI == 0) return arg_fail(h, "no interior leaves");
+    h->NI = NI; h->NG = NG; h->NC = NC;
+    // 3. slots, values, centres
+    FDM_CK(h, h->lslot.ensure(n * 4));
+    FDM_CK(h, h->slot_leaf.ensure(n * 4));
+    k_slots<<<nblk(n, TB), TB, 0, s>>>(n, NI, NG, fI, fG, sI, sG, sC, h->lslot.as<int32_t>(), h->slot_leaf.as<int32_t>());
+    FDM_CK(h, h->lcx.ensure(n * 8));
+    FDM_CK(h, h->lcy.ensure(n * 8));
+    k_centers<<<nblk(n, TB), TB, 0, s>>>(n, lkey, h->G, h->lcx.as<double>(), h->lcy.as<double>());
+    // 4. stencil resolution
+    const int64_t ne = NI * 8;
+    FDM_CK(h, h->ist.ensure(ne * 4));
+    FDM_CK(h, h->ilvl.ensure(NI));
+    FDM_CK(h, h->tmp[3].ensure(ne * (4 + 4 + 8 + 8 + 8 + 4 + 4)));
+    ResolveOut RO;
+    char *base = h->tmp[3].as<char>();
+    RO.slot = (int32_t *)base;
+    RO.kind = (int32_t *)(base + ne * 4);
+    RO.ref = (int64_t *)(base + ne * 8);
+    RO.tx = (double *)(base + ne * 16);
+    RO.ty = (double *)(base + ne * 24);
+    int32_t *rflag = (int32_t *)(base + ne * 32);
+    int32_t *ridx = (int32_t *)(base + ne * 36);
+    {
+        Tables T = h->tables();
+        k_resolve<<<nblk(NI, 128), 128, 0, s>>>(T, h->G, RO, h->ilvl.as<uint8_t>(), err);
+    }
+    k_req_flags<<<nblk(ne, TB), TB, 0, s>>>(ne, RO.slot, rflag);
+    FDM_RC(scan_i32(h, rflag, ridx, ne));
+    int64_t NR;
+    FDM_RC(scan_total(h, rflag, ridx, ne, NR));
+    {
+        int32_t he[8];
+        FDM_CK(h, cudaMemcpy(he, err, sizeof(he), cudaMemcpyDeviceToHost));
+        if (he[BE_NULLNB]) return arg_fail(h, "an interior leaf has a null stencil neighbour (fewer than 3 ghost layers?)");
+    }
+    h->NR = NR;
+    h->NS = NI + NG + NC + NR;
+    const int64_t VS0 = NI + NG + NC;
+    const int64_t nrq = NR > 0 ? NR : 1;
+    FDM_CK(h, h->tmp[4].ensure(nrq * (4 + 8 + 8 + 8)));
+    ReqDesc RD;
+    char *rb = h->tmp[4].as<char>();
+    RD.kind = (int32_t *)rb;
+    RD.ref = (int64_t *)(rb + nrq * 8);
+    RD.tx = (double *)(rb + nrq * 16);
+    RD.ty = (double *)(rb + nrq * 24);
+    k_emit<<<nblk(ne, TB), TB, 0, s>>>(ne, VS0, RO, ridx, h->ist.as<int32_t>(), RD);
+    // 5. requests: gather + WLS geometry
+    FDM_CK(h, h->rq_kind.ensure(nrq * 4));
+    FDM_CK(h, h->rq_m.ensure(nrq * 8));
+    FDM_CK(h, h->rq_mem.ensure(nrq * WLS_MAXM * 4));
+    FDM_CK(h, h->rq_geo.ensure(nrq * RQ_GEO * 8));
+    FDM_CK(h, h->tmp[5].ensure(64));
+    unsigned long long *counts = h->tmp[5].as<unsigned long long>();
+    FDM_CK(h, cudaMemsetAsync(counts, 0, 64, s));
+    if (NR > 0) {
+        Tables T = h->tables();
+        ReqOut O{h->rq_kind.as<int32_t>(), h->rq_m.as<int32_t>(), h->rq_mem.as<int32_t>(),
+                 h->rq_geo.as<double>(), counts};
+        k_gather<<<nblk(NR, 64), 64, 0, s>>>(T, h->G, RD, O, err);
+    }
+    // 6. ghosts
+    const int64_t ngh = NG > 0 ? NG : 1;
+    FDM_CK(h, h->gh_kind.ensure(ngh * 4));
+    FDM_CK(h, h->gh_a.ensure(ngh * 4));
+    FDM_CK(h, h->gh_b.ensure(ngh * 4));
+    FDM_CK(h, h->gh_flip.ensure(ngh * 4));
+    FDM_CK(h, h->gh_x.ensure(ngh * 8));
+    FDM_CK(h, h->gh_y.ensure(ngh * 8));
+    if (NG > 0) {
+        Tables T = h->tables();
+        GhostOut O{h->gh_kind.as<int32_t>(), h->gh_a.as<int32_t>(), h->gh_b.as<int32_t>(),
+                   h->gh_flip.as<int32_t>(), h->gh_x.as<double>(), h->gh_y.as<double>()};
+        k_ghosts<<<nblk(NG, 128), 128, 0, s>>>(T, h->G, h->p, O);
+    }
+    // 7. faces
+    FDM_CK(h, h->tmp[6].ensure(NI * 4 * 4));
+    int32_t *ux = h->tmp[6].as<int32_t>(), *uy = ux + NI, *sx = uy + NI, *sy = sx + NI;
+    {
+        Tables T = h->tables();
+        k_face_flags<<<nblk(NI, TB), TB, 0, s>>>(T, ux, uy);
+    }
+    FDM_RC(scan_i32(h, ux, sx, NI));
+    FDM_RC(scan_i32(h, uy, sy, NI));
+    int64_t nux, nuy;
+    FDM_RC(scan_total(h, ux, sx, NI, nux));
+    FDM_RC(scan_total(h, uy, sy, NI, nuy));
+    h->nux = nux; h->nuy = nuy;
+    FDM_CK(h, h->ifxl.ensure(NI * 4));
+    FDM_CK(h, h->ifyl.ensure(NI * 4));
+    FDM_CK(h, h->uxl.ensure((nux > 0 ? nux : 1) * 4));
+    FDM_CK(h, h->uyl.ensure((nuy > 0 ? nuy : 1) * 4));
+    {
+        Tables T = h->tables();
+        k_face_assign<<<nblk(NI, TB), TB, 0, s>>>(T, ux, uy, sx, sy, h->ifxl.as<int32_t>(), h->ifyl.as<int32_t>(),
+                                                  h->uxl.as<int32_t>(), h->uyl.as<int32_t>());
+    }
+    // 8. state buffers (corner values copied into all three)
+    const int64_t NS = h->NS;
+    for (int b = 0; b < 3; ++b) FDM_CK(h, h->B[b].ensure(NS * 32));
+    FDM_CK(h, h->Fx.ensure((NI + nux) * 32));
+    FDM_CK(h, h->Fy.ensure((NI + nuy) * 32));
+    FDM_CK(h, h->Ut.ensure(NI * 32));
+    k_scatter<<<nblk(n, TB), TB, 0, s>>>(n, perm, h->lslot.as<int32_t>(), prim_in, h->B[0].as<double4>());
+    if (NC > 0)
+        for (int b = 1; b < 3; ++b)
+            FDM_CK(h, cudaMemcpyAsync(h->B[b].as<double4>() + NI + NG, h->B[0].as<double4>() + NI + NG, NC * 32,
+                                      cudaMemcpyDeviceToDevice, s));
+    // 9. l_max
+    int32_t *dl = err + 7;
+    FDM_CK(h, cudaMemsetAsync(dl, 0, 4, s));
+    k_lmax<<<nblk(NI, TB), TB, 0, s>>>(NI, h->ilvl.as<uint8_t>(), dl);
+    int32_t he[8];
+    unsigned long long hc[4];
+    FDM_CK(h, cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, s));
+    FDM_CK(h, cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    FDM_CK(h, cudaStreamSynchronize(s));
+    FDM_CK(h, cudaGetLastError());
+    if (he[BE_OVERFLOW]) return arg_fail(h, "hanging-node stencil larger than supported");
+    h->l_max = he[7];
+    FDM_CK(h, cudaMemcpy(&h->scal.as<DevScalars>()->l_max, &h->l_max, 4, cudaMemcpyHostToDevice));
+    h->n_singular += (int64_t)hc[0];
+    h->n_restrict = (int64_t)hc[2];
+    h->table_version++;
+    h->lam_fresh = false;
+    h->loaded = true;
+    return FDM_OK;
+}
+
+}  // namespace fdm

@@ -1,0 +1,140 @@
+// handle.cuh — host-side state of one libfdm handle.
+#pragma once
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fdm_common.cuh"
+
+namespace fdm {
+
+// Device buffer that only grows; freed with the handle.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t nbytes) {
+        if (nbytes <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t nb = nbytes ? nbytes : 16;
+        cudaError_t e = cudaMalloc(&p, nb);
+        if (e == cudaSuccess) bytes = nb;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+}  // namespace fdm
+
+struct fdm_handle {
+    fdm_params p{};
+    fdm::Geometry G{};
+    fdm::LevelTab lt{};
+    int device = 0;
+    cudaStream_t s = nullptr;
+    std::string err;
+
+    // leaf set sizes
+    int64_t NL = 0, NI = 0, NG = 0, NC = 0, NR = 0, NS = 0, nux = 0, nuy = 0;
+    int32_t l_max = 0;
+    bool loaded = false;
+    bool lam_fresh = false;
+    int cur_buf = 0;         // split API: buffer holding the latest interior values
+    int64_t n_singular = 0, n_regrids = 0, n_restrict = 0;
+
+    // tables
+    fdm::DevBuf lkey, lslot, slot_leaf, lcx, lcy, lcross;
+    fdm::DevBuf ist, ilvl, ifxl, ifyl, uxl, uyl;
+    fdm::DevBuf rq_kind, rq_m, rq_mem, rq_geo;
+    fdm::DevBuf gh_kind, gh_a, gh_b, gh_flip, gh_x, gh_y;
+    // state: three slot arrays (step start / stage 1 / stage 2)
+    fdm::DevBuf B[3];
+    fdm::DevBuf Fx, Fy, Ut;
+    fdm::DevBuf scal;        // DevScalars
+    fdm::DevBuf res_part;    // per-block residual partials
+    // scratch for table building
+    fdm::DevBuf tmp[8];
+    fdm::DevBuf cub_tmp;
+    fdm::DevBuf flag;        // device error flags (int32[8])
+    fdm::DevScalars *hs = nullptr;   // pinned host mirror of the scalars
+
+    // CUDA graph of one RK3 step (captured lazily, dropped at regrid)
+    cudaGraphExec_t step_graph = nullptr;
+    int64_t graph_version = -1;
+    int64_t table_version = 0;
+
+    fdm::Tables tables() const {
+        fdm::Tables T{};
+        T.NL = NL; T.NI = NI; T.NG = NG; T.NC = NC; T.NR = NR; T.NS = NS;
+        T.lkey = lkey.as<uint64_t>();
+        T.lslot = lslot.as<int32_t>();
+        T.slot_leaf = slot_leaf.as<int32_t>();
+        T.lcx = lcx.as<double>();
+        T.lcy = lcy.as<double>();
+        T.ist = ist.as<int32_t>();
+        T.ilvl = ilvl.as<uint8_t>();
+        T.ifxl = ifxl.as<int32_t>();
+        T.ifyl = ifyl.as<int32_t>();
+        T.uxl = uxl.as<int32_t>();
+        T.uyl = uyl.as<int32_t>();
+        T.nux = nux; T.nuy = nuy;
+        T.rq_kind = rq_kind.as<int32_t>();
+        T.rq_m = rq_m.as<int32_t>();
+        T.rq_mem = rq_mem.as<int32_t>();
+        T.rq_geo = rq_geo.as<double>();
+        T.gh_kind = gh_kind.as<int32_t>();
+        T.gh_a = gh_a.as<int32_t>();
+        T.gh_b = gh_b.as<int32_t>();
+        T.gh_flip = gh_flip.as<int32_t>();
+        T.gh_x = gh_x.as<double>();
+        T.gh_y = gh_y.as<double>();
+        return T;
+    }
+};
+
+namespace fdm {
+
+// error helpers: record a message in the handle and return a status
+inline int cuda_fail(fdm_handle *h, cudaError_t e, const char *what) {
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    h->err = buf;
+    return e == cudaErrorMemoryAllocation ? FDM_ERR_NOMEM : FDM_ERR_CUDA;
+}
+#define FDM_CK(h, call)                                        \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return fdm::cuda_fail(h, e_, #call); \
+    } while (0)
+
+inline int arg_fail(fdm_handle *h, const char *msg) {
+    h->err = msg;
+    return FDM_ERR_ARG;
+}
+
+// table construction (build.cu)
+int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_dev, const double *prim_dev);
+// per-stage pipeline (stage.cu)
+void launch_requests(fdm_handle *h, const double4 *cur);
+void launch_faces(fdm_handle *h, const double4 *cur);
+void launch_cells(fdm_handle *h, const double4 *cur, const double4 *un, double4 *next, int krk,
+                  int mode);
+void launch_ghosts(fdm_handle *h, double4 *next, int j);
+void launch_blend(fdm_handle *h, const double4 *un, double4 *cur, int krk);
+void launch_lambda(fdm_handle *h, const double4 *cur);
+void launch_step_control(fdm_handle *h);
+void launch_step_end(fdm_handle *h);
+void launch_set_tstep(fdm_handle *h, double tstep);
+void launch_res_finalize(fdm_handle *h);
+int launch_stage(fdm_handle *h, int krk);
+// AMR (amr.cu)
+int run_amr(fdm_handle *h);
+
+}  // namespace fdm

@@ -1,0 +1,489 @@
+// libfdm.cu — the extern "C" boundary (include/fdm.h).
+#include <cmath>
+#include <cstdlib>
+#include <new>
+
+#include "handle.cuh"
+#include "topo.cuh"
+
+using namespace fdm;
+
+namespace fdm {
+
+static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+__global__ void k_reset_lam(DevScalars *sc) {
+    if (threadIdx.x || blockIdx.x) return;
+    sc->lam_next_x = 0.0;
+    sc->lam_next_y = 0.0;
+}
+
+__global__ void k_out(int64_t NL, const int32_t *lslot, const double4 *B0, double *prim) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    const double4 v = B0[lslot[k]];
+    prim[4 * k] = v.x; prim[4 * k + 1] = v.y; prim[4 * k + 2] = v.z; prim[4 * k + 3] = v.w;
+}
+__global__ void k_in(int64_t NL, const int32_t *lslot, double4 *B0, const double *prim) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    B0[lslot[k]] = make_double4(prim[4 * k], prim[4 * k + 1], prim[4 * k + 2], prim[4 * k + 3]);
+}
+__global__ void k_stencil_out(Tables T, const double4 *B, double *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= T.NI) return;
+    for (int s = 0; s < 8; ++s) {
+        const double4 v = B[T.ist[i * 8 + s]];
+        double *o = out + (i * 8 + s) * 4;
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+}
+__global__ void k_neighbors_out(Tables T, Geometry G, uint64_t *out) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= T.NL) return;
+    NodeRef c;
+    c.n = node_of_key(T.lkey[k]);
+    c.leaf = (int32_t)k;
+    c.valid = 1;
+    NodeRef nb[8];
+    nb[0] = face_nb(T, G, c, DIR_UP);
+    nb[1] = face_nb(T, G, c, DIR_DOWN);
+    nb[2] = face_nb(T, G, c, DIR_RIGHT);
+    nb[3] = face_nb(T, G, c, DIR_LEFT);
+    if (root_cross(G, c.n.root) >= 0) {
+        nb[4] = upleft_nb(T, G, c);
+        nb[5] = upright_nb(T, G, c);
+        nb[6] = downleft_nb(T, G, c);
+        nb[7] = downright_nb(T, G, c);
+    } else {
+        for (int d = 4; d < 8; ++d) nb[d] = null_ref();
+    }
+    for (int d = 0; d < 8; ++d) out[k * 8 + d] = nb[d].valid ? node_key(nb[d].n) : ~0ull;
+}
+
+static int sync_scalars_from_device(fdm_handle *h) {
+    FDM_CK(h, cudaMemcpyAsync(h->hs, h->scal.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+static int push_scalars(fdm_handle *h) {
+    FDM_CK(h, cudaMemcpyAsync(h->scal.p, h->hs, sizeof(DevScalars), cudaMemcpyHostToDevice, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+
+static int ensure_lambda(fdm_handle *h) {
+    if (h->lam_fresh) return FDM_OK;
+    k_reset_lam<<<1, 32, 0, h->s>>>(h->scal.as<DevScalars>());
+    launch_lambda(h, h->B[0].as<double4>());
+    h->lam_fresh = true;
+    return FDM_OK;
+}
+
+// getRKn + 3 x (solution_cell, updateRK, body_boundary_RK)
+static void enqueue_rk(fdm_handle *h) {
+    launch_stage(h, 1);
+    launch_stage(h, 2);
+    k_reset_lam<<<1, 32, 0, h->s>>>(h->scal.as<DevScalars>());
+    launch_stage(h, 3);
+}
+
+// one solute iteration without AMR: step control, RK3, tt/residual/NaN
+static void enqueue_solute_iteration(fdm_handle *h) {
+    launch_step_control(h);
+    enqueue_rk(h);
+    launch_step_end(h);
+}
+
+static int prepare_buffers(fdm_handle *h) {
+    const int64_t nb = nblk(h->NI, 256);
+    FDM_CK(h, h->res_part.ensure((size_t)(nb > 0 ? nb : 1) * 8 * sizeof(double)));
+    return FDM_OK;
+}
+
+static void drop_graph(fdm_handle *h) {
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+    h->graph_version = -1;
+}
+
+// CUDA graph of one solute iteration; re-captured after every rebuild of the
+// tables (upload / regrid), replayed otherwise.
+static int step_graph(fdm_handle *h, cudaGraphExec_t *out) {
+    if (h->step_graph && h->graph_version == h->table_version) {
+        *out = h->step_graph;
+        return FDM_OK;
+    }
+    drop_graph(h);
+    cudaGraph_t g = nullptr;
+    FDM_CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    enqueue_solute_iteration(h);
+    cudaError_t e = cudaStreamEndCapture(h->s, &g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->step_graph = nullptr;
+        return cuda_fail(h, e, "cudaGraphInstantiate");
+    }
+    h->graph_version = h->table_version;
+    *out = h->step_graph;
+    return FDM_OK;
+}
+
+static bool amr_due(const fdm_handle *h, int64_t it) {
+    return h->p.iflag_amr && it >= h->p.nstep_adapt && h->p.pstep_adapt != 0 &&
+           (it % h->p.pstep_adapt) == 1;
+}
+
+}  // namespace fdm
+
+#define CHECK_H(h)                    \
+    do {                              \
+        if (!(h)) return FDM_ERR_ARG; \
+    } while (0)
+#define CHECK_LOADED(h)                                                            \
+    do {                                                                           \
+        if (!(h)->loaded) { (h)->err = "no leaf set uploaded"; return FDM_ERR_STATE; } \
+    } while (0)
+#define RC(x)                \
+    do {                     \
+        int rc_ = (x);       \
+        if (rc_) return rc_; \
+    } while (0)
+
+extern "C" {
+
+int fdm_create(const fdm_params *p, fdm_handle **out) {
+    if (!p || !out) return FDM_ERR_ARG;
+    *out = nullptr;
+    if (!(p->h > 0.0) || !(p->x_factor > 0.0) || p->m < 7 || p->n < 7) return FDM_ERR_ARG;
+    const int m = (int)((p->xmax - p->xmin) / (p->x_factor * p->h));
+    const int n = (int)((p->ymax - p->ymin) / p->h);
+    if (m != p->m || n != p->n) return FDM_ERR_ARG;
+    if ((int64_t)p->m * p->n >= (1ll << 30)) return FDM_ERR_ARG;
+    if (p->lvl_amr < 0 || p->lvl_amr > MAXLVL_TAB - 2) return FDM_ERR_ARG;
+    if (p->flux_variant != 0) return FDM_ERR_UNSUPPORTED;
+    fdm_handle *h = new (std::nothrow) fdm_handle();
+    if (!h) return FDM_ERR_NOMEM;
+    h->p = *p;
+    h->G.xmin = p->xmin; h->G.ymin = p->ymin; h->G.h = p->h; h->G.xf = p->x_factor;
+    h->G.gama = p->gama; h->G.cv = p->cv; h->G.m = p->m; h->G.n = p->n;
+    for (int l = 0; l < MAXLVL_TAB; ++l) {
+        const double dy = p->h / (double)(1ll << l);
+        const double dx = p->x_factor * dy;
+        h->lt.dx[l] = dx;
+        h->lt.dy[l] = dy;
+        h->lt.cxa[l] = 4.0 / (3.0 * dx);
+        h->lt.cxb[l] = 1.0 / (6.0 * dx);
+        h->lt.cya[l] = 4.0 / 3.0 / dy;
+        h->lt.cyb[l] = 1.0 / 6.0 / dy;
+        h->lt.dxdy[l] = 0.0;
+        h->lt.p15[l] = std::pow(dy, 1.5);
+    }
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hs, sizeof(DevScalars));
+    if (e == cudaSuccess) e = h->scal.ensure(sizeof(DevScalars));
+    if (e == cudaSuccess) e = h->flag.ensure(8 * sizeof(int32_t));
+    if (e != cudaSuccess) {
+        fdm_destroy(h);
+        return e == cudaErrorMemoryAllocation ? FDM_ERR_NOMEM : FDM_ERR_CUDA;
+    }
+    std::memset(h->hs, 0, sizeof(DevScalars));
+    h->hs->tstep = p->tstep;
+    h->hs->t_end = p->t_end;
+    h->hs->done = 0;
+    if (push_scalars(h)) {
+        fdm_destroy(h);
+        return FDM_ERR_CUDA;
+    }
+    *out = h;
+    return FDM_OK;
+}
+
+void fdm_destroy(fdm_handle *h) {
+    if (!h) return;
+    if (h->s) cudaStreamSynchronize(h->s);
+    drop_graph(h);
+    DevBuf *bufs[] = {&h->lkey, &h->lslot, &h->slot_leaf, &h->lcx, &h->lcy, &h->lcross, &h->ist, &h->ilvl,
+                      &h->ifxl, &h->ifyl, &h->uxl, &h->uyl, &h->rq_kind, &h->rq_m, &h->rq_mem, &h->rq_geo,
+                      &h->gh_kind, &h->gh_a, &h->gh_b, &h->gh_flip, &h->gh_x, &h->gh_y, &h->B[0], &h->B[1],
+                      &h->B[2], &h->Fx, &h->Fy, &h->Ut, &h->scal, &h->res_part, &h->cub_tmp, &h->flag};
+    for (DevBuf *b : bufs) b->release();
+    for (auto &t : h->tmp) t.release();
+    if (h->hs) cudaFreeHost(h->hs);
+    if (h->s) cudaStreamDestroy(h->s);
+    delete h;
+}
+
+int fdm_last_error(const fdm_handle *h, char *buf, size_t n) {
+    if (!h || !buf || n == 0) return FDM_ERR_ARG;
+    size_t k = h->err.size() < n - 1 ? h->err.size() : n - 1;
+    std::memcpy(buf, h->err.data(), k);
+    buf[k] = 0;
+    return FDM_OK;
+}
+
+int fdm_upload_leaves(fdm_handle *h, int64_t n, const uint64_t *keys, const double *prim) {
+    CHECK_H(h);
+    if (n <= 0 || !keys || !prim) return arg_fail(h, "empty leaf set");
+    DevBuf dk, dp;
+    FDM_CK(h, dk.ensure(n * 8));
+    FDM_CK(h, dp.ensure(n * 32));
+    FDM_CK(h, cudaMemcpyAsync(dk.p, keys, n * 8, cudaMemcpyHostToDevice, h->s));
+    FDM_CK(h, cudaMemcpyAsync(dp.p, prim, n * 32, cudaMemcpyHostToDevice, h->s));
+    int rc = build_tables(h, n, dk.as<uint64_t>(), dp.as<double>());
+    cudaStreamSynchronize(h->s);
+    dk.release();
+    dp.release();
+    if (rc) { h->loaded = false; return rc; }
+    return prepare_buffers(h);
+}
+
+int64_t fdm_num_leaves(const fdm_handle *h) { return h && h->loaded ? h->NL : 0; }
+
+int fdm_download_leaves(fdm_handle *h, int64_t cap, int64_t *n_out, uint64_t *keys, double *prim) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (n_out) *n_out = h->NL;
+    if (cap < h->NL) return arg_fail(h, "capacity below the leaf count");
+    DevBuf dp;
+    FDM_CK(h, dp.ensure(h->NL * 32));
+    k_out<<<nblk(h->NL, 256), 256, 0, h->s>>>(h->NL, h->lslot.as<int32_t>(), h->B[0].as<double4>(), dp.as<double>());
+    if (keys) FDM_CK(h, cudaMemcpyAsync(keys, h->lkey.p, h->NL * 8, cudaMemcpyDeviceToHost, h->s));
+    if (prim) FDM_CK(h, cudaMemcpyAsync(prim, dp.p, h->NL * 32, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    dp.release();
+    return FDM_OK;
+}
+
+int fdm_set_values(fdm_handle *h, int64_t n, const double *prim) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (n != h->NL || !prim) return arg_fail(h, "value count differs from the leaf count");
+    DevBuf dp;
+    FDM_CK(h, dp.ensure(n * 32));
+    FDM_CK(h, cudaMemcpyAsync(dp.p, prim, n * 32, cudaMemcpyHostToDevice, h->s));
+    k_in<<<nblk(n, 256), 256, 0, h->s>>>(n, h->lslot.as<int32_t>(), h->B[0].as<double4>(), dp.as<double>());
+    if (h->NC > 0)
+        for (int b = 1; b < 3; ++b)
+            FDM_CK(h, cudaMemcpyAsync(h->B[b].as<double4>() + h->NI + h->NG, h->B[0].as<double4>() + h->NI + h->NG,
+                                      h->NC * 32, cudaMemcpyDeviceToDevice, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    dp.release();
+    h->lam_fresh = false;
+    return FDM_OK;
+}
+
+int fdm_get_scalars(fdm_handle *h, double *lambda_x, double *lambda_y, double *tstep, double *tt, int64_t *it,
+                    int32_t *l_max) {
+    CHECK_H(h);
+    RC(sync_scalars_from_device(h));
+    if (lambda_x) *lambda_x = h->hs->lambda_x;
+    if (lambda_y) *lambda_y = h->hs->lambda_y;
+    if (tstep) *tstep = h->hs->tstep;
+    if (tt) *tt = h->hs->tt;
+    if (it) *it = h->hs->it;
+    if (l_max) *l_max = h->l_max;
+    return FDM_OK;
+}
+
+int fdm_set_scalars(fdm_handle *h, double lambda_x, double lambda_y, double tstep, double tt, int64_t it) {
+    CHECK_H(h);
+    RC(sync_scalars_from_device(h));
+    h->hs->lambda_x = lambda_x;
+    h->hs->lambda_y = lambda_y;
+    h->hs->tstep = tstep;
+    h->hs->tt = tt;
+    h->hs->it = it;
+    h->hs->t_end = h->p.t_end;
+    h->hs->done = !(tt < h->p.t_end);
+    h->hs->status = 0;
+    return push_scalars(h);
+}
+
+int fdm_step_control(fdm_handle *h, double *tstep, double *lambda_x, double *lambda_y, int32_t *l_max) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    RC(ensure_lambda(h));
+    launch_step_control(h);
+    RC(sync_scalars_from_device(h));
+    if (tstep) *tstep = h->hs->tstep;
+    if (lambda_x) *lambda_x = h->hs->lambda_x;
+    if (lambda_y) *lambda_y = h->hs->lambda_y;
+    if (l_max) *l_max = h->l_max;
+    return FDM_OK;
+}
+
+int fdm_time_advance_rk(fdm_handle *h, double tstep) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    launch_set_tstep(h, tstep);
+    enqueue_rk(h);
+    h->lam_fresh = true;
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    FDM_CK(h, cudaGetLastError());
+    return FDM_OK;
+}
+
+int fdm_get_rkn(fdm_handle *h) {
+    // B0 holds Un for the whole step (stages never overwrite it before
+    // stage 3), so getRKn needs no copy.
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    return FDM_OK;
+}
+
+// split API: stage krk reads buffer (krk-1) and writes Ut; update_rk blends
+// into buffer krk % 3; body_boundary fills its ghosts.
+int fdm_solution_cells(fdm_handle *h, int32_t krk) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (krk < 1 || krk > 3) return arg_fail(h, "krk must be 1..3");
+    const double4 *cur = h->B[krk - 1].as<double4>();
+    launch_requests(h, cur);
+    launch_faces(h, cur);
+    launch_cells(h, cur, h->B[0].as<double4>(), h->Ut.as<double4>(), krk, 1);
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+int fdm_update_rk(fdm_handle *h, int32_t krk) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (krk < 1 || krk > 3) return arg_fail(h, "krk must be 1..3");
+    launch_blend(h, h->B[0].as<double4>(), h->B[krk % 3].as<double4>(), krk);
+    h->cur_buf = krk % 3;
+    h->lam_fresh = false;
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+int fdm_body_boundary(fdm_handle *h, int32_t j) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    // ghosts of the buffer that holds the latest interior values
+    launch_ghosts(h, h->B[h->cur_buf].as<double4>(), j);
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+
+int fdm_residual(fdm_handle *h, double res_max[4], double res_rms[4]) {
+    CHECK_H(h);
+    RC(sync_scalars_from_device(h));
+    for (int n = 0; n < 4; ++n) {
+        if (res_max) res_max[n] = h->hs->res_max[n];
+        if (res_rms) res_rms[n] = h->hs->res_rms[n];
+    }
+    return FDM_OK;
+}
+
+int fdm_solute_step(fdm_handle *h) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    RC(ensure_lambda(h));
+    enqueue_solute_iteration(h);
+    h->lam_fresh = true;
+    RC(sync_scalars_from_device(h));
+    FDM_CK(h, cudaGetLastError());
+    if (h->hs->status == FDM_ERR_NAN) {
+        h->err = "NaN in the residual RMS (the reference stops here)";
+        return FDM_ERR_NAN;
+    }
+    if (amr_due(h, h->hs->it)) {
+        RC(fdm_amr(h));
+    }
+    if (h->p.iflag_amr) {
+        launch_ghosts(h, h->B[0].as<double4>(), 1);
+        FDM_CK(h, cudaStreamSynchronize(h->s));
+    }
+    return FDM_OK;
+}
+
+int fdm_solute(fdm_handle *h, int64_t nsteps, int64_t *steps_done) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    int64_t k = 0;
+    int rc = FDM_OK;
+    RC(sync_scalars_from_device(h));
+    while (k < nsteps && h->hs->tt < h->p.t_end) {
+        rc = fdm_solute_step(h);
+        ++k;
+        if (rc) break;
+    }
+    if (steps_done) *steps_done = k;
+    return rc;
+}
+
+// Device-only loop of solute iterations through the captured step graph:
+// no host synchronisation and no regrid inside (the caller keeps the window
+// between regrids).  Used for the timed windows of the benchmark.
+int fdm_advance(fdm_handle *h, int64_t nsteps) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    RC(ensure_lambda(h));
+    cudaGraphExec_t g = nullptr;
+    RC(step_graph(h, &g));
+    for (int64_t k = 0; k < nsteps; ++k) FDM_CK(h, cudaGraphLaunch(g, h->s));
+    h->lam_fresh = true;
+    return FDM_OK;
+}
+
+int fdm_amr(fdm_handle *h) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    return run_amr(h);
+}
+
+int fdm_get_counters(fdm_handle *h, fdm_counters *c) {
+    CHECK_H(h);
+    if (!c) return FDM_ERR_ARG;
+    std::memset(c, 0, sizeof(*c));
+    c->n_leaves = h->NL;
+    c->n_interior = h->NI;
+    c->n_ghost = h->NG;
+    c->n_wls_requests = h->NR - h->n_restrict;
+    c->n_restrict_requests = h->n_restrict;
+    c->n_faces_x = h->NI + h->nux;
+    c->n_faces_y = h->NI + h->nuy;
+    c->n_singular = h->n_singular;
+    c->n_regrids = h->n_regrids;
+    return FDM_OK;
+}
+
+int fdm_debug_stencil(fdm_handle *h, int64_t cap, double *out) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (cap < h->NI) return arg_fail(h, "capacity below the interior leaf count");
+    launch_requests(h, h->B[0].as<double4>());
+    DevBuf d;
+    FDM_CK(h, d.ensure(h->NI * 8 * 32));
+    k_stencil_out<<<nblk(h->NI, 128), 128, 0, h->s>>>(h->tables(), h->B[0].as<double4>(), d.as<double>());
+    FDM_CK(h, cudaMemcpyAsync(out, d.p, h->NI * 8 * 32, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    d.release();
+    return FDM_OK;
+}
+
+int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (cap < h->NL) return arg_fail(h, "capacity below the leaf count");
+    DevBuf d;
+    FDM_CK(h, d.ensure(h->NL * 8 * 8));
+    k_neighbors_out<<<nblk(h->NL, 128), 128, 0, h->s>>>(h->tables(), h->G, d.as<uint64_t>());
+    FDM_CK(h, cudaMemcpyAsync(out, d.p, h->NL * 64, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    d.release();
+    return FDM_OK;
+}
+
+int fdm_device_state(fdm_handle *h, void **stream, double **prim_dev, int64_t *n) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (stream) *stream = (void *)h->s;
+    if (prim_dev) *prim_dev = h->B[0].as<double>();
+    if (n) *n = h->NS;
+    return FDM_OK;
+}
+
+}  // extern "C"

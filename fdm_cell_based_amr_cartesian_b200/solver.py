@@ -1,0 +1,419 @@
+"""Host-side mirror of the reference's driver (program main / solute,
+src/MAIN.F90:1-25, src/solution.F90:171-238) over the libfdm C-ABI.
+
+The names follow the reference: ``creat_mesh`` builds the background grid
+(src/mesh.F90:9-47), ``initial`` evaluates the initial state on the host
+(src/solution.F90:9-69; the vortex formulas are evaluated with the C
+library's exp/pow exactly as written there), ``solute`` runs the time loop,
+``time_advance_rk`` / ``amr`` / ``step_control`` are the device calls.  There
+is no CPU fallback: constructing a Solver without a CUDA device or without
+libfdm.so raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from . import params as P
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfdm.so")
+
+FDM_OK = 0
+FDM_ERR_NAN = 3
+ERRORS = {1: "FDM_ERR_ARG", 2: "FDM_ERR_CUDA", 3: "FDM_ERR_NAN", 4: "FDM_ERR_TIMEOUT",
+          5: "FDM_ERR_NOMEM", 6: "FDM_ERR_STATE", 7: "FDM_ERR_UNSUPPORTED"}
+
+# every extern "C" symbol declared in include/fdm.h
+EXPORTS = [
+    "fdm_create", "fdm_destroy", "fdm_last_error", "fdm_upload_leaves", "fdm_num_leaves",
+    "fdm_download_leaves", "fdm_set_values", "fdm_get_scalars", "fdm_set_scalars",
+    "fdm_step_control", "fdm_time_advance_rk", "fdm_get_rkn", "fdm_solution_cells",
+    "fdm_update_rk", "fdm_body_boundary", "fdm_residual", "fdm_solute_step", "fdm_solute",
+    "fdm_advance", "fdm_amr", "fdm_get_counters", "fdm_debug_stencil", "fdm_debug_neighbors",
+    "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak",
+]
+
+
+class FdmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class FdmCounters(ctypes.Structure):
+    _fields_ = [("n_leaves", ctypes.c_int64), ("n_interior", ctypes.c_int64),
+                ("n_ghost", ctypes.c_int64), ("n_wls_requests", ctypes.c_int64),
+                ("n_restrict_requests", ctypes.c_int64), ("n_faces_x", ctypes.c_int64),
+                ("n_faces_y", ctypes.c_int64), ("n_singular", ctypes.c_int64),
+                ("n_regrids", ctypes.c_int64), ("reserved", ctypes.c_int64 * 8)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libfdm.so and declare the C signatures.  Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run __graft_entry__.build() first")
+    L = ctypes.CDLL(path)
+    vp, i64, i32, dp = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    L.fdm_create.argtypes = [ctypes.POINTER(P.FdmParams), ctypes.POINTER(vp)]
+    L.fdm_destroy.argtypes = [vp]
+    L.fdm_destroy.restype = None
+    L.fdm_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    L.fdm_upload_leaves.argtypes = [vp, i64, u64p, dp]
+    L.fdm_num_leaves.argtypes = [vp]
+    L.fdm_num_leaves.restype = i64
+    L.fdm_download_leaves.argtypes = [vp, i64, ctypes.POINTER(i64), u64p, dp]
+    L.fdm_set_values.argtypes = [vp, i64, dp]
+    L.fdm_get_scalars.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(i64), ctypes.POINTER(i32)]
+    L.fdm_set_scalars.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, i64]
+    L.fdm_step_control.argtypes = [vp, dp, dp, dp, ctypes.POINTER(i32)]
+    L.fdm_time_advance_rk.argtypes = [vp, ctypes.c_double]
+    L.fdm_get_rkn.argtypes = [vp]
+    L.fdm_solution_cells.argtypes = [vp, i32]
+    L.fdm_update_rk.argtypes = [vp, i32]
+    L.fdm_body_boundary.argtypes = [vp, i32]
+    L.fdm_residual.argtypes = [vp, dp, dp]
+    L.fdm_solute_step.argtypes = [vp]
+    L.fdm_solute.argtypes = [vp, i64, ctypes.POINTER(i64)]
+    L.fdm_advance.argtypes = [vp, i64]
+    L.fdm_amr.argtypes = [vp]
+    L.fdm_get_counters.argtypes = [vp, ctypes.POINTER(FdmCounters)]
+    L.fdm_debug_stencil.argtypes = [vp, i64, dp]
+    L.fdm_debug_neighbors.argtypes = [vp, i64, u64p]
+    L.fdm_debug_rot_div.argtypes = [vp, i64, dp, dp, dp]
+    L.fdm_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(dp), ctypes.POINTER(i64)]
+    L.fdm_time_kernels.argtypes = [vp, i32, dp]
+    L.fdm_fp64_peak.argtypes = [dp]
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _u64p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+# ------------------------------------------------------------ host mesh
+def root_keys(m: int, n: int) -> np.ndarray:
+    """Keys of the background cells, cell(1..m*n) (src/mesh.F90:15-37)."""
+    return (np.arange(m * n, dtype=np.uint64) << np.uint64(34))
+
+
+def node_centers(cfg: P.Config, keys: np.ndarray):
+    """Centres by the reference's chain of operations: creat_mesh for the
+    background cell, then one Refine_cell offset per level
+    (src/mesh.F90:25-26, 205-248)."""
+    p = cfg.params
+    keys = np.asarray(keys, dtype=np.uint64)
+    root = (keys >> np.uint64(34)).astype(np.int64)
+    lvl = (keys & np.uint64(15)).astype(np.int64)
+    path = ((keys >> np.uint64(4)) & np.uint64((1 << 30) - 1)).astype(np.int64)
+    nj = (root % p.m + 1).astype(np.float64)
+    ni = (root // p.m + 1).astype(np.float64)
+    cx = 0.5 * (2.0 * nj - 1.0) * p.x_factor * p.h + p.xmin
+    cy = (ni - 0.5) * p.h + p.ymin
+    for k in range(1, int(lvl.max(initial=0)) + 1):
+        act = lvl >= k
+        q = (path >> (2 * (15 - k))) & 3
+        qx = p.x_factor * p.h / float(1 << (k + 1))
+        qy = p.h / float(1 << (k + 1))
+        cx = np.where(act, np.where(q & 1, cx + qx, cx - qx), cx)
+        cy = np.where(act, np.where(q & 2, cy + qy, cy - qy), cy)
+    return cx, cy
+
+
+def initial_state(cfg: P.Config, keys: np.ndarray) -> np.ndarray:
+    """Initial primitive state (rho,u,v,p) per leaf (src/solution.F90:31-69
+    for the vortex; quadrant and oblique-shock states for the extensions)."""
+    p = cfg.params
+    cx, cy = node_centers(cfg, keys)
+    out = np.zeros((len(keys), 4))
+    g = p.gama
+    if cfg.ic_kind == P.IC_VORTEX:
+        cc, pi = 5.0, 3.1415926535897932
+        for i in range(len(keys)):
+            x, y = float(cx[i]), float(cy[i])
+            rr = (x - 5.0) * (x - 5.0) + (y - 5.0) * (y - 5.0)
+            dT = -(g - 1.0) * (cc * cc) * math.exp(1.0 - rr) / (8.0 * g * pi * pi)
+            out[i, 0] = 1.0 + math.pow(1.0 + dT, 1.0 / (g - 1.0)) - 1.0
+            out[i, 1] = 1.0 - (y - 5.0) * cc / (2.0 * pi) * math.exp(0.5 * (1.0 - rr))
+            out[i, 2] = 1.0 + (x - 5.0) * cc / (2.0 * pi) * math.exp(0.5 * (1.0 - rr))
+            out[i, 3] = 1.0 + math.pow(1.0 + dT, g / (g - 1.0)) - 1.0
+    elif cfg.ic_kind == P.IC_QUADRANTS:
+        icp = cfg.ic_params
+        st = np.asarray(icp[2:18], dtype=np.float64).reshape(4, 4)
+        east = cx > icp[0]
+        north = cy > icp[1]
+        q = np.where(north, np.where(east, 0, 1), np.where(east, 3, 2))
+        out[:] = st[q]
+    else:
+        x0, cot = cfg.ic_params[0], cfg.ic_params[1]
+        post = np.array(list(p.dmr_post))
+        pre = np.array(list(p.dmr_pre))
+        xs = x0 + cy * cot
+        out[:] = np.where((cx < xs)[:, None], post[None, :], pre[None, :])
+    return out
+
+
+class Solver:
+    """One solver instance on the current CUDA device (a libfdm handle)."""
+
+    def __init__(self, cfg: P.Config):
+        self.cfg = cfg
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        rc = self.L.fdm_create(ctypes.byref(cfg.params), ctypes.byref(h))
+        if rc:
+            raise FdmError(rc, "fdm_create failed (no CUDA device, or inconsistent parameters)")
+        self.h = h
+
+    # ---- error handling
+    def _check(self, rc: int):
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            self.L.fdm_last_error(self.h, buf, 512)
+            raise FdmError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fdm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- mesh + state
+    def creat_mesh_and_initial(self):
+        """creat_mesh + initial (src/mesh.F90:9-47, src/solution.F90:9-29):
+        background grid, initial state, periodic/extension ghost fill."""
+        keys = root_keys(self.cfg.m, self.cfg.n)
+        prim = initial_state(self.cfg, keys)
+        self.upload(keys, prim)
+        self.body_boundary(1)
+        return keys
+
+    def upload(self, keys, prim):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        prim = np.ascontiguousarray(prim, np.float64)
+        self._check(self.L.fdm_upload_leaves(self.h, len(keys), _u64p(keys), _dp(prim)))
+
+    def set_values(self, prim):
+        prim = np.ascontiguousarray(prim, np.float64)
+        self._check(self.L.fdm_set_values(self.h, len(prim), _dp(prim)))
+
+    def num_leaves(self) -> int:
+        return int(self.L.fdm_num_leaves(self.h))
+
+    def leaves(self):
+        n = self.num_leaves()
+        keys = np.zeros(n, np.uint64)
+        prim = np.zeros((n, 4))
+        nout = ctypes.c_int64()
+        self._check(self.L.fdm_download_leaves(self.h, n, ctypes.byref(nout), _u64p(keys), _dp(prim)))
+        return keys, prim
+
+    def scalars(self) -> dict:
+        lx, ly, dt, tt = (ctypes.c_double() for _ in range(4))
+        it = ctypes.c_int64()
+        lm = ctypes.c_int32()
+        self._check(self.L.fdm_get_scalars(self.h, ctypes.byref(lx), ctypes.byref(ly), ctypes.byref(dt),
+                                           ctypes.byref(tt), ctypes.byref(it), ctypes.byref(lm)))
+        return dict(lambda_x=lx.value, lambda_y=ly.value, tstep=dt.value, tt=tt.value, it=it.value,
+                    l_max=lm.value)
+
+    def set_scalars(self, lambda_x, lambda_y, tstep, tt, it):
+        self._check(self.L.fdm_set_scalars(self.h, lambda_x, lambda_y, tstep, tt, int(it)))
+
+    def counters(self) -> dict:
+        c = FdmCounters()
+        self._check(self.L.fdm_get_counters(self.h, ctypes.byref(c)))
+        return {k: getattr(c, k) for k, _ in FdmCounters._fields_ if k != "reserved"}
+
+    # ---- time loop (reference names)
+    def step_control(self):
+        dt, lx, ly = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        lm = ctypes.c_int32()
+        self._check(self.L.fdm_step_control(self.h, ctypes.byref(dt), ctypes.byref(lx), ctypes.byref(ly),
+                                            ctypes.byref(lm)))
+        return dt.value
+
+    def time_advance_rk(self, tstep: float):
+        self._check(self.L.fdm_time_advance_rk(self.h, float(tstep)))
+
+    def solution_cells(self, krk: int):
+        self._check(self.L.fdm_solution_cells(self.h, krk))
+
+    def update_rk(self, krk: int):
+        self._check(self.L.fdm_update_rk(self.h, krk))
+
+    def body_boundary(self, j: int):
+        self._check(self.L.fdm_body_boundary(self.h, j))
+
+    def residual(self):
+        rmax = np.zeros(4)
+        rrms = np.zeros(4)
+        self._check(self.L.fdm_residual(self.h, _dp(rmax), _dp(rrms)))
+        return rmax, rrms
+
+    def solute_step(self):
+        self._check(self.L.fdm_solute_step(self.h))
+
+    def solute(self, nsteps: int) -> int:
+        done = ctypes.c_int64()
+        self._check(self.L.fdm_solute(self.h, int(nsteps), ctypes.byref(done)))
+        return done.value
+
+    def advance(self, nsteps: int):
+        self._check(self.L.fdm_advance(self.h, int(nsteps)))
+
+    def amr(self):
+        self._check(self.L.fdm_amr(self.h))
+
+    def stencil(self):
+        n = self.counters()["n_interior"]
+        out = np.zeros((n, 8, 4))
+        self._check(self.L.fdm_debug_stencil(self.h, n, _dp(out)))
+        return out
+
+    def neighbors(self):
+        n = self.num_leaves()
+        out = np.zeros((n, 8), np.uint64)
+        self._check(self.L.fdm_debug_neighbors(self.h, n, _u64p(out)))
+        return out
+
+    def rot_div(self):
+        n = self.counters()["n_interior"]
+        rot = np.zeros(n)
+        div = np.zeros(n)
+        sums = np.zeros(3)
+        self._check(self.L.fdm_debug_rot_div(self.h, n, _dp(rot), _dp(div), _dp(sums)))
+        return rot, div, sums
+
+    def time_kernels(self, reps: int = 10):
+        """Average ms per launch: faces (x+y), cells, hanging nodes, ghosts."""
+        ms = np.zeros(4)
+        self._check(self.L.fdm_time_kernels(self.h, int(reps), _dp(ms)))
+        return dict(faces=ms[0], cells=ms[1], requests=ms[2], ghosts=ms[3])
+
+    def device_state(self):
+        s = ctypes.c_void_p()
+        p = ctypes.POINTER(ctypes.c_double)()
+        n = ctypes.c_int64()
+        self._check(self.L.fdm_device_state(self.h, ctypes.byref(s), ctypes.byref(p), ctypes.byref(n)))
+        return s.value, ctypes.cast(p, ctypes.c_void_p).value, n.value
+
+    # ---- diagnostics (output_error, src/output_ADT.F90:18-75)
+    def output_error(self):
+        """L1/L2/Linf density error of the interior leaves against the t = 0
+        vortex, area-weighted as output_error does."""
+        keys, prim = self.leaves()
+        return vortex_error(self.cfg, keys, prim)
+
+
+def vortex_error(cfg: P.Config, keys, prim):
+    p = cfg.params
+    root = (np.asarray(keys, np.uint64) >> np.uint64(34)).astype(np.int64)
+    row, col = root // p.m, root % p.m
+    inter = (row >= 3) & (row < p.n - 3) & (col >= 3) & (col < p.m - 3)
+    lvl = (np.asarray(keys, np.uint64) & np.uint64(15)).astype(np.int64)
+    cx, cy = node_centers(cfg, keys)
+    g = p.gama
+    rr = (cx - 5.0) ** 2 + (cy - 5.0) ** 2
+    dT = -(g - 1.0) * 25.0 * np.exp(1.0 - rr) / (8.0 * g * math.pi ** 2)
+    err = prim[:, 0] - (1.0 + dT) ** (1.0 / (g - 1.0))
+    dy = p.h / (2.0 ** lvl)
+    area = p.x_factor * dy * dy
+    e, a = err[inter], area[inter]
+    return dict(L1=float(np.sum(np.abs(e) * a) / np.sum(a)),
+                L2=float(math.sqrt(np.sum(e * e * a) / np.sum(a))),
+                Linf=float(np.max(np.abs(e))))
+
+
+# ------------------------------------------------- static distance refinement
+def distance_refined_keys(cfg: P.Config, lines, dist_by_level) -> np.ndarray:
+    """Leaf keys of a statically refined mesh, in the manner of the
+    reference's BlockDis_refi (src/mesh.F90:144-172): a leaf at level l is
+    refined when its centre lies within dist_by_level[l] of any of the given
+    axis-parallel lines ("x", c) / ("y", c).  Distances must shrink by at
+    least two cells of the finer level per level so that the result keeps the
+    2:1 balance.  Only interior background cells are refined."""
+    p = cfg.params
+    m, n = cfg.m, cfg.n
+    root = np.arange(m * n, dtype=np.int64)
+    row, col = root // m, root % m
+    lvl = np.zeros_like(root)
+    ix = np.zeros_like(root)
+    iy = np.zeros_like(root)
+    inter = (row >= 3) & (row < n - 3) & (col >= 3) & (col < m - 3)
+    done_r, done_l, done_x, done_y = [], [], [], []
+    cur_r, cur_l, cur_x, cur_y, cur_i = root, lvl, ix, iy, inter
+    for L in range(len(dist_by_level) + 1):
+        hx = p.x_factor * p.h / (1 << L)
+        hy = p.h / (1 << L)
+        cx = p.xmin + col_of(cur_r, m) * p.x_factor * p.h + (cur_x + 0.5) * hx
+        cy = p.ymin + (cur_r // m) * p.h + (cur_y + 0.5) * hy
+        refine = np.zeros(len(cur_r), bool)
+        if L < len(dist_by_level):
+            d = dist_by_level[L]
+            for ax, c in lines:
+                refine |= np.abs((cx if ax == "x" else cy) - c) < d
+            refine &= cur_i
+        keep = ~refine
+        done_r.append(cur_r[keep]); done_l.append(cur_l[keep])
+        done_x.append(cur_x[keep]); done_y.append(cur_y[keep])
+        if not refine.any():
+            break
+        r, l, x, y, it = cur_r[refine], cur_l[refine], cur_x[refine], cur_y[refine], cur_i[refine]
+        cur_r = np.repeat(r, 4)
+        cur_l = np.repeat(l + 1, 4)
+        q = np.tile(np.arange(4), len(r))
+        cur_x = np.repeat(2 * x, 4) + (q & 1)
+        cur_y = np.repeat(2 * y, 4) + (q >> 1)
+        cur_i = np.repeat(it, 4)
+    r = np.concatenate(done_r); l = np.concatenate(done_l)
+    x = np.concatenate(done_x); y = np.concatenate(done_y)
+    s = 15 - l
+    path = morton(x << s, y << s)
+    keys = (r.astype(np.uint64) << np.uint64(34)) | (path.astype(np.uint64) << np.uint64(4)) | l.astype(np.uint64)
+    return np.sort(keys)
+
+
+def col_of(r, m):
+    return r % m
+
+
+def morton(x, y):
+    x = np.asarray(x, np.uint64)
+    y = np.asarray(y, np.uint64)
+    out = np.zeros_like(x)
+    for b in range(15):
+        out |= ((x >> np.uint64(b)) & np.uint64(1)) << np.uint64(2 * b)
+        out |= ((y >> np.uint64(b)) & np.uint64(1)) << np.uint64(2 * b + 1)
+    return out
+
+
+def fp64_peak_tflops() -> float:
+    """Measured FP64 FMA throughput of the current device."""
+    L = load_library()
+    v = ctypes.c_double()
+    rc = L.fdm_fp64_peak(ctypes.byref(v))
+    if rc:
+        raise FdmError(rc, "fdm_fp64_peak failed")
+    return v.value

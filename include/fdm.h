@@ -1,0 +1,227 @@
+/*
+ * fdm.h — C-ABI of libfdm: the B200 (sm_100a) implementation of the
+ * leaf-cell hot path of the cell-based quadtree AMR WCNS solver
+ * (Jian-cd/FDM-cell-based-AMR-Cartesian).
+ *
+ * Every entry point replaces one OpenMP loop or subroutine of the reference
+ * Fortran; the citation on each declaration names it (path:line within the
+ * reference project).  A Fortran host binds these with ISO_C_BINDING
+ * (`bind(C, name="fdm_time_advance_rk")`, `type(c_ptr), value :: h`); the
+ * signatures use only plain pointers, sizes and C scalars.
+ *
+ * Ownership: the caller owns every host array (copied in/out on the call);
+ * the library owns the device buffers, streams and CUDA graphs of a handle
+ * for the handle's lifetime.  A handle is single-threaded: calls are
+ * serialised on the handle's stream and outputs are synchronous on return.
+ * The library never calls exit/abort and never throws across this ABI.
+ */
+#ifndef FDM_H
+#define FDM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define FDM_OK            0
+#define FDM_ERR_ARG       1   /* bad argument / size / inconsistent leaf set        */
+#define FDM_ERR_CUDA      2   /* a CUDA runtime call failed (message in last_error) */
+#define FDM_ERR_NAN       3   /* NaN residual: the reference stops here
+                                 (src/solution.F90:209-215)                         */
+#define FDM_ERR_TIMEOUT   4   /* a bounded device wait ran out                      */
+#define FDM_ERR_NOMEM     5   /* device allocation failed                           */
+#define FDM_ERR_STATE     6   /* call out of order (e.g. step before upload)        */
+#define FDM_ERR_UNSUPPORTED 7 /* configuration outside what the kernels implement   */
+
+/* -------------------------------------------------------- boundary kinds */
+/* BCcyc = 6 is the only kind of the reference (src/module.F90:7).  The other
+ * kinds are extensions for the four-quadrant Riemann and Mach-10 wall cases;
+ * the reference has no counterpart for them. */
+#define FDM_BC_PERIODIC      6
+#define FDM_BC_TRANSMISSIVE  2
+#define FDM_BC_WALL          3   /* reflecting wall (mirror, normal velocity negated) */
+#define FDM_BC_INFLOW        4   /* fixed state bc_state[side]                        */
+#define FDM_BC_DMR_BOTTOM    5   /* inflow for x <= dmr_x0, reflecting wall beyond    */
+#define FDM_BC_DMR_TOP       7   /* exact moving oblique shock (post/pre states)      */
+
+/* sides for bc_state[] */
+#define FDM_SIDE_XM 0
+#define FDM_SIDE_XP 1
+#define FDM_SIDE_YM 2
+#define FDM_SIDE_YP 3
+
+/* ---------------------------------------------------------------- leaf keys
+ * A quadtree node is named by a 64-bit key
+ *     key = root << 34 | path << 4 | lvl
+ * root : 0-based row-major index of the background cell, i.e. cell(root+1)
+ *        of src/mesh.F90:15-37 (num(1) = root / m + 1, num(2) = root % m + 1)
+ * lvl  : refinement level (0 = background cell), lvl <= FDM_LMAX
+ * path : 2 bits per level, level 1 in the most significant pair of the 30-bit
+ *        field; the pair is the child quadrant q = xbit | ybit << 1, so
+ *        son1 (SW) = 0, son2 (SE) = 1, son4 (NW) = 2, son3 (NE) = 3
+ *        (child placement of Refine_cell, src/mesh.F90:204-258).
+ * Sorting leaf keys ascending yields exactly the reference leaf-list order of
+ * IDNSgrid (roots row-major, children son1, son2, son4, son3 —
+ * src/solution.F90:655-670). */
+#define FDM_LMAX 15
+#define FDM_KEY(root, lvl, path) \
+    (((uint64_t)(root) << 34) | ((uint64_t)(path) << 4) | (uint64_t)(lvl))
+#define FDM_KEY_ROOT(k) ((uint64_t)(k) >> 34)
+#define FDM_KEY_LVL(k)  ((uint32_t)((k) & 15u))
+#define FDM_KEY_PATH(k) (((uint64_t)(k) >> 4) & ((1ull << 30) - 1ull))
+
+/* ------------------------------------------------------------- parameters
+ * Mirrors the run parameters of module Global_Var (src/module.F90:16-68) as
+ * set_parameter leaves them (src/MAIN.F90:29-71): the domain is already
+ * padded by the three ghost layers, and every value is the one the Fortran
+ * holds at run time (a REAL(4) literal such as gama = 1.4 is passed as its
+ * promoted value 1.399999976158142). */
+typedef struct fdm_params {
+    double xmin, xmax, ymin, ymax;   /* padded domain (src/MAIN.F90:55-56)      */
+    double h;                        /* background cell size                    */
+    double x_factor;                 /* aspect factor dx = x_factor * dy        */
+    int32_t m, n;                    /* background columns / rows incl. ghosts  */
+    double gama, cv, ma;             /* cv = 1/(gama (gama-1) Ma^2)             */
+
+    int32_t iflag_amr;               /* AMR on/off (src/solution.F90:221)       */
+    int32_t lvl_amr;                 /* maximum AMR level                       */
+    int32_t lvl_max;
+    int32_t nstep_adapt, pstep_adapt;/* regrid when it>=Nstep and mod(it,P)==1  */
+    double refine_goal_rot, refine_goal_div;
+    double coarse_goal_rot, coarse_goal_div;
+
+    int32_t kind_xpbc, kind_xmbc, kind_ypbc, kind_ymbc;
+
+    int32_t iflag_localdt;           /* CFL time step (src/solution.F90:195)    */
+    double cfl, tstep, t_end;
+
+    /* boundary-extension data (no reference counterpart) */
+    double bc_state[4][4];           /* (rho,u,v,p) per side for FDM_BC_INFLOW  */
+    double dmr_x0;                   /* wall start for FDM_BC_DMR_BOTTOM        */
+    double dmr_post[4], dmr_pre[4];  /* post/pre-shock states for the DMR BCs   */
+    double dmr_shock_speed;          /* x-speed of the shock foot on y = ymax   */
+    double dmr_angle_cot;            /* cot(angle) of the shock                 */
+    int32_t flux_variant;            /* 0 = exact (reference op order, no FMA),
+                                        1 = fast (FMA contraction)              */
+    int32_t reserved[7];
+} fdm_params;
+
+typedef struct fdm_handle fdm_handle;
+
+/* Counters the reference only prints (brinv "real matrix singularity!",
+ * src/XuanGua.F90:616-619) or never notices. */
+typedef struct fdm_counters {
+    int64_t n_leaves;          /* all leaves incl. ghosts and corners         */
+    int64_t n_interior;        /* nResgrid (src/solution.F90:599-613)         */
+    int64_t n_ghost;           /* nBCgrid                                     */
+    int64_t n_wls_requests;    /* hanging-node WLS-WENO evaluations per stage */
+    int64_t n_restrict_requests;
+    int64_t n_faces_x, n_faces_y;
+    int64_t n_singular;        /* brinv singular pivots in the WLS geometry   */
+    int64_t n_regrids;
+    int64_t reserved[8];
+} fdm_counters;
+
+/* ------------------------------------------------------------- lifecycle */
+/* Create a handle on the current CUDA device.  Replaces nothing: the
+ * reference keeps its state in module globals (src/module.F90:13-69). */
+int fdm_create(const fdm_params *p, fdm_handle **out);
+void fdm_destroy(fdm_handle *h);
+int fdm_last_error(const fdm_handle *h, char *buf, size_t n);
+
+/* Upload a complete leaf set (interior, ghost and corner leaves in any order)
+ * with primitive values prim[4*i .. 4*i+3] = (rho, u, v, p).  Builds the
+ * device leaf order, neighbour tables, stencil tables and hanging-node
+ * requests.  Equivalent of the tree the reference holds after creat_mesh /
+ * AMR + idneighbor + IDgrid (src/mesh.F90:9-47, src/neighbor.F90:399-449,
+ * src/solution.F90:593-615). */
+int fdm_upload_leaves(fdm_handle *h, int64_t n, const uint64_t *keys,
+                      const double *prim);
+int64_t fdm_num_leaves(const fdm_handle *h);
+/* Download all leaves in key order; cap is the capacity of keys/prim. */
+int fdm_download_leaves(fdm_handle *h, int64_t cap, int64_t *n_out,
+                        uint64_t *keys, double *prim);
+/* Overwrite the primitive values of the current leaf set (same keys as the
+ * last upload/regrid, in key order).  No table rebuild. */
+int fdm_set_values(fdm_handle *h, int64_t n, const double *prim);
+
+/* Scalars of the time loop: lambda_x, lambda_y, tstep, tt, it, l_max. */
+int fdm_get_scalars(fdm_handle *h, double *lambda_x, double *lambda_y,
+                    double *tstep, double *tt, int64_t *it, int32_t *l_max);
+int fdm_set_scalars(fdm_handle *h, double lambda_x, double lambda_y,
+                    double tstep, double tt, int64_t it);
+
+/* ------------------------------------------------------------ time loop */
+/* lambda / time-step control: monotone max of |u|+c, |v|+c over the interior
+ * leaves, l_max, CFL step and t_end clamp (src/solution.F90:185-201). */
+int fdm_step_control(fdm_handle *h, double *tstep, double *lambda_x,
+                     double *lambda_y, int32_t *l_max);
+/* One SSP-RK3 step with the current tstep: getRKn, 3 x (solution_cell loop,
+ * updateRK, body_boundary_RK loop) — Time_advance_RK,
+ * src/solution.F90:267-298. */
+int fdm_time_advance_rk(fdm_handle *h, double tstep);
+/* Fine-grained pieces of Time_advance_RK. */
+int fdm_get_rkn(fdm_handle *h);                       /* src/solution.F90:372-384 */
+int fdm_solution_cells(fdm_handle *h, int32_t krk);   /* src/solution.F90:279-284 */
+int fdm_update_rk(fdm_handle *h, int32_t krk);        /* src/solution.F90:386-404 */
+int fdm_body_boundary(fdm_handle *h, int32_t j);      /* src/solution.F90:288-293 */
+/* Residual norms of the last stage, as Res_max / Res_rms after the
+ * sqrt of src/solution.F90:209-210 (4 equations). */
+int fdm_residual(fdm_handle *h, double res_max[4], double res_rms[4]);
+/* One iteration of the solute loop (src/solution.F90:182-236) without file
+ * output: step control, Time_advance_RK, tt update, NaN check, and AMR +
+ * boundary refill when iflag_amr.  Returns FDM_ERR_NAN on a NaN residual. */
+int fdm_solute_step(fdm_handle *h);
+/* Run solute steps until tt >= t_end or nsteps were taken. */
+int fdm_solute(fdm_handle *h, int64_t nsteps, int64_t *steps_done);
+
+/* Run nsteps solute iterations on the device (step control, RK3 step,
+ * tt/residual/NaN bookkeeping) through a captured CUDA graph, without host
+ * synchronisation and without regrid: the timed window between two regrids
+ * of the solute loop (src/solution.F90:182-219).  Returns when enqueued;
+ * fdm_get_scalars synchronises. */
+int fdm_advance(fdm_handle *h, int64_t nsteps);
+
+/* AMR driver: indicators, refine/coarsen flags, smoothing / 2:1 balance,
+ * neighbour and leaf-list rebuild (src/solution.F90:408-421). */
+int fdm_amr(fdm_handle *h);
+
+int fdm_get_counters(fdm_handle *h, fdm_counters *c);
+
+/* ----------------------------------------------- test / integration hooks */
+/* The 8 stencil values per interior leaf (Tip, Tim, Tjp, Tjm, Tipp, Timm,
+ * Tjpp, Tjmm of src/XuanGua.F90:401-590) for the current values, in interior
+ * key order: out[(i*8 + s)*4 + v].  For parity tests. */
+int fdm_debug_stencil(fdm_handle *h, int64_t cap, double *out);
+/* Face-neighbour and diagonal-neighbour keys per leaf in key order
+ * (idnei, src/neighbor.F90:412-449): out[i*8 + d], d = up, down, right,
+ * left, upleft, upright, downleft, downright; ~0ull for a null pointer. */
+int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out);
+/* AMR indicators rot/div of the interior leaves (src/solution.F90:424-466). */
+int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double *div,
+                      double *srot_sdiv_ne);
+
+/* Device-resident state for in-process callers (bench, Python mirror):
+ * the CUDA stream of the handle and the device pointer of the (rho,u,v,p)
+ * 32-byte slot records: interior leaves in key order, then ghost leaves,
+ * corner leaves and hanging-node values; n receives the slot count. */
+int fdm_device_state(fdm_handle *h, void **stream, double **prim_dev,
+                     int64_t *n);
+
+/* Measurement hooks.  fdm_time_kernels times the kernels of one stage on
+ * the current state with CUDA events on the handle's stream, averaged over
+ * reps launches: ms[0] face fluxes (x and y), ms[1] residual + RK update,
+ * ms[2] hanging-node values, ms[3] ghost fill.  The stage-1/2 buffers are
+ * scratch for this call.  fdm_fp64_peak measures the FP64 FMA throughput of
+ * the current device (TFLOP/s, 2 flops per DFMA).  No reference
+ * counterpart. */
+int fdm_time_kernels(fdm_handle *h, int32_t reps, double *ms);
+int fdm_fp64_peak(double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDM_H */

@@ -1,0 +1,183 @@
+"""GPU (libfdm, sm_100a) vs oracle parity through the C-ABI.
+
+Bar (stated tolerance): conserved/primitive fields within 1e-12 relative per
+step; neighbour tables bit-exact.  The exact build of libfdm keeps the
+reference's operation order without FMA, so most cases are expected to be
+bit-identical; the tests assert the stated tolerance and, where the inputs
+are identical and no library transcendental is involved, bit equality."""
+import numpy as np
+import pytest
+
+from fdm_cell_based_amr_cartesian_b200 import params as P
+from fdm_cell_based_amr_cartesian_b200.solver import FdmError, Solver
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+def snapshot(o):
+    keys, prim, _ = o.leaves()
+    s = o.scalars()
+    return keys, prim, s
+
+
+def gpu_from(cfg, keys, prim, s):
+    g = Solver(cfg)
+    g.upload(keys, prim)
+    g.set_scalars(s["lambda_x"], s["lambda_y"], s["tstep"], s["tt"], s["it"])
+    return g
+
+
+def rel_err(a, b):
+    scale = np.maximum(np.abs(b), 1e-300)
+    return float(np.max(np.abs(a - b) / np.maximum(scale, 1e-14)))
+
+
+def assert_state_close(g, o, exact=False):
+    kg, pg = g.leaves()
+    ko, po, _ = o.leaves()
+    assert np.array_equal(kg, ko), "leaf sets differ"
+    err = rel_err(pg, po)
+    assert err <= REL, f"max relative difference {err:.3e}"
+    if exact:
+        assert np.array_equal(pg, po), f"not bit-identical (max rel {err:.3e})"
+    return err
+
+
+def _run_pair(cfg, pre_steps, steps, oracle_mod, exact=False):
+    o = oracle_mod.Oracle(cfg)
+    o.solute(pre_steps)
+    keys, prim, s = snapshot(o)
+    g = gpu_from(cfg, keys, prim, s)
+    for _ in range(steps):
+        o.solute_step()
+        g.solute_step()
+        assert_state_close(g, o, exact)
+        so, sg = o.scalars(), g.scalars()
+        assert sg["lambda_x"] == so["lambda_x"] and sg["lambda_y"] == so["lambda_y"]
+        assert sg["tstep"] == so["tstep"] and sg["tt"] == so["tt"]
+    return o, g
+
+
+def test_uniform_vortex_steps_bit_exact(oracle_mod):
+    cfg = P.vortex(lvl_amr=0)
+    _run_pair(cfg, 2, 5, oracle_mod, exact=True)
+
+
+def test_amr_vortex_steps(oracle_mod):
+    """Vortex after two regrids: hanging faces with WLS-WENO values."""
+    cfg = P.vortex()
+    o, g = _run_pair(cfg, 12, 6, oracle_mod, exact=True)
+    c = g.counters()
+    assert c["n_wls_requests"] > 0
+
+
+def test_neighbor_tables_bit_exact(oracle_mod):
+    cfg = P.vortex()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(21)
+    keys, prim, s = snapshot(o)
+    g = gpu_from(cfg, keys, prim, s)
+    assert np.array_equal(g.neighbors(), o.neighbors())
+
+
+def test_stencil_values_bit_exact(oracle_mod):
+    cfg = P.vortex()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(21)
+    keys, prim, s = snapshot(o)
+    g = gpu_from(cfg, keys, prim, s)
+    sg, so = g.stencil(), o.stencil()
+    assert sg.shape == so.shape
+    assert np.array_equal(sg, so), f"max abs diff {np.max(np.abs(sg - so)):.3e}"
+
+
+def test_rot_div_and_ordered_sums(oracle_mod):
+    cfg = P.vortex()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(21)
+    keys, prim, s = snapshot(o)
+    g = gpu_from(cfg, keys, prim, s)
+    rg, dg, sums = g.rot_div()
+    ro, do = o.rot_div()
+    so = o.scalars()
+    assert np.array_equal(rg, ro) and np.array_equal(dg, do)
+    assert sums[0] == so["srot"] and sums[1] == so["sdiv"] and int(sums[2]) == so["ne"]
+
+
+def test_riemann4_transmissive_steps(oracle_mod):
+    cfg = P.riemann4(base=32, lvl_amr=2)
+    _run_pair(cfg, 12, 4, oracle_mod)
+
+
+def test_double_mach_wall_inflow_steps(oracle_mod):
+    cfg = P.double_mach(base_y=12, lvl_amr=2)
+    _run_pair(cfg, 6, 4, oracle_mod)
+
+
+def test_split_api_equals_fused(oracle_mod):
+    cfg = P.vortex()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(12)
+    keys, prim, s = snapshot(o)
+    a = gpu_from(cfg, keys, prim, s)
+    b = gpu_from(cfg, keys, prim, s)
+    dt = a.step_control()
+    assert b.step_control() == dt
+    a.time_advance_rk(dt)
+    for krk in (1, 2, 3):
+        b.solution_cells(krk)
+        b.update_rk(krk)
+        b.body_boundary(3)
+    ka, pa = a.leaves()
+    kb, pb = b.leaves()
+    assert np.array_equal(pa, pb)
+
+
+def test_graph_advance_equals_steps(oracle_mod):
+    cfg = P.vortex()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(12)
+    keys, prim, s = snapshot(o)
+    a = gpu_from(cfg, keys, prim, s)
+    b = gpu_from(cfg, keys, prim, s)
+    for _ in range(5):
+        a.solute_step()
+    b.advance(5)
+    assert np.array_equal(a.leaves()[1], b.leaves()[1])
+    assert a.scalars() == b.scalars()
+
+
+def test_invalid_leaf_sets_rejected():
+    cfg = P.vortex(lvl_amr=0)
+    g = Solver(cfg)
+    with pytest.raises(FdmError) as e:
+        g.stencil()
+    assert e.value.code == 6  # FDM_ERR_STATE before any upload
+    m, n = cfg.m, cfg.n
+    keys = (np.arange(m * n, dtype=np.uint64) << np.uint64(34))
+    prim = np.tile([1.0, 0.0, 0.0, 1.0], (len(keys), 1))
+    with pytest.raises(FdmError) as e:          # a missing background cell
+        g.upload(keys[:-1], prim[:-1])
+    assert e.value.code == 1
+    dup = keys.copy()
+    dup[5] = dup[4]
+    with pytest.raises(FdmError) as e:          # duplicate leaf
+        g.upload(dup, prim)
+    assert e.value.code == 1
+    over = np.concatenate([keys, [keys[100] | np.uint64(1)]])
+    with pytest.raises(FdmError):               # a leaf inside another leaf
+        g.upload(over, np.vstack([prim, prim[:1]]))
+    g.upload(keys, prim)                        # the valid set still loads
+
+
+def test_nan_state_stops(oracle_mod):
+    cfg = P.vortex(lvl_amr=0)
+    o = oracle_mod.Oracle(cfg)
+    keys, prim, s = snapshot(o)
+    prim[(cfg.n // 2) * cfg.m + cfg.m // 2, 0] = np.nan   # an interior leaf
+    g = gpu_from(cfg, keys, prim, s)
+    with pytest.raises(FdmError) as e:
+        g.solute_step()
+    assert e.value.code == 3
