@@ -53,9 +53,11 @@ __global__ void k_ordered_sums(int64_t NI, const int32_t *order, const double *r
 static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3) {
     const int64_t NI = h->NI;
     launch_requests(h, h->B[0].as<double4>());
-    FDM_CK(h, h->tmp[0].ensure(NI * 8 * 2 + NI * 4 * 2));
-    uint64_t *k0 = h->tmp[0].as<uint64_t>(), *k1 = k0 + NI;
-    int32_t *i0 = (int32_t *)(k1 + NI), *i1 = i0 + NI;
+    Carve cv;
+    cv.add(NI * 8); cv.add(NI * 8); cv.add(NI * 4); cv.add(NI * 4);
+    FDM_CK(h, h->tmp[0].ensure(cv.total));
+    uint64_t *k0 = cv.at<uint64_t>(h->tmp[0], 0), *k1 = cv.at<uint64_t>(h->tmp[0], 1);
+    int32_t *i0 = cv.at<int32_t>(h->tmp[0], 2), *i1 = cv.at<int32_t>(h->tmp[0], 3);
     k_rot_div<<<nblk(NI, 256), 256, 0, h->s>>>(h->tables(), h->lt, h->B[0].as<double4>(), rot, div, k0, i0);
     size_t bytes = 0;
     FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0, k1, i0, i1, (int)NI, 0, 64, h->s));
@@ -78,8 +80,10 @@ extern "C" int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double
     if (!h->loaded) return FDM_ERR_STATE;
     if (cap < h->NI) return arg_fail(h, "capacity below the interior leaf count");
     DevBuf d;
-    FDM_CK(h, d.ensure(h->NI * 16 + 64));
-    double *dr = d.as<double>(), *dd = dr + h->NI, *ds = dd + h->NI;
+    Carve cv;
+    cv.add(h->NI * 8); cv.add(h->NI * 8); cv.add(3 * 8);
+    FDM_CK(h, d.ensure(cv.total));
+    double *dr = cv.at<double>(d, 0), *dd = cv.at<double>(d, 1), *ds = cv.at<double>(d, 2);
     int rc = compute_rot_div(h, dr, dd, ds);
     if (rc) return rc;
     if (rot) FDM_CK(h, cudaMemcpyAsync(rot, dr, h->NI * 8, cudaMemcpyDeviceToHost, h->s));

@@ -17,7 +17,7 @@ namespace fdm {
 #define FDM_ATAN_BIAS 1.000000013351432e-10   /* REAL(4) 1e-10, src/XuanGua.F90:40 */
 #define FDM_PI_REF 3.1415926535897932
 
-enum BuildErr { BE_PARTITION = 0, BE_NULLNB = 1, BE_OVERFLOW = 2, BE_ROOT = 3, BE_LEVEL = 4 };
+enum BuildErr { BE_PARTITION = 0, BE_NULLNB = 1, BE_OVERFLOW = 2, BE_ROOT = 3, BE_LEVEL = 4, BE_INDEX = 5 };
 
 static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
@@ -271,6 +271,7 @@ struct ReqOut {
     int32_t *m;
     int32_t *mem;
     double *geo;
+    uint64_t *node;
     unsigned long long *counts;   // [0] singular, [1] wls, [2] restrict, [3] copy
 };
 
@@ -295,6 +296,10 @@ __global__ void k_gather(Tables T, Geometry G, ReqDesc D, ReqOut O, int32_t *err
         c.valid = 1;
         node_center(G, c.n, x, y);
         xx = x; yy = y;
+        O.node[r] = node_key(c.n);
+        geo[G_ORIGIN] = 0.0;
+        geo[G_XX] = xx;
+        geo[G_YY] = yy;
         const int qs[4] = {0, 1, 3, 2};
         for (int t = 0; t < 4; ++t) g_search(T, child_ref(T, c, qs[t]), x, y, g);
         if (g.m1 + g.m2 < 8) {
@@ -320,6 +325,10 @@ __global__ void k_gather(Tables T, Geometry G, ReqDesc D, ReqOut O, int32_t *err
         c.valid = 1;
         x = T.lcx[L]; y = T.lcy[L];
         xx = D.tx[r]; yy = D.ty[r];
+        O.node[r] = T.lkey[L];
+        geo[G_ORIGIN] = 1.0;
+        geo[G_XX] = xx;
+        geo[G_YY] = yy;
         g.n1[g.m1++] = L;
         const bool diag = root_cross(G, c.n.root) >= 0;
         const NodeRef nul = null_ref();
@@ -552,6 +561,49 @@ __global__ void k_lmax(int64_t NI, const uint8_t *ilvl, int32_t *out) {
     if ((threadIdx.x & 31) == 0) atomicMax(out, v);
 }
 
+// Every index a stage kernel will dereference is checked once here, so that
+// no stage kernel can read or write outside its buffers.
+__global__ void k_validate(Tables T, int32_t *err) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t NLEAF = T.NI + T.NG + T.NC;
+    bool bad = false;
+    if (t < T.NI * 8) {
+        const int32_t s = T.ist[t];
+        bad |= s < 0 || s >= T.NS;
+    }
+    if (t < T.NI) {
+        bad |= T.ifxl[t] < 0 || T.ifxl[t] >= T.NI + T.nux;
+        bad |= T.ifyl[t] < 0 || T.ifyl[t] >= T.NI + T.nuy;
+    }
+    if (t < T.nux) bad |= T.uxl[t] < 0 || T.uxl[t] >= T.NI;
+    if (t < T.nuy) bad |= T.uyl[t] < 0 || T.uyl[t] >= T.NI;
+    if (t < T.NR) {
+        const int k = T.rq_kind[t];
+        const int32_t a = T.rq_m[2 * t], b = T.rq_m[2 * t + 1];
+        const int32_t *mem = T.rq_mem + t * WLS_MAXM;
+        if (k == RQ_WLS) {
+            bad |= a < 0 || b < 0 || a + b > WLS_MAXM;
+            if (!bad)
+                for (int i = 0; i < a + b; ++i) bad |= mem[i] < 0 || mem[i] >= NLEAF;
+        } else if (k == RQ_RESTRICT) {
+            bad |= a < 0 || b <= a || b > T.NL;
+        } else if (k == RQ_COPY) {
+            bad |= mem[0] < 0 || mem[0] >= NLEAF;
+        } else {
+            bad = true;
+        }
+    }
+    if (t < T.NG) {
+        const int k = T.gh_kind[t];
+        const int32_t a = T.gh_a[t], b = T.gh_b[t];
+        if (k == GH_COPY) bad |= a < 0 || a >= NLEAF;
+        else if (k == GH_RESTRICT) bad |= a < 0 || b <= a || b > T.NL;
+        else if (k == GH_STATE) bad |= a < 0 || a >= 6;
+        else if (k != GH_DMR_TOP && k != GH_NONE) bad = true;
+    }
+    if (bad) atomicExch(err + BE_INDEX, 1);
+}
+
 // ------------------------------------------------------------ host side
 static int scan_i32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n) {
     size_t bytes = 0;
@@ -604,9 +656,11 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     const uint64_t *lkey = h->lkey.as<uint64_t>();
     const int32_t *perm = h->tmp[1].as<int32_t>();
     // 2. classify + partition check
-    FDM_CK(h, h->tmp[2].ensure(n * 4 * 6));
-    int32_t *fI = h->tmp[2].as<int32_t>(), *fG = fI + n, *fC = fG + n;
-    int32_t *sI = fC + n, *sG = sI + n, *sC = sG + n;
+    Carve c2;
+    for (int q = 0; q < 6; ++q) c2.add(n * 4);
+    FDM_CK(h, h->tmp[2].ensure(c2.total));
+    int32_t *fI = c2.at<int32_t>(h->tmp[2], 0), *fG = c2.at<int32_t>(h->tmp[2], 1), *fC = c2.at<int32_t>(h->tmp[2], 2);
+    int32_t *sI = c2.at<int32_t>(h->tmp[2], 3), *sG = c2.at<int32_t>(h->tmp[2], 4), *sC = c2.at<int32_t>(h->tmp[2], 5);
     FDM_CK(h, h->lcross.ensure(n));
     k_classify<<<nblk(n, TB), TB, 0, s>>>(lkey, n, h->G, fI, fG, fC, h->lcross.as<int8_t>(), err);
     FDM_RC(scan_i32(h, fI, sI, n));
@@ -636,16 +690,17 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     const int64_t ne = NI * 8;
     FDM_CK(h, h->ist.ensure(ne * 4));
     FDM_CK(h, h->ilvl.ensure(NI));
-    FDM_CK(h, h->tmp[3].ensure(ne * (4 + 4 + 8 + 8 + 8 + 4 + 4)));
+    Carve c3;
+    c3.add(ne * 4); c3.add(ne * 4); c3.add(ne * 8); c3.add(ne * 8); c3.add(ne * 8); c3.add(ne * 4); c3.add(ne * 4);
+    FDM_CK(h, h->tmp[3].ensure(c3.total));
     ResolveOut RO;
-    char *base = h->tmp[3].as<char>();
-    RO.slot = (int32_t *)base;
-    RO.kind = (int32_t *)(base + ne * 4);
-    RO.ref = (int64_t *)(base + ne * 8);
-    RO.tx = (double *)(base + ne * 16);
-    RO.ty = (double *)(base + ne * 24);
-    int32_t *rflag = (int32_t *)(base + ne * 32);
-    int32_t *ridx = (int32_t *)(base + ne * 36);
+    RO.slot = c3.at<int32_t>(h->tmp[3], 0);
+    RO.kind = c3.at<int32_t>(h->tmp[3], 1);
+    RO.ref = c3.at<int64_t>(h->tmp[3], 2);
+    RO.tx = c3.at<double>(h->tmp[3], 3);
+    RO.ty = c3.at<double>(h->tmp[3], 4);
+    int32_t *rflag = c3.at<int32_t>(h->tmp[3], 5);
+    int32_t *ridx = c3.at<int32_t>(h->tmp[3], 6);
     {
         Tables T = h->tables();
         k_resolve<<<nblk(NI, 128), 128, 0, s>>>(T, h->G, RO, h->ilvl.as<uint8_t>(), err);
@@ -663,26 +718,28 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     h->NS = NI + NG + NC + NR;
     const int64_t VS0 = NI + NG + NC;
     const int64_t nrq = NR > 0 ? NR : 1;
-    FDM_CK(h, h->tmp[4].ensure(nrq * (4 + 8 + 8 + 8)));
+    Carve c4;
+    c4.add(nrq * 4); c4.add(nrq * 8); c4.add(nrq * 8); c4.add(nrq * 8);
+    FDM_CK(h, h->tmp[4].ensure(c4.total));
     ReqDesc RD;
-    char *rb = h->tmp[4].as<char>();
-    RD.kind = (int32_t *)rb;
-    RD.ref = (int64_t *)(rb + nrq * 8);
-    RD.tx = (double *)(rb + nrq * 16);
-    RD.ty = (double *)(rb + nrq * 24);
+    RD.kind = c4.at<int32_t>(h->tmp[4], 0);
+    RD.ref = c4.at<int64_t>(h->tmp[4], 1);
+    RD.tx = c4.at<double>(h->tmp[4], 2);
+    RD.ty = c4.at<double>(h->tmp[4], 3);
     k_emit<<<nblk(ne, TB), TB, 0, s>>>(ne, VS0, RO, ridx, h->ist.as<int32_t>(), RD);
     // 5. requests: gather + WLS geometry
     FDM_CK(h, h->rq_kind.ensure(nrq * 4));
     FDM_CK(h, h->rq_m.ensure(nrq * 8));
     FDM_CK(h, h->rq_mem.ensure(nrq * WLS_MAXM * 4));
     FDM_CK(h, h->rq_geo.ensure(nrq * RQ_GEO * 8));
+    FDM_CK(h, h->rq_node.ensure(nrq * 8));
     FDM_CK(h, h->tmp[5].ensure(64));
     unsigned long long *counts = h->tmp[5].as<unsigned long long>();
     FDM_CK(h, cudaMemsetAsync(counts, 0, 64, s));
     if (NR > 0) {
         Tables T = h->tables();
         ReqOut O{h->rq_kind.as<int32_t>(), h->rq_m.as<int32_t>(), h->rq_mem.as<int32_t>(),
-                 h->rq_geo.as<double>(), counts};
+                 h->rq_geo.as<double>(), h->rq_node.as<uint64_t>(), counts};
         k_gather<<<nblk(NR, 64), 64, 0, s>>>(T, h->G, RD, O, err);
     }
     // 6. ghosts
@@ -700,8 +757,11 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
         k_ghosts<<<nblk(NG, 128), 128, 0, s>>>(T, h->G, h->p, O);
     }
     // 7. faces
-    FDM_CK(h, h->tmp[6].ensure(NI * 4 * 4));
-    int32_t *ux = h->tmp[6].as<int32_t>(), *uy = ux + NI, *sx = uy + NI, *sy = sx + NI;
+    Carve c6;
+    for (int q = 0; q < 4; ++q) c6.add(NI * 4);
+    FDM_CK(h, h->tmp[6].ensure(c6.total));
+    int32_t *ux = c6.at<int32_t>(h->tmp[6], 0), *uy = c6.at<int32_t>(h->tmp[6], 1);
+    int32_t *sx = c6.at<int32_t>(h->tmp[6], 2), *sy = c6.at<int32_t>(h->tmp[6], 3);
     {
         Tables T = h->tables();
         k_face_flags<<<nblk(NI, TB), TB, 0, s>>>(T, ux, uy);
@@ -732,7 +792,15 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
         for (int b = 1; b < 3; ++b)
             FDM_CK(h, cudaMemcpyAsync(h->B[b].as<double4>() + NI + NG, h->B[0].as<double4>() + NI + NG, NC * 32,
                                       cudaMemcpyDeviceToDevice, s));
-    // 9. l_max
+    // 9. index validation of every table the stage kernels use
+    {
+        Tables T = h->tables();
+        int64_t nv = NI * 8;
+        const int64_t others[5] = {nux, nuy, NR, NG, NI};
+        for (int q = 0; q < 5; ++q) nv = nv > others[q] ? nv : others[q];
+        k_validate<<<nblk(nv, TB), TB, 0, s>>>(T, err);
+    }
+    // 10. l_max
     int32_t *dl = err + 7;
     FDM_CK(h, cudaMemsetAsync(dl, 0, 4, s));
     k_lmax<<<nblk(NI, TB), TB, 0, s>>>(NI, h->ilvl.as<uint8_t>(), dl);
@@ -743,6 +811,7 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     FDM_CK(h, cudaStreamSynchronize(s));
     FDM_CK(h, cudaGetLastError());
     if (he[BE_OVERFLOW]) return arg_fail(h, "hanging-node stencil larger than supported");
+    if (he[BE_INDEX]) return arg_fail(h, "internal table check failed: an index is out of range");
     h->l_max = he[7];
     FDM_CK(h, cudaMemcpy(&h->scal.as<DevScalars>()->l_max, &h->l_max, 4, cudaMemcpyHostToDevice));
     h->n_singular += (int64_t)hc[0];

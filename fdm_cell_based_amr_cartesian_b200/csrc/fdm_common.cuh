@@ -66,6 +66,7 @@ struct Tables {
     const int32_t *rq_m;              // [NR][2]  (m1, m2) or (lo, hi) range
     const int32_t *rq_mem;            // [NR][WLS_MAXM] member slots
     const double *rq_geo;             // [NR][RQ_GEO] geometry block
+    const uint64_t *rq_node;          // [NR] key of the node the value belongs to
     // ghosts (slots NI .. NI+NG)
     const int32_t *gh_kind;           // [NG]
     const int32_t *gh_a;              // [NG] source slot / range lo
@@ -84,6 +85,7 @@ constexpr int G_L = G_W + WLS_MAXM;               // inverse 6x6
 constexpr int G_A = G_L + 36;                     // inverse 3x3 (axis points)
 constexpr int G_B = G_A + 9;                      // inverse 3x3 (diagonal points)
 constexpr int G_LVL = G_B + 9;                    // level (restrict) as double
+constexpr int G_ORIGIN = G_LVL + 1;               // 0 parent_value_weno, 1 child_value_weno
 constexpr int RQ_GEO = G_LVL + 2;                 // 96 doubles
 
 // Device-side scalars of the time loop.

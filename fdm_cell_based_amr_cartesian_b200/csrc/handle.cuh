@@ -13,6 +13,10 @@ namespace fdm {
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
     cudaError_t ensure(size_t nbytes) {
         if (nbytes <= bytes && p) return cudaSuccess;
         if (p) cudaFree(p);
@@ -29,6 +33,21 @@ struct DevBuf {
         bytes = 0;
     }
     template <class T> T *as() const { return (T *)p; }
+};
+
+// Carves several arrays out of one scratch buffer: offsets and the total
+// size come from the same list, 256-byte aligned.
+struct Carve {
+    size_t off[16];
+    size_t total = 0;
+    int n = 0;
+    size_t add(size_t bytes) {
+        total = (total + 255) & ~size_t(255);
+        off[n++] = total;
+        total += bytes;
+        return off[n - 1];
+    }
+    template <class T> T *at(const DevBuf &b, int i) const { return (T *)((char *)b.p + off[i]); }
 };
 
 }  // namespace fdm
@@ -52,7 +71,7 @@ struct fdm_handle {
     // tables
     fdm::DevBuf lkey, lslot, slot_leaf, lcx, lcy, lcross;
     fdm::DevBuf ist, ilvl, ifxl, ifyl, uxl, uyl;
-    fdm::DevBuf rq_kind, rq_m, rq_mem, rq_geo;
+    fdm::DevBuf rq_kind, rq_m, rq_mem, rq_geo, rq_node;
     fdm::DevBuf gh_kind, gh_a, gh_b, gh_flip, gh_x, gh_y;
     // state: three slot arrays (step start / stage 1 / stage 2)
     fdm::DevBuf B[3];
@@ -89,6 +108,7 @@ struct fdm_handle {
         T.rq_m = rq_m.as<int32_t>();
         T.rq_mem = rq_mem.as<int32_t>();
         T.rq_geo = rq_geo.as<double>();
+        T.rq_node = rq_node.as<uint64_t>();
         T.gh_kind = gh_kind.as<int32_t>();
         T.gh_a = gh_a.as<int32_t>();
         T.gh_b = gh_b.as<int32_t>();

@@ -61,6 +61,40 @@ __global__ void k_neighbors_out(Tables T, Geometry G, uint64_t *out) {
     for (int d = 0; d < 8; ++d) out[k * 8 + d] = nb[d].valid ? node_key(nb[d].n) : ~0ull;
 }
 
+// hanging-node stencil of every (interior leaf, entry), in the encoding of
+// the oracle's gather export: 0 leaf copy, 1 parent WLS, 2 parent interpA,
+// 3 child WLS, 4 child copy
+__global__ void k_requests_out(Tables T, int32_t *kind, uint64_t *node, double *xy, int32_t *m12,
+                               uint64_t *mem) {
+    const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= T.NI * 8) return;
+    const int32_t s = T.ist[o];
+    const int64_t VS0 = T.NI + T.NG + T.NC;
+    for (int k = 0; k < 16; ++k) mem[o * 16 + k] = ~0ull;
+    if (s < VS0) {
+        kind[o] = 0;
+        node[o] = T.lkey[T.slot_leaf[s]];
+        xy[2 * o] = 0.0; xy[2 * o + 1] = 0.0;
+        m12[2 * o] = 0; m12[2 * o + 1] = 0;
+        return;
+    }
+    const int64_t r = s - VS0;
+    const double *geo = T.rq_geo + r * RQ_GEO;
+    const int k = T.rq_kind[r];
+    const bool child = geo[G_ORIGIN] != 0.0;
+    kind[o] = child ? (k == RQ_WLS ? 3 : 4) : (k == RQ_WLS ? 1 : 2);
+    node[o] = T.rq_node[r];
+    xy[2 * o] = geo[G_XX];
+    xy[2 * o + 1] = geo[G_YY];
+    if (k == RQ_WLS) {
+        const int m1 = T.rq_m[2 * r], m2 = T.rq_m[2 * r + 1];
+        m12[2 * o] = m1; m12[2 * o + 1] = m2;
+        for (int i = 0; i < m1 + m2 && i < 16; ++i) mem[o * 16 + i] = T.lkey[T.slot_leaf[T.rq_mem[r * WLS_MAXM + i]]];
+    } else {
+        m12[2 * o] = -1; m12[2 * o + 1] = -1;
+    }
+}
+
 static int sync_scalars_from_device(fdm_handle *h) {
     FDM_CK(h, cudaMemcpyAsync(h->hs, h->scal.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
@@ -207,7 +241,7 @@ void fdm_destroy(fdm_handle *h) {
     if (h->s) cudaStreamSynchronize(h->s);
     drop_graph(h);
     DevBuf *bufs[] = {&h->lkey, &h->lslot, &h->slot_leaf, &h->lcx, &h->lcy, &h->lcross, &h->ist, &h->ilvl,
-                      &h->ifxl, &h->ifyl, &h->uxl, &h->uyl, &h->rq_kind, &h->rq_m, &h->rq_mem, &h->rq_geo,
+                      &h->ifxl, &h->ifyl, &h->uxl, &h->uyl, &h->rq_kind, &h->rq_m, &h->rq_mem, &h->rq_geo, &h->rq_node,
                       &h->gh_kind, &h->gh_a, &h->gh_b, &h->gh_flip, &h->gh_x, &h->gh_y, &h->B[0], &h->B[1],
                       &h->B[2], &h->Fx, &h->Fy, &h->Ut, &h->scal, &h->res_part, &h->cub_tmp, &h->flag};
     for (DevBuf *b : bufs) b->release();
@@ -459,6 +493,32 @@ int fdm_debug_stencil(fdm_handle *h, int64_t cap, double *out) {
     FDM_CK(h, d.ensure(h->NI * 8 * 32));
     k_stencil_out<<<nblk(h->NI, 128), 128, 0, h->s>>>(h->tables(), h->B[0].as<double4>(), d.as<double>());
     FDM_CK(h, cudaMemcpyAsync(out, d.p, h->NI * 8 * 32, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    d.release();
+    return FDM_OK;
+}
+
+int fdm_debug_requests(fdm_handle *h, int64_t cap, int32_t *kind, uint64_t *node, double *xy, int32_t *m12,
+                       uint64_t *mem) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (cap < h->NI) return arg_fail(h, "capacity below the interior leaf count");
+    const int64_t ne = h->NI * 8;
+    DevBuf d;
+    Carve cv;
+    cv.add(ne * 4); cv.add(ne * 8); cv.add(ne * 16); cv.add(ne * 8); cv.add(ne * 128);
+    FDM_CK(h, d.ensure(cv.total));
+    int32_t *dk = cv.at<int32_t>(d, 0);
+    uint64_t *dn = cv.at<uint64_t>(d, 1);
+    double *dxy = cv.at<double>(d, 2);
+    int32_t *dm = cv.at<int32_t>(d, 3);
+    uint64_t *dmem = cv.at<uint64_t>(d, 4);
+    k_requests_out<<<nblk(ne, 128), 128, 0, h->s>>>(h->tables(), dk, dn, dxy, dm, dmem);
+    FDM_CK(h, cudaMemcpyAsync(kind, dk, ne * 4, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(node, dn, ne * 8, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(xy, dxy, ne * 16, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(m12, dm, ne * 8, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(mem, dmem, ne * 128, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     d.release();
     return FDM_OK;

@@ -34,6 +34,7 @@ EXPORTS = [
     "fdm_step_control", "fdm_time_advance_rk", "fdm_get_rkn", "fdm_solution_cells",
     "fdm_update_rk", "fdm_body_boundary", "fdm_residual", "fdm_solute_step", "fdm_solute",
     "fdm_advance", "fdm_amr", "fdm_get_counters", "fdm_debug_stencil", "fdm_debug_neighbors",
+    "fdm_debug_requests",
     "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak",
 ]
 
@@ -91,6 +92,8 @@ def load_library(path: str = LIB_PATH):
     L.fdm_get_counters.argtypes = [vp, ctypes.POINTER(FdmCounters)]
     L.fdm_debug_stencil.argtypes = [vp, i64, dp]
     L.fdm_debug_neighbors.argtypes = [vp, i64, u64p]
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    L.fdm_debug_requests.argtypes = [vp, i64, i32p, u64p, dp, i32p, u64p]
     L.fdm_debug_rot_div.argtypes = [vp, i64, dp, dp, dp]
     L.fdm_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(dp), ctypes.POINTER(i64)]
     L.fdm_time_kernels.argtypes = [vp, i32, dp]
@@ -297,6 +300,20 @@ class Solver:
         out = np.zeros((n, 8), np.uint64)
         self._check(self.L.fdm_debug_neighbors(self.h, n, _u64p(out)))
         return out
+
+    def requests(self):
+        """Hanging-node stencils per (interior leaf, entry) in the oracle's
+        gather encoding (see fdm_debug_requests)."""
+        n = self.counters()["n_interior"]
+        kind = np.zeros((n, 8), np.int32)
+        node = np.zeros((n, 8), np.uint64)
+        xy = np.zeros((n, 8, 2))
+        m12 = np.zeros((n, 8, 2), np.int32)
+        mem = np.zeros((n, 8, 16), np.uint64)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        self._check(self.L.fdm_debug_requests(self.h, n, kind.ctypes.data_as(i32p), _u64p(node), _dp(xy),
+                                              m12.ctypes.data_as(i32p), _u64p(mem)))
+        return dict(kind=kind, node=node, xy=xy, m12=m12, mem=mem)
 
     def rot_div(self):
         n = self.counters()["n_interior"]

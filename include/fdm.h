@@ -200,6 +200,14 @@ int fdm_debug_stencil(fdm_handle *h, int64_t cap, double *out);
  * (idnei, src/neighbor.F90:412-449): out[i*8 + d], d = up, down, right,
  * left, upleft, upright, downleft, downright; ~0ull for a null pointer. */
 int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out);
+/* Hanging-node stencils per interior leaf and entry (key order, entries as
+ * in fdm_debug_stencil): kind 0 same-level leaf, 1 parent_value_weno WLS,
+ * 2 parent_value_weno interpA fallback, 3 child_value_weno WLS, 4
+ * child_value_weno copy fallback (src/XuanGua.F90:45-150); the node key the
+ * value belongs to, the target point, (m1, m2) and up to 16 member keys of
+ * the WLS stencil in the reference's list order. */
+int fdm_debug_requests(fdm_handle *h, int64_t cap, int32_t *kind, uint64_t *node,
+                       double *xy, int32_t *m12, uint64_t *mem);
 /* AMR indicators rot/div of the interior leaves (src/solution.F90:424-466). */
 int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double *div,
                       double *srot_sdiv_ne);

@@ -522,6 +522,24 @@ static void interpA(Grid *c, double var[NVAR]) {               // :359-398
     for (int k = 0; k < 7; ++k) var[k] = 0.25 * (s1[k] + s2[k] + s3[k] + s4[k]);
 }
 
+// Optional record of the stencil gathered by the next parent/child call
+// (test hook: lets the tests compare the hanging-node stencils themselves).
+struct GatherRec {
+    int kind;           // 0 leaf copy, 1 parent WLS, 2 parent interpA, 3 child WLS, 4 child copy
+    uint64_t node;      // key of the node the value is taken from
+    double xx, yy;
+    int m1, m2;
+    uint64_t mem[16];
+};
+static thread_local GatherRec *tl_rec = nullptr;
+static void rec_lists(const NList &n1, const NList &n2) {
+    if (!tl_rec) return;
+    tl_rec->m1 = n1.n;
+    tl_rec->m2 = n2.n;
+    for (int i = 0; i < n1.n; ++i) tl_rec->mem[i] = n1.a[i]->key;
+    for (int i = 0; i < n2.n; ++i) tl_rec->mem[n1.n + i] = n2.a[i]->key;
+}
+
 static void parent_value_weno(Solver &S, Grid *c, double var[NVAR]) {  // :45-94
     NList n1, n2;
     bool used[8] = {false, false, false, false, false, false, false, false};
@@ -537,6 +555,7 @@ static void parent_value_weno(Solver &S, Grid *c, double var[NVAR]) {  // :45-94
             if (nb[q]) search_cell_5(nb[q], x, y, n1, n2, used);
     }
     m = n1.n + n2.n;
+    if (tl_rec) { rec_lists(n1, n2); tl_rec->node = c->key; tl_rec->xx = x; tl_rec->yy = y; tl_rec->kind = m < 7 ? 2 : 1; }
     if (m < 7) {
         interpA(c, var);
 #pragma omp atomic
@@ -557,6 +576,7 @@ static void child_value_weno(Solver &S, double xx, double yy, Grid *c,
     for (int q = 0; q < 8; ++q)
         if (nb[q]) search_cell_5(nb[q], x, y, n1, n2, used);
     int m = n1.n + n2.n;
+    if (tl_rec) { rec_lists(n1, n2); tl_rec->node = c->key; tl_rec->xx = xx; tl_rec->yy = yy; tl_rec->kind = m < 7 ? 4 : 3; }
     if (m < 7) {
         for (int k = 0; k < 7; ++k) var[k] = c->U[k];
 #pragma omp atomic
@@ -568,6 +588,7 @@ static void child_value_weno(Solver &S, double xx, double yy, Grid *c,
 
 static inline void copyU(const Grid *c, double var[NVAR]) {
     for (int k = 0; k < 7; ++k) var[k] = c->U[k];
+    if (tl_rec) { tl_rec->kind = 0; tl_rec->node = c->key; tl_rec->m1 = 0; tl_rec->m2 = 0; }
 }
 
 // Tip/Tim/Tjp/Tjm (src/XuanGua.F90:401-419, 449-467, 497-515, 545-563)
@@ -1462,6 +1483,32 @@ int orc_export_stencil(void *h, int64_t cap, double *out) {
     }
     return 0;
 }
+// hanging-node stencils of every interior leaf and entry (Tip, Tim, Tjp, Tjm,
+// Tipp, Timm, Tjpp, Tjmm): kind (GatherRec), node key, target, m1/m2 and
+// up to 16 member keys
+int orc_export_gather(void *h, int64_t cap, int32_t *kind, uint64_t *node, double *xy, int32_t *m12,
+                      uint64_t *mem) {
+    Solver *S = (Solver *)h;
+    const int64_t nn = (int64_t)S->cell_NS.size();
+    if (nn > cap) return FDM_ERR_ARG;
+    for (int64_t i = 0; i < nn; ++i) {
+        Grid *c = S->cell_NS[(size_t)i];
+        for (int e = 0; e < 8; ++e) {
+            GatherRec r{};
+            tl_rec = &r;
+            double var[NVAR];
+            const int d = e % 4 == 0 ? D_RIGHT : e % 4 == 1 ? D_LEFT : e % 4 == 2 ? D_UP : D_DOWN;
+            if (e < 4) T1(*S, c, d, var); else T2(*S, c, d, var);
+            tl_rec = nullptr;
+            const int64_t o = i * 8 + e;
+            kind[o] = r.kind; node[o] = r.node; xy[2 * o] = r.xx; xy[2 * o + 1] = r.yy;
+            m12[2 * o] = r.m1; m12[2 * o + 1] = r.m2;
+            for (int k = 0; k < 16; ++k) mem[o * 16 + k] = k < r.m1 + r.m2 ? r.mem[k] : ~0ull;
+        }
+    }
+    return 0;
+}
+
 // cached neighbour keys per leaf (key order): up, down, right, left,
 // upleft, upright, downleft, downright; ~0 for null
 int orc_export_neighbors(void *h, int64_t cap, uint64_t *out) {

@@ -60,6 +60,8 @@ def lib():
         L.orc_export_stencil.argtypes = [vp, i64, dp]
         L.orc_export_neighbors.argtypes = [vp, i64, u64p]
         L.orc_counters.argtypes = [vp, i64p]
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        L.orc_export_gather.argtypes = [vp, i64, i32p, u64p, dp, i32p, u64p]
         L.orc_residual.argtypes = [vp, dp, dp]
         L.orc_wcns_z3.argtypes = [dp, dp, dp, dp, dp]
         L.orc_eigen.argtypes = [ctypes.c_double, i32, dp, dp, dp]
@@ -184,6 +186,21 @@ class Oracle:
         out = np.zeros((n, 8, 4))
         self.L.orc_export_stencil(self.h, n, _dp(out))
         return out
+
+    def gather(self):
+        """Hanging-node stencil of every (interior leaf, entry): kind
+        (0 leaf copy, 1 parent WLS, 2 parent interpA, 3 child WLS, 4 child
+        copy), node key, target (xx, yy), (m1, m2) and member keys."""
+        n = self.num_interior()
+        kind = np.zeros((n, 8), np.int32)
+        node = np.zeros((n, 8), np.uint64)
+        xy = np.zeros((n, 8, 2))
+        m12 = np.zeros((n, 8, 2), np.int32)
+        mem = np.zeros((n, 8, 16), np.uint64)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        self.L.orc_export_gather(self.h, n, kind.ctypes.data_as(i32p), _u64p(node), _dp(xy),
+                                 m12.ctypes.data_as(i32p), _u64p(mem))
+        return dict(kind=kind, node=node, xy=xy, m12=m12, mem=mem)
 
     def neighbors(self):
         n = self.num_leaves()

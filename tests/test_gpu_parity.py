@@ -93,6 +93,28 @@ def test_stencil_values_bit_exact(oracle_mod):
     assert np.array_equal(sg, so), f"max abs diff {np.max(np.abs(sg - so)):.3e}"
 
 
+@pytest.mark.parametrize("name", ["vortex", "riemann4", "double_mach"])
+def test_hanging_node_stencils_bit_exact(oracle_mod, name):
+    """Every hanging-node value: kind (WLS / interpA / copy fallback), node,
+    target point and the WLS member list in the reference's order."""
+    cfg = {"vortex": lambda: P.vortex(),
+           "riemann4": lambda: P.riemann4(base=32, lvl_amr=2),
+           "double_mach": lambda: P.double_mach(base_y=12, lvl_amr=2)}[name]()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(12)
+    keys, prim, s = snapshot(o)
+    g = gpu_from(cfg, keys, prim, s)
+    og, gg = o.gather(), g.requests()
+    assert np.array_equal(gg["kind"], og["kind"])
+    assert np.array_equal(gg["node"], og["node"])
+    req = og["kind"] > 0
+    assert np.array_equal(gg["xy"][req], og["xy"][req])
+    wls = (og["kind"] == 1) | (og["kind"] == 3)
+    assert np.array_equal(gg["m12"][wls], og["m12"][wls])
+    assert np.array_equal(gg["mem"][wls], og["mem"][wls])
+    assert np.array_equal(g.stencil(), o.stencil())
+
+
 def test_rot_div_and_ordered_sums(oracle_mod):
     cfg = P.vortex()
     o = oracle_mod.Oracle(cfg)
