@@ -205,6 +205,74 @@ __device__ __forceinline__ void face_flux(const Prim &s0, const Prim &s1, const 
     for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
 }
 
+// ------------------------------------------------ face flux, 4 lanes/face
+// Lane r of a group of four computes characteristic component r: its row of
+// Ri, the four WCNS_Z3 reconstructions of that component, and, after the
+// reconstructed components are exchanged within the group, row r of R*uL
+// and flux component r.  Every value is formed by the same operations in
+// the same order as in face_flux, so both give identical bits.
+struct EigRow {
+    double u, v, a, q2, H1, H2;
+    double ri[4];   // row r of Ri
+};
+
+template <int DIR>
+__device__ __forceinline__ void eigen_row(const double Um[4], double g, int r, EigRow &E) {
+    const double r0 = Um[0];
+    const double u = Um[1] / Um[0];
+    const double v = Um[2] / Um[0];
+    const double p = (g - 1.0) * r0 * (Um[3] / r0 - 0.5 * (u * u + v * v));
+    const double a = sqrt(g * p / r0);
+    const double q2 = 0.5 * (u * u + v * v);
+    const double aa = a * a, a2 = 2.0 * a * a;
+    E.u = u; E.v = v; E.a = a; E.q2 = q2;
+    const double c = DIR == 0 ? u : v;
+    E.H1 = a * a / (g - 1) + q2 - c * a;
+    E.H2 = a * a / (g - 1) + q2 + c * a;
+    if (r == 0) {
+        E.ri[0] = ((g - 1.0) * q2 + a * c) / a2;
+        E.ri[1] = DIR == 0 ? ((1.0 - g) * u - a) / a2 : ((1.0 - g) * u) / a2;
+        E.ri[2] = DIR == 0 ? ((1.0 - g) * v) / a2 : ((1.0 - g) * v - a) / a2;
+        E.ri[3] = (g - 1.0) / a2;
+    } else if (r == 1) {
+        E.ri[0] = (aa - (g - 1.0) * q2) / aa;
+        E.ri[1] = ((g - 1.0) * u) / aa;
+        E.ri[2] = ((g - 1.0) * v) / aa;
+        E.ri[3] = (1.0 - g) / aa;
+    } else if (r == 2) {
+        E.ri[0] = ((g - 1.0) * q2 - a * c) / a2;
+        E.ri[1] = DIR == 0 ? ((1.0 - g) * u + a) / a2 : ((1.0 - g) * u) / a2;
+        E.ri[2] = DIR == 0 ? ((1.0 - g) * v) / a2 : ((1.0 - g) * v + a) / a2;
+        E.ri[3] = (g - 1.0) / a2;
+    } else {
+        E.ri[0] = DIR == 0 ? v : -u;
+        E.ri[1] = 0.0;
+        E.ri[2] = 0.0;
+        E.ri[3] = 0.0;
+    }
+}
+
+// component r of Ri * X
+template <int DIR>
+__device__ __forceinline__ double project_row(const EigRow &E, int r, const double X[4]) {
+    if (r < 3) return E.ri[0] * X[0] + E.ri[1] * X[1] + E.ri[2] * X[2] + E.ri[3] * X[3];
+    return DIR == 0 ? E.ri[0] * X[0] + -X[2] : E.ri[0] * X[0] + X[1];
+}
+
+// row r of R * uL
+template <int DIR>
+__device__ __forceinline__ double back_row(const EigRow &E, int r, const double uL[4]) {
+    if (r == 0) return uL[0] + uL[1] + uL[2];
+    if (DIR == 0) {
+        if (r == 1) return (E.u - E.a) * uL[0] + E.u * uL[1] + (E.u + E.a) * uL[2];
+        if (r == 2) return E.v * uL[0] + E.v * uL[1] + E.v * uL[2] + -uL[3];
+        return E.H1 * uL[0] + E.q2 * uL[1] + E.H2 * uL[2] + -E.v * uL[3];
+    }
+    if (r == 1) return E.u * uL[0] + E.u * uL[1] + E.u * uL[2] + uL[3];
+    if (r == 2) return (E.v - E.a) * uL[0] + E.v * uL[1] + (E.v + E.a) * uL[2];
+    return E.H1 * uL[0] + E.q2 * uL[1] + E.H2 * uL[2] + E.u * uL[3];
+}
+
 // ------------------------------------------------------------ WLS-WENO
 // integrate_square_poly (src/XuanGua.F90:342-355)
 __device__ __forceinline__ double isq_poly(double k0, double k1, double k2, const double *box) {

@@ -21,31 +21,55 @@ static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 // interpA over a subtree whose leaves are [lo, hi) of the sorted array
 // (src/XuanGua.F90:359-398): children combined as
 // 0.25*(son1 + son2 + son3 + son4) = 0.25*(((q0 + q1) + q3) + q2).
-__device__ double4 restrict_mean(const Tables &T, const double4 *__restrict__ buf, int64_t lo, int64_t hi) {
-    double4 st[48];
-    int sl[48];
+// One warp: the lanes stage the subtree's leaves in shared memory, lane 0
+// folds them in key order with a stack of pending sibling groups.
+constexpr int RW_CAP = 256;     // leaves staged per pass
+constexpr int RW_STACK = 48;    // >= 3 pending siblings x 15 levels + 1
+struct RestrictSmem {
+    double4 v[RW_CAP];
+    int8_t l[RW_CAP];
+    double4 st[RW_STACK];
+    int8_t sl[RW_STACK];
+};
+
+__device__ double4 restrict_warp(const Tables &T, const double4 *__restrict__ buf, int64_t lo, int64_t hi,
+                                 RestrictSmem &sm) {
+    const int lane = threadIdx.x & 31;
     int top = 0;
-    for (int64_t k = lo; k < hi; ++k) {
-        const uint64_t key = __ldg(T.lkey + k);
-        st[top] = buf[__ldg(T.lslot + k)];
-        sl[top] = (int)(key & 15u);
-        ++top;
-        while (top >= 4 && sl[top - 1] == sl[top - 2] && sl[top - 1] == sl[top - 3] && sl[top - 1] == sl[top - 4]) {
-            const double4 e0 = st[top - 4], e1 = st[top - 3], e2 = st[top - 2], e3 = st[top - 1];
-            double4 v;
-            v.x = 0.25 * (e0.x + e1.x + e3.x + e2.x);
-            v.y = 0.25 * (e0.y + e1.y + e3.y + e2.y);
-            v.z = 0.25 * (e0.z + e1.z + e3.z + e2.z);
-            v.w = 0.25 * (e0.w + e1.w + e3.w + e2.w);
-            const int l = sl[top - 1] - 1;
-            top -= 4;
-            st[top] = v;
-            sl[top] = l;
-            ++top;
+    for (int64_t base = lo; base < hi; base += RW_CAP) {
+        const int n = (int)min((int64_t)RW_CAP, hi - base);
+        for (int k = lane; k < n; k += 32) {
+            sm.v[k] = buf[__ldg(T.lslot + base + k)];
+            sm.l[k] = (int8_t)(__ldg(T.lkey + base + k) & 15u);
         }
-        if (top > 44) break;  // cannot happen for a valid subtree
+        __syncwarp();
+        if (lane == 0) {
+            for (int k = 0; k < n; ++k) {
+                if (top >= RW_STACK) break;  // cannot happen for a valid subtree
+                sm.st[top] = sm.v[k];
+                sm.sl[top] = sm.l[k];
+                ++top;
+                while (top >= 4 && sm.sl[top - 1] == sm.sl[top - 2] && sm.sl[top - 1] == sm.sl[top - 3] &&
+                       sm.sl[top - 1] == sm.sl[top - 4]) {
+                    const double4 e0 = sm.st[top - 4], e1 = sm.st[top - 3], e2 = sm.st[top - 2], e3 = sm.st[top - 1];
+                    double4 v;
+                    v.x = 0.25 * (e0.x + e1.x + e3.x + e2.x);
+                    v.y = 0.25 * (e0.y + e1.y + e3.y + e2.y);
+                    v.z = 0.25 * (e0.z + e1.z + e3.z + e2.z);
+                    v.w = 0.25 * (e0.w + e1.w + e3.w + e2.w);
+                    const int8_t l = (int8_t)(sm.sl[top - 1] - 1);
+                    top -= 4;
+                    sm.st[top] = v;
+                    sm.sl[top] = l;
+                    ++top;
+                }
+            }
+        }
+        __syncwarp();
     }
-    return st[0];
+    double4 r = sm.st[0];
+    __syncwarp();
+    return r;
 }
 
 __global__ void __launch_bounds__(64) k_requests(Tables T, double4 *cur) {
@@ -58,10 +82,7 @@ __global__ void __launch_bounds__(64) k_requests(Tables T, double4 *cur) {
         cur[out] = cur[mem[0]];
         return;
     }
-    if (kind == RQ_RESTRICT) {
-        cur[out] = restrict_mean(T, cur, T.rq_m[2 * r], T.rq_m[2 * r + 1]);
-        return;
-    }
+    if (kind == RQ_RESTRICT) return;   // k_requests_restrict
     const int m1 = T.rq_m[2 * r], m2 = T.rq_m[2 * r + 1];
     const int m = m1 + m2;
     const double *geo = T.rq_geo + r * RQ_GEO;
@@ -78,12 +99,23 @@ __global__ void __launch_bounds__(64) k_requests(Tables T, double4 *cur) {
     cur[out] = v;
 }
 
+// interpA fallbacks of parent_value_weno: one warp per request
+__global__ void __launch_bounds__(128) k_requests_restrict(Tables T, double4 *cur) {
+    __shared__ RestrictSmem sm[4];
+    const int64_t r = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (r >= T.NR) return;
+    if (T.rq_kind[r] != RQ_RESTRICT) return;
+    const double4 v = restrict_warp(T, cur, T.rq_m[2 * r], T.rq_m[2 * r + 1], sm[threadIdx.x >> 5]);
+    if ((threadIdx.x & 31) == 0) cur[T.NI + T.NG + T.NC + r] = v;
+}
+
 // One thread per face.  Faces [0, NI) are the right (top) faces of the
 // interior leaves; faces [NI, NI+nu) are left (bottom) faces that are not
-// shared with a same-level neighbour.
-template <int DIR>
-__global__ void __launch_bounds__(128) k_faces(Tables T, const double4 *__restrict__ cur, double4 *F,
-                                                const DevScalars *__restrict__ sc, double g) {
+// shared with a same-level neighbour.  TB threads per block, at least MINB
+// blocks per SM (the register budget follows from both).
+template <int DIR, int TB, int MINB>
+__global__ void __launch_bounds__(TB, MINB) k_faces(Tables T, const double4 *__restrict__ cur, double4 *F,
+                                                    const DevScalars *__restrict__ sc, double g) {
     const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t nu = DIR == 0 ? T.nux : T.nuy;
     if (f >= T.NI + nu) return;
@@ -103,6 +135,67 @@ __global__ void __launch_bounds__(128) k_faces(Tables T, const double4 *__restri
     double out[4];
     face_flux<DIR>(p0, p1, p2, p3, g, lam, out);
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
+}
+
+// Four lanes per face (see face_flux in numerics.cuh for the per-face
+// algebra).  All 32 lanes of a warp run the shuffles; lanes past the last
+// face work on a clamped face and do not store.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_faces4(Tables T, const double4 *__restrict__ cur, double4 *F,
+                                                const DevScalars *__restrict__ sc, double g) {
+    const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nf = T.NI + (DIR == 0 ? T.nux : T.nuy);
+    const int r = (int)(gt & 3);
+    int64_t f = gt >> 2;
+    const bool store = f < nf;
+    if (!store) f = nf - 1;
+    int32_t a, b, c, d;
+    if (f < T.NI) {
+        const int32_t *s = T.ist + f * 8;
+        if (DIR == 0) { a = s[1]; b = (int32_t)f; c = s[0]; d = s[4]; }
+        else { a = s[3]; b = (int32_t)f; c = s[2]; d = s[6]; }
+    } else {
+        const int32_t i = DIR == 0 ? T.uxl[f - T.NI] : T.uyl[f - T.NI];
+        const int32_t *s = T.ist + (int64_t)i * 8;
+        if (DIR == 0) { a = s[5]; b = s[1]; c = i; d = s[0]; }
+        else { a = s[7]; b = s[3]; c = i; d = s[2]; }
+    }
+    const Prim P[4] = {load_prim(cur, a), load_prim(cur, b), load_prim(cur, c), load_prim(cur, d)};
+    const double lam = DIR == 0 ? sc->lambda_x : sc->lambda_y;
+    double Um[4];
+    {
+        double U1[4], U2[4], Fd[4];
+        cons_flux<DIR>(P[1], g, U1, Fd);
+        cons_flux<DIR>(P[2], g, U2, Fd);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Um[k] = (U1[k] + U2[k]) / 2.0;
+    }
+    EigRow E;
+    eigen_row<DIR>(Um, g, r, E);
+    double w[4], q[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double Uk[4], Fk[4];
+        cons_flux<DIR>(P[k], g, Uk, Fk);
+        w[k] = project_row<DIR>(E, r, Uk);
+        q[k] = project_row<DIR>(E, r, Fk);
+    }
+    const double uwL = wcns_z3(w[0], w[1], w[2]);
+    const double uwR = wcns_z3(w[3], w[2], w[1]);
+    const double ugL = wcns_z3(q[0], q[1], q[2]);
+    const double ugR = wcns_z3(q[3], q[2], q[1]);
+    double awL[4], awR[4], agL[4], agR[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        awL[k] = __shfl_sync(0xffffffffu, uwL, k, 4);
+        awR[k] = __shfl_sync(0xffffffffu, uwR, k, 4);
+        agL[k] = __shfl_sync(0xffffffffu, ugL, k, 4);
+        agR[k] = __shfl_sync(0xffffffffu, ugR, k, 4);
+    }
+    const double wL = back_row<DIR>(E, r, awL), wR = back_row<DIR>(E, r, awR);
+    const double gL = back_row<DIR>(E, r, agL), gR = back_row<DIR>(E, r, agR);
+    const double out = 0.5 * (gL + gR - lam * (wR - wL));
+    if (store) reinterpret_cast<double *>(F + f)[r] = out;
 }
 
 // Residual + forward-Euler candidate (LXL) fused with updateRK.
@@ -221,16 +314,20 @@ struct GhostStates {
     double x0, cot, speed;
 };
 
-__global__ void k_ghost(Tables T, double4 *buf, GhostStates GS, const DevScalars *__restrict__ sc, int j) {
-    const int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// one warp per ghost leaf (interpA images can span hundreds of leaves)
+__global__ void __launch_bounds__(128) k_ghost(Tables T, double4 *buf, GhostStates GS,
+                                               const DevScalars *__restrict__ sc, int j) {
+    __shared__ RestrictSmem sm[4];
+    const int64_t gi = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (gi >= T.NG) return;
     const int kind = T.gh_kind[gi];
     if (kind == GH_NONE) return;
     double4 v;
-    if (kind == GH_COPY) {
+    if (kind == GH_RESTRICT) {
+        v = restrict_warp(T, buf, T.gh_a[gi], T.gh_b[gi], sm[threadIdx.x >> 5]);
+    } else if (kind == GH_COPY) {
         v = buf[T.gh_a[gi]];
-    } else if (kind == GH_RESTRICT) {
-        v = restrict_mean(T, buf, T.gh_a[gi], T.gh_b[gi]);
     } else {
         // boundary time of body_boundary_RK (src/solution.F90:320-326)
         double t = sc->tt;
@@ -243,6 +340,7 @@ __global__ void k_ghost(Tables T, double4 *buf, GhostStates GS, const DevScalars
         }
         v = make_double4(GS.s[st][0], GS.s[st][1], GS.s[st][2], GS.s[st][3]);
     }
+    if (lane != 0) return;
     const int fl = T.gh_flip[gi];
     if (fl == 1) v.y = -v.y;
     else if (fl == 2) v.z = -v.z;
@@ -283,13 +381,28 @@ __global__ void k_step_control(DevScalars *sc, fdm_params P, int use_dt) {
     if (sc->tt + sc->tstep > P.t_end) sc->tstep = P.t_end - sc->tt;
 }
 
-__global__ void k_res_finalize(const double *res_part, int nb, DevScalars *sc) {
-    if (threadIdx.x >= 8 || blockIdx.x) return;
-    const int n = threadIdx.x;
-    double v = res_part[n];
-    for (int b = 1; b < nb; ++b) v = n < 4 ? fmax(v, res_part[b * 8 + n]) : v + res_part[b * 8 + n];
-    if (n < 4) sc->res_max[n] = v;
-    else sc->res_rms[n - 4] = v;
+// residual partials -> Res_max / Res_rms sums; fixed reduction tree, so the
+// result is identical run to run
+__global__ void __launch_bounds__(256) k_res_finalize(const double *__restrict__ res_part, int nb, DevScalars *sc) {
+    __shared__ double sh[256][8];
+    double v[8];
+    for (int n = 0; n < 8; ++n) v[n] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 256)
+        for (int n = 0; n < 8; ++n) v[n] = n < 4 ? fmax(v[n], res_part[b * 8 + n]) : v[n] + res_part[b * 8 + n];
+    for (int n = 0; n < 8; ++n) sh[threadIdx.x][n] = v[n];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int n = 0; n < 8; ++n)
+                sh[threadIdx.x][n] = n < 4 ? fmax(sh[threadIdx.x][n], sh[threadIdx.x + w][n])
+                                           : sh[threadIdx.x][n] + sh[threadIdx.x + w][n];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) {
+        const int n = threadIdx.x;
+        if (n < 4) sc->res_max[n] = sh[0][n];
+        else sc->res_rms[n - 4] = sh[0][n];
+    }
 }
 
 // end of one solute iteration: tt, rms, NaN stop, t_end (src/solution.F90:205-215)
@@ -314,18 +427,51 @@ __global__ void k_set_tstep(DevScalars *sc, double tstep) {
 void launch_requests(fdm_handle *h, const double4 *cur) {
     if (h->NR == 0) return;
     k_requests<<<nblk(h->NR, 64), 64, 0, h->s>>>(h->tables(), (double4 *)cur);
+    if (h->n_restrict > 0) k_requests_restrict<<<nblk(h->NR, 4), 128, 0, h->s>>>(h->tables(), (double4 *)cur);
 }
-void launch_faces(fdm_handle *h, const double4 *cur) {
+// Launch shapes of the face kernel that the autotuner chooses from.
+template <int TB, int MINB>
+static void faces_1lane(fdm_handle *h, const double4 *cur) {
     const Tables T = h->tables();
     const DevScalars *sc = h->scal.as<DevScalars>();
-    k_faces<0><<<nblk(h->NI + h->nux, 128), 128, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, h->G.gama);
-    k_faces<1><<<nblk(h->NI + h->nuy, 128), 128, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, h->G.gama);
+    k_faces<0, TB, MINB><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, h->G.gama);
+    k_faces<1, TB, MINB><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, h->G.gama);
 }
+static void faces_4lane(fdm_handle *h, const double4 *cur) {
+    const Tables T = h->tables();
+    const DevScalars *sc = h->scal.as<DevScalars>();
+    k_faces4<0><<<nblk(4 * (h->NI + h->nux), 256), 256, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, h->G.gama);
+    k_faces4<1><<<nblk(4 * (h->NI + h->nuy), 256), 256, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, h->G.gama);
+}
+
+const char *face_variant_name(int v) {
+    switch (v) {
+        case 0: return "1 thread/face, 128 threads, >=3 blocks/SM";
+        case 1: return "1 thread/face, 128 threads, >=4 blocks/SM";
+        case 2: return "1 thread/face, 64 threads, >=7 blocks/SM";
+        case 3: return "1 thread/face, 256 threads, >=2 blocks/SM";
+        case 4: return "4 threads/face, 256 threads";
+        default: return "?";
+    }
+}
+
+void launch_faces(fdm_handle *h, const double4 *cur) {
+    switch (h->face_variant) {
+        case 1: faces_1lane<128, 4>(h, cur); break;
+        case 2: faces_1lane<64, 7>(h, cur); break;
+        case 3: faces_1lane<256, 2>(h, cur); break;
+        case 4: faces_4lane(h, cur); break;
+        default: faces_1lane<128, 3>(h, cur); break;
+    }
+}
+
 void launch_cells(fdm_handle *h, const double4 *cur, const double4 *un, double4 *next, int krk, int mode) {
     const int nb = nblk(h->NI, 256);
     k_cells<<<nb, 256, 0, h->s>>>(h->tables(), h->lt, cur, un, next, h->Fx.as<double4>(), h->Fy.as<double4>(),
                                   h->scal.as<DevScalars>(), h->res_part.as<double>(), krk, mode, h->G.gama);
-    k_res_finalize<<<1, 32, 0, h->s>>>(h->res_part.as<double>(), nb, h->scal.as<DevScalars>());
+    // Res_max / Res_rms are reset every stage and read after the last one
+    // (src/solution.F90:276-277, 209-210): reduce them once, after stage 3
+    if (krk == 3 || mode == 1) k_res_finalize<<<1, 256, 0, h->s>>>(h->res_part.as<double>(), nb, h->scal.as<DevScalars>());
 }
 void launch_ghosts(fdm_handle *h, double4 *next, int j) {
     if (h->NG == 0) return;
@@ -336,7 +482,7 @@ void launch_ghosts(fdm_handle *h, double4 *next, int j) {
     GS.x0 = h->p.dmr_x0;
     GS.cot = h->p.dmr_angle_cot;
     GS.speed = h->p.dmr_shock_speed;
-    k_ghost<<<nblk(h->NG, 256), 256, 0, h->s>>>(h->tables(), next, GS, h->scal.as<DevScalars>(), j);
+    k_ghost<<<nblk(h->NG, 4), 128, 0, h->s>>>(h->tables(), next, GS, h->scal.as<DevScalars>(), j);
 }
 void launch_blend(fdm_handle *h, const double4 *un, double4 *cur, int krk) {
     k_blend<<<nblk(h->NI, 256), 256, 0, h->s>>>(h->NI, un, h->Ut.as<double4>(), cur, krk);

@@ -47,6 +47,52 @@ extern "C" int fdm_time_kernels(fdm_handle *h, int32_t reps, double *ms) {
     return FDM_OK;
 }
 
+namespace fdm {
+const char *face_variant_name(int v);
+constexpr int N_FACE_VARIANTS = 5;
+}
+
+// Autotuner: times every launch shape of the face kernel on the current leaf
+// set (CUDA events on the handle's stream, reps launches each, after one
+// untimed launch) and keeps the fastest.  ms[v] receives the average ms per
+// (x + y) launch pair of variant v.
+extern "C" int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms) {
+    if (!h || reps <= 0) return FDM_ERR_ARG;
+    if (!h->loaded) return FDM_ERR_STATE;
+    cudaEvent_t e[2];
+    FDM_CK(h, cudaEventCreate(&e[0]));
+    FDM_CK(h, cudaEventCreate(&e[1]));
+    const int keep = h->face_variant;
+    double bt = 1e30;
+    int bv = keep;
+    for (int v = 0; v < N_FACE_VARIANTS; ++v) {
+        h->face_variant = v;
+        launch_faces(h, h->B[0].as<double4>());
+        FDM_CK(h, cudaEventRecord(e[0], h->s));
+        for (int r = 0; r < reps; ++r) launch_faces(h, h->B[0].as<double4>());
+        FDM_CK(h, cudaEventRecord(e[1], h->s));
+        FDM_CK(h, cudaEventSynchronize(e[1]));
+        float t = 0.f;
+        FDM_CK(h, cudaEventElapsedTime(&t, e[0], e[1]));
+        const double avg = (double)t / reps;
+        if (ms) ms[v] = avg;
+        if (avg < bt) { bt = avg; bv = v; }
+    }
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+    h->face_variant = bv;
+    h->graph_version = -1;   // the step graph holds the old launch shape
+    if (best) *best = bv;
+    return FDM_OK;
+}
+
+extern "C" int fdm_set_variant(fdm_handle *h, int32_t face_variant) {
+    if (!h || face_variant < 0 || face_variant >= N_FACE_VARIANTS) return FDM_ERR_ARG;
+    h->face_variant = face_variant;
+    h->graph_version = -1;
+    return FDM_OK;
+}
+
 extern "C" int fdm_fp64_peak(double *tflops) {
     if (!tflops) return FDM_ERR_ARG;
     int dev = 0, sms = 0;

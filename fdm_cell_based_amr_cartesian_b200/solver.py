@@ -35,7 +35,8 @@ EXPORTS = [
     "fdm_update_rk", "fdm_body_boundary", "fdm_residual", "fdm_solute_step", "fdm_solute",
     "fdm_advance", "fdm_amr", "fdm_get_counters", "fdm_debug_stencil", "fdm_debug_neighbors",
     "fdm_debug_requests",
-    "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak",
+    "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
+    "fdm_set_variant",
 ]
 
 
@@ -98,6 +99,8 @@ def load_library(path: str = LIB_PATH):
     L.fdm_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(dp), ctypes.POINTER(i64)]
     L.fdm_time_kernels.argtypes = [vp, i32, dp]
     L.fdm_fp64_peak.argtypes = [dp]
+    L.fdm_autotune.argtypes = [vp, i32, ctypes.POINTER(i32), dp]
+    L.fdm_set_variant.argtypes = [vp, i32]
     _lib = L
     return L
 
@@ -328,6 +331,16 @@ class Solver:
         ms = np.zeros(4)
         self._check(self.L.fdm_time_kernels(self.h, int(reps), _dp(ms)))
         return dict(faces=ms[0], cells=ms[1], requests=ms[2], ghosts=ms[3])
+
+    def autotune(self, reps: int = 5):
+        """Pick the fastest face-kernel launch shape for this leaf set."""
+        best = ctypes.c_int32()
+        ms = np.zeros(5)
+        self._check(self.L.fdm_autotune(self.h, int(reps), ctypes.byref(best), _dp(ms)))
+        return best.value, ms
+
+    def set_variant(self, v: int):
+        self._check(self.L.fdm_set_variant(self.h, int(v)))
 
     def device_state(self):
         s = ctypes.c_void_p()
