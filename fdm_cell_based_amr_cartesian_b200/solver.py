@@ -36,7 +36,7 @@ EXPORTS = [
     "fdm_advance", "fdm_amr", "fdm_get_counters", "fdm_debug_stencil", "fdm_debug_neighbors",
     "fdm_debug_requests",
     "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
-    "fdm_set_variant",
+    "fdm_set_variant", "fdm_time_advance_rk_uniform_static",
 ]
 
 
@@ -101,6 +101,9 @@ def load_library(path: str = LIB_PATH):
     L.fdm_fp64_peak.argtypes = [dp]
     L.fdm_autotune.argtypes = [vp, i32, ctypes.POINTER(i32), dp]
     L.fdm_set_variant.argtypes = [vp, i32]
+    L.fdm_time_advance_rk_uniform_static.argtypes = [vp, vp, i32, i32, ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_double, vp]
     _lib = L
     return L
 

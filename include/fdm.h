@@ -234,6 +234,41 @@ int fdm_fp64_peak(double *tflops);
 int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms);
 int fdm_set_variant(fdm_handle *h, int32_t face_variant);
 
+/* ------------------------------------------------- no-allocation entry point
+ * One SSP-RK3 step (the three stages of Time_advance_RK with periodic ghost
+ * fill) on a uniform periodic grid of nx x ny cells, without allocating any
+ * device memory.  No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc — a host whose GPU memory belongs to its own
+ * allocator (an OpenACC or CUDA Fortran runtime that owns the device heap),
+ * code that runs under a memory budget fixed at start-up, or a process that
+ * forbids device allocation after initialisation.
+ *
+ * prim_in / prim_out: device arrays of (nx+6)*(ny+6) 32-byte records
+ * (rho,u,v,p), 32-byte aligned, row-major over the background grid with its
+ * three ghost layers (the order of cell(1..m*n)); prim_in holds filled
+ * ghosts, prim_out receives the new interior, its periodic ghosts and the
+ * input corners.  lambda_x/lambda_y are the global Lax-Friedrichs speeds of
+ * the step.  Enqueued on `stream` (0 = legacy default stream); synchronise
+ * before reading prim_out.
+ *
+ * Working memory (the two intermediate stage states and the face fluxes) is
+ * a fixed 8.5 MiB static device array that every GPU loading libfdm holds
+ * until the process exits.  Limits: 3 <= nx, ny <= FDM_STATIC_MAX_SIDE and
+ * nx*ny <= FDM_STATIC_MAX_CELLS; larger sizes return FDM_ERR_ARG and enqueue
+ * nothing.  Every call shares that array and every record a call reads was
+ * written earlier by the same call, so nothing carries over from a previous
+ * call; calls that overlap on the GPU (different streams, or different host
+ * threads on one device) race on it and must be serialised by the caller.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. */
+#define FDM_STATIC_MAX_SIDE  1024
+#define FDM_STATIC_MAX_CELLS 65536
+int fdm_time_advance_rk_uniform_static(const double *prim_in, double *prim_out,
+                                       int32_t nx, int32_t ny, double h, double x_factor,
+                                       double gama, double lambda_x, double lambda_y,
+                                       double tstep, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
