@@ -67,9 +67,902 @@ static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3
     return FDM_OK;
 }
 
+// ===================================================================
+// Regrid.  The tree is handled as a node set: every leaf and every internal
+// node, sorted by key, each with a value.  Internal nodes carry the value
+// the reference leaves in a refined cell (its U when it was refined, or the
+// interpA mean when it was coarsened), because gridmodify4 can copy it back
+// into new leaves (Refine_cell of a non-leaf, src/mesh.F90:389-392).
+// ===================================================================
+
+struct NodeSet {
+    int64_t n = 0;
+    uint64_t *key = nullptr;
+    uint8_t *leaf = nullptr;
+    double4 *val = nullptr;
+};
+
+enum { D_NONE = 0, D_REFINE = 1, D_COARSEN = 2 };
+enum { PF_LEAF = 1, PF_DELETED = 2 };
+
+__device__ __forceinline__ int64_t find_key(const uint64_t *__restrict__ keys, int64_t n, uint64_t k) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const uint64_t v = keys[mid];
+        if (v < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && keys[lo] == k) ? lo : -1;
+}
+
+FDM_HD uint64_t parent_key(uint64_t k) {
+    Node n = node_of_key(k);
+    n.lvl -= 1;
+    n.ix >>= 1;
+    n.iy >>= 1;
+    return node_key(n);
+}
+FDM_HD uint64_t child_key(uint64_t k, int q) {
+    Node n = node_of_key(k);
+    n.lvl += 1;
+    n.ix = 2u * n.ix + (uint32_t)(q & 1);
+    n.iy = 2u * n.iy + (uint32_t)(q >> 1);
+    return node_key(n);
+}
+// same-level neighbour node key across a face; false across the grid edge
+FDM_HD bool shift_key(const Geometry &G, uint64_t k, int dir, uint64_t &out) {
+    Node n = node_of_key(k);
+    int64_t row = n.root / G.m, col = n.root % G.m;
+    const uint32_t N = 1u << n.lvl;
+    switch (dir) {
+        case DIR_UP:
+            if (n.iy + 1 == N) { if (row + 1 >= G.n) return false; ++row; n.iy = 0; } else ++n.iy;
+            break;
+        case DIR_DOWN:
+            if (n.iy == 0) { if (row == 0) return false; --row; n.iy = N - 1; } else --n.iy;
+            break;
+        case DIR_RIGHT:
+            if (n.ix + 1 == N) { if (col + 1 >= G.m) return false; ++col; n.ix = 0; } else ++n.ix;
+            break;
+        default:
+            if (n.ix == 0) { if (col == 0) return false; --col; n.ix = N - 1; } else --n.ix;
+            break;
+    }
+    n.root = row * G.m + col;
+    out = node_key(n);
+    return true;
+}
+// traversal rank of gridmodify4 / solute_div_rot (sons 1,2,3,4): Morton path
+// with the digits of son3 and son4 swapped
+FDM_HD uint64_t dfs_rank(uint64_t k) {
+    const uint64_t path = key_pos(k) & ((1ull << 30) - 1ull);
+    return ((k >> 34) << 30) | (path ^ ((path & 0x2AAAAAAAull) >> 1));
+}
+// post-order rank of gridmodify1 (a node after all of its descendants):
+// 3 bits per level, sons 1,2,3,4 -> 0,1,2,3 and 4 below the node's level
+FDM_HD uint64_t post_rank(uint64_t k) {
+    const Node n = node_of_key(k);
+    const uint64_t path = key_pos(k) & ((1ull << 30) - 1ull);
+    uint64_t r = 0;
+    for (int l = 1; l <= LMAX; ++l) {
+        uint64_t dgt = 4;
+        if (l <= n.lvl) {
+            const uint64_t q = (path >> (2 * (LMAX - l))) & 3u;
+            dgt = q ^ (q >> 1);
+        }
+        r = (r << 3) | dgt;
+    }
+    return ((uint64_t)n.root << 45) | r;
+}
+
+__device__ __forceinline__ double4 mean4(const double4 &c0, const double4 &c1, const double4 &c2, const double4 &c3) {
+    // interpA: 0.25*(son1 + son2 + son3 + son4) with son3 = q3, son4 = q2
+    double4 v;
+    v.x = 0.25 * (c0.x + c1.x + c3.x + c2.x);
+    v.y = 0.25 * (c0.y + c1.y + c3.y + c2.y);
+    v.z = 0.25 * (c0.z + c1.z + c3.z + c2.z);
+    v.w = 0.25 * (c0.w + c1.w + c3.w + c2.w);
+    return v;
+}
+
+// ---------------------------------------------------- internal node values
+__global__ void k_anc_count(int64_t NL, const uint64_t *lkey, int32_t *cnt) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < NL) cnt[k] = (int32_t)(lkey[k] & 15u);
+}
+__global__ void k_anc_emit(int64_t NL, const uint64_t *lkey, const int32_t *off, uint64_t *out) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NL) return;
+    uint64_t a = lkey[k];
+    const int l = (int)(a & 15u);
+    for (int j = 0; j < l; ++j) {
+        a = parent_key(a);
+        out[off[k] + j] = a;
+    }
+}
+// interpA of internal nodes at one level from their children (leaves or
+// deeper internal nodes, already done)
+__global__ void k_internal_vals(int64_t NInt, const uint64_t *ikey, double4 *ival, int lvl, const uint64_t *lkey,
+                                int64_t NL, const int32_t *lslot, const double4 *B0) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= NInt) return;
+    const uint64_t k = ikey[i];
+    if ((int)(k & 15u) != lvl) return;
+    double4 c[4];
+    for (int q = 0; q < 4; ++q) {
+        const uint64_t ck = child_key(k, q);
+        const int64_t li = find_key(lkey, NL, ck);
+        if (li >= 0) c[q] = B0[lslot[li]];
+        else {
+            const int64_t ii = find_key(ikey, NInt, ck);
+            c[q] = ii >= 0 ? ival[ii] : make_double4(0, 0, 0, 0);
+        }
+    }
+    ival[i] = mean4(c[0], c[1], c[2], c[3]);
+}
+
+// ------------------------------------------------------------- sorting
+__global__ void k_iota(int64_t n, int32_t *o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) o[i] = (int32_t)i;
+}
+__global__ void k_gather_nodes(int64_t n, const int32_t *perm, const uint8_t *leaf_in, const double4 *val_in,
+                               uint8_t *leaf_out, double4 *val_out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    leaf_out[i] = leaf_in[perm[i]];
+    val_out[i] = val_in[perm[i]];
+}
+
+struct AmrCtx {
+    fdm_handle *h;
+    NodeSet A, B;          // current / next node set
+    int a = 0;             // which buffer triple (amr[0..2] or amr[3..5]) holds A
+    int64_t cap = 0;       // capacity of both triples
+};
+
+static void bind_sets(fdm_handle *h, AmrCtx &X) {
+    const int64_t na = X.A.n, nb = X.B.n;
+    NodeSet *S[2] = {&X.A, &X.B};
+    for (int s = 0; s < 2; ++s) {
+        const int b = s == 0 ? X.a : 1 - X.a;
+        S[s]->key = h->amr[3 * b + 0].as<uint64_t>();
+        S[s]->leaf = h->amr[3 * b + 1].as<uint8_t>();
+        S[s]->val = h->amr[3 * b + 2].as<double4>();
+    }
+    X.A.n = na;
+    X.B.n = nb;
+}
+static void swap_sets(fdm_handle *h, AmrCtx &X) {
+    X.a = 1 - X.a;
+    std::swap(X.A.n, X.B.n);
+    bind_sets(h, X);
+}
+// room for n nodes in both triples; the contents of both are dropped when
+// they have to grow (callers grow only before writing into B, after A's last
+// reader has finished)
+static int grow_nodes(fdm_handle *h, AmrCtx &X, int64_t n) {
+    if (n <= X.cap) return FDM_OK;
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    const int64_t c = n + n / 2 + 1024;
+    for (int s = 0; s < 2; ++s) {
+        FDM_CK(h, h->amr[3 * s + 0].ensure(c * 8));
+        FDM_CK(h, h->amr[3 * s + 1].ensure(c));
+        FDM_CK(h, h->amr[3 * s + 2].ensure(c * 32));
+    }
+    X.cap = c;
+    bind_sets(h, X);
+    return FDM_OK;
+}
+
+// sort (keys, leaf, val) of length n (unsorted, in the given device arrays)
+// into the node set `out`
+static int sort_into(fdm_handle *h, int64_t n, const uint64_t *keys, const uint8_t *leaf, const double4 *val,
+                     NodeSet &out) {
+    const int TB = 256;
+    FDM_CK(h, h->amr[6].ensure(n * 4 + 16));
+    FDM_CK(h, h->amr[7].ensure(n * 4 + 16));
+    int32_t *iota = h->amr[6].as<int32_t>(), *perm = h->amr[7].as<int32_t>();
+    k_iota<<<nblk(n, TB), TB, 0, h->s>>>(n, iota);
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, out.key, iota, perm, (int)n, 0, 64, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys, out.key, iota, perm, (int)n, 0, 64, h->s));
+    k_gather_nodes<<<nblk(n, TB), TB, 0, h->s>>>(n, perm, leaf, val, out.leaf, out.val);
+    out.n = n;
+    return FDM_OK;
+}
+
+static int scan_total32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n, int64_t &total) {
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceScan::ExclusiveSum(h->cub_tmp.p, bytes, in, out, (int)n, h->s));
+    int32_t a = 0, b = 0;
+    FDM_CK(h, cudaMemcpyAsync(&a, in + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(&b, out + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    total = (int64_t)a + b;
+    return FDM_OK;
+}
+
+// internal nodes and their interpA values from the current leaf set
+// (values as the reference's import of a leaf set would give them)
+int init_internal(fdm_handle *h) {
+    const int TB = 256;
+    const int64_t NL = h->NL;
+    Carve cv;
+    cv.add(NL * 4); cv.add(NL * 4);
+    FDM_CK(h, h->amr[8].ensure(cv.total));
+    int32_t *cnt = cv.at<int32_t>(h->amr[8], 0), *off = cv.at<int32_t>(h->amr[8], 1);
+    k_anc_count<<<nblk(NL, TB), TB, 0, h->s>>>(NL, h->lkey.as<uint64_t>(), cnt);
+    int64_t na = 0;
+    int rc = scan_total32(h, cnt, off, NL, na);
+    if (rc) return rc;
+    h->NInt = 0;
+    if (na == 0) return FDM_OK;
+    FDM_CK(h, h->amr[9].ensure(na * 8 * 2 + 64));
+    uint64_t *anc = h->amr[9].as<uint64_t>(), *srt = anc + na;
+    k_anc_emit<<<nblk(NL, TB), TB, 0, h->s>>>(NL, h->lkey.as<uint64_t>(), off, anc);
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceRadixSort::SortKeys(nullptr, bytes, anc, srt, (int)na, 0, 64, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceRadixSort::SortKeys(h->cub_tmp.p, bytes, anc, srt, (int)na, 0, 64, h->s));
+    FDM_CK(h, h->ikey.ensure(na * 8));
+    FDM_CK(h, h->amr[10].ensure(16));
+    int64_t *nsel = h->amr[10].as<int64_t>();
+    bytes = 0;
+    FDM_CK(h, cub::DeviceSelect::Unique(nullptr, bytes, srt, h->ikey.as<uint64_t>(), nsel, (int)na, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceSelect::Unique(h->cub_tmp.p, bytes, srt, h->ikey.as<uint64_t>(), nsel, (int)na, h->s));
+    int64_t ni = 0;
+    FDM_CK(h, cudaMemcpyAsync(&ni, nsel, 8, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    h->NInt = ni;
+    FDM_CK(h, h->ival.ensure(ni * 32 + 32));
+    for (int l = MAXLVL_TAB - 2; l >= 0; --l)
+        k_internal_vals<<<nblk(ni, TB), TB, 0, h->s>>>(ni, h->ikey.as<uint64_t>(), h->ival.as<double4>(), l,
+                                                      h->lkey.as<uint64_t>(), NL, h->lslot.as<int32_t>(),
+                                                      h->B[0].as<double4>());
+    FDM_CK(h, cudaGetLastError());
+    return FDM_OK;
+}
+
+// ----------------------------------------------------------- solute_ref
+// refine flags of the leaves (solute_ref_sub, src/solution.F90:519-535)
+__global__ void k_refine_flags(Tables T, Geometry G, fdm_params P, const double *rot_slot, const double *div_slot,
+                               const double *sums, int8_t *rflag) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= T.NL) return;
+    const uint64_t key = T.lkey[k];
+    const int lvl = (int)(key & 15u);
+    const int cr = root_cross(G, (int64_t)(key >> 34));
+    const int32_t s = T.lslot[k];
+    rflag[k] = 0;
+    if ((cr == 0 || cr == 1) && lvl < P.lvl_amr && s < T.NI) {
+        const double arot = sqrt(sums[0] / sums[2]);
+        const double adiv = sqrt(sums[1] / sums[2]);
+        if (rot_slot[s] > P.refine_goal_rot * arot || div_slot[s] > P.refine_goal_div * adiv) rflag[k] = 1;
+    }
+}
+// coarsen flags of internal nodes (solute_coarse_sub, src/solution.F90:490-517):
+// all four sons are leaves, none refined in this pass, means below the goals
+__global__ void k_coarsen_flags(int64_t NInt, const uint64_t *ikey, Tables T, fdm_params P, const double *rot_slot,
+                                const double *div_slot, const double *sums, const int8_t *rflag, int8_t *cflag) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= NInt) return;
+    cflag[i] = 0;
+    const uint64_t k = ikey[i];
+    if ((int)(k & 15u) >= P.lvl_amr) return;
+    double r[4], d[4];
+    for (int q = 0; q < 4; ++q) {
+        const int64_t li = find_key(T.lkey, T.NL, child_key(k, q));
+        if (li < 0 || rflag[li]) return;
+        const int32_t s = T.lslot[li];
+        r[q] = s < T.NI ? rot_slot[s] : 0.0;
+        d[q] = s < T.NI ? div_slot[s] : 0.0;
+    }
+    const double arot = sqrt(sums[0] / sums[2]);
+    const double adiv = sqrt(sums[1] / sums[2]);
+    // son1 + son2 + son3 + son4 = q0 + q1 + q3 + q2
+    if ((r[0] + r[1] + r[3] + r[2]) / 4 < P.coarse_goal_rot * arot &&
+        (d[0] + d[1] + d[3] + d[2]) / 4 < P.coarse_goal_div * adiv)
+        cflag[i] = 1;
+}
+__global__ void k_ref_count(Tables T, const int8_t *rflag, const uint64_t *ikey, int64_t NInt, const int8_t *cflag,
+                            int32_t *cnt) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < T.NL) {
+        const uint64_t key = T.lkey[k];
+        int c = rflag[k] ? 5 : 1;
+        if ((key & 15u) > 0) {
+            const int64_t pi = find_key(ikey, NInt, parent_key(key));
+            if (pi >= 0 && cflag[pi]) c = 0;
+        }
+        cnt[k] = c;
+    } else if (k < T.NL + NInt) {
+        cnt[k] = 1;
+    }
+}
+__global__ void k_ref_emit(Tables T, const double4 *B0, const int8_t *rflag, const uint64_t *ikey, const double4 *ival,
+                           int64_t NInt, const int8_t *cflag, const int32_t *off, uint64_t *okey, uint8_t *oleaf,
+                           double4 *oval) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < T.NL) {
+        const uint64_t key = T.lkey[k];
+        if ((key & 15u) > 0) {
+            const int64_t pi = find_key(ikey, NInt, parent_key(key));
+            if (pi >= 0 && cflag[pi]) return;
+        }
+        const double4 v = B0[T.lslot[k]];
+        int64_t o = off[k];
+        okey[o] = key; oleaf[o] = rflag[k] ? 0 : 1; oval[o] = v;
+        if (rflag[k]) {   // Refine_cell: sons copy U (src/mesh.F90:210-252)
+            for (int q = 0; q < 4; ++q) {
+                okey[o + 1 + q] = child_key(key, q); oleaf[o + 1 + q] = 1; oval[o + 1 + q] = v;
+            }
+        }
+    } else if (k < T.NL + NInt) {
+        const int64_t i = k - T.NL;
+        const uint64_t key = ikey[i];
+        const int64_t o = off[k];
+        okey[o] = key;
+        if (cflag[i]) {   // Coarse_cell: interpA of the four leaf sons (src/mesh.F90:397-408)
+            double4 c[4];
+            for (int q = 0; q < 4; ++q) c[q] = B0[T.lslot[find_key(T.lkey, T.NL, child_key(key, q))]];
+            oleaf[o] = 1;
+            oval[o] = mean4(c[0], c[1], c[2], c[3]);
+        } else {
+            oleaf[o] = 0;
+            oval[o] = ival[i];
+        }
+    }
+}
+
+// ----------------------------------------------------------- gridmodify1
+struct Links {
+    int32_t *parent, *child, *nb, *rank;   // child[4 n], nb[4 n] (up, down, right, left)
+    uint8_t *leaf0;
+    int8_t *cross;
+};
+__global__ void k_gm1_links(NodeSet A, Geometry G, Links L, uint64_t *pkey, int32_t *pidx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const uint64_t k = A.key[i];
+    const int lvl = (int)(k & 15u);
+    L.parent[i] = lvl > 0 ? (int32_t)find_key(A.key, A.n, parent_key(k)) : -1;
+    L.leaf0[i] = A.leaf[i];
+    L.cross[i] = (int8_t)root_cross(G, (int64_t)(k >> 34));
+    for (int q = 0; q < 4; ++q)
+        L.child[4 * i + q] = A.leaf[i] ? -1 : (int32_t)find_key(A.key, A.n, child_key(k, q));
+    for (int d = 0; d < 4; ++d) {
+        uint64_t nk;
+        L.nb[4 * i + d] = shift_key(G, k, d, nk) ? (int32_t)find_key(A.key, A.n, nk) : -1;
+    }
+    pkey[i] = post_rank(k);
+    pidx[i] = (int32_t)i;
+}
+__global__ void k_scatter_rank(int64_t n, const int32_t *sorted_idx, int32_t *rank) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < n) rank[sorted_idx[r]] = (int32_t)r;
+}
+// "the same-level node N exists and has sons" when x is visited: decisions
+// of earlier-visited nodes applied
+__device__ __forceinline__ bool gm1_has_son(const Links &L, const int8_t *d, int32_t N, int32_t rx) {
+    if (N < 0) return false;
+    for (int32_t a = L.parent[N]; a >= 0; a = L.parent[a])
+        if (d[a] == D_COARSEN && L.rank[a] < rx) return false;
+    if (!L.leaf0[N]) return !(d[N] == D_COARSEN && L.rank[N] < rx);
+    return d[N] == D_REFINE && L.rank[N] < rx;
+}
+// gridmodify1 decision of one node (src/mesh.F90:305-353) given the current
+// estimate of all decisions; a decision only reads decisions of nodes that
+// are visited earlier, so iterating to a fixpoint gives the sequential result
+__global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, int32_t *changed) {
+    const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (x >= n) return;
+    int8_t r = D_NONE;
+    if (L.cross[x] == 0) {
+        const int32_t rx = L.rank[x];
+        const bool up = gm1_has_son(L, d, L.nb[4 * x + DIR_UP], rx);
+        const bool down = gm1_has_son(L, d, L.nb[4 * x + DIR_DOWN], rx);
+        const bool left = gm1_has_son(L, d, L.nb[4 * x + DIR_LEFT], rx);
+        const bool right = gm1_has_son(L, d, L.nb[4 * x + DIR_RIGHT], rx);
+        if (L.leaf0[x]) {
+            if ((left && right) || (up && down)) r = D_REFINE;
+        } else {
+            bool all_leaf = true;
+            for (int q = 0; q < 4; ++q) {
+                const int32_t c = L.child[4 * x + q];
+                const bool lf = c >= 0 && ((L.leaf0[c] && d[c] != D_REFINE) || (!L.leaf0[c] && d[c] == D_COARSEN));
+                all_leaf = all_leaf && lf;
+            }
+            if (all_leaf && ((!left && !right) || (!up && !down))) r = D_COARSEN;
+        }
+    }
+    dn[x] = r;
+    if (r != d[x]) atomicExch(changed, 1);
+}
+// values of coarsened nodes, deepest level first (interpA of the sons as they
+// are at the node's visit)
+__global__ void k_gm1_vals(NodeSet A, Links L, const int8_t *d, int lvl) {
+    const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (x >= A.n || d[x] != D_COARSEN || (int)(A.key[x] & 15u) != lvl) return;
+    const int32_t *c = L.child + 4 * x;
+    A.val[x] = mean4(A.val[c[0]], A.val[c[1]], A.val[c[2]], A.val[c[3]]);
+}
+__device__ __forceinline__ bool ancestor_coarsened(const Links &L, const int8_t *d, int32_t x) {
+    for (int32_t a = L.parent[x]; a >= 0; a = L.parent[a])
+        if (d[a] == D_COARSEN) return true;
+    return false;
+}
+__global__ void k_gm1_count(int64_t n, Links L, const int8_t *d, int32_t *cnt) {
+    const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (x >= n) return;
+    cnt[x] = ancestor_coarsened(L, d, (int32_t)x) ? 0 : (d[x] == D_REFINE ? 5 : 1);
+}
+__global__ void k_gm1_emit(NodeSet A, Links L, const int8_t *d, const int32_t *off, uint64_t *okey, uint8_t *oleaf,
+                           double4 *oval) {
+    const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (x >= A.n || ancestor_coarsened(L, d, (int32_t)x)) return;
+    const int64_t o = off[x];
+    const uint64_t k = A.key[x];
+    const double4 v = A.val[x];
+    okey[o] = k;
+    oval[o] = v;
+    if (d[x] == D_REFINE) {
+        oleaf[o] = 0;
+        for (int q = 0; q < 4; ++q) { okey[o + 1 + q] = child_key(k, q); oleaf[o + 1 + q] = 1; oval[o + 1 + q] = v; }
+    } else if (d[x] == D_COARSEN) {
+        oleaf[o] = 1;
+    } else {
+        oleaf[o] = A.leaf[x];
+    }
+}
+
+// ----------------------------------------------------------- gridmodify4
+// live neighbour (src/neighbor.F90:65-196) on a sorted node set: the
+// same-level node, else the deepest existing ancestor of it (a leaf)
+__device__ int64_t live_nb_set(const NodeSet &A, const Geometry &G, uint64_t k, int dir) {
+    uint64_t t;
+    if (!shift_key(G, k, dir, t)) return -1;
+    for (;;) {
+        const int64_t i = find_key(A.key, A.n, t);
+        if (i >= 0) return i;
+        if ((t & 15u) == 0) return -1;
+        t = parent_key(t);
+    }
+}
+// leaves that can act in gridmodify4 (a neighbour, or the neighbour's
+// neighbour, two or more levels coarser); later refinements only make
+// neighbours finer, so no other initial leaf can act when visited
+__global__ void k_gm4_triggers(NodeSet A, Geometry G, int32_t *flag, uint64_t *rank, int32_t *idx) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= A.n) return;
+    int f = 0;
+    if (A.leaf[c]) {
+        const uint64_t k = A.key[c];
+        const int lc = (int)(k & 15u);
+        const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
+        for (int t = 0; t < 4 && !f; ++t) {
+            const int64_t nb = live_nb_set(A, G, k, dirs[t]);
+            if (nb < 0) continue;
+            if ((int)(A.key[nb] & 15u) <= lc - 2) { f = 1; break; }
+            const int64_t nn = live_nb_set(A, G, A.key[nb], dirs[t]);
+            if (nn >= 0 && (int)(A.key[nn] & 15u) <= lc - 2) f = 1;
+        }
+    }
+    flag[c] = f;
+    rank[c] = dfs_rank(A.key[c]);
+    idx[c] = (int32_t)c;
+}
+
+struct Pool {
+    uint64_t *key;
+    uint8_t *flags;
+    int32_t *gen;
+    double4 *val;
+    int32_t *slot;       // hash slots -> pool index, -1 empty
+    uint64_t mask;       // slots - 1
+    int64_t cap;         // pool capacity
+    int64_t *n;          // pool size (device counter)
+    uint64_t *hrank;     // heap of new leaves
+    int32_t *hidx, *hgen;
+    int64_t hcap;
+    int32_t *err;        // [0] capacity exceeded, [1] visits, [2] non-leaf refines
+};
+__device__ __forceinline__ uint64_t hmix(uint64_t k) {
+    k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+    return k;
+}
+__global__ void k_pool_init(NodeSet A, Pool P) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    P.key[i] = A.key[i];
+    P.flags[i] = A.leaf[i] ? PF_LEAF : 0;
+    P.gen[i] = 0;
+    P.val[i] = A.val[i];
+    uint64_t hsh = hmix(A.key[i]) & P.mask;
+    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
+        const int32_t old = atomicCAS(P.slot + hsh, -1, (int32_t)i);
+        if (old == -1) return;
+        hsh = (hsh + 1) & P.mask;
+    }
+    atomicExch(P.err, 1);
+}
+// pool index of a live node, or -1
+__device__ int32_t hfind(const Pool &P, uint64_t k) {
+    uint64_t hsh = hmix(k) & P.mask;
+    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
+        const int32_t s = P.slot[hsh];
+        if (s < 0) return -1;
+        if (P.key[s] == k) return (P.flags[s] & PF_DELETED) ? -1 : s;
+        hsh = (hsh + 1) & P.mask;
+    }
+    return -1;
+}
+// insert or revive a leaf with value v; returns its pool index or -1
+__device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v) {
+    uint64_t hsh = hmix(k) & P.mask;
+    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
+        const int32_t s = P.slot[hsh];
+        if (s < 0) {
+            const int64_t i = *P.n;
+            if (i >= P.cap) return -1;
+            *P.n = i + 1;
+            P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
+            P.slot[hsh] = (int32_t)i;
+            return (int32_t)i;
+        }
+        if (P.key[s] == k) {
+            P.flags[s] = PF_LEAF;
+            P.gen[s] = P.gen[s] + 1;
+            P.val[s] = v;
+            return s;
+        }
+        hsh = (hsh + 1) & P.mask;
+    }
+    return -1;
+}
+__device__ int32_t live_nb_pool(const Pool &P, const Geometry &G, uint64_t k, int dir) {
+    uint64_t t;
+    if (!shift_key(G, k, dir, t)) return -1;
+    for (;;) {
+        const int32_t i = hfind(P, t);
+        if (i >= 0) return i;
+        if ((t & 15u) == 0) return -1;
+        t = parent_key(t);
+    }
+}
+__device__ void heap_push(Pool &P, int64_t &hn, uint64_t r, int32_t idx, int32_t gen) {
+    if (hn >= P.hcap) { P.err[0] = 1; return; }
+    int64_t i = hn++;
+    while (i > 0) {
+        const int64_t pa = (i - 1) >> 1;
+        if (P.hrank[pa] <= r) break;
+        P.hrank[i] = P.hrank[pa]; P.hidx[i] = P.hidx[pa]; P.hgen[i] = P.hgen[pa];
+        i = pa;
+    }
+    P.hrank[i] = r; P.hidx[i] = idx; P.hgen[i] = gen;
+}
+__device__ void heap_pop(Pool &P, int64_t &hn, uint64_t &r, int32_t &idx, int32_t &gen) {
+    r = P.hrank[0]; idx = P.hidx[0]; gen = P.hgen[0];
+    --hn;
+    const uint64_t lr = P.hrank[hn];
+    const int32_t li = P.hidx[hn], lg = P.hgen[hn];
+    int64_t i = 0;
+    for (;;) {
+        int64_t c = 2 * i + 1;
+        if (c >= hn) break;
+        if (c + 1 < hn && P.hrank[c + 1] < P.hrank[c]) ++c;
+        if (P.hrank[c] >= lr) break;
+        P.hrank[i] = P.hrank[c]; P.hidx[i] = P.hidx[c]; P.hgen[i] = P.hgen[c];
+        i = c;
+    }
+    if (hn > 0) { P.hrank[i] = lr; P.hidx[i] = li; P.hgen[i] = lg; }
+}
+// Refine_cell (src/mesh.F90:199-260) of a leaf, or of a non-leaf whose old
+// subtree is dropped and whose new sons copy its stale value
+__device__ void refine_pool(Pool &P, int64_t &hn, int32_t p, uint64_t cur_rank) {
+    const uint64_t pk = P.key[p];
+    if (!(P.flags[p] & PF_LEAF)) {
+        P.err[2] += 1;
+        uint64_t st[64];
+        int sp = 0;
+        st[sp++] = pk;
+        while (sp > 0) {
+            const uint64_t k = st[--sp];
+            for (int q = 0; q < 4; ++q) {
+                const int32_t c = hfind(P, child_key(k, q));
+                if (c < 0) continue;
+                if (!(P.flags[c] & PF_LEAF) && sp < 64) st[sp++] = P.key[c];
+                P.flags[c] |= PF_DELETED;
+            }
+        }
+    }
+    P.flags[p] = 0;   // internal, value kept
+    const double4 v = P.val[p];
+    for (int q = 0; q < 4; ++q) {
+        const uint64_t ck = child_key(pk, q);
+        const int32_t c = hinsert(P, ck, v);
+        if (c < 0) { P.err[0] = 1; return; }
+        const uint64_t r = dfs_rank(ck);
+        if (r > cur_rank) heap_push(P, hn, r, c, P.gen[c]);
+    }
+}
+// gridmodify4 (src/mesh.F90:355-395) over one pass of the tree: the initial
+// leaves that can act, and every leaf created ahead of the traversal, are
+// visited in traversal order by one thread
+__global__ void k_gm4_seq(Pool P, Geometry G, const uint64_t *trank, const int32_t *tidx, int64_t ntrig) {
+    if (threadIdx.x || blockIdx.x) return;
+    int64_t ti = 0, hn = 0;
+    const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
+    const int64_t limit = ntrig + P.hcap + 1;
+    for (int64_t step = 0; step < limit; ++step) {
+        uint64_t r;
+        int32_t c, gen;
+        if (hn > 0 && (ti >= ntrig || P.hrank[0] < trank[ti])) heap_pop(P, hn, r, c, gen);
+        else if (ti < ntrig) { r = trank[ti]; c = tidx[ti]; gen = 0; ++ti; }
+        else break;
+        if (P.gen[c] != gen || (P.flags[c] & PF_DELETED) || !(P.flags[c] & PF_LEAF)) continue;
+        P.err[1] += 1;
+        const int lc = (int)(P.key[c] & 15u);
+        for (int t = 0; t < 4; ++t) {
+            const int32_t nb = live_nb_pool(P, G, P.key[c], dirs[t]);
+            if (nb < 0) continue;
+            if ((int)(P.key[nb] & 15u) <= lc - 2) refine_pool(P, hn, nb, r);
+            if (P.err[0]) return;
+            const int32_t nn = live_nb_pool(P, G, P.key[nb], dirs[t]);
+            if (nn >= 0 && (int)(P.key[nn] & 15u) <= lc - 2) refine_pool(P, hn, nn, r);
+            if (P.err[0]) return;
+        }
+    }
+}
+__global__ void k_pool_live(int64_t n, const uint8_t *flags, int32_t *live) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) live[i] = !(flags[i] & PF_DELETED);
+}
+__global__ void k_pool_emit(int64_t n, const uint8_t *flags, const uint64_t *key, const double4 *val,
+                            const int32_t *off, uint64_t *okey, uint8_t *oleaf, double4 *oval) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n || (flags[i] & PF_DELETED)) return;
+    okey[off[i]] = key[i];
+    oleaf[off[i]] = (flags[i] & PF_LEAF) ? 1 : 0;
+    oval[off[i]] = val[i];
+}
+
+// ------------------------------------------------------------ extraction
+__global__ void k_split_count(int64_t n, const uint8_t *leaf, int32_t *fl, int32_t *fi) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) { fl[i] = leaf[i] ? 1 : 0; fi[i] = leaf[i] ? 0 : 1; }
+}
+__global__ void k_split_emit(NodeSet A, const int32_t *ol, const int32_t *oi, uint64_t *lk, double4 *lv, uint64_t *ik,
+                             double4 *iv) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    if (A.leaf[i]) { lk[ol[i]] = A.key[i]; lv[ol[i]] = A.val[i]; }
+    else { ik[oi[i]] = A.key[i]; iv[oi[i]] = A.val[i]; }
+}
+
+// emission helper: count kernel already ran into cnt; scan; emit kernel fills
+// the unsorted arrays (B's storage); sort into the other set
+struct Emit {
+    uint64_t *key;
+    uint8_t *leaf;
+    double4 *val;
+};
+static int emit_buffers(fdm_handle *h, int64_t n, Emit &E) {
+    FDM_CK(h, h->amr[11].ensure(n * 8 + 16));
+    FDM_CK(h, h->amr[12].ensure(n + 16));
+    FDM_CK(h, h->amr[13].ensure(n * 32 + 32));
+    E.key = h->amr[11].as<uint64_t>();
+    E.leaf = h->amr[12].as<uint8_t>();
+    E.val = h->amr[13].as<double4>();
+    return FDM_OK;
+}
+
+#define AMR_RC(x)            \
+    do {                     \
+        int rc_ = (x);       \
+        if (rc_) return rc_; \
+    } while (0)
+
+// one gridmodify1 pass over the node set A -> A
+static int gridmodify1_pass(fdm_handle *h, AmrCtx &X) {
+    const int TB = 256;
+    const int64_t n = X.A.n;
+    Carve cv;
+    cv.add(n * 4); cv.add(n * 16); cv.add(n * 16); cv.add(n * 4); cv.add(n); cv.add(n);
+    cv.add(n * 8); cv.add(n * 4); cv.add(n * 8); cv.add(n * 4); cv.add(n); cv.add(n); cv.add(16);
+    cv.add(n * 4); cv.add(n * 4);
+    FDM_CK(h, h->amr[14].ensure(cv.total));
+    DevBuf &b = h->amr[14];
+    Links L;
+    L.parent = cv.at<int32_t>(b, 0); L.child = cv.at<int32_t>(b, 1); L.nb = cv.at<int32_t>(b, 2);
+    L.rank = cv.at<int32_t>(b, 3); L.leaf0 = cv.at<uint8_t>(b, 4); L.cross = cv.at<int8_t>(b, 5);
+    uint64_t *pk = cv.at<uint64_t>(b, 6), *pk2 = cv.at<uint64_t>(b, 8);
+    int32_t *pi = cv.at<int32_t>(b, 7), *pi2 = cv.at<int32_t>(b, 9);
+    int8_t *d0 = cv.at<int8_t>(b, 10), *d1 = cv.at<int8_t>(b, 11);
+    int32_t *changed = cv.at<int32_t>(b, 12);
+    int32_t *cnt = cv.at<int32_t>(b, 13), *off = cv.at<int32_t>(b, 14);
+    k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L, pk, pi);
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, pk, pk2, pi, pi2, (int)n, 0, 64, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, pk, pk2, pi, pi2, (int)n, 0, 64, h->s));
+    k_scatter_rank<<<nblk(n, TB), TB, 0, h->s>>>(n, pi2, L.rank);
+    FDM_CK(h, cudaMemsetAsync(d0, 0, n, h->s));
+    int8_t *cur = d0, *nxt = d1;
+    int64_t it = 0;
+    for (;; ++it) {
+        if (it > n + 2) { h->err = "gridmodify1 decisions did not settle"; return FDM_ERR_UNSUPPORTED; }
+        FDM_CK(h, cudaMemsetAsync(changed, 0, 4, h->s));
+        k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed);
+        int32_t hc = 0;
+        FDM_CK(h, cudaMemcpyAsync(&hc, changed, 4, cudaMemcpyDeviceToHost, h->s));
+        FDM_CK(h, cudaStreamSynchronize(h->s));
+        std::swap(cur, nxt);
+        if (!hc) break;
+    }
+    h->gm1_iters += it + 1;
+    for (int l = MAXLVL_TAB - 2; l >= 0; --l) k_gm1_vals<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, l);
+    k_gm1_count<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, cnt);
+    int64_t total = 0;
+    AMR_RC(scan_total32(h, cnt, off, n, total));
+    Emit E;
+    AMR_RC(emit_buffers(h, total, E));
+    k_gm1_emit<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, off, E.key, E.leaf, E.val);
+    AMR_RC(grow_nodes(h, X, total));
+    AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
+    swap_sets(h, X);
+    return FDM_OK;
+}
+
+// one gridmodify4 pass over the node set A -> A
+static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
+    const int TB = 256;
+    const int64_t n = X.A.n;
+    Carve cv;
+    cv.add(n * 4); cv.add(n * 8); cv.add(n * 4); cv.add(n * 8); cv.add(n * 4); cv.add(n * 4); cv.add(16);
+    FDM_CK(h, h->amr[15].ensure(cv.total));
+    DevBuf &b = h->amr[15];
+    int32_t *flag = cv.at<int32_t>(b, 0), *idx = cv.at<int32_t>(b, 2), *sidx = cv.at<int32_t>(b, 4);
+    uint64_t *rk = cv.at<uint64_t>(b, 1), *srk = cv.at<uint64_t>(b, 3);
+    int32_t *foff = cv.at<int32_t>(b, 5);
+    int64_t *nsel = cv.at<int64_t>(b, 6);
+    k_gm4_triggers<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, flag, rk, idx);
+    // keep the triggering leaves, sorted by traversal rank
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceSelect::Flagged(nullptr, bytes, rk, flag, srk, nsel, (int)n, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceSelect::Flagged(h->cub_tmp.p, bytes, rk, flag, srk, nsel, (int)n, h->s));
+    FDM_CK(h, cub::DeviceSelect::Flagged(nullptr, bytes, idx, flag, sidx, nsel + 1, (int)n, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceSelect::Flagged(h->cub_tmp.p, bytes, idx, flag, sidx, nsel + 1, (int)n, h->s));
+    int64_t ntrig = 0;
+    FDM_CK(h, cudaMemcpyAsync(&ntrig, nsel, 8, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    if (ntrig == 0) return FDM_OK;
+    // key order is Morton order (son4 before son3); the traversal visits
+    // son3 first, so sort the triggers by traversal rank
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, srk, rk, sidx, idx, (int)ntrig, 0, 64, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, srk, rk, sidx, idx, (int)ntrig, 0, 64, h->s));
+    // pool + hash of all nodes, room for new ones
+    const int64_t cap = 2 * n + 4096;
+    uint64_t slots = 1;
+    while (slots < (uint64_t)(2 * cap)) slots <<= 1;
+    Carve cp;
+    cp.add(cap * 8); cp.add(cap); cp.add(cap * 4); cp.add(cap * 32); cp.add(slots * 4); cp.add(16);
+    cp.add(cap * 8); cp.add(cap * 4); cp.add(cap * 4); cp.add(16);
+    FDM_CK(h, h->amr[16].ensure(cp.total));
+    DevBuf &pb = h->amr[16];
+    Pool P;
+    P.key = cp.at<uint64_t>(pb, 0); P.flags = cp.at<uint8_t>(pb, 1); P.gen = cp.at<int32_t>(pb, 2);
+    P.val = cp.at<double4>(pb, 3); P.slot = cp.at<int32_t>(pb, 4); P.n = cp.at<int64_t>(pb, 5);
+    P.hrank = cp.at<uint64_t>(pb, 6); P.hidx = cp.at<int32_t>(pb, 7); P.hgen = cp.at<int32_t>(pb, 8);
+    P.err = cp.at<int32_t>(pb, 9);
+    P.mask = slots - 1;
+    P.cap = cap;
+    P.hcap = cap;
+    FDM_CK(h, cudaMemsetAsync(P.slot, 0xff, slots * 4, h->s));
+    FDM_CK(h, cudaMemsetAsync(P.err, 0, 16, h->s));
+    FDM_CK(h, cudaMemcpyAsync(P.n, &n, 8, cudaMemcpyHostToDevice, h->s));
+    k_pool_init<<<nblk(n, TB), TB, 0, h->s>>>(X.A, P);
+    k_gm4_seq<<<1, 32, 0, h->s>>>(P, h->G, rk, idx, ntrig);
+    int32_t herr[4] = {0, 0, 0, 0};
+    int64_t pn = 0;
+    FDM_CK(h, cudaMemcpyAsync(herr, P.err, 16, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(&pn, P.n, 8, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    if (herr[0]) { h->err = "gridmodify4 cascade exceeded its node pool"; return FDM_ERR_UNSUPPORTED; }
+    h->gm4_visits += herr[1];
+    h->gm4_nonleaf += herr[2];
+    // live nodes back into a sorted node set
+    Carve ce;
+    ce.add(pn * 4); ce.add(pn * 4);
+    FDM_CK(h, h->amr[17].ensure(ce.total));
+    int32_t *live = ce.at<int32_t>(h->amr[17], 0), *loff = ce.at<int32_t>(h->amr[17], 1);
+    k_pool_live<<<nblk(pn, TB), TB, 0, h->s>>>(pn, P.flags, live);
+    int64_t total = 0;
+    AMR_RC(scan_total32(h, live, loff, pn, total));
+    Emit E;
+    AMR_RC(emit_buffers(h, total, E));
+    k_pool_emit<<<nblk(pn, TB), TB, 0, h->s>>>(pn, P.flags, P.key, P.val, loff, E.key, E.leaf, E.val);
+    AMR_RC(grow_nodes(h, X, total));
+    AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
+    swap_sets(h, X);
+    return FDM_OK;
+}
+
+// AMR (src/solution.F90:408-421) after the trigger test: indicators,
+// refine/coarsen, lvlAMR rounds of gridmodify1 + gridmodify4, new tables.
 int run_amr(fdm_handle *h) {
-    h->err = "device regrid not built yet";
-    return FDM_ERR_UNSUPPORTED;
+    const int TB = 256;
+    const int64_t NL = h->NL, NI = h->NI, NInt = h->NInt;
+    if ((int64_t)h->p.m * h->p.n >= (1ll << 19)) {
+        h->err = "device regrid supports up to 2^19 background cells";
+        return FDM_ERR_UNSUPPORTED;
+    }
+    // 1. indicators and their ordered sums
+    Carve ci;
+    ci.add(NI * 8); ci.add(NI * 8); ci.add(32); ci.add(NL); ci.add((NInt > 0 ? NInt : 1));
+    FDM_CK(h, h->amr[18].ensure(ci.total));
+    double *rot = ci.at<double>(h->amr[18], 0), *div = ci.at<double>(h->amr[18], 1), *sums = ci.at<double>(h->amr[18], 2);
+    int8_t *rflag = ci.at<int8_t>(h->amr[18], 3), *cflag = ci.at<int8_t>(h->amr[18], 4);
+    AMR_RC(compute_rot_div(h, rot, div, sums));
+    // 2. solute_ref: refine and coarsen flags, applied at once
+    const Tables T = h->tables();
+    k_refine_flags<<<nblk(NL, TB), TB, 0, h->s>>>(T, h->G, h->p, rot, div, sums, rflag);
+    if (NInt > 0)
+        k_coarsen_flags<<<nblk(NInt, TB), TB, 0, h->s>>>(NInt, h->ikey.as<uint64_t>(), T, h->p, rot, div, sums, rflag,
+                                                        cflag);
+    const int64_t nn = NL + NInt;
+    FDM_CK(h, h->amr[19].ensure(nn * 8 + 16));
+    int32_t *cnt = h->amr[19].as<int32_t>(), *off = cnt + nn;
+    k_ref_count<<<nblk(nn, TB), TB, 0, h->s>>>(T, rflag, h->ikey.as<uint64_t>(), NInt, cflag, cnt);
+    int64_t total = 0;
+    AMR_RC(scan_total32(h, cnt, off, nn, total));
+    Emit E;
+    AMR_RC(emit_buffers(h, total, E));
+    k_ref_emit<<<nblk(nn, TB), TB, 0, h->s>>>(T, h->B[0].as<double4>(), rflag, h->ikey.as<uint64_t>(),
+                                              h->ival.as<double4>(), NInt, cflag, off, E.key, E.leaf, E.val);
+    AmrCtx X;
+    X.h = h;
+    AMR_RC(grow_nodes(h, X, total));
+    bind_sets(h, X);
+    AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
+    swap_sets(h, X);
+    // 3. solute_gridmodify: lvlAMR rounds (src/solution.F90:537-556)
+    for (int k = 1; k <= h->p.lvl_amr; ++k) {
+        AMR_RC(gridmodify1_pass(h, X));
+        AMR_RC(gridmodify4_pass(h, X));
+    }
+    // 4. split leaves / internal nodes, rebuild the tables (idneighbor + IDgrid)
+    const int64_t n = X.A.n;
+    Carve cs;
+    cs.add(n * 4); cs.add(n * 4); cs.add(n * 4); cs.add(n * 4);
+    FDM_CK(h, h->amr[8].ensure(cs.total));
+    int32_t *fl = cs.at<int32_t>(h->amr[8], 0), *fi = cs.at<int32_t>(h->amr[8], 1);
+    int32_t *ol = cs.at<int32_t>(h->amr[8], 2), *oi = cs.at<int32_t>(h->amr[8], 3);
+    k_split_count<<<nblk(n, TB), TB, 0, h->s>>>(n, X.A.leaf, fl, fi);
+    int64_t nleaf = 0, nint = 0;
+    AMR_RC(scan_total32(h, fl, ol, n, nleaf));
+    AMR_RC(scan_total32(h, fi, oi, n, nint));
+    DevBuf lk, lv;
+    FDM_CK(h, lk.ensure(nleaf * 8 + 8));
+    FDM_CK(h, lv.ensure(nleaf * 32 + 32));
+    FDM_CK(h, h->ikey.ensure(nint * 8 + 8));
+    FDM_CK(h, h->ival.ensure(nint * 32 + 32));
+    k_split_emit<<<nblk(n, TB), TB, 0, h->s>>>(X.A, ol, oi, lk.as<uint64_t>(), lv.as<double4>(),
+                                               h->ikey.as<uint64_t>(), h->ival.as<double4>());
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    h->NInt = nint;
+    const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>());
+    if (rc) return rc;
+    h->n_regrids++;
+    return FDM_OK;
 }
 
 }  // namespace fdm

@@ -85,6 +85,13 @@ struct fdm_handle {
     fdm::DevBuf flag;        // device error flags (int32[8])
     fdm::DevScalars *hs = nullptr;   // pinned host mirror of the scalars
 
+    // internal nodes of the tree and their values (the reference keeps a
+    // stale U in every refined node; gridmodify4 can copy it back)
+    fdm::DevBuf ikey, ival;
+    int64_t NInt = 0;
+    fdm::DevBuf amr[20];     // regrid scratch
+    int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0;
+
     // CUDA graph of one RK3 step (captured lazily, dropped at regrid)
     cudaGraphExec_t step_graph = nullptr;
     int64_t graph_version = -1;
@@ -157,5 +164,6 @@ void launch_res_finalize(fdm_handle *h);
 int launch_stage(fdm_handle *h, int krk);
 // AMR (amr.cu)
 int run_amr(fdm_handle *h);
+int init_internal(fdm_handle *h);
 
 }  // namespace fdm

@@ -272,7 +272,9 @@ int fdm_upload_leaves(fdm_handle *h, int64_t n, const uint64_t *keys, const doub
     dk.release();
     dp.release();
     if (rc) { h->loaded = false; return rc; }
-    return prepare_buffers(h);
+    rc = prepare_buffers(h);
+    if (rc) return rc;
+    return init_internal(h);
 }
 
 int64_t fdm_num_leaves(const fdm_handle *h) { return h && h->loaded ? h->NL : 0; }
@@ -465,7 +467,9 @@ int fdm_advance(fdm_handle *h, int64_t nsteps) {
 int fdm_amr(fdm_handle *h) {
     CHECK_H(h);
     CHECK_LOADED(h);
-    return run_amr(h);
+    int rc = run_amr(h);
+    if (rc) return rc;
+    return prepare_buffers(h);
 }
 
 int fdm_get_counters(fdm_handle *h, fdm_counters *c) {
@@ -481,6 +485,10 @@ int fdm_get_counters(fdm_handle *h, fdm_counters *c) {
     c->n_faces_y = h->NI + h->nuy;
     c->n_singular = h->n_singular;
     c->n_regrids = h->n_regrids;
+    c->n_internal = h->NInt;
+    c->n_gm1_iterations = h->gm1_iters;
+    c->n_gm4_visits = h->gm4_visits;
+    c->n_gm4_nonleaf = h->gm4_nonleaf;
     return FDM_OK;
 }
 

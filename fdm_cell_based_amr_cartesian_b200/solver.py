@@ -51,7 +51,9 @@ class FdmCounters(ctypes.Structure):
                 ("n_ghost", ctypes.c_int64), ("n_wls_requests", ctypes.c_int64),
                 ("n_restrict_requests", ctypes.c_int64), ("n_faces_x", ctypes.c_int64),
                 ("n_faces_y", ctypes.c_int64), ("n_singular", ctypes.c_int64),
-                ("n_regrids", ctypes.c_int64), ("reserved", ctypes.c_int64 * 8)]
+                ("n_regrids", ctypes.c_int64), ("n_internal", ctypes.c_int64),
+                ("n_gm1_iterations", ctypes.c_int64), ("n_gm4_visits", ctypes.c_int64),
+                ("n_gm4_nonleaf", ctypes.c_int64), ("reserved", ctypes.c_int64 * 4)]
 
 
 _lib = None

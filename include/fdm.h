@@ -122,7 +122,12 @@ typedef struct fdm_counters {
     int64_t n_faces_x, n_faces_y;
     int64_t n_singular;        /* brinv singular pivots in the WLS geometry   */
     int64_t n_regrids;
-    int64_t reserved[8];
+    int64_t n_internal;        /* internal nodes of the tree                  */
+    int64_t n_gm1_iterations;  /* fixpoint sweeps of gridmodify1 (all passes) */
+    int64_t n_gm4_visits;      /* leaves gridmodify4 acted from               */
+    int64_t n_gm4_nonleaf;     /* Refine_cell of a non-leaf by gridmodify4
+                                  (src/mesh.F90:389-392)                      */
+    int64_t reserved[4];
 } fdm_counters;
 
 /* ------------------------------------------------------------- lifecycle */
