@@ -217,11 +217,9 @@ def run_ours(args):
                 g.advance(1)
                 ev[k][1].record(ext)
         torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
+    from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), device="cuda")
     if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     value = NI * world * args.steps / (ms / 1e3)
     clocks = clk.summary()
@@ -254,8 +252,39 @@ def run_ours(args):
         e2e = {"value": NI * world * n_e2e / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(len(keys) * 32), "d2h_bytes_per_step": int(len(keys) * 40)}
 
-    launches_per_step = 1 + 1 + 1 + 3 * (2 + 2 + (1 if cnt["n_wls_requests"] + cnt["n_restrict_requests"] else 0)
-                                          + (1 if cnt["n_ghost"] else 0))
+    # step control, lambda reset, step end, residual reduction (stage 3) and,
+    # per stage: 2 face kernels, the update, hanging nodes (+ interpA
+    # fallbacks), ghosts
+    per_stage = 2 + 1 + (1 if cnt["n_wls_requests"] + cnt["n_restrict_requests"] else 0) \
+        + (1 if cnt["n_restrict_requests"] else 0) + (1 if cnt["n_ghost"] else 0)
+    launches_per_step = 4 + 3 * per_stage
+
+    # the full configuration as the reference runs it: t = 0 -> 0.3 with the
+    # device regrid every 10 steps (time to solution, all regrids included)
+    full = None
+    if not args.no_full_run:
+        gf = S.Solver(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
+        gf.creat_mesh_and_initial()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps = 0
+        upd = 0
+        while True:
+            before = gf.scalars()["tt"]
+            if before >= 0.3:
+                break
+            ni = gf.counters()["n_interior"]
+            n = gf.solute(10)
+            steps += n
+            upd += n * ni
+            if n == 0:
+                break
+        t_full = time.perf_counter() - t0
+        cf = gf.counters()
+        full = {"workload": "riemann4 128^2, 4 levels, t = 0 -> 0.3, regrid every 10 steps",
+                "seconds": t_full, "steps": steps, "regrids": cf["n_regrids"],
+                "mean_updates_per_s": upd / t_full, "leaves_at_end": cf["n_leaves"]}
+        gf.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -280,7 +309,7 @@ def run_ours(args):
                              "frac": step_gbs / hbm_peak},
                 "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
-                "counters": cnt, "cpu_baseline": cpu}
+                "counters": cnt, "cpu_baseline": cpu, "full_run": full}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -296,6 +325,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-full-run", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
