@@ -177,6 +177,90 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------- GPU arm
+def timed_window(g, steps, warmup, flush):
+    """Device time (ms) of `steps` solute iterations (step graph replays)
+    on the handle's stream, L2 flushed before each, after `warmup` untimed."""
+    import torch
+    for _ in range(warmup):
+        g.advance(1)
+    torch.cuda.synchronize()
+    stream_ptr, _, _ = g.device_state()
+    ext = torch.cuda.ExternalStream(stream_ptr)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(ext):
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(ext)
+            g.advance(1)
+            ev[k][1].record(ext)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def learned_window(args, cfg, keys, prim, NI, flush, world):
+    """The learned-gated solver on the same mesh and window as the plain
+    one: updates/s, the gated face share, and the density error against a
+    plain run over the same steps."""
+    import torch
+    from fdm_cell_based_amr_cartesian_b200 import learned as LG
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+    from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
+    if not os.path.exists(LG.PARAMS_PATH):
+        return {"unavailable": "no trained gate parameters"}
+    gl = S.Solver(cfg)
+    gl.upload(keys, prim)
+    gl.body_boundary(1)
+    gl.step_control()
+    LG.enable(gl)
+    ms = max_over_ranks(timed_window(gl, args.steps, args.warmup, flush), device="cuda")
+    gated, total = LG.stats(gl)
+    ref = S.Solver(cfg)
+    ref.upload(keys, prim)
+    ref.body_boundary(1)
+    ref.step_control()
+    ref.advance(args.warmup + args.steps)
+    torch.cuda.synchronize()
+    l1, linf = LG.density_errors(cfg, ref.leaves(), gl.leaves())
+    kt = gl.time_kernels(reps=5)
+    gl.close()
+    ref.close()
+    return {"value": NI * world * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "gated_face_fraction": gated / max(total, 1), "threshold": LG.THRESHOLD,
+            "l1_density_vs_plain": l1, "linf_density_vs_plain": linf,
+            "error_window_steps": args.warmup + args.steps, "kernel_ms": kt}
+
+
+def full_run(S, gate):
+    import torch
+    gf = S.Solver(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
+    gf.creat_mesh_and_initial()
+    if gate:
+        from fdm_cell_based_amr_cartesian_b200 import learned as LG
+        LG.enable(gf)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    steps = 0
+    upd = 0
+    while True:
+        before = gf.scalars()["tt"]
+        if before >= 0.3:
+            break
+        ni = gf.counters()["n_interior"]
+        n = gf.solute(10)
+        steps += n
+        upd += n * ni
+        if n == 0:
+            break
+    t_full = time.perf_counter() - t0
+    cf = gf.counters()
+    out = {"workload": "riemann4 128^2, 4 levels, t = 0 -> 0.3, regrid every 10 steps",
+           "seconds": t_full, "steps": steps, "regrids": cf["n_regrids"],
+           "mean_updates_per_s": upd / t_full, "leaves_at_end": cf["n_leaves"]}
+    leaves = gf.leaves()
+    gf.close()
+    return out, leaves
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -219,6 +303,11 @@ def run_ours(args):
         torch.cuda.synchronize()
     from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
     ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), device="cuda")
+    # the timed steps must have advanced a valid flow
+    _, after = g.leaves()
+    finite = bool(np.isfinite(after).all() and after[:, 0].min() > 0 and after[:, 3].min() > 0)
+    if not finite:
+        raise RuntimeError("benchmark state is not finite/positive after the timed steps")
     if world > 1:
         dist.barrier()
     value = NI * world * args.steps / (ms / 1e3)
@@ -259,32 +348,22 @@ def run_ours(args):
         + (1 if cnt["n_restrict_requests"] else 0) + (1 if cnt["n_ghost"] else 0)
     launches_per_step = 4 + 3 * per_stage
 
+    # learned-gated path on the same workload and window
+    gated = None
+    if not args.no_learned:
+        gated = learned_window(args, cfg, keys, prim, NI, flush, world)
+
     # the full configuration as the reference runs it: t = 0 -> 0.3 with the
-    # device regrid every 10 steps (time to solution, all regrids included)
+    # device regrid every 10 steps (time to solution, all regrids included),
+    # plain and learned-gated, and the gated run's density error at t = 0.3
     full = None
     if not args.no_full_run:
-        gf = S.Solver(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
-        gf.creat_mesh_and_initial()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        steps = 0
-        upd = 0
-        while True:
-            before = gf.scalars()["tt"]
-            if before >= 0.3:
-                break
-            ni = gf.counters()["n_interior"]
-            n = gf.solute(10)
-            steps += n
-            upd += n * ni
-            if n == 0:
-                break
-        t_full = time.perf_counter() - t0
-        cf = gf.counters()
-        full = {"workload": "riemann4 128^2, 4 levels, t = 0 -> 0.3, regrid every 10 steps",
-                "seconds": t_full, "steps": steps, "regrids": cf["n_regrids"],
-                "mean_updates_per_s": upd / t_full, "leaves_at_end": cf["n_leaves"]}
-        gf.close()
+        full, leaves_plain = full_run(S, gate=False)
+        if gated is not None:
+            full_g, leaves_gated = full_run(S, gate=True)
+            from fdm_cell_based_amr_cartesian_b200 import learned as LG
+            l1, linf = LG.density_errors(P.riemann4(base=128, lvl_amr=4), leaves_plain, leaves_gated)
+            full["gated"] = dict(full_g, l1_density_vs_plain=l1, linf_density_vs_plain=linf)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -309,7 +388,8 @@ def run_ours(args):
                              "frac": step_gbs / hbm_peak},
                 "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
-                "counters": cnt, "cpu_baseline": cpu, "full_run": full}
+                "counters": cnt, "state_finite_after_timed_steps": finite, "cpu_baseline": cpu,
+                "learned": gated, "full_run": full}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -326,6 +406,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-full-run", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

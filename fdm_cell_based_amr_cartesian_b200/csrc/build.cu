@@ -817,6 +817,7 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     h->n_singular += (int64_t)hc[0];
     h->n_restrict = (int64_t)hc[2];
     h->table_version++;
+    h->gate_stage1_valid = false;
     h->lam_fresh = false;
     h->loaded = true;
     return FDM_OK;

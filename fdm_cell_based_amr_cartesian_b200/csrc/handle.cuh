@@ -92,6 +92,12 @@ struct fdm_handle {
     fdm::DevBuf amr[20];     // regrid scratch
     int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0;
 
+    // learned gate of the face flux
+    fdm::DevBuf gate_params, gate_flag;   // gate_flag: per-stage hard-face lists
+    float gate_logit_thr = 0.f;
+    bool gate_on = false;
+    bool gate_stage1_valid = false;   // stage-1 decisions exist for the current tables
+
     // CUDA graph of one RK3 step (captured lazily, dropped at regrid)
     cudaGraphExec_t step_graph = nullptr;
     int64_t graph_version = -1;
@@ -151,7 +157,7 @@ inline int arg_fail(fdm_handle *h, const char *msg) {
 int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_dev, const double *prim_dev);
 // per-stage pipeline (stage.cu)
 void launch_requests(fdm_handle *h, const double4 *cur);
-void launch_faces(fdm_handle *h, const double4 *cur);
+void launch_faces(fdm_handle *h, const double4 *cur, int krk);
 void launch_cells(fdm_handle *h, const double4 *cur, const double4 *un, double4 *next, int krk,
                   int mode);
 void launch_ghosts(fdm_handle *h, double4 *next, int j);
@@ -162,6 +168,8 @@ void launch_step_end(fdm_handle *h);
 void launch_set_tstep(fdm_handle *h, double tstep);
 void launch_res_finalize(fdm_handle *h);
 int launch_stage(fdm_handle *h, int krk);
+void launch_gated_faces(fdm_handle *h, const double4 *cur, int krk);
+size_t gate_list_bytes(const fdm_handle *h);
 // AMR (amr.cu)
 int run_amr(fdm_handle *h);
 int init_internal(fdm_handle *h);

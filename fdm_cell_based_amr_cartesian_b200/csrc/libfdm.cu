@@ -132,6 +132,7 @@ static void enqueue_solute_iteration(fdm_handle *h) {
 static int prepare_buffers(fdm_handle *h) {
     const int64_t nb = nblk(h->NI, 256);
     FDM_CK(h, h->res_part.ensure((size_t)(nb > 0 ? nb : 1) * 8 * sizeof(double)));
+    FDM_CK(h, h->gate_flag.ensure(gate_list_bytes(h)));
     return FDM_OK;
 }
 
@@ -243,7 +244,8 @@ void fdm_destroy(fdm_handle *h) {
     DevBuf *bufs[] = {&h->lkey, &h->lslot, &h->slot_leaf, &h->lcx, &h->lcy, &h->lcross, &h->ist, &h->ilvl,
                       &h->ifxl, &h->ifyl, &h->uxl, &h->uyl, &h->rq_kind, &h->rq_m, &h->rq_mem, &h->rq_geo, &h->rq_node,
                       &h->gh_kind, &h->gh_a, &h->gh_b, &h->gh_flip, &h->gh_x, &h->gh_y, &h->B[0], &h->B[1],
-                      &h->B[2], &h->Fx, &h->Fy, &h->Ut, &h->scal, &h->res_part, &h->cub_tmp, &h->flag};
+                      &h->B[2], &h->Fx, &h->Fy, &h->Ut, &h->scal, &h->res_part, &h->cub_tmp, &h->flag,
+                      &h->gate_params, &h->gate_flag, &h->ikey, &h->ival};
     for (DevBuf *b : bufs) b->release();
     for (auto &t : h->tmp) t.release();
     if (h->hs) cudaFreeHost(h->hs);
@@ -379,7 +381,7 @@ int fdm_solution_cells(fdm_handle *h, int32_t krk) {
     if (krk < 1 || krk > 3) return arg_fail(h, "krk must be 1..3");
     const double4 *cur = h->B[krk - 1].as<double4>();
     launch_requests(h, cur);
-    launch_faces(h, cur);
+    launch_faces(h, cur, krk);
     launch_cells(h, cur, h->B[0].as<double4>(), h->Ut.as<double4>(), krk, 1);
     FDM_CK(h, cudaStreamSynchronize(h->s));
     return FDM_OK;

@@ -455,7 +455,11 @@ const char *face_variant_name(int v) {
     }
 }
 
-void launch_faces(fdm_handle *h, const double4 *cur) {
+void launch_faces(fdm_handle *h, const double4 *cur, int krk) {
+    if (h->gate_on) {
+        launch_gated_faces(h, cur, krk);
+        return;
+    }
     switch (h->face_variant) {
         case 1: faces_1lane<128, 4>(h, cur); break;
         case 2: faces_1lane<64, 7>(h, cur); break;
@@ -507,7 +511,7 @@ int launch_stage(fdm_handle *h, int krk) {
     const double4 *cur = krk == 1 ? b0 : krk == 2 ? b1 : b2;
     double4 *next = krk == 1 ? b1 : krk == 2 ? b2 : b0;
     launch_requests(h, cur);
-    launch_faces(h, cur);
+    launch_faces(h, cur, krk);
     launch_cells(h, cur, b0, next, krk, 0);
     launch_ghosts(h, next, 3);
     return FDM_OK;

@@ -31,7 +31,7 @@ extern "C" int fdm_time_kernels(fdm_handle *h, int32_t reps, double *ms) {
         // one untimed launch, then reps timed launches
         for (int r = 0; r <= reps; ++r) {
             if (r == 1) FDM_CK(h, cudaEventRecord(e[0], h->s));
-            if (which == 0) launch_faces(h, b0);
+            if (which == 0) launch_faces(h, b0, 1 + r % 3);   // gated: stage-1 and stage-2/3 kinds in turn
             else if (which == 1) launch_cells(h, b0, b0, b1, 2, 0);
             else if (which == 2) launch_requests(h, b0);
             else launch_ghosts(h, b1, 3);
@@ -67,9 +67,9 @@ extern "C" int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *
     int bv = keep;
     for (int v = 0; v < N_FACE_VARIANTS; ++v) {
         h->face_variant = v;
-        launch_faces(h, h->B[0].as<double4>());
+        launch_faces(h, h->B[0].as<double4>(), 1);
         FDM_CK(h, cudaEventRecord(e[0], h->s));
-        for (int r = 0; r < reps; ++r) launch_faces(h, h->B[0].as<double4>());
+        for (int r = 0; r < reps; ++r) launch_faces(h, h->B[0].as<double4>(), 1);
         FDM_CK(h, cudaEventRecord(e[1], h->s));
         FDM_CK(h, cudaEventSynchronize(e[1]));
         float t = 0.f;

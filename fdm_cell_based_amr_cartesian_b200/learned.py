@@ -1,0 +1,260 @@
+"""Learned smoothness gate of the face flux: data, training, evaluation.
+
+The plain solver emits per-face samples (8 features, target exp(-dev/tau)
+with dev the largest effect of the nonlinear WCNS weights' deviation from
+the linear ones on a reconstruction) on randomized four-quadrant problems;
+the MLP is trained on the GPU by libfdm's tensor-core forward/backward
+kernels (fdm_gate_train_step).  The trained parameters are kept in
+gate_params.npy next to this file:
+
+    python -m fdm_cell_based_amr_cartesian_b200.learned --train
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import os
+import time
+
+import numpy as np
+
+from . import params as P
+from .solver import FdmError, Solver, load_library
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PARAMS_PATH = os.path.join(HERE, "gate_params.npy")
+N_PARAMS = 1377
+TAU = 1e-3          # target = exp(-dev / TAU): above 0.9 for dev < 1.05e-4
+THRESHOLD = 0.9     # gate >= 0.9 takes the linear path
+NEG_WEIGHT = 4.0    # weight of the non-smooth term of the loss (false "smooth" costs more)
+
+
+def _lib():
+    L = load_library()
+    vp, i64, f32p = ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)
+    L.fdm_gate_param_count.restype = ctypes.c_int
+    L.fdm_gate_set.argtypes = [vp, f32p, ctypes.c_float, ctypes.c_int32]
+    L.fdm_gate_samples.argtypes = [vp, i64, i64, ctypes.c_double, vp, vp, i64, i64, ctypes.POINTER(i64)]
+    L.fdm_gate_train_step.argtypes = [vp, vp, i64, i64, i64, i64, ctypes.c_float, vp, vp, vp, vp, i64,
+                                      ctypes.c_float, vp, vp]
+    L.fdm_gate_eval.argtypes = [vp, i64, vp, vp, vp]
+    L.fdm_gate_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    return L
+
+
+def stats(solver: Solver):
+    """(faces on the linear path in the last stage, all faces)."""
+    L = _lib()
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    rc = L.fdm_gate_stats(solver.h, ctypes.byref(a), ctypes.byref(b))
+    if rc:
+        raise FdmError(rc, "fdm_gate_stats failed")
+    return a.value, b.value
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """Scaled-normal initialisation of W1[32][8], b1, W2[32][32], b2, w3, b3."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(N_PARAMS, np.float32)
+    p[0:256] = rng.normal(0, 1 / np.sqrt(8), 256)
+    p[288:1312] = rng.normal(0, 1 / np.sqrt(32), 1024)
+    p[1344:1376] = rng.normal(0, 1 / np.sqrt(32), 32)
+    p[1376] = 2.0          # start biased toward "smooth" (most faces are)
+    return p
+
+
+def enable(solver: Solver, params: np.ndarray | None = None, threshold: float = THRESHOLD):
+    L = _lib()
+    p = np.ascontiguousarray(load_params() if params is None else params, np.float32)
+    rc = L.fdm_gate_set(solver.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), threshold, 1)
+    if rc:
+        raise FdmError(rc, "fdm_gate_set failed")
+
+
+def disable(solver: Solver):
+    L = _lib()
+    rc = L.fdm_gate_set(solver.h, None, 0.5, 0)
+    if rc:
+        raise FdmError(rc, "fdm_gate_set failed")
+
+
+def load_params() -> np.ndarray:
+    return np.load(PARAMS_PATH).astype(np.float32)
+
+
+def collect(seeds, base=64, lvl_amr=3, steps=200, every=10, stride=3, tau=TAU, cap=12_000_000):
+    """(features, targets) on the GPU (torch tensors) from plain runs of
+    random four-quadrant problems (rho, p ~ U[0.1,2], u, v ~ U[-1,1])."""
+    import torch
+    L = _lib()
+    X = torch.empty((cap, 8), dtype=torch.float32, device="cuda")
+    Y = torch.empty((cap,), dtype=torch.float32, device="cuda")
+    n = 0
+    phase = 0
+    for seed in seeds:
+        cfg = P.random_riemann4(seed, base=base, lvl_amr=lvl_amr, t_end=1e9)
+        g = Solver(cfg)
+        g.creat_mesh_and_initial()
+        for k in range(steps):
+            g.solute_step()
+            if k % every == every - 1 and n < cap:
+                w = ctypes.c_int64()
+                rc = L.fdm_gate_samples(g.h, stride, phase % stride, tau, X.data_ptr(), Y.data_ptr(), n, cap,
+                                        ctypes.byref(w))
+                if rc:
+                    raise FdmError(rc, "fdm_gate_samples failed")
+                n += w.value
+                phase += 1
+        g.close()
+        if n >= cap:
+            break
+    torch.cuda.synchronize()
+    return X[:n], Y[:n]
+
+
+def train(X, Y, steps=3000, batch=65536, lr=3e-3, seed=0, params=None, log_every=0, neg_weight=NEG_WEIGHT,
+          cosine=False):
+    """Adam on the weighted cross entropy of minibatches (cosine-decayed
+    learning rate if asked); returns (params, loss history)."""
+    import torch
+    L = _lib()
+    n = X.shape[0]
+    p = torch.tensor(init_params(seed) if params is None else params, device="cuda")
+    grad = torch.zeros_like(p)
+    m = torch.zeros_like(p)
+    v = torch.zeros_like(p)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(seed)
+    hist = []
+    for t in range(1, steps + 1):
+        idx0 = int(rng.integers(0, n))
+        step = int(rng.choice([1, 3, 7, 11, 13, 17, 19, 23]))   # strided, wrapped minibatch
+        lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * (t - 1) / steps)) if cosine else lr
+        rc = L.fdm_gate_train_step(X.data_ptr(), Y.data_ptr(), n, idx0, step, min(batch, n), neg_weight,
+                                   p.data_ptr(), grad.data_ptr(), m.data_ptr(), v.data_ptr(), t, lr_t,
+                                   loss.data_ptr(), ctypes.c_void_p(stream))
+        if rc:
+            raise FdmError(rc, "fdm_gate_train_step failed")
+        if log_every and (t % log_every == 0 or t == 1):
+            hist.append((t, float(loss.item()) / min(batch, n)))
+    torch.cuda.synchronize()
+    return p.cpu().numpy(), hist
+
+
+def gradients(X, Y, params, batch, idx0=0, step=1, neg_weight=1.0):
+    """Mean-loss gradients of one minibatch from the GPU kernels (lr = 0)."""
+    import torch
+    L = _lib()
+    p = torch.tensor(params, device="cuda")
+    grad = torch.zeros_like(p)
+    m = torch.zeros_like(p)
+    v = torch.zeros_like(p)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    rc = L.fdm_gate_train_step(X.data_ptr(), Y.data_ptr(), X.shape[0], idx0, step, batch, neg_weight,
+                               p.data_ptr(), grad.data_ptr(), m.data_ptr(), v.data_ptr(), 1, 0.0,
+                               loss.data_ptr(), None)
+    if rc:
+        raise FdmError(rc, "fdm_gate_train_step failed")
+    torch.cuda.synchronize()
+    return grad.cpu().numpy(), float(loss.item())
+
+
+def probabilities(X, params):
+    import torch
+    L = _lib()
+    p = torch.tensor(params, device="cuda")
+    out = torch.empty(X.shape[0], dtype=torch.float32, device="cuda")
+    rc = L.fdm_gate_eval(X.data_ptr(), X.shape[0], p.data_ptr(), out.data_ptr(), None)
+    if rc:
+        raise FdmError(rc, "fdm_gate_eval failed")
+    torch.cuda.synchronize()
+    return out
+
+
+def fine_density(cfg: P.Config, keys, prim, level=None):
+    """Leaf densities painted onto the uniform grid of the finest level
+    (each leaf covers 4^(L - lvl) fine cells) over all m x n roots."""
+    p = cfg.params
+    keys = np.asarray(keys, dtype=np.uint64)
+    lvl = (keys & np.uint64(15)).astype(np.int64)
+    L = int(lvl.max(initial=0)) if level is None else level
+    root = (keys >> np.uint64(34)).astype(np.int64)
+    path = ((keys >> np.uint64(4)) & np.uint64((1 << 30) - 1)).astype(np.int64)
+    ix = (root % p.m) << L
+    iy = (root // p.m) << L
+    for k in range(1, L + 1):
+        act = lvl >= k
+        q = (path >> (2 * (15 - k))) & 3
+        ix = ix + np.where(act, (q & 1) << (L - k), 0)
+        iy = iy + np.where(act, (q >> 1) << (L - k), 0)
+    out = np.zeros(((p.n << L), (p.m << L)), np.float64)
+    side = 1 << (L - lvl)
+    for s in np.unique(side):
+        sel = side == s
+        for dy in range(s):
+            for dx in range(s):
+                out[iy[sel] + dy, ix[sel] + dx] = prim[sel, 0]
+    return out
+
+
+def density_errors(cfg: P.Config, plain, gated):
+    """(L1, Linf) of the gated density against the plain one, area-weighted
+    on the finest uniform grid, relative to the plain density's L1 / Linf."""
+    kp, pp = plain
+    kg, pg = gated
+    L = int(max((np.asarray(kp, np.uint64) & np.uint64(15)).max(), (np.asarray(kg, np.uint64) & np.uint64(15)).max()))
+    a = fine_density(cfg, kp, pp, L)
+    b = fine_density(cfg, kg, pg, L)
+    d = np.abs(b - a)
+    return float(d.sum() / np.abs(a).sum()), float(d.max() / np.abs(a).max())
+
+
+def compare(cfg: P.Config, steps: int, params=None, threshold: float = THRESHOLD):
+    """Run the plain and the gated solver side by side for `steps` solute
+    iterations; returns the density errors, the gated face fraction of the
+    last stage and the leaf counts."""
+    plain, gated = Solver(cfg), Solver(cfg)
+    plain.creat_mesh_and_initial()
+    gated.creat_mesh_and_initial()
+    enable(gated, params, threshold)
+    plain.solute(steps)
+    gated.solute(steps)
+    g, n = stats(gated)
+    pl, gl = plain.leaves(), gated.leaves()
+    l1, linf = density_errors(cfg, pl, gl)
+    plain.close()
+    gated.close()
+    return {"l1": l1, "linf": linf, "gated_fraction": g / max(n, 1), "leaves_plain": len(pl[0]),
+            "leaves_gated": len(gl[0])}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", action="store_true")
+    ap.add_argument("--seeds", type=int, default=24)
+    ap.add_argument("--steps", type=int, default=3000)
+    args = ap.parse_args()
+    if args.train:
+        import torch
+        t0 = time.time()
+        X, Y = collect(range(args.seeds))
+        print(f"samples {X.shape[0]} collected in {time.time() - t0:.1f}s; smooth fraction "
+              f"{float((Y > THRESHOLD).float().mean()):.3f}")
+        params, hist = train(X, Y, steps=args.steps, log_every=500, cosine=True)
+        for t, l in hist:
+            print(f"step {t} loss {l:.5f}")
+        Xe, Ye = collect(range(1000, 1004))
+        prob = probabilities(Xe, params)
+        gate = prob >= THRESHOLD
+        smooth = Ye >= THRESHOLD
+        dev = -TAU * torch.log(Ye.clamp(min=1e-30))
+        print(f"held-out: smooth fraction {float(smooth.float().mean()):.3f}, gated fraction "
+              f"{float(gate.float().mean()):.3f}, precision {float((gate & smooth).sum() / gate.sum().clamp(min=1)):.4f}, "
+              f"largest dev among gated {float(dev[gate].max()) if bool(gate.any()) else 0.0:.3e}")
+        np.save(PARAMS_PATH, params)
+        print("saved", PARAMS_PATH, f"{time.time() - t0:.1f}s")
+
+
+if __name__ == "__main__":
+    main()

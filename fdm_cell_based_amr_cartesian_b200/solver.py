@@ -36,7 +36,8 @@ EXPORTS = [
     "fdm_advance", "fdm_amr", "fdm_get_counters", "fdm_debug_stencil", "fdm_debug_neighbors",
     "fdm_debug_requests",
     "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
-    "fdm_set_variant", "fdm_time_advance_rk_uniform_static",
+    "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
+    "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats",
 ]
 
 
@@ -388,7 +389,11 @@ def distance_refined_keys(cfg: P.Config, lines, dist_by_level) -> np.ndarray:
     refined when its centre lies within dist_by_level[l] of any of the given
     axis-parallel lines ("x", c) / ("y", c).  Distances must shrink by at
     least two cells of the finer level per level so that the result keeps the
-    2:1 balance.  Only interior background cells are refined."""
+    2:1 balance.  Ghost background cells follow the same rule, so the balance
+    also holds across the domain boundary (the reference's gridmodify refines
+    ghost cells next to refined interior cells in the same way); a refined
+    interior cell beside an unrefined ghost would break the hanging-node
+    stencils there."""
     p = cfg.params
     m, n = cfg.m, cfg.n
     root = np.arange(m * n, dtype=np.int64)
@@ -396,7 +401,7 @@ def distance_refined_keys(cfg: P.Config, lines, dist_by_level) -> np.ndarray:
     lvl = np.zeros_like(root)
     ix = np.zeros_like(root)
     iy = np.zeros_like(root)
-    inter = (row >= 3) & (row < n - 3) & (col >= 3) & (col < m - 3)
+    inter = np.ones(m * n, dtype=bool)
     done_r, done_l, done_x, done_y = [], [], [], []
     cur_r, cur_l, cur_x, cur_y, cur_i = root, lvl, ix, iy, inter
     for L in range(len(dist_by_level) + 1):

@@ -239,6 +239,37 @@ int fdm_fp64_peak(double *tflops);
 int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms);
 int fdm_set_variant(fdm_handle *h, int32_t face_variant);
 
+/* ------------------------------------------------------------ learned gate
+ * No reference counterpart.  A BF16 MLP (8 -> 32 -> 32 -> 1, GELU, sigmoid,
+ * FP32 accumulation on the tensor cores) decides per face whether the
+ * linear WCNS weights suffice; such faces take a component-wise linear
+ * reconstruction, all others the plain scheme.  Parameters are FP32, layout
+ * W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3 (fdm_gate_param_count()
+ * floats).  fdm_gate_set enables the gate on a handle (g >= threshold takes
+ * the linear path) or disables it (enable = 0: the exact path).
+ * fdm_gate_samples writes (features[8], target) of every stride-th face of
+ * the current state to caller device buffers; target = exp(-dev/tau) with
+ * dev the largest effect of a nonlinear-weight deviation on the face's 16
+ * WCNS_Z3 reconstructions, |w1 - l1| |p1 - p2| over the magnitude of the
+ * characteristic component on the stencil.  fdm_gate_train_step runs one
+ * Adam step (forward and backward on the tensor cores) on a minibatch of B
+ * samples idx0 + k*step (mod n) of caller device arrays, minimising
+ * -(y log g + neg_weight (1-y) log(1-g)); loss receives the batch sum.
+ * fdm_gate_eval: gate probabilities of feature rows. */
+int fdm_gate_param_count(void);
+int fdm_gate_set(fdm_handle *h, const float *params, float threshold, int32_t enable);
+int fdm_gate_samples(fdm_handle *h, int64_t stride, int64_t phase, double tau,
+                     float *feat_dev, float *target_dev, int64_t offset, int64_t cap,
+                     int64_t *n_written);
+int fdm_gate_train_step(const float *X, const float *Y, int64_t n, int64_t idx0,
+                        int64_t step, int64_t B, float neg_weight, float *params,
+                        float *grad, float *adam_m, float *adam_v, int64_t t,
+                        float lr, float *loss, void *stream);
+int fdm_gate_eval(const float *X, int64_t n, const float *params, float *prob,
+                  void *stream);
+/* faces that took the linear path in the last gated stage / all faces */
+int fdm_gate_stats(fdm_handle *h, int64_t *gated, int64_t *total);
+
 /* ------------------------------------------------- no-allocation entry point
  * One SSP-RK3 step (the three stages of Time_advance_RK with periodic ghost
  * fill) on a uniform periodic grid of nx x ny cells, without allocating any

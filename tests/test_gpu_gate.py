@@ -1,0 +1,161 @@
+"""Learned gate on the GPU: tensor-core forward and backward against the
+CPU oracle (tests/mlp_ref.py), training, and the gated solver's accuracy
+against the plain one."""
+import os
+
+import numpy as np
+import pytest
+
+import mlp_ref
+from fdm_cell_based_amr_cartesian_b200 import learned
+from fdm_cell_based_amr_cartesian_b200 import params as P
+from fdm_cell_based_amr_cartesian_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.uniform(-1, 1, (n, 8)).astype(np.float32)
+    Y = (1 / (1 + np.exp(-(X[:, 0] - 0.5 * X[:, 3] + 0.3)))).astype(np.float32)
+    return X, Y
+
+
+def test_forward_matches_oracle():
+    import torch
+    X, _ = _data(4096, 1)
+    p = learned.init_params(5)
+    prob = learned.probabilities(torch.tensor(X, device="cuda"), p).cpu().numpy()
+    z = mlp_ref.forward(p, X)[-1]
+    ref = 1 / (1 + np.exp(-z))
+    assert np.max(np.abs(prob - ref)) < 2e-3
+
+
+@pytest.mark.parametrize("neg_weight", [1.0, 4.0])
+def test_gradients_match_oracle(neg_weight):
+    import torch
+    X, Y = _data(2048, 2)
+    p = learned.init_params(7)
+    g_gpu, loss_gpu = learned.gradients(torch.tensor(X, device="cuda"), torch.tensor(Y, device="cuda"), p, 2048,
+                                        neg_weight=neg_weight)
+    loss, g = mlp_ref.loss_and_grads(p, X, Y, neg_weight=neg_weight)
+    assert abs(loss_gpu / 2048 - loss) < 1e-3 * abs(loss) + 1e-5
+    rel = np.linalg.norm(g_gpu - g) / np.linalg.norm(g)
+    assert rel < 2e-2, rel
+    # every block of the gradient, not only the norm
+    for a, b in ((0, 256), (256, 288), (288, 1312), (1312, 1344), (1344, 1376)):
+        assert np.linalg.norm(g_gpu[a:b] - g[a:b]) <= 3e-2 * np.linalg.norm(g[a:b]) + 1e-7, (a, b)
+
+
+def test_training_reduces_loss():
+    import torch
+    X, Y = _data(65536, 3)
+    Xd, Yd = torch.tensor(X, device="cuda"), torch.tensor(Y, device="cuda")
+    _, hist = learned.train(Xd, Yd, steps=400, batch=8192, lr=3e-3, log_every=100)
+    assert hist[-1][1] < 0.9 * hist[0][1]
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+@pytest.mark.parametrize("name", ["vortex", "riemann4"])
+def test_gated_solver_accuracy(name):
+    """Area-weighted L1 density error of the gated run against the plain run
+    <= 1e-3 (relative), with a real share of the faces on the linear path."""
+    cfg = {"vortex": lambda: P.vortex(), "riemann4": lambda: P.riemann4(base=64, lvl_amr=3, t_end=0.3)}[name]()
+    steps = 200 if name == "vortex" else 400
+    r = learned.compare(cfg, steps)
+    print(name, r)
+    assert r["l1"] <= 1e-3, r
+    assert r["gated_fraction"] >= {"vortex": 0.01, "riemann4": 0.1}[name], r
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+def test_gated_path_is_faster_at_bounded_error():
+    """What the trained network buys: on a statically refined four-quadrant
+    mesh (base 64, 4 levels) the gated step is at least 1.25x faster than the
+    plain one, with the density error after 20 steps <= 1e-3."""
+    import torch
+    from fdm_cell_based_amr_cartesian_b200.solver import distance_refined_keys, initial_state
+    cfg = P.riemann4(base=64, lvl_amr=4, pstep_adapt=1000)
+    keys = distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], [0.2, 0.15, 0.1, 0.05])
+    prim = initial_state(cfg, keys)
+    out = {}
+    for gate in (False, True):
+        g = Solver(cfg)
+        g.upload(keys, prim)
+        g.body_boundary(1)
+        g.step_control()
+        if gate:
+            learned.enable(g)
+        sp, _, _ = g.device_state()
+        ext = torch.cuda.ExternalStream(sp)
+        g.advance(3)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            a.record(ext)
+            g.advance(17)
+            b.record(ext)
+        torch.cuda.synchronize()
+        out[gate] = (a.elapsed_time(b), g.leaves())
+        g.close()
+    l1, _ = learned.density_errors(cfg, out[False][1], out[True][1])
+    print("plain ms", out[False][0], "gated ms", out[True][0], "l1", l1)
+    assert l1 <= 1e-3
+    assert out[True][0] * 1.25 <= out[False][0]
+
+
+def _const_gate(bias):
+    p = np.zeros(learned.N_PARAMS, np.float32)
+    p[-1] = bias
+    return p
+
+
+def test_gate_rejecting_everything_is_exact(oracle_mod):
+    """A gate that sends every face to the hard list reproduces the plain
+    scheme bit for bit (compaction and the list kernel cover every face)."""
+    cfg = P.riemann4(base=32, lvl_amr=2, t_end=0.3)
+    o = oracle_mod.Oracle(cfg)
+    o.solute(5)
+    keys, prim, _ = o.leaves()
+    s = o.scalars()
+    g = Solver(cfg)
+    g.upload(keys, prim)
+    g.set_scalars(s["lambda_x"], s["lambda_y"], s["tstep"], s["tt"], s["it"])
+    learned.enable(g, _const_gate(-50.0))
+    for _ in range(3):
+        o.solute_step()
+        g.solute_step()
+    assert learned.stats(g)[0] == 0
+    assert np.array_equal(g.leaves()[1], o.leaves()[1])
+
+
+def test_gate_accepting_everything_is_linear_scheme():
+    """Every face on the linear path: the statistics count all faces, and
+    the smooth vortex stays close to the plain run."""
+    cfg = P.vortex()
+    plain, lin = Solver(cfg), Solver(cfg)
+    plain.creat_mesh_and_initial()
+    lin.creat_mesh_and_initial()
+    learned.enable(lin, _const_gate(50.0))
+    plain.solute(10)
+    lin.solute(10)
+    g, n = learned.stats(lin)
+    assert g >= 0.95 * n          # stage-3 count: the guard may send a few faces back
+    l1, _ = learned.density_errors(cfg, plain.leaves(), lin.leaves())
+    assert 0.0 < l1 < 1e-3, l1
+
+
+def test_gate_off_is_exact(oracle_mod):
+    cfg = P.vortex()
+    o = oracle_mod.Oracle(cfg)
+    o.solute(12)
+    keys, prim, _ = o.leaves()
+    s = o.scalars()
+    g = Solver(cfg)
+    g.upload(keys, prim)
+    g.set_scalars(s["lambda_x"], s["lambda_y"], s["tstep"], s["tt"], s["it"])
+    learned.enable(g, learned.init_params(0))
+    learned.disable(g)
+    o.solute_step()
+    g.solute_step()
+    assert np.array_equal(g.leaves()[1], o.leaves()[1])

@@ -203,3 +203,24 @@ def test_nan_state_stops(oracle_mod):
     with pytest.raises(FdmError) as e:
         g.solute_step()
     assert e.value.code == 3
+
+
+def test_distance_refined_mesh_steps(oracle_mod):
+    """The benchmark's kind of mesh (statically refined bands, 4 levels,
+    ghost cells refined with the interior) uploaded to both sides."""
+    from fdm_cell_based_amr_cartesian_b200.solver import distance_refined_keys, initial_state
+    cfg = P.riemann4(base=32, lvl_amr=4, pstep_adapt=1000)
+    keys = distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], [0.2, 0.15, 0.1, 0.05])
+    prim = initial_state(cfg, keys)
+    o = oracle_mod.Oracle(cfg, initial=False)
+    o.set_leaves(keys, prim)
+    g = Solver(cfg)
+    g.upload(keys, prim)
+    for _ in range(3):
+        dt = g.step_control()
+        o.step_control()
+        assert dt == o.scalars()["tstep"]
+        o.time_advance_rk()
+        g.time_advance_rk(dt)
+        assert_state_close(g, o)
+    assert np.isfinite(g.leaves()[1]).all()

@@ -1,0 +1,44 @@
+"""The benchmark's statically refined mesh (no GPU): 2:1 balance across the
+whole root grid, ghost cells included, and a finite, positive state after
+a few RK3 steps of the oracle."""
+import numpy as np
+
+from fdm_cell_based_amr_cartesian_b200 import learned
+from fdm_cell_based_amr_cartesian_b200 import params as P
+from fdm_cell_based_amr_cartesian_b200.solver import distance_refined_keys, initial_state
+
+BAND = [0.2, 0.15, 0.1, 0.05]
+
+
+def _small():
+    cfg = P.riemann4(base=32, lvl_amr=4, pstep_adapt=1000)
+    keys = distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], BAND)
+    return cfg, keys
+
+
+def test_distance_refined_mesh_is_balanced():
+    cfg, keys = _small()
+    lvl = (keys & np.uint64(15)).astype(np.float64)
+    vals = np.zeros((len(keys), 4))
+    vals[:, 0] = lvl
+    F = learned.fine_density(cfg, keys, vals)
+    assert F.shape == (cfg.n << 4, cfg.m << 4)
+    assert F.max() == 4
+    # face neighbours of every fine cell differ by at most one level
+    assert np.abs(np.diff(F, axis=0)).max() <= 1
+    assert np.abs(np.diff(F, axis=1)).max() <= 1
+    # the mesh reaches the boundary rows: the ghost rows are refined too
+    assert F[:3 << 4].max() >= 3
+
+
+def test_distance_refined_mesh_stays_finite(oracle_mod):
+    cfg, keys = _small()
+    prim = initial_state(cfg, keys)
+    o = oracle_mod.Oracle(cfg, initial=False)
+    o.set_leaves(keys, prim)
+    for _ in range(3):
+        o.step_control()
+        o.time_advance_rk()
+    _, p, _ = o.leaves()
+    assert np.isfinite(p).all()
+    assert p[:, 0].min() > 0.1 and p[:, 3].min() > 0.02
