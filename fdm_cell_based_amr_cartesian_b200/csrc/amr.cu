@@ -35,18 +35,62 @@ __global__ void k_rot_div(Tables T, LevelTab LT, const double4 *__restrict__ B, 
 
 // Srot = Srot + rot**2 ... in traversal order: one thread, the sum is a
 // sequence of roundings that no parallel order reproduces
-__global__ void k_ordered_sums(int64_t NI, const int32_t *order, const double *rot, const double *div,
-                               double *out) {
-    if (threadIdx.x || blockIdx.x) return;
+// squares in traversal order (the products are rounded exactly as in the
+// sequential loop: no FMA in this build)
+__global__ void k_ordered_squares(int64_t NI, const int32_t *__restrict__ order, const double *__restrict__ rot,
+                                  const double *__restrict__ div, double2 *__restrict__ sq) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= NI) return;
+    const int32_t i = order[k];
+    sq[k] = make_double2(rot[i] * rot[i], div[i] * div[i]);
+}
+
+// Srot, Sdiv: left-to-right sums in traversal order, as the reference's
+// recursive loop forms them (one lane adds; the warp streams the squares
+// through shared memory with cp.async, one chunk ahead)
+constexpr int SUM_CHUNK = 1024;   // double2 per chunk: 16 KB
+__device__ __forceinline__ void cp16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__global__ void __launch_bounds__(32) k_ordered_sums(int64_t NI, const double2 *__restrict__ sq, double *out) {
+    __shared__ double2 buf[2][SUM_CHUNK];
+    const int lane = threadIdx.x;
+    const int64_t nch = (NI + SUM_CHUNK - 1) / SUM_CHUNK;
+    auto fetch = [&](int64_t c) {
+        const int64_t base = c * SUM_CHUNK;
+        for (int j = lane; j < SUM_CHUNK; j += 32)
+            if (base + j < NI) cp16(&buf[c & 1][j], sq + base + j);
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
     double sr = 0.0, sd = 0.0;
-    for (int64_t k = 0; k < NI; ++k) {
-        const int32_t i = order[k];
-        sr = sr + rot[i] * rot[i];
-        sd = sd + div[i] * div[i];
+    if (nch > 0) fetch(0);
+    for (int64_t c = 0; c < nch; ++c) {
+        if (c + 1 < nch) {
+            fetch(c + 1);
+            asm volatile("cp.async.wait_group 1;\n" ::);
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int64_t rest = NI - c * SUM_CHUNK;
+            const int m = rest < SUM_CHUNK ? (int)rest : SUM_CHUNK;
+            const double2 *b = buf[c & 1];
+#pragma unroll 8
+            for (int j = 0; j < m; ++j) {
+                const double2 v = b[j];
+                sr = sr + v.x;
+                sd = sd + v.y;
+            }
+        }
+        __syncwarp();
     }
-    out[0] = sr;
-    out[1] = sd;
-    out[2] = (double)NI;
+    if (lane == 0) {
+        out[0] = sr;
+        out[1] = sd;
+        out[2] = (double)NI;
+    }
 }
 
 // rot/div of the current state into rot/div buffers; ordered sums to out3
@@ -54,16 +98,18 @@ static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3
     const int64_t NI = h->NI;
     launch_requests(h, h->B[0].as<double4>());
     Carve cv;
-    cv.add(NI * 8); cv.add(NI * 8); cv.add(NI * 4); cv.add(NI * 4);
+    cv.add(NI * 8); cv.add(NI * 8); cv.add(NI * 4); cv.add(NI * 4); cv.add(NI * 16);
     FDM_CK(h, h->tmp[0].ensure(cv.total));
     uint64_t *k0 = cv.at<uint64_t>(h->tmp[0], 0), *k1 = cv.at<uint64_t>(h->tmp[0], 1);
     int32_t *i0 = cv.at<int32_t>(h->tmp[0], 2), *i1 = cv.at<int32_t>(h->tmp[0], 3);
+    double2 *sq = cv.at<double2>(h->tmp[0], 4);
     k_rot_div<<<nblk(NI, 256), 256, 0, h->s>>>(h->tables(), h->lt, h->B[0].as<double4>(), rot, div, k0, i0);
     size_t bytes = 0;
     FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0, k1, i0, i1, (int)NI, 0, 64, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
     FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, k0, k1, i0, i1, (int)NI, 0, 64, h->s));
-    k_ordered_sums<<<1, 32, 0, h->s>>>(NI, i1, rot, div, out3);
+    k_ordered_squares<<<nblk(NI, 256), 256, 0, h->s>>>(NI, i1, rot, div, sq);
+    k_ordered_sums<<<1, 32, 0, h->s>>>(NI, sq, out3);
     return FDM_OK;
 }
 
@@ -83,7 +129,7 @@ struct NodeSet {
 };
 
 enum { D_NONE = 0, D_REFINE = 1, D_COARSEN = 2 };
-enum { PF_LEAF = 1, PF_DELETED = 2 };
+enum { PF_LEAF = 1, PF_DELETED = 2, PF_VISITED = 4 };
 
 __device__ __forceinline__ int64_t find_key(const uint64_t *__restrict__ keys, int64_t n, uint64_t k) {
     int64_t lo = 0, hi = n;
@@ -535,8 +581,10 @@ __device__ int64_t live_nb_set(const NodeSet &A, const Geometry &G, uint64_t k, 
     }
 }
 // leaves that can act in gridmodify4 (a neighbour, or the neighbour's
-// neighbour, two or more levels coarser); later refinements only make
-// neighbours finer, so no other initial leaf can act when visited
+// neighbour, two or more levels coarser).  Later refinements of leaves only
+// make neighbours finer; the one way a region gets coarser during the pass
+// (a non-leaf refinement dropping a deep subtree) queues the leaves around
+// it (push_ring)
 __global__ void k_gm4_triggers(NodeSet A, Geometry G, int32_t *flag, uint64_t *rank, int32_t *idx) {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= A.n) return;
@@ -563,15 +611,17 @@ struct Pool {
     uint8_t *flags;
     int32_t *gen;
     double4 *val;
-    int32_t *slot;       // hash slots -> pool index, -1 empty
+    int32_t *slot;       // hash slots -> pool index (| SLOT_DEL when deleted), -1 empty
+    uint64_t *skey;      // the key held by each slot
     uint64_t mask;       // slots - 1
     int64_t cap;         // pool capacity
     int64_t *n;          // pool size (device counter)
-    uint64_t *hrank;     // heap of new leaves
+    uint64_t *hrank;     // heap of leaves to visit ahead of the traversal
     int32_t *hidx, *hgen;
     int64_t hcap;
-    int32_t *err;        // [0] capacity exceeded, [1] visits, [2] non-leaf refines
+    int32_t *err;        // [0] capacity exceeded, [1] visits, [2] non-leaf refines, [3] step limit
 };
+constexpr int32_t SLOT_DEL = 0x40000000;
 __device__ __forceinline__ uint64_t hmix(uint64_t k) {
     k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
     return k;
@@ -586,51 +636,67 @@ __global__ void k_pool_init(NodeSet A, Pool P) {
     uint64_t hsh = hmix(A.key[i]) & P.mask;
     for (uint64_t probe = 0; probe <= P.mask; ++probe) {
         const int32_t old = atomicCAS(P.slot + hsh, -1, (int32_t)i);
-        if (old == -1) return;
+        if (old == -1) {
+            P.skey[hsh] = A.key[i];
+            return;
+        }
         hsh = (hsh + 1) & P.mask;
     }
-    atomicExch(P.err, 1);
 }
-// pool index of a live node, or -1
-__device__ int32_t hfind(const Pool &P, uint64_t k) {
+// slot position of key k (live or deleted), or -1; the slot word and the
+// slot key are independent loads, so a probe costs one memory round trip
+__device__ __forceinline__ int64_t hpos(const Pool &P, uint64_t k, int32_t &s) {
     uint64_t hsh = hmix(k) & P.mask;
     for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        const int32_t s = P.slot[hsh];
-        if (s < 0) return -1;
-        if (P.key[s] == k) return (P.flags[s] & PF_DELETED) ? -1 : s;
+        s = P.slot[hsh];
+        const uint64_t sk = P.skey[hsh];
+        if (s == -1) return -1;
+        if (sk == k) return (int64_t)hsh;
         hsh = (hsh + 1) & P.mask;
     }
     return -1;
 }
+// pool index of the live node with key k, or -1
+__device__ __forceinline__ int32_t hfind(const Pool &P, uint64_t k) {
+    int32_t s;
+    if (hpos(P, k, s) < 0) return -1;
+    return (s & SLOT_DEL) ? -1 : s;
+}
 // insert or revive a leaf with value v; returns its pool index or -1
 __device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v) {
+    int32_t s;
+    const int64_t pos = hpos(P, k, s);
+    if (pos >= 0) {
+        const int32_t i = s & ~SLOT_DEL;
+        P.slot[pos] = i;
+        P.flags[i] = PF_LEAF;
+        P.gen[i] = P.gen[i] + 1;
+        P.val[i] = v;
+        return i;
+    }
     uint64_t hsh = hmix(k) & P.mask;
     for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        const int32_t s = P.slot[hsh];
-        if (s < 0) {
+        if (P.slot[hsh] == -1) {
             const int64_t i = *P.n;
             if (i >= P.cap) return -1;
             *P.n = i + 1;
             P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
             P.slot[hsh] = (int32_t)i;
+            P.skey[hsh] = k;
             return (int32_t)i;
-        }
-        if (P.key[s] == k) {
-            P.flags[s] = PF_LEAF;
-            P.gen[s] = P.gen[s] + 1;
-            P.val[s] = v;
-            return s;
         }
         hsh = (hsh + 1) & P.mask;
     }
     return -1;
 }
-__device__ int32_t live_nb_pool(const Pool &P, const Geometry &G, uint64_t k, int dir) {
+// live neighbour in the pool: the same-level node, else the deepest existing
+// ancestor of it; its key in nk
+__device__ int32_t live_nb_pool(const Pool &P, const Geometry &G, uint64_t k, int dir, uint64_t &nk) {
     uint64_t t;
     if (!shift_key(G, k, dir, t)) return -1;
     for (;;) {
         const int32_t i = hfind(P, t);
-        if (i >= 0) return i;
+        if (i >= 0) { nk = t; return i; }
         if ((t & 15u) == 0) return -1;
         t = parent_key(t);
     }
@@ -662,22 +728,63 @@ __device__ void heap_pop(Pool &P, int64_t &hn, uint64_t &r, int32_t &idx, int32_
     }
     if (hn > 0) { P.hrank[i] = lr; P.hidx[i] = li; P.hgen[i] = lg; }
 }
+// After a non-leaf Refine_cell dropped a subtree two or more levels deep,
+// the region of pk (level l0) is coarser than before: leaves at level
+// >= l0 + 3 in the four edge-adjacent level-l0 cells can now find one of the
+// new sons as a neighbour (or neighbour's neighbour) two levels coarser.  The
+// reference visits every leaf, so those ahead of the traversal are queued.
+__device__ void push_ring(Pool &P, const Geometry &G, int64_t &hn, uint64_t pk, uint64_t cur_rank, int32_t &nl) {
+    const int l0 = (int)(pk & 15u);
+    const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
+    for (int d = 0; d < 4; ++d) {
+        uint64_t t;
+        if (!shift_key(G, pk, dirs[d], t)) continue;
+        const int32_t s0 = hfind(P, t);
+        if (s0 < 0 || (P.flags[s0] & PF_LEAF)) continue;
+        uint64_t st[64];
+        int sp = 0;
+        st[sp++] = t;
+        while (sp > 0) {
+            const uint64_t k = st[--sp];
+            for (int q = 0; q < 4; ++q) {
+                const uint64_t ck = child_key(k, q);
+                const int32_t c = hfind(P, ck);
+                if (c < 0) continue;
+                if (P.flags[c] & PF_LEAF) {
+                    const uint64_t r = dfs_rank(ck);
+                    if ((int)(ck & 15u) >= l0 + 3 && r > cur_rank) heap_push(P, hn, r, c, P.gen[c]);
+                } else if (sp < 64) {
+                    st[sp++] = ck;
+                } else {
+                    P.err[0] = 1;
+                }
+            }
+        }
+    }
+}
 // Refine_cell (src/mesh.F90:199-260) of a leaf, or of a non-leaf whose old
-// subtree is dropped and whose new sons copy its stale value
-__device__ void refine_pool(Pool &P, int64_t &hn, int32_t p, uint64_t cur_rank) {
+// subtree is dropped and whose new sons copy its stale value (counted in nl)
+__device__ void refine_pool(Pool &P, const Geometry &G, int64_t &hn, int32_t p, uint64_t cur_rank, int32_t &nl) {
     const uint64_t pk = P.key[p];
+    bool deep = false;
     if (!(P.flags[p] & PF_LEAF)) {
-        P.err[2] += 1;
+        nl += 1;
         uint64_t st[64];
         int sp = 0;
         st[sp++] = pk;
         while (sp > 0) {
             const uint64_t k = st[--sp];
             for (int q = 0; q < 4; ++q) {
-                const int32_t c = hfind(P, child_key(k, q));
-                if (c < 0) continue;
-                if (!(P.flags[c] & PF_LEAF) && sp < 64) st[sp++] = P.key[c];
-                P.flags[c] |= PF_DELETED;
+                int32_t s;
+                const int64_t pos = hpos(P, child_key(k, q), s);
+                if (pos < 0 || (s & SLOT_DEL)) continue;
+                if (!(P.flags[s] & PF_LEAF)) {
+                    if (k != pk) deep = true;
+                    if (sp < 64) st[sp++] = P.key[s];
+                    else P.err[0] = 1;
+                }
+                P.flags[s] |= PF_DELETED;
+                P.slot[pos] = s | SLOT_DEL;
             }
         }
     }
@@ -690,33 +797,125 @@ __device__ void refine_pool(Pool &P, int64_t &hn, int32_t p, uint64_t cur_rank) 
         const uint64_t r = dfs_rank(ck);
         if (r > cur_rank) heap_push(P, hn, r, c, P.gen[c]);
     }
+    if (deep) push_ring(P, G, hn, pk, cur_rank, nl);
 }
-// gridmodify4 (src/mesh.F90:355-395) over one pass of the tree: the initial
-// leaves that can act, and every leaf created ahead of the traversal, are
-// visited in traversal order by one thread
-__global__ void k_gm4_seq(Pool P, Geometry G, const uint64_t *trank, const int32_t *tidx, int64_t ntrig) {
-    if (threadIdx.x || blockIdx.x) return;
-    int64_t ti = 0, hn = 0;
+// gridmodify4 (src/mesh.F90:355-395) over one pass of the tree, by one
+// warp.  The leaves that can act (the initial triggers, sorted by traversal
+// rank, and every leaf queued ahead of the traversal) are visited in
+// traversal order.  Up to 8 upcoming trigger leaves are looked at together:
+// 4 lanes per leaf find its right/left/up/down neighbour and that
+// neighbour's neighbour at once.  The decisions are then applied leaf by
+// leaf in order; the batch ends after a leaf that refined something, and
+// within that leaf every later lookup is repeated on lane 0 after the
+// refinement, so the result is the sequential traversal's.
+constexpr int GM4_BATCH = 8;
+__global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint64_t *__restrict__ trank,
+                                                 const int32_t *__restrict__ tidx, int64_t ntrig, int64_t max_steps) {
+    const int lane = threadIdx.x, grp = lane >> 2, tl = lane & 3;
+    const unsigned FULL = 0xffffffffu;
     const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
-    const int64_t limit = ntrig + P.hcap + 1;
-    for (int64_t step = 0; step < limit; ++step) {
-        uint64_t r;
-        int32_t c, gen;
-        if (hn > 0 && (ti >= ntrig || P.hrank[0] < trank[ti])) heap_pop(P, hn, r, c, gen);
-        else if (ti < ntrig) { r = trank[ti]; c = tidx[ti]; gen = 0; ++ti; }
-        else break;
-        if (P.gen[c] != gen || (P.flags[c] & PF_DELETED) || !(P.flags[c] & PF_LEAF)) continue;
-        P.err[1] += 1;
-        const int lc = (int)(P.key[c] & 15u);
-        for (int t = 0; t < 4; ++t) {
-            const int32_t nb = live_nb_pool(P, G, P.key[c], dirs[t]);
-            if (nb < 0) continue;
-            if ((int)(P.key[nb] & 15u) <= lc - 2) refine_pool(P, hn, nb, r);
-            if (P.err[0]) return;
-            const int32_t nn = live_nb_pool(P, G, P.key[nb], dirs[t]);
-            if (nn >= 0 && (int)(P.key[nn] & 15u) <= lc - 2) refine_pool(P, hn, nn, r);
-            if (P.err[0]) return;
+    int64_t ti = 0, hn = 0;   // uniform
+    int64_t step = 0;
+    int32_t visits = 0, nonleaf = 0;   // lane 0's counts, stored at the end
+    for (;; ++step) {
+        if (step >= max_steps) { if (lane == 0) P.err[3] = 1; break; }
+        // the next items in traversal order
+        const uint64_t htop = hn > 0 ? P.hrank[0] : ~0ull;
+        int cnt = 0;
+        bool from_heap = false;
+        uint64_t r = 0;
+        int32_t c = -1, gen = 0;
+        if (hn > 0 && (ti >= ntrig || htop < trank[ti])) {
+            from_heap = true;
+            cnt = 1;
+            if (lane == 0) heap_pop(P, hn, r, c, gen);
+            r = __shfl_sync(FULL, r, 0);
+            c = __shfl_sync(FULL, c, 0);
+            gen = __shfl_sync(FULL, gen, 0);
+            hn = __shfl_sync(FULL, hn, 0);
+            __syncwarp();
+        } else if (ti < ntrig) {
+            const int64_t j = ti + grp;
+            bool ok = grp < GM4_BATCH && j < ntrig;
+            if (ok) {
+                r = trank[j];
+                c = tidx[j];
+                ok = r <= htop;   // a tie is the same leaf queued twice
+            }
+            const unsigned m = __ballot_sync(FULL, ok && tl == 0);
+            cnt = __popc(m);   // the ranks are sorted, so the ok items form a prefix
+        } else {
+            break;
         }
+        // speculative lookups: lane (grp, tl) handles direction tl of item grp
+        bool valid = false;
+        uint64_t ck = 0, nbk = 0, nnk = 0;
+        int32_t nb = -1, nn = -1;
+        uint8_t fl = 0;
+        if (grp < cnt) {
+            fl = P.flags[c];
+            const int32_t gc = P.gen[c];
+            ck = P.key[c];
+            valid = gc == gen && (fl & (PF_LEAF | PF_DELETED | PF_VISITED)) == PF_LEAF;
+            if (valid) {
+                nb = live_nb_pool(P, G, ck, dirs[tl], nbk);
+                if (nb >= 0) nn = live_nb_pool(P, G, nbk, dirs[tl], nnk);
+            }
+        }
+        int consumed = 0;
+        for (int b = 0; b < cnt; ++b) {
+            const bool vb = __shfl_sync(FULL, valid, b * 4);
+            const uint64_t rb = __shfl_sync(FULL, r, b * 4);
+            const int32_t cb = __shfl_sync(FULL, c, b * 4);
+            const uint64_t kb = __shfl_sync(FULL, ck, b * 4);
+            const uint8_t fb = (uint8_t)__shfl_sync(FULL, (int)fl, b * 4);
+            consumed = b + 1;
+            if (!vb) continue;
+            const int lc = (int)(kb & 15u);
+            bool dirty = false;   // a refinement since the lookups were made
+            if (lane == 0) {
+                P.flags[cb] = fb | PF_VISITED;
+                ++visits;
+            }
+            for (int t = 0; t < 4; ++t) {
+                int32_t nbt = __shfl_sync(FULL, nb, b * 4 + t);
+                uint64_t nbkt = __shfl_sync(FULL, nbk, b * 4 + t);
+                int32_t nnt = __shfl_sync(FULL, nn, b * 4 + t);
+                uint64_t nnkt = __shfl_sync(FULL, nnk, b * 4 + t);
+                if (dirty) {   // repeat the lookup after a refinement (lane 0)
+                    if (lane == 0) nbt = live_nb_pool(P, G, kb, dirs[t], nbkt);
+                    nbt = __shfl_sync(FULL, nbt, 0);
+                    nbkt = __shfl_sync(FULL, nbkt, 0);
+                }
+                if (nbt < 0) continue;
+                if ((int)(nbkt & 15u) <= lc - 2) {
+                    if (lane == 0) refine_pool(P, G, hn, nbt, rb, nonleaf);
+                    hn = __shfl_sync(FULL, hn, 0);
+                    __syncwarp();
+                    dirty = true;
+                    if (__shfl_sync(FULL, lane == 0 ? P.err[0] : 0, 0)) return;
+                }
+                if (dirty) {   // the neighbour's neighbour is looked up after Refine_cell(nbor)
+                    if (lane == 0) nnt = live_nb_pool(P, G, nbkt, dirs[t], nnkt);
+                    nnt = __shfl_sync(FULL, nnt, 0);
+                    nnkt = __shfl_sync(FULL, nnkt, 0);
+                }
+                if (nnt >= 0 && (int)(nnkt & 15u) <= lc - 2) {
+                    if (lane == 0) refine_pool(P, G, hn, nnt, rb, nonleaf);
+                    hn = __shfl_sync(FULL, hn, 0);
+                    __syncwarp();
+                    dirty = true;
+                    if (__shfl_sync(FULL, lane == 0 ? P.err[0] : 0, 0)) return;
+                }
+            }
+            if (dirty) break;   // later items are looked up again
+        }
+        if (!from_heap) ti += consumed;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        P.err[1] = visits;
+        P.err[2] = nonleaf;
     }
 }
 __global__ void k_pool_live(int64_t n, const uint8_t *flags, int32_t *live) {
@@ -855,7 +1054,7 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     while (slots < (uint64_t)(2 * cap)) slots <<= 1;
     Carve cp;
     cp.add(cap * 8); cp.add(cap); cp.add(cap * 4); cp.add(cap * 32); cp.add(slots * 4); cp.add(16);
-    cp.add(cap * 8); cp.add(cap * 4); cp.add(cap * 4); cp.add(16);
+    cp.add(cap * 8); cp.add(cap * 4); cp.add(cap * 4); cp.add(16); cp.add(slots * 8);
     FDM_CK(h, h->amr[16].ensure(cp.total));
     DevBuf &pb = h->amr[16];
     Pool P;
@@ -863,6 +1062,7 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     P.val = cp.at<double4>(pb, 3); P.slot = cp.at<int32_t>(pb, 4); P.n = cp.at<int64_t>(pb, 5);
     P.hrank = cp.at<uint64_t>(pb, 6); P.hidx = cp.at<int32_t>(pb, 7); P.hgen = cp.at<int32_t>(pb, 8);
     P.err = cp.at<int32_t>(pb, 9);
+    P.skey = cp.at<uint64_t>(pb, 10);
     P.mask = slots - 1;
     P.cap = cap;
     P.hcap = cap;
@@ -870,13 +1070,15 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     FDM_CK(h, cudaMemsetAsync(P.err, 0, 16, h->s));
     FDM_CK(h, cudaMemcpyAsync(P.n, &n, 8, cudaMemcpyHostToDevice, h->s));
     k_pool_init<<<nblk(n, TB), TB, 0, h->s>>>(X.A, P);
-    k_gm4_seq<<<1, 32, 0, h->s>>>(P, h->G, rk, idx, ntrig);
+    // every step consumes a trigger or a queued leaf, or ends the pass
+    k_gm4_warp<<<1, 32, 0, h->s>>>(P, h->G, rk, idx, ntrig, ntrig + P.hcap + 16);
     int32_t herr[4] = {0, 0, 0, 0};
     int64_t pn = 0;
     FDM_CK(h, cudaMemcpyAsync(herr, P.err, 16, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaMemcpyAsync(&pn, P.n, 8, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     if (herr[0]) { h->err = "gridmodify4 cascade exceeded its node pool"; return FDM_ERR_UNSUPPORTED; }
+    if (herr[3]) { h->err = "gridmodify4 replay did not finish"; return FDM_ERR_UNSUPPORTED; }
     h->gm4_visits += herr[1];
     h->gm4_nonleaf += herr[2];
     // live nodes back into a sorted node set
@@ -905,6 +1107,9 @@ int run_amr(fdm_handle *h) {
         h->err = "device regrid supports up to 2^19 background cells";
         return FDM_ERR_UNSUPPORTED;
     }
+    for (int k = 0; k <= fdm_handle::AMR_PHASES; ++k)
+        if (!h->amr_ev[k]) FDM_CK(h, cudaEventCreate(&h->amr_ev[k]));
+    FDM_CK(h, cudaEventRecord(h->amr_ev[0], h->s));
     // 1. indicators and their ordered sums
     Carve ci;
     ci.add(NI * 8); ci.add(NI * 8); ci.add(32); ci.add(NL); ci.add((NInt > 0 ? NInt : 1));
@@ -912,6 +1117,7 @@ int run_amr(fdm_handle *h) {
     double *rot = ci.at<double>(h->amr[18], 0), *div = ci.at<double>(h->amr[18], 1), *sums = ci.at<double>(h->amr[18], 2);
     int8_t *rflag = ci.at<int8_t>(h->amr[18], 3), *cflag = ci.at<int8_t>(h->amr[18], 4);
     AMR_RC(compute_rot_div(h, rot, div, sums));
+    FDM_CK(h, cudaEventRecord(h->amr_ev[1], h->s));
     // 2. solute_ref: refine and coarsen flags, applied at once
     const Tables T = h->tables();
     k_refine_flags<<<nblk(NL, TB), TB, 0, h->s>>>(T, h->G, h->p, rot, div, sums, rflag);
@@ -934,11 +1140,13 @@ int run_amr(fdm_handle *h) {
     bind_sets(h, X);
     AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
     swap_sets(h, X);
+    FDM_CK(h, cudaEventRecord(h->amr_ev[2], h->s));
     // 3. solute_gridmodify: lvlAMR rounds (src/solution.F90:537-556)
     for (int k = 1; k <= h->p.lvl_amr; ++k) {
         AMR_RC(gridmodify1_pass(h, X));
         AMR_RC(gridmodify4_pass(h, X));
     }
+    FDM_CK(h, cudaEventRecord(h->amr_ev[3], h->s));
     // 4. split leaves / internal nodes, rebuild the tables (idneighbor + IDgrid)
     const int64_t n = X.A.n;
     Carve cs;
@@ -957,15 +1165,32 @@ int run_amr(fdm_handle *h) {
     FDM_CK(h, h->ival.ensure(nint * 32 + 32));
     k_split_emit<<<nblk(n, TB), TB, 0, h->s>>>(X.A, ol, oi, lk.as<uint64_t>(), lv.as<double4>(),
                                                h->ikey.as<uint64_t>(), h->ival.as<double4>());
+    FDM_CK(h, cudaEventRecord(h->amr_ev[4], h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     h->NInt = nint;
     const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>());
     if (rc) return rc;
+    FDM_CK(h, cudaEventRecord(h->amr_ev[5], h->s));
+    FDM_CK(h, cudaEventSynchronize(h->amr_ev[5]));
+    for (int k = 0; k < fdm_handle::AMR_PHASES; ++k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, h->amr_ev[k], h->amr_ev[k + 1]);
+        h->amr_phase_ms[k] = t;
+    }
     h->n_regrids++;
     return FDM_OK;
 }
 
 }  // namespace fdm
+
+// Device-timeline milliseconds of the last regrid's phases: indicators and
+// ordered sums, refine/coarsen flags and the first node sort, the lvlAMR
+// gridmodify rounds, the leaf/internal split, the table rebuild.
+extern "C" int fdm_amr_phase_ms(const fdm_handle *h, double *ms) {
+    if (!h || !ms) return FDM_ERR_ARG;
+    for (int k = 0; k < fdm_handle::AMR_PHASES; ++k) ms[k] = h->amr_phase_ms[k];
+    return FDM_OK;
+}
 
 extern "C" int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double *div, double *sums) {
     using namespace fdm;

@@ -91,6 +91,10 @@ struct fdm_handle {
     int64_t NInt = 0;
     fdm::DevBuf amr[20];     // regrid scratch
     int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0;
+    // device-timeline phases of the last regrid (events recorded on the stream)
+    static constexpr int AMR_PHASES = 5;
+    cudaEvent_t amr_ev[AMR_PHASES + 1] = {};
+    double amr_phase_ms[AMR_PHASES] = {};
 
     // learned gate of the face flux
     fdm::DevBuf gate_params, gate_flag;   // gate_flag: per-stage hard-face lists

@@ -248,6 +248,8 @@ void fdm_destroy(fdm_handle *h) {
                       &h->gate_params, &h->gate_flag, &h->ikey, &h->ival};
     for (DevBuf *b : bufs) b->release();
     for (auto &t : h->tmp) t.release();
+    for (cudaEvent_t e : h->amr_ev)
+        if (e) cudaEventDestroy(e);
     if (h->hs) cudaFreeHost(h->hs);
     if (h->s) cudaStreamDestroy(h->s);
     delete h;

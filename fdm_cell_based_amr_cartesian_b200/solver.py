@@ -37,7 +37,7 @@ EXPORTS = [
     "fdm_debug_requests",
     "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
     "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
-    "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats",
+    "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
 ]
 
 
@@ -102,6 +102,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(dp), ctypes.POINTER(i64)]
     L.fdm_time_kernels.argtypes = [vp, i32, dp]
     L.fdm_fp64_peak.argtypes = [dp]
+    L.fdm_amr_phase_ms.argtypes = [vp, dp]
     L.fdm_autotune.argtypes = [vp, i32, ctypes.POINTER(i32), dp]
     L.fdm_set_variant.argtypes = [vp, i32]
     L.fdm_time_advance_rk_uniform_static.argtypes = [vp, vp, i32, i32, ctypes.c_double, ctypes.c_double,
@@ -331,6 +332,12 @@ class Solver:
         sums = np.zeros(3)
         self._check(self.L.fdm_debug_rot_div(self.h, n, _dp(rot), _dp(div), _dp(sums)))
         return rot, div, sums
+
+    def amr_phase_ms(self) -> dict:
+        """Device-timeline ms of the last regrid's phases."""
+        a = np.zeros(5)
+        self._check(self.L.fdm_amr_phase_ms(self.h, _dp(a)))
+        return dict(zip(("indicators", "flags", "gridmodify", "split", "tables"), a.tolist()))
 
     def time_kernels(self, reps: int = 10):
         """Average ms per launch: faces (x+y), cells, hanging nodes, ghosts."""

@@ -270,6 +270,12 @@ int fdm_gate_eval(const float *X, int64_t n, const float *params, float *prob,
 /* faces that took the linear path in the last gated stage / all faces */
 int fdm_gate_stats(fdm_handle *h, int64_t *gated, int64_t *total);
 
+/* Diagnostics, no reference counterpart: device-timeline milliseconds of
+ * the last regrid's five phases (indicators + ordered sums; flags + first
+ * node sort; the lvlAMR gridmodify rounds; leaf/internal split; table
+ * rebuild). */
+int fdm_amr_phase_ms(const fdm_handle *h, double ms[5]);
+
 /* ------------------------------------------------- no-allocation entry point
  * One SSP-RK3 step (the three stages of Time_advance_RK with periodic ghost
  * fill) on a uniform periodic grid of nx x ny cells, without allocating any
