@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfdm.so")
-SOURCES = ["build.cu", "stage.cu", "amr.cu", "libfdm.cu", "timing.cu", "static_uniform.cu", "gate.cu"]
+SOURCES = ["build.cu", "stage.cu", "amr.cu", "libfdm.cu", "timing.cu", "static_uniform.cu", "gate.cu", "batch.cu"]
 HEADERS = ["fdm_common.cuh", "handle.cuh", "numerics.cuh", "topo.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1,0 +1,695 @@
+// batch.cu — many independent meshes advanced together: one persistent
+// kernel launch per SSP-RK3 stage covers every member of an ensemble.
+//
+// No reference counterpart (the reference runs one mesh per process).  Each
+// member is an ordinary handle (its own tables, state buffers and scalars);
+// the batch only schedules their work.  A launch runs the phases of one
+// stage (step control, hanging-node requests, faces, hard faces of the
+// learned gate, cells, ghosts and, at stage 3, the residual and the end of
+// the step) for all members, separated by a grid barrier.  Inside a phase
+// the blocks take (member, tile) pairs from one atomic counter, so members
+// of very different sizes share the machine without a static split.  The
+// per-item arithmetic is the single-mesh code (items.cuh, gate_items.cuh),
+// so a member advanced in a batch matches the same handle advanced alone.
+//
+// The launch is cooperative (all blocks resident), and every wait in the
+// grid barrier has an iteration limit: a barrier that does not complete
+// sets an error word and the kernel returns, which the host reports.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "gate_items.cuh"
+
+struct fdm_batch;
+
+namespace fdm {
+
+__host__ __device__ __forceinline__ int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+constexpr int BT = 256;        // threads per block
+constexpr int BW = BT / 32;    // warps per block
+
+enum { PH_REQ = 0, PH_FACE, PH_HARD, PH_CELL, PH_GHOST, PH_GHOST1, N_PHASE };
+
+struct Member {
+    Tables T;
+    LevelTab LT;
+    double4 *B0, *B1, *B2;
+    double4 *Fx, *Fy;
+    DevScalars *sc;
+    double *res_part;
+    GhostStates GS;
+    double gama;
+    // step control (src/solution.F90:185-201)
+    fdm_params p;
+    int32_t amr_on;          // body_boundary(1) after each step
+    int32_t has_restrict;
+    // learned gate
+    int32_t gate_on;
+    float logit_thr;
+    const float *gate_P;
+    GateLists GL;
+    int64_t nfx, nfy;
+};
+
+struct GridBar {
+    unsigned count;
+    unsigned gen;
+    int err;
+    int pad;
+};
+
+struct BatchArgs {
+    const Member *mem;
+    int nmem;
+    int any_gate;
+    const int64_t *off;            // [N_PHASE][nmem + 1] tile offsets (PH_HARD filled on the device)
+    int64_t *off_hard;             // = off + PH_HARD * (nmem + 1)
+    unsigned long long *ctr;       // [N_PHASE] tile counters, zero at launch
+    GridBar *bar;
+    int32_t *act;                  // member not finished at the start of the step
+    const int32_t *skip_j1;        // host: a regrid follows this step (no body_boundary(1) here)
+};
+
+constexpr unsigned long long BAR_SPIN_LIMIT = 1ull << 24;   // x >= 64 ns of sleep: about a second
+
+// Grid-wide barrier among the co-resident blocks of a cooperative launch.
+// Returns false when any block gave up waiting; the caller then returns.
+__device__ bool grid_bar(GridBar *b, unsigned nblocks) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = &b->gen;
+        const unsigned g0 = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&b->count, 1u);
+        if (arrived == nblocks - 1) {
+            b->count = 0;
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*vgen == g0) {
+                if (++spins > BAR_SPIN_LIMIT || *(volatile int *)&b->err) {
+                    atomicExch(&b->err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int *)&b->err == 0;
+}
+
+// Work stealing over the tiles of one phase: fn(member, tile) for every
+// tile, each taken by one block from the phase's counter.
+template <class Fn>
+__device__ __forceinline__ void run_tiles(const BatchArgs &A, int ph, const int64_t *off, int64_t *s_t, Fn &&fn) {
+    const int64_t total = off[A.nmem];
+    for (;;) {
+        if (threadIdx.x == 0) *s_t = (int64_t)atomicAdd(A.ctr + ph, 1ull);
+        __syncthreads();
+        const int64_t t = *s_t;
+        __syncthreads();
+        if (t >= total) break;
+        int lo = 0, hi = A.nmem;   // off[lo] <= t < off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (off[mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        fn(lo, t - off[lo]);
+    }
+}
+
+struct GateSmem {
+    GateWeights W;
+    XTile xt[BW];
+};
+union BatchSmem {
+    GateSmem gate;
+    RestrictSmem rs[BW];
+    CellsSmem cells;
+    double fin[BT][8];
+};
+
+__device__ __forceinline__ const double4 *stage_cur(const Member &M, int krk) {
+    return krk == 1 ? M.B0 : krk == 2 ? M.B1 : M.B2;
+}
+__device__ __forceinline__ double4 *stage_next(const Member &M, int krk) {
+    return krk == 1 ? M.B1 : krk == 2 ? M.B2 : M.B0;
+}
+
+// One RK stage (krk) of every member; MINB resident blocks per SM (the
+// register budget follows: 128 per thread at 2, up to 255 at 1).
+template <int MINB>
+__global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSmem &S = *reinterpret_cast<BatchSmem *>(smem_raw);
+    __shared__ int64_t s_t;
+    __shared__ const float *s_loaded;
+    const unsigned nb = gridDim.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int np1 = A.nmem + 1;
+
+    // ---- step control / per-stage resets (one thread per member)
+    if (blockIdx.x == 0) {
+        for (int m = threadIdx.x; m < A.nmem; m += BT) {
+            const Member &M = A.mem[m];
+            if (krk == 1) {
+                A.act[m] = (!M.sc->done && M.sc->tt < M.p.t_end) ? 1 : 0;
+                if (A.act[m]) step_control_item(M.sc, M.p, 1);
+            }
+            if (!A.act[m]) continue;
+            if (krk == 3) { M.sc->lam_next_x = 0.0; M.sc->lam_next_y = 0.0; }
+            if (M.gate_on) {
+                if (krk == 1) { M.GL.cnt[0] = 0; M.GL.cnt[1] = 0; }
+                else { M.GL.cnt[0] = M.GL.cnt[2]; M.GL.cnt[1] = M.GL.cnt[3]; }
+            }
+        }
+    }
+    if (!grid_bar(A.bar, nb)) return;
+
+    // ---- hanging-node requests
+    run_tiles(A, PH_REQ, A.off + PH_REQ * np1, &s_t, [&](int m, int64_t t) {
+        const Member &M = A.mem[m];
+        if (!A.act[m]) return;
+        double4 *cur = const_cast<double4 *>(stage_cur(M, krk));
+        const int64_t nthr = cdiv(M.T.NR, BT);
+        if (t < nthr) {
+            const int64_t r = t * BT + threadIdx.x;
+            if (r < M.T.NR) request_item(M.T, cur, r);
+        } else {
+            const int64_t r = (t - nthr) * BW + wid;
+            if (r < M.T.NR) request_restrict_warp(M.T, cur, r, S.rs[wid]);
+        }
+    });
+    if (!grid_bar(A.bar, nb)) return;
+
+    // ---- faces: plain flux, or gate / guard with the linear flux
+    if (threadIdx.x == 0) s_loaded = nullptr;
+    __syncthreads();
+    run_tiles(A, PH_FACE, A.off + PH_FACE * np1, &s_t, [&](int m, int64_t t) {
+        const Member &M = A.mem[m];
+        if (!A.act[m]) return;
+        const double4 *cur = stage_cur(M, krk);
+        const int64_t tx = cdiv(M.nfx, BT);
+        const int dir = t < tx ? 0 : 1;
+        const int64_t lt = dir == 0 ? t : t - tx;
+        const int64_t nf = dir == 0 ? M.nfx : M.nfy;
+        const double lam = dir == 0 ? M.sc->lambda_x : M.sc->lambda_y;
+        if (!M.gate_on) {
+            const int64_t f = lt * BT + threadIdx.x;
+            if (f < nf) {
+                if (dir == 0) face_item<0>(M.T, cur, M.Fx, lam, M.gama, f);
+                else face_item<1>(M.T, cur, M.Fy, lam, M.gama, f);
+            }
+            return;
+        }
+        const double ig1 = 1.0 / (M.gama - 1.0);
+        const int64_t w = lt * BW + wid;   // warp chunk of 32 faces
+        if (krk == 1) {
+            if (s_loaded != M.gate_P) {
+                __syncthreads();
+                load_weights_smem(S.gate.W, M.gate_P);
+                for (int k = GF; k < XLD; ++k) S.gate.xt[wid].X[lane][k] = __float2bfloat16_rn(0.f);
+                if (threadIdx.x == 0) s_loaded = M.gate_P;
+                __syncthreads();
+            }
+            if (w * 32 < nf) {
+                if (dir == 0)
+                    gate_linear_chunk<0>(M.T, cur, M.Fx, S.gate.W, S.gate.xt[wid], M.logit_thr, lam, ig1, M.gama,
+                                         M.GL.hx, M.GL.cnt, M.GL.jx, w);
+                else
+                    gate_linear_chunk<1>(M.T, cur, M.Fy, S.gate.W, S.gate.xt[wid], M.logit_thr, lam, ig1, M.gama,
+                                         M.GL.hy, M.GL.cnt + 1, M.GL.jy, w);
+            }
+        } else if (w * 32 < nf) {
+            if (dir == 0)
+                guard_linear_chunk<0>(M.T, cur, M.Fx, M.GL.jx, lam, ig1, M.gama, M.GL.hx, M.GL.cnt, w);
+            else
+                guard_linear_chunk<1>(M.T, cur, M.Fy, M.GL.jy, lam, ig1, M.gama, M.GL.hy, M.GL.cnt + 1, w);
+        }
+    });
+    if (!grid_bar(A.bar, nb)) return;
+
+    // ---- hard faces of gated members (full WCNS flux)
+    if (A.any_gate) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            int64_t acc = 0;
+            for (int m = 0; m < A.nmem; ++m) {
+                A.off_hard[m] = acc;
+                const Member &M = A.mem[m];
+                if (!A.act[m] || !M.gate_on) continue;
+                if (krk == 1) { M.GL.cnt[2] = M.GL.cnt[0]; M.GL.cnt[3] = M.GL.cnt[1]; }
+                acc += cdiv(M.GL.cnt[0], BT) + cdiv(M.GL.cnt[1], BT);
+            }
+            A.off_hard[A.nmem] = acc;
+        }
+        if (!grid_bar(A.bar, nb)) return;
+        run_tiles(A, PH_HARD, A.off_hard, &s_t, [&](int m, int64_t t) {
+            const Member &M = A.mem[m];
+            const double4 *cur = stage_cur(M, krk);
+            const int64_t tx = cdiv(M.GL.cnt[0], BT);
+            if (t < tx) {
+                const int64_t i = t * BT + threadIdx.x;
+                if (i < M.GL.cnt[0]) face_item<0>(M.T, cur, M.Fx, M.sc->lambda_x, M.gama, M.GL.hx[i]);
+            } else {
+                const int64_t i = (t - tx) * BT + threadIdx.x;
+                if (i < M.GL.cnt[1]) face_item<1>(M.T, cur, M.Fy, M.sc->lambda_y, M.gama, M.GL.hy[i]);
+            }
+        });
+        if (!grid_bar(A.bar, nb)) return;
+    }
+
+    // ---- cells: residual, candidate, RK blend, residual partials, lambda
+    run_tiles(A, PH_CELL, A.off + PH_CELL * np1, &s_t, [&](int m, int64_t t) {
+        const Member &M = A.mem[m];
+        if (!A.act[m]) return;
+        const int64_t i = t * BT + threadIdx.x;
+        double rm[4] = {0.0, 0.0, 0.0, 0.0}, rs[4] = {0.0, 0.0, 0.0, 0.0};
+        double lx = 0.0, ly = 0.0;
+        if (i < M.T.NI)
+            cell_item(M.T, M.LT, stage_cur(M, krk), M.B0, stage_next(M, krk), M.Fx, M.Fy, M.sc->tstep, krk, 0,
+                      M.gama, i, rm, rs, lx, ly);
+        cells_block_reduce(rm, rs, lx, ly, M.res_part + t * 8, M.sc, krk == 3, S.cells);
+    });
+    if (!grid_bar(A.bar, nb)) return;
+
+    // ---- ghosts of the new stage value (body_boundary_RK)
+    run_tiles(A, PH_GHOST, A.off + PH_GHOST * np1, &s_t, [&](int m, int64_t t) {
+        const Member &M = A.mem[m];
+        if (!A.act[m]) return;
+        const int64_t gi = t * BW + wid;
+        if (gi < M.T.NG) ghost_warp(M.T, stage_next(M, krk), M.GS, M.sc, 3, gi, S.rs[wid]);
+    });
+    if (krk != 3) return;
+    if (!grid_bar(A.bar, nb)) return;
+
+    // ---- end of the step: residual norms, tt, it, NaN, t_end
+    for (int m = blockIdx.x; m < A.nmem; m += nb) {
+        const Member &M = A.mem[m];
+        if (!A.act[m]) continue;
+        res_finalize_block(M.res_part, (int)cdiv(M.T.NI, BT), M.sc, S.fin);
+        if (threadIdx.x == 0) step_end_item(M.sc, M.T.NI);
+        __syncthreads();
+    }
+    if (!grid_bar(A.bar, nb)) return;
+
+    // ---- body_boundary(1) after the step on AMR members
+    run_tiles(A, PH_GHOST1, A.off + PH_GHOST1 * np1, &s_t, [&](int m, int64_t t) {
+        const Member &M = A.mem[m];
+        if (!A.act[m] || !M.amr_on || A.skip_j1[m]) return;
+        const int64_t gi = t * BW + wid;
+        if (gi < M.T.NG) ghost_warp(M.T, M.B0, M.GS, M.sc, 1, gi, S.rs[wid]);
+    });
+}
+
+}  // namespace fdm
+
+using namespace fdm;
+
+struct fdm_batch {
+    std::vector<fdm_handle *> mem;
+    int device = 0;
+    cudaStream_t s = nullptr;
+    DevBuf d_mem, d_off, d_ctr, d_bar, d_act, d_skip;
+    std::vector<int32_t> h_skip;
+    int grid = 0, blocks_per_sm = 0, want_bps = 2;
+    size_t smem = 0;
+    bool any_gate = false;
+    cudaGraphExec_t graph = nullptr;
+    bool use_graph = true;           // off when cooperative launches cannot be captured here
+    std::vector<int64_t> versions;   // member table versions the descriptors were built for
+    std::vector<bool> gates;
+    std::vector<float> thr;
+    cudaEvent_t ev = nullptr;
+    std::string err;
+};
+
+static int batch_fail(fdm_batch *b, cudaError_t e, const char *what) {
+    b->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return FDM_ERR_CUDA;
+}
+#define BCK(b, x)                                             \
+    do {                                                      \
+        cudaError_t e_ = (x);                                 \
+        if (e_ != cudaSuccess) return batch_fail(b, e_, #x);  \
+    } while (0)
+
+static void drop_batch_graph(fdm_batch *b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+}
+
+// Member descriptors and tile offsets from the members' current tables.
+static int batch_refresh(fdm_batch *b) {
+    const int n = (int)b->mem.size();
+    std::vector<Member> M(n);
+    std::vector<int64_t> off((size_t)N_PHASE * (n + 1), 0);
+    b->any_gate = false;
+    for (int m = 0; m < n; ++m) {
+        fdm_handle *h = b->mem[m];
+        Member &d = M[m];
+        std::memset(&d, 0, sizeof d);
+        d.T = h->tables();
+        d.LT = h->lt;
+        d.B0 = h->B[0].as<double4>();
+        d.B1 = h->B[1].as<double4>();
+        d.B2 = h->B[2].as<double4>();
+        d.Fx = h->Fx.as<double4>();
+        d.Fy = h->Fy.as<double4>();
+        d.sc = h->scal.as<DevScalars>();
+        d.res_part = h->res_part.as<double>();
+        d.GS = ghost_states(h->p);
+        d.gama = h->G.gama;
+        d.p = h->p;
+        d.amr_on = h->p.iflag_amr ? 1 : 0;
+        d.has_restrict = h->n_restrict > 0;
+        d.nfx = h->NI + h->nux;
+        d.nfy = h->NI + h->nuy;
+        d.gate_on = h->gate_on;
+        if (h->gate_on) {
+            b->any_gate = true;
+            d.logit_thr = h->gate_logit_thr;
+            d.gate_P = h->gate_params.as<float>();
+            d.GL = gate_lists(h->gate_flag.p, d.nfx, d.nfy);
+        }
+        const int64_t tiles[N_PHASE] = {
+            cdiv(h->NR, BT) + (d.has_restrict ? cdiv(h->NR, BW) : 0),   // PH_REQ
+            cdiv(d.nfx, BT) + cdiv(d.nfy, BT),                          // PH_FACE
+            0,                                                          // PH_HARD (device)
+            cdiv(h->NI, BT),                                            // PH_CELL
+            cdiv(h->NG, BW),                                            // PH_GHOST
+            cdiv(h->NG, BW)};                                           // PH_GHOST1
+        for (int ph = 0; ph < N_PHASE; ++ph) off[(size_t)ph * (n + 1) + m + 1] = off[(size_t)ph * (n + 1) + m] + tiles[ph];
+    }
+    BCK(b, b->d_mem.ensure(sizeof(Member) * n));
+    BCK(b, b->d_off.ensure(sizeof(int64_t) * off.size()));
+    BCK(b, cudaMemcpyAsync(b->d_mem.p, M.data(), sizeof(Member) * n, cudaMemcpyHostToDevice, b->s));
+    BCK(b, cudaMemcpyAsync(b->d_off.p, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice, b->s));
+    BCK(b, cudaStreamSynchronize(b->s));
+    b->versions.resize(n);
+    b->gates.resize(n);
+    b->thr.resize(n);
+    for (int m = 0; m < n; ++m) {
+        b->versions[m] = b->mem[m]->table_version;
+        b->gates[m] = b->mem[m]->gate_on;
+        b->thr[m] = b->mem[m]->gate_logit_thr;
+    }
+    drop_batch_graph(b);
+    return FDM_OK;
+}
+
+static bool batch_stale(const fdm_batch *b) {
+    for (size_t m = 0; m < b->mem.size(); ++m)
+        if (b->versions[m] != b->mem[m]->table_version || b->gates[m] != b->mem[m]->gate_on ||
+            b->thr[m] != b->mem[m]->gate_logit_thr)
+            return true;
+    return false;
+}
+
+static int batch_grid(fdm_batch *b) {
+    int sms = 0, bps = 0;
+    BCK(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    if (b->want_bps == 1) {
+        BCK(b, cudaFuncSetAttribute(k_batch_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        BCK(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_stage<1>, BT, b->smem));
+    } else {
+        BCK(b, cudaFuncSetAttribute(k_batch_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        BCK(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_stage<2>, BT, b->smem));
+    }
+    if (bps <= 0) { b->err = "the batch kernel does not fit on an SM"; return FDM_ERR_UNSUPPORTED; }
+    b->blocks_per_sm = std::min(bps, b->want_bps);
+    b->grid = sms * b->blocks_per_sm;
+    return FDM_OK;
+}
+
+static int enqueue_batch_stage(fdm_batch *b, int krk) {
+    BatchArgs A;
+    A.mem = b->d_mem.as<Member>();
+    A.nmem = (int)b->mem.size();
+    A.any_gate = b->any_gate ? 1 : 0;
+    A.off = b->d_off.as<int64_t>();
+    A.off_hard = const_cast<int64_t *>(A.off) + PH_HARD * (A.nmem + 1);
+    A.ctr = b->d_ctr.as<unsigned long long>();
+    A.bar = b->d_bar.as<GridBar>();
+    A.act = b->d_act.as<int32_t>();
+    A.skip_j1 = b->d_skip.as<int32_t>();
+    BCK(b, cudaMemsetAsync(A.ctr, 0, sizeof(unsigned long long) * N_PHASE, b->s));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->grid);
+    cfg.blockDim = dim3(BT);
+    cfg.dynamicSmemBytes = b->smem;
+    cfg.stream = b->s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (b->want_bps == 1) BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<1>, A, krk));
+    else BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<2>, A, krk));
+    return FDM_OK;
+}
+
+// CUDA graph of one step of every member (three cooperative launches);
+// captured again whenever a member's tables or gate change.  Where the
+// capture of a cooperative launch is refused, the three launches are issued
+// directly instead.
+static int batch_graph(fdm_batch *b) {
+    if (batch_stale(b)) {
+        int rc = batch_refresh(b);
+        if (rc) return rc;
+    }
+    if (b->graph || !b->use_graph) return FDM_OK;
+    cudaGraph_t g = nullptr;
+    BCK(b, cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
+    int rc = FDM_OK;
+    for (int krk = 1; krk <= 3 && !rc; ++krk) rc = enqueue_batch_stage(b, krk);
+    cudaError_t e = cudaStreamEndCapture(b->s, &g);
+    if (!rc && e == cudaSuccess) {
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        if (e != cudaSuccess) b->graph = nullptr;
+    }
+    if (g) cudaGraphDestroy(g);
+    if (rc || e != cudaSuccess || !b->graph) {
+        cudaGetLastError();
+        b->use_graph = false;
+        b->err.clear();
+    }
+    return FDM_OK;
+}
+
+static int launch_step(fdm_batch *b) {
+    if (b->graph) {
+        BCK(b, cudaGraphLaunch(b->graph, b->s));
+        return FDM_OK;
+    }
+    for (int krk = 1; krk <= 3; ++krk) {
+        int rc = enqueue_batch_stage(b, krk);
+        if (rc) return rc;
+    }
+    return FDM_OK;
+}
+
+// members' queued work before the batch's, the batch's before theirs after
+static int join_members(fdm_batch *b) {
+    for (fdm_handle *h : b->mem) {
+        BCK(b, cudaEventRecord(b->ev, h->s));
+        BCK(b, cudaStreamWaitEvent(b->s, b->ev, 0));
+    }
+    return FDM_OK;
+}
+static int release_members(fdm_batch *b) {
+    BCK(b, cudaEventRecord(b->ev, b->s));
+    for (fdm_handle *h : b->mem) BCK(b, cudaStreamWaitEvent(h->s, b->ev, 0));
+    return FDM_OK;
+}
+
+static int check_barrier(fdm_batch *b) {
+    GridBar gb;
+    BCK(b, cudaMemcpyAsync(&gb, b->d_bar.p, sizeof gb, cudaMemcpyDeviceToHost, b->s));
+    BCK(b, cudaStreamSynchronize(b->s));
+    if (gb.err) { b->err = "a grid barrier of the batch kernel timed out"; return FDM_ERR_CUDA; }
+    return FDM_OK;
+}
+
+extern "C" {
+
+int fdm_batch_create(fdm_handle *const *members, int32_t n, fdm_batch **out) {
+    if (!members || n <= 0 || !out) return FDM_ERR_ARG;
+    *out = nullptr;
+    int dev = -1;
+    for (int m = 0; m < n; ++m) {
+        if (!members[m] || !members[m]->loaded) return FDM_ERR_STATE;
+        if (dev < 0) dev = members[m]->device;
+        if (members[m]->device != dev) return FDM_ERR_ARG;
+        for (int k = 0; k < m; ++k)
+            if (members[k] == members[m]) return FDM_ERR_ARG;
+    }
+    fdm_batch *b = new fdm_batch();
+    b->mem.assign(members, members + n);
+    b->device = dev;
+    b->smem = sizeof(BatchSmem);
+    cudaSetDevice(dev);
+    int rc = FDM_OK;
+    if (cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess)
+        rc = FDM_ERR_CUDA;
+    if (!rc && (b->d_ctr.ensure(sizeof(unsigned long long) * N_PHASE) != cudaSuccess ||
+                b->d_bar.ensure(sizeof(GridBar)) != cudaSuccess || b->d_act.ensure(sizeof(int32_t) * n) != cudaSuccess ||
+                b->d_skip.ensure(sizeof(int32_t) * n) != cudaSuccess))
+        rc = FDM_ERR_CUDA;
+    if (!rc) {
+        cudaMemsetAsync(b->d_bar.p, 0, sizeof(GridBar), b->s);
+        cudaMemsetAsync(b->d_skip.p, 0, sizeof(int32_t) * n, b->s);
+        b->h_skip.assign(n, 0);
+        rc = batch_grid(b);
+    }
+    if (!rc) rc = batch_refresh(b);
+    if (rc) {
+        fdm_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return FDM_OK;
+}
+
+void fdm_batch_destroy(fdm_batch *b) {
+    if (!b) return;
+    if (b->s) cudaStreamSynchronize(b->s);
+    drop_batch_graph(b);
+    b->d_mem.release(); b->d_off.release(); b->d_ctr.release(); b->d_bar.release();
+    b->d_act.release(); b->d_skip.release();
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->s) cudaStreamDestroy(b->s);
+    delete b;
+}
+
+int fdm_batch_last_error(const fdm_batch *b, char *buf, size_t n) {
+    if (!b || !buf || n == 0) return FDM_ERR_ARG;
+    const size_t k = std::min(b->err.size(), n - 1);
+    std::memcpy(buf, b->err.data(), k);
+    buf[k] = 0;
+    return FDM_OK;
+}
+
+// nsteps solute iterations of every unfinished member, no regrid and no
+// host synchronisation (graph replays on the batch stream).
+int fdm_batch_advance(fdm_batch *b, int64_t nsteps) {
+    if (!b || nsteps < 0) return FDM_ERR_ARG;
+    cudaSetDevice(b->device);
+    for (fdm_handle *h : b->mem) {
+        int rc = member_ready(h);
+        if (rc) { b->err = "member: " + h->err; return rc; }
+    }
+    std::fill(b->h_skip.begin(), b->h_skip.end(), 0);
+    int rc = join_members(b);
+    if (rc) return rc;
+    BCK(b, cudaMemcpyAsync(b->d_skip.p, b->h_skip.data(), sizeof(int32_t) * b->h_skip.size(), cudaMemcpyHostToDevice,
+                           b->s));
+    rc = batch_graph(b);
+    if (rc) return rc;
+    for (int64_t k = 0; k < nsteps; ++k) {
+        rc = launch_step(b);
+        if (rc) return rc;
+    }
+    for (fdm_handle *h : b->mem) member_stepped(h);
+    return release_members(b);
+}
+
+// nsteps solute iterations with the members' regrids, as fdm_solute_step
+// does for one mesh: after each step the scalars are read back; a NaN stops
+// the batch (status of the first member that has it), and members whose
+// regrid is due are regridded before the next step.  steps_done: steps
+// taken.  Members past t_end are left alone.
+int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done) {
+    if (!b || nsteps < 0) return FDM_ERR_ARG;
+    cudaSetDevice(b->device);
+    const int n = (int)b->mem.size();
+    int64_t k = 0;
+    int rc = FDM_OK;
+    std::vector<DevScalars> hs(n);
+    for (fdm_handle *h : b->mem) {
+        rc = member_ready(h);
+        if (rc) { b->err = "member: " + h->err; return rc; }
+    }
+    for (; k < nsteps; ++k) {
+        // scalars before the step: finished members and regrids due after it
+        rc = join_members(b);
+        if (rc) break;
+        for (int m = 0; m < n; ++m)
+            BCK(b, cudaMemcpyAsync(&hs[m], b->mem[m]->scal.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, b->s));
+        BCK(b, cudaStreamSynchronize(b->s));
+        bool any = false;
+        for (int m = 0; m < n; ++m) {
+            const bool active = !hs[m].done && hs[m].tt < b->mem[m]->p.t_end;
+            any = any || active;
+            b->h_skip[m] = active && member_amr_due(b->mem[m], hs[m].it + 1) ? 1 : 0;
+        }
+        if (!any) break;
+        BCK(b, cudaMemcpyAsync(b->d_skip.p, b->h_skip.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, b->s));
+        rc = batch_graph(b);
+        if (rc) break;
+        rc = launch_step(b);
+        if (rc) break;
+        rc = check_barrier(b);
+        if (rc) break;
+        for (int m = 0; m < n; ++m)
+            BCK(b, cudaMemcpyAsync(&hs[m], b->mem[m]->scal.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, b->s));
+        BCK(b, cudaStreamSynchronize(b->s));
+        for (fdm_handle *h : b->mem) member_stepped(h);
+        for (int m = 0; m < n && !rc; ++m) {
+            if (hs[m].status == FDM_ERR_NAN) {
+                b->err = "member " + std::to_string(m) + ": NaN in the residual RMS";
+                rc = FDM_ERR_NAN;
+            }
+        }
+        if (rc) { ++k; break; }
+        for (int m = 0; m < n && !rc; ++m) {
+            if (!b->h_skip[m]) continue;
+            fdm_handle *h = b->mem[m];
+            rc = member_regrid(h);
+            if (rc) b->err = "member " + std::to_string(m) + " regrid: " + h->err;
+        }
+        if (rc) { ++k; break; }
+    }
+    if (steps_done) *steps_done = k;
+    if (!rc) rc = release_members(b);
+    return rc;
+}
+
+int fdm_batch_sync(fdm_batch *b) {
+    if (!b) return FDM_ERR_ARG;
+    return check_barrier(b);
+}
+
+// 1 or 2 resident blocks per SM for the persistent kernel; the next graph
+// uses the new grid.
+int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t bps) {
+    if (!b || bps < 1 || bps > 2) return FDM_ERR_ARG;
+    b->want_bps = bps;
+    int rc = batch_grid(b);
+    if (rc) return rc;
+    drop_batch_graph(b);
+    return FDM_OK;
+}
+
+int fdm_batch_info(const fdm_batch *b, int32_t *grid, int32_t *blocks_per_sm, int64_t *smem_bytes) {
+    if (!b) return FDM_ERR_ARG;
+    if (grid) *grid = b->grid;
+    if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
+    if (smem_bytes) *smem_bytes = (int64_t)b->smem;
+    return FDM_OK;
+}
+
+// the batch stream (events, timing)
+int fdm_batch_stream(const fdm_batch *b, void **stream) {
+    if (!b || !stream) return FDM_ERR_ARG;
+    *stream = (void *)b->s;
+    return FDM_OK;
+}
+
+}  // extern "C"

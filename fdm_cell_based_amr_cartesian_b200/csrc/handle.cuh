@@ -167,6 +167,11 @@ void launch_cells(fdm_handle *h, const double4 *cur, const double4 *un, double4 
 void launch_ghosts(fdm_handle *h, double4 *next, int j);
 void launch_blend(fdm_handle *h, const double4 *un, double4 *cur, int krk);
 void launch_lambda(fdm_handle *h, const double4 *cur);
+// batched path (batch.cu) <-> single-mesh bookkeeping (libfdm.cu)
+int member_ready(fdm_handle *h);
+void member_stepped(fdm_handle *h);
+bool member_amr_due(const fdm_handle *h, int64_t it);
+int member_regrid(fdm_handle *h);
 void launch_step_control(fdm_handle *h);
 void launch_step_end(fdm_handle *h);
 void launch_set_tstep(fdm_handle *h, double tstep);

@@ -559,3 +559,28 @@ int fdm_device_state(fdm_handle *h, void **stream, double **prim_dev, int64_t *n
 }
 
 }  // extern "C"
+
+namespace fdm {
+
+// hooks of the batched path (batch.cu): the same host-side bookkeeping as
+// fdm_solute_step around steps that the batch kernel takes
+int member_ready(fdm_handle *h) {
+    if (!h->loaded) { h->err = "no leaf set uploaded"; return FDM_ERR_STATE; }
+    return ensure_lambda(h);
+}
+void member_stepped(fdm_handle *h) {
+    h->lam_fresh = true;
+    if (h->gate_on) h->gate_stage1_valid = true;
+}
+bool member_amr_due(const fdm_handle *h, int64_t it) { return amr_due(h, it); }
+int member_regrid(fdm_handle *h) {
+    int rc = fdm_amr(h);
+    if (rc) return rc;
+    if (h->p.iflag_amr) {
+        launch_ghosts(h, h->B[0].as<double4>(), 1);
+        FDM_CK(h, cudaStreamSynchronize(h->s));
+    }
+    return FDM_OK;
+}
+
+}  // namespace fdm

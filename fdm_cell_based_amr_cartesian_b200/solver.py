@@ -38,6 +38,8 @@ EXPORTS = [
     "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
     "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
     "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
+    "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
+    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream",
 ]
 
 
@@ -108,6 +110,16 @@ def load_library(path: str = LIB_PATH):
     L.fdm_time_advance_rk_uniform_static.argtypes = [vp, vp, i32, i32, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_double, vp]
+    L.fdm_batch_create.argtypes = [ctypes.POINTER(vp), i32, ctypes.POINTER(vp)]
+    L.fdm_batch_destroy.argtypes = [vp]
+    L.fdm_batch_destroy.restype = None
+    L.fdm_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    L.fdm_batch_advance.argtypes = [vp, i64]
+    L.fdm_batch_solute.argtypes = [vp, i64, ctypes.POINTER(i64)]
+    L.fdm_batch_sync.argtypes = [vp]
+    L.fdm_batch_set_blocks_per_sm.argtypes = [vp, i32]
+    L.fdm_batch_info.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64)]
+    L.fdm_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     _lib = L
     return L
 
@@ -368,6 +380,65 @@ class Solver:
         vortex, area-weighted as output_error does."""
         keys, prim = self.leaves()
         return vortex_error(self.cfg, keys, prim)
+
+
+class Batch:
+    """An ensemble of loaded solvers on one GPU advanced together: one
+    persistent kernel launch per RK3 stage covers every member (libfdm's
+    fdm_batch_*).  The solvers stay usable on their own between calls."""
+
+    def __init__(self, solvers):
+        self.L = load_library()
+        self.members = list(solvers)
+        arr = (ctypes.c_void_p * len(self.members))(*[s.h.value for s in self.members])
+        b = ctypes.c_void_p()
+        rc = self.L.fdm_batch_create(arr, len(self.members), ctypes.byref(b))
+        if rc:
+            raise FdmError(rc, "fdm_batch_create failed")
+        self.b = b
+
+    def _check(self, rc: int):
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            self.L.fdm_batch_last_error(self.b, buf, 512)
+            raise FdmError(rc, buf.value.decode(errors="replace"))
+
+    def advance(self, nsteps: int):
+        """nsteps steps of every unfinished member, no regrid, no host sync."""
+        self._check(self.L.fdm_batch_advance(self.b, int(nsteps)))
+
+    def solute(self, nsteps: int) -> int:
+        """nsteps steps with the members' regrids when due; returns the steps taken."""
+        k = ctypes.c_int64()
+        self._check(self.L.fdm_batch_solute(self.b, int(nsteps), ctypes.byref(k)))
+        return k.value
+
+    def sync(self):
+        self._check(self.L.fdm_batch_sync(self.b))
+
+    def set_blocks_per_sm(self, k: int):
+        self._check(self.L.fdm_batch_set_blocks_per_sm(self.b, int(k)))
+
+    def info(self) -> dict:
+        g, bps, sm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        self._check(self.L.fdm_batch_info(self.b, ctypes.byref(g), ctypes.byref(bps), ctypes.byref(sm)))
+        return {"grid": g.value, "blocks_per_sm": bps.value, "smem_bytes": sm.value}
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.L.fdm_batch_stream(self.b, ctypes.byref(s)))
+        return s.value or 0
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.fdm_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def vortex_error(cfg: P.Config, keys, prim):

@@ -276,6 +276,35 @@ int fdm_gate_stats(fdm_handle *h, int64_t *gated, int64_t *total);
  * rebuild). */
 int fdm_amr_phase_ms(const fdm_handle *h, double ms[5]);
 
+/* ------------------------------------------------------------ ensembles
+ * No reference counterpart (the reference runs one mesh per process).  A
+ * batch advances many loaded handles of one GPU together: one persistent,
+ * cooperative kernel launch per RK3 stage covers every member, the blocks
+ * taking (member, tile) work from a shared counter, with a grid barrier
+ * (bounded waits) between the phases of a stage.  Each member keeps its own
+ * tables, state, scalars and learned-gate setting, and ends in the state
+ * that the same number of fdm_solute_step calls gives.  A member's regrid
+ * rebuilds its tables; the batch notices and captures its step graph again.
+ *
+ * fdm_batch_advance: nsteps steps of every unfinished member without regrids
+ * or host synchronisation (graph replays on the batch stream, ordered after
+ * and before the members' own streams).  fdm_batch_solute: nsteps steps with
+ * each member's regrids when due, stopping with FDM_ERR_NAN at a NaN.
+ * fdm_batch_sync waits for the batch and reports a barrier that timed out.
+ * Members must stay alive and must not be used from another thread while
+ * the batch exists. */
+typedef struct fdm_batch fdm_batch;
+int fdm_batch_create(fdm_handle *const *members, int32_t n, fdm_batch **out);
+void fdm_batch_destroy(fdm_batch *b);
+int fdm_batch_last_error(const fdm_batch *b, char *buf, size_t n);
+int fdm_batch_advance(fdm_batch *b, int64_t nsteps);
+int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done);
+int fdm_batch_sync(fdm_batch *b);
+int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t blocks_per_sm);
+int fdm_batch_info(const fdm_batch *b, int32_t *grid, int32_t *blocks_per_sm,
+                   int64_t *smem_bytes);
+int fdm_batch_stream(const fdm_batch *b, void **stream);
+
 /* ------------------------------------------------- no-allocation entry point
  * One SSP-RK3 step (the three stages of Time_advance_RK with periodic ghost
  * fill) on a uniform periodic grid of nx x ny cells, without allocating any
