@@ -230,6 +230,117 @@ def learned_window(args, cfg, keys, prim, NI, flush, world):
             "error_window_steps": args.warmup + args.steps, "kernel_ms": kt}
 
 
+def ensemble_window(args, world):
+    """The ensemble configuration: 64 random four-quadrant problems (maximum
+    level drawn from 2..5, band-refined meshes, 66M leaves in all) on one GPU
+    with learned gating, advanced by the batched path (one persistent launch
+    per RK3 stage over all members).  Timed beside the same members with the
+    gate off, and beside the single-mesh path (one step graph per member,
+    each on its own stream).  Inputs far exceed L2, so no flush is needed."""
+    import torch
+    from fdm_cell_based_amr_cartesian_b200 import ensemble as E
+    from fdm_cell_based_amr_cartesian_b200 import learned as LG
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+    from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
+    if not os.path.exists(LG.PARAMS_PATH):
+        return {"unavailable": "no trained gate parameters"}
+    t_setup = time.perf_counter()
+    cfgs = E.ensemble_configs()
+    meshes = E.ensemble_meshes(cfgs)
+    sols = []
+    for cfg, (k, p) in zip(cfgs, meshes):
+        g = S.Solver(cfg)
+        g.upload(k, p)
+        g.body_boundary(1)
+        LG.enable(g)
+        sols.append(g)
+    NI = sum(g.counters()["n_interior"] for g in sols)
+    batch = S.Batch(sols)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t_setup
+    ext = torch.cuda.ExternalStream(batch.stream())
+
+    def timed_batch():
+        batch.advance(args.warmup)
+        batch.sync()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            a.record(ext)
+            batch.advance(args.steps)
+            b.record(ext)
+        batch.sync()
+        return max_over_ranks(a.elapsed_time(b), device="cuda")
+
+    # the persistent kernel at 1 or 2 resident blocks per SM: the faster one
+    tune = {}
+    for bps in (1, 2):
+        batch.set_blocks_per_sm(bps)
+        batch.advance(2)
+        batch.sync()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            a.record(ext)
+            batch.advance(3)
+            b.record(ext)
+        batch.sync()
+        tune[bps] = a.elapsed_time(b) / 3
+    batch.set_blocks_per_sm(min(tune, key=tune.get))
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        ms_gated = timed_batch()
+    gated, total = 0, 0
+    for g in sols:
+        a, b = LG.stats(g)
+        gated += a
+        total += b
+    info = batch.info()
+    for g in sols:
+        LG.disable(g)
+    ms_plain = timed_batch()
+    # the single-mesh path on the same members: one step graph per member,
+    # members on their own streams (host-timed: the launches are the cost)
+    for g in sols:
+        LG.enable(g)
+        g.advance(args.warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for g in sols:
+        g.advance(args.steps)
+    torch.cuda.synchronize()
+    ms_single = max_over_ranks((time.perf_counter() - t0) * 1e3, device="cuda")
+    finite = all(bool(np.isfinite(g.leaves()[1]).all()) for g in sols[:4])
+    batch.close()
+    for g in sols:
+        g.close()
+    # accuracy of the gate: one member per level, gated against plain
+    acc = {}
+    for L in (2, 3, 4, 5):
+        i = next(j for j, c in enumerate(cfgs) if int(c.params.lvl_amr) == L)
+        pair = []
+        for gate in (False, True):
+            g = S.Solver(cfgs[i])
+            g.upload(*meshes[i])
+            g.body_boundary(1)
+            if gate:
+                LG.enable(g)
+            g.advance(args.warmup + args.steps)
+            pair.append(g.leaves())
+            g.close()
+        l1, linf = LG.density_errors(cfgs[i], pair[0], pair[1])
+        acc[f"level{L}_seed{E.ENSEMBLE_SEEDS[i]}"] = {"l1": l1, "linf": linf}
+    per = lambda ms: NI * world * args.steps / (ms / 1e3)
+    return {"workload": f"64 random four-quadrant problems (seeds 1000-1063, rho,p~U[0.1,2], u,v~U[-1,1]), "
+                        f"base {E.ENSEMBLE_BASE}^2, max level U{{2..5}}, band-refined meshes, learned gate on",
+            "blocks_per_sm_ms_per_step": tune,
+            "members": len(cfgs), "interior_leaves": int(NI), "value": per(ms_gated), "unit": UNIT,
+            "ms_per_step": ms_gated / args.steps, "gated_face_fraction": gated / max(total, 1),
+            "plain_batched": {"value": per(ms_plain), "ms_per_step": ms_plain / args.steps},
+            "single_mesh_graphs": {"value": per(ms_single), "ms_per_step": ms_single / args.steps,
+                                   "note": "same members, one step graph each, own streams, host-timed"},
+            "density_error_vs_plain": acc, "launch": info, "setup_s": t_setup, "clocks": clk.summary(),
+            "state_finite": finite,
+            "gpu_launches_per_step": 3}
+
+
 def full_run(S, gate):
     import torch
     gf = S.Solver(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
@@ -353,6 +464,11 @@ def run_ours(args):
     if not args.no_learned:
         gated = learned_window(args, cfg, keys, prim, NI, flush, world)
 
+    # the batched ensemble (configuration 5)
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_window(args, world)
+
     # the full configuration as the reference runs it: t = 0 -> 0.3 with the
     # device regrid every 10 steps (time to solution, all regrids included),
     # plain and learned-gated, and the gated run's density error at t = 0.3
@@ -389,7 +505,7 @@ def run_ours(args):
                 "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
                 "counters": cnt, "state_finite_after_timed_steps": finite, "cpu_baseline": cpu,
-                "learned": gated, "full_run": full}
+                "learned": gated, "ensemble": ens, "full_run": full}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -407,6 +523,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-full-run", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -70,7 +70,14 @@ struct BatchArgs {
     GridBar *bar;
     int32_t *act;                  // member not finished at the start of the step
     const int32_t *skip_j1;        // host: a regrid follows this step (no body_boundary(1) here)
+    unsigned long long *stamp;     // [3][16] global-timer stamps at the phase ends of each stage
 };
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 constexpr unsigned long long BAR_SPIN_LIMIT = 1ull << 24;   // x >= 64 ns of sleep: about a second
 
@@ -105,8 +112,16 @@ __device__ bool grid_bar(GridBar *b, unsigned nblocks) {
 
 // Work stealing over the tiles of one phase: fn(member, tile) for every
 // tile, each taken by one block from the phase's counter.
+constexpr int OFF_CAP = 513;   // tile offsets kept in shared memory (members + 1)
 template <class Fn>
-__device__ __forceinline__ void run_tiles(const BatchArgs &A, int ph, const int64_t *off, int64_t *s_t, Fn &&fn) {
+__device__ __forceinline__ void run_tiles(const BatchArgs &A, int ph, const int64_t *goff, int64_t *s_t,
+                                          int64_t *s_off, Fn &&fn) {
+    const int64_t *off = goff;
+    if (A.nmem + 1 <= OFF_CAP) {
+        for (int k = threadIdx.x; k <= A.nmem; k += blockDim.x) s_off[k] = goff[k];
+        __syncthreads();
+        off = s_off;
+    }
     const int64_t total = off[A.nmem];
     for (;;) {
         if (threadIdx.x == 0) *s_t = (int64_t)atomicAdd(A.ctr + ph, 1ull);
@@ -122,6 +137,7 @@ __device__ __forceinline__ void run_tiles(const BatchArgs &A, int ph, const int6
         }
         fn(lo, t - off[lo]);
     }
+    __syncthreads();   // s_off is reloaded by the next phase
 }
 
 struct GateSmem {
@@ -135,12 +151,38 @@ union BatchSmem {
     double fin[BT][8];
 };
 
+// 256 ghost leaves: copies and boundary states one per thread, then the
+// interpA images of the tile one per warp
+__device__ __forceinline__ void ghost_tile(const Tables &T, double4 *buf, const GhostStates &GS,
+                                           const DevScalars *__restrict__ sc, int j, int64_t t, int32_t *rlist,
+                                           int *rn, RestrictSmem *rs) {
+    const int64_t gi = t * BT + threadIdx.x;
+    if (threadIdx.x == 0) *rn = 0;
+    __syncthreads();
+    if (gi < T.NG) {
+        const int kind = T.gh_kind[gi];
+        if (kind == GH_RESTRICT) rlist[atomicAdd(rn, 1)] = (int32_t)threadIdx.x;
+        else if (kind != GH_NONE) ghost_store(T, buf, gi, ghost_simple_value(T, buf, GS, sc, j, gi, kind));
+    }
+    __syncthreads();
+    const int n = *rn, wid = threadIdx.x >> 5;
+    for (int k = wid; k < n; k += BW) ghost_warp(T, buf, GS, sc, j, t * BT + rlist[k], rs[wid]);
+    __syncthreads();
+}
+
 __device__ __forceinline__ const double4 *stage_cur(const Member &M, int krk) {
     return krk == 1 ? M.B0 : krk == 2 ? M.B1 : M.B2;
 }
 __device__ __forceinline__ double4 *stage_next(const Member &M, int krk) {
     return krk == 1 ? M.B1 : krk == 2 ? M.B2 : M.B0;
 }
+
+// barrier, then block 0 stamps the time (phase k of stage krk ended)
+#define BAR_STAMP(k)                                                                   \
+    do {                                                                               \
+        if (!grid_bar(A.bar, nb)) return;                                              \
+        if (blockIdx.x == 0 && threadIdx.x == 0) A.stamp[(krk - 1) * 16 + (k)] = gtimer(); \
+    } while (0)
 
 // One RK stage (krk) of every member; MINB resident blocks per SM (the
 // register budget follows: 128 per thread at 2, up to 255 at 1).
@@ -149,10 +191,14 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BatchSmem &S = *reinterpret_cast<BatchSmem *>(smem_raw);
     __shared__ int64_t s_t;
+    __shared__ int64_t s_off[OFF_CAP];
     __shared__ const float *s_loaded;
+    __shared__ int32_t s_rlist[BT];
+    __shared__ int s_rn;
     const unsigned nb = gridDim.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int np1 = A.nmem + 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.stamp[(krk - 1) * 16] = gtimer();
 
     // ---- step control / per-stage resets (one thread per member)
     if (blockIdx.x == 0) {
@@ -170,10 +216,10 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
             }
         }
     }
-    if (!grid_bar(A.bar, nb)) return;
+    BAR_STAMP(1);
 
     // ---- hanging-node requests
-    run_tiles(A, PH_REQ, A.off + PH_REQ * np1, &s_t, [&](int m, int64_t t) {
+    run_tiles(A, PH_REQ, A.off + PH_REQ * np1, &s_t, s_off, [&](int m, int64_t t) {
         const Member &M = A.mem[m];
         if (!A.act[m]) return;
         double4 *cur = const_cast<double4 *>(stage_cur(M, krk));
@@ -186,12 +232,12 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
             if (r < M.T.NR) request_restrict_warp(M.T, cur, r, S.rs[wid]);
         }
     });
-    if (!grid_bar(A.bar, nb)) return;
+    BAR_STAMP(2);
 
     // ---- faces: plain flux, or gate / guard with the linear flux
     if (threadIdx.x == 0) s_loaded = nullptr;
     __syncthreads();
-    run_tiles(A, PH_FACE, A.off + PH_FACE * np1, &s_t, [&](int m, int64_t t) {
+    run_tiles(A, PH_FACE, A.off + PH_FACE * np1, &s_t, s_off, [&](int m, int64_t t) {
         const Member &M = A.mem[m];
         if (!A.act[m]) return;
         const double4 *cur = stage_cur(M, krk);
@@ -233,7 +279,7 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
                 guard_linear_chunk<1>(M.T, cur, M.Fy, M.GL.jy, lam, ig1, M.gama, M.GL.hy, M.GL.cnt + 1, w);
         }
     });
-    if (!grid_bar(A.bar, nb)) return;
+    BAR_STAMP(3);
 
     // ---- hard faces of gated members (full WCNS flux)
     if (A.any_gate) {
@@ -248,8 +294,8 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
             }
             A.off_hard[A.nmem] = acc;
         }
-        if (!grid_bar(A.bar, nb)) return;
-        run_tiles(A, PH_HARD, A.off_hard, &s_t, [&](int m, int64_t t) {
+        BAR_STAMP(4);
+        run_tiles(A, PH_HARD, A.off_hard, &s_t, s_off, [&](int m, int64_t t) {
             const Member &M = A.mem[m];
             const double4 *cur = stage_cur(M, krk);
             const int64_t tx = cdiv(M.GL.cnt[0], BT);
@@ -261,11 +307,11 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
                 if (i < M.GL.cnt[1]) face_item<1>(M.T, cur, M.Fy, M.sc->lambda_y, M.gama, M.GL.hy[i]);
             }
         });
-        if (!grid_bar(A.bar, nb)) return;
+        BAR_STAMP(5);
     }
 
     // ---- cells: residual, candidate, RK blend, residual partials, lambda
-    run_tiles(A, PH_CELL, A.off + PH_CELL * np1, &s_t, [&](int m, int64_t t) {
+    run_tiles(A, PH_CELL, A.off + PH_CELL * np1, &s_t, s_off, [&](int m, int64_t t) {
         const Member &M = A.mem[m];
         if (!A.act[m]) return;
         const int64_t i = t * BT + threadIdx.x;
@@ -276,17 +322,16 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
                       M.gama, i, rm, rs, lx, ly);
         cells_block_reduce(rm, rs, lx, ly, M.res_part + t * 8, M.sc, krk == 3, S.cells);
     });
-    if (!grid_bar(A.bar, nb)) return;
+    BAR_STAMP(6);
 
     // ---- ghosts of the new stage value (body_boundary_RK)
-    run_tiles(A, PH_GHOST, A.off + PH_GHOST * np1, &s_t, [&](int m, int64_t t) {
+    run_tiles(A, PH_GHOST, A.off + PH_GHOST * np1, &s_t, s_off, [&](int m, int64_t t) {
         const Member &M = A.mem[m];
         if (!A.act[m]) return;
-        const int64_t gi = t * BW + wid;
-        if (gi < M.T.NG) ghost_warp(M.T, stage_next(M, krk), M.GS, M.sc, 3, gi, S.rs[wid]);
+        ghost_tile(M.T, stage_next(M, krk), M.GS, M.sc, 3, t, s_rlist, &s_rn, S.rs);
     });
     if (krk != 3) return;
-    if (!grid_bar(A.bar, nb)) return;
+    BAR_STAMP(7);
 
     // ---- end of the step: residual norms, tt, it, NaN, t_end
     for (int m = blockIdx.x; m < A.nmem; m += nb) {
@@ -296,14 +341,13 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
         if (threadIdx.x == 0) step_end_item(M.sc, M.T.NI);
         __syncthreads();
     }
-    if (!grid_bar(A.bar, nb)) return;
+    BAR_STAMP(8);
 
     // ---- body_boundary(1) after the step on AMR members
-    run_tiles(A, PH_GHOST1, A.off + PH_GHOST1 * np1, &s_t, [&](int m, int64_t t) {
+    run_tiles(A, PH_GHOST1, A.off + PH_GHOST1 * np1, &s_t, s_off, [&](int m, int64_t t) {
         const Member &M = A.mem[m];
         if (!A.act[m] || !M.amr_on || A.skip_j1[m]) return;
-        const int64_t gi = t * BW + wid;
-        if (gi < M.T.NG) ghost_warp(M.T, M.B0, M.GS, M.sc, 1, gi, S.rs[wid]);
+        ghost_tile(M.T, M.B0, M.GS, M.sc, 1, t, s_rlist, &s_rn, S.rs);
     });
 }
 
@@ -315,7 +359,7 @@ struct fdm_batch {
     std::vector<fdm_handle *> mem;
     int device = 0;
     cudaStream_t s = nullptr;
-    DevBuf d_mem, d_off, d_ctr, d_bar, d_act, d_skip;
+    DevBuf d_mem, d_off, d_ctr, d_bar, d_act, d_skip, d_stamp;
     std::vector<int32_t> h_skip;
     int grid = 0, blocks_per_sm = 0, want_bps = 2;
     size_t smem = 0;
@@ -382,8 +426,8 @@ static int batch_refresh(fdm_batch *b) {
             cdiv(d.nfx, BT) + cdiv(d.nfy, BT),                          // PH_FACE
             0,                                                          // PH_HARD (device)
             cdiv(h->NI, BT),                                            // PH_CELL
-            cdiv(h->NG, BW),                                            // PH_GHOST
-            cdiv(h->NG, BW)};                                           // PH_GHOST1
+            cdiv(h->NG, BT),                                            // PH_GHOST
+            cdiv(h->NG, BT)};                                           // PH_GHOST1
         for (int ph = 0; ph < N_PHASE; ++ph) off[(size_t)ph * (n + 1) + m + 1] = off[(size_t)ph * (n + 1) + m] + tiles[ph];
     }
     BCK(b, b->d_mem.ensure(sizeof(Member) * n));
@@ -438,6 +482,7 @@ static int enqueue_batch_stage(fdm_batch *b, int krk) {
     A.bar = b->d_bar.as<GridBar>();
     A.act = b->d_act.as<int32_t>();
     A.skip_j1 = b->d_skip.as<int32_t>();
+    A.stamp = b->d_stamp.as<unsigned long long>();
     BCK(b, cudaMemsetAsync(A.ctr, 0, sizeof(unsigned long long) * N_PHASE, b->s));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)b->grid);
@@ -540,11 +585,13 @@ int fdm_batch_create(fdm_handle *const *members, int32_t n, fdm_batch **out) {
         rc = FDM_ERR_CUDA;
     if (!rc && (b->d_ctr.ensure(sizeof(unsigned long long) * N_PHASE) != cudaSuccess ||
                 b->d_bar.ensure(sizeof(GridBar)) != cudaSuccess || b->d_act.ensure(sizeof(int32_t) * n) != cudaSuccess ||
-                b->d_skip.ensure(sizeof(int32_t) * n) != cudaSuccess))
+                b->d_skip.ensure(sizeof(int32_t) * n) != cudaSuccess ||
+                b->d_stamp.ensure(sizeof(unsigned long long) * 48) != cudaSuccess))
         rc = FDM_ERR_CUDA;
     if (!rc) {
         cudaMemsetAsync(b->d_bar.p, 0, sizeof(GridBar), b->s);
         cudaMemsetAsync(b->d_skip.p, 0, sizeof(int32_t) * n, b->s);
+        cudaMemsetAsync(b->d_stamp.p, 0, sizeof(unsigned long long) * 48, b->s);
         b->h_skip.assign(n, 0);
         rc = batch_grid(b);
     }
@@ -562,7 +609,7 @@ void fdm_batch_destroy(fdm_batch *b) {
     if (b->s) cudaStreamSynchronize(b->s);
     drop_batch_graph(b);
     b->d_mem.release(); b->d_off.release(); b->d_ctr.release(); b->d_bar.release();
-    b->d_act.release(); b->d_skip.release();
+    b->d_act.release(); b->d_skip.release(); b->d_stamp.release();
     if (b->ev) cudaEventDestroy(b->ev);
     if (b->s) cudaStreamDestroy(b->s);
     delete b;
@@ -682,6 +729,23 @@ int fdm_batch_info(const fdm_batch *b, int32_t *grid, int32_t *blocks_per_sm, in
     if (grid) *grid = b->grid;
     if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
     if (smem_bytes) *smem_bytes = (int64_t)b->smem;
+    return FDM_OK;
+}
+
+// Microseconds spent in each phase of the last step, per stage: row krk-1,
+// column k = phase k (0 step control, then requests, faces, [hard-list
+// offsets, hard faces,] cells, ghosts, [step end, level-1 ghosts]); unused
+// entries are 0.
+int fdm_batch_phase_us(fdm_batch *b, double *us) {
+    if (!b || !us) return FDM_ERR_ARG;
+    unsigned long long st[48];
+    BCK(b, cudaMemcpyAsync(st, b->d_stamp.p, sizeof st, cudaMemcpyDeviceToHost, b->s));
+    BCK(b, cudaStreamSynchronize(b->s));
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 16; ++k) {
+            const unsigned long long a = st[r * 16 + k], c = k < 15 ? st[r * 16 + k + 1] : 0;
+            us[r * 16 + k] = (k < 15 && c > a && a) ? (double)(c - a) * 1e-3 : 0.0;
+        }
     return FDM_OK;
 }
 

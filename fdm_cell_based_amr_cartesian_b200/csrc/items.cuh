@@ -249,6 +249,30 @@ struct GhostStates {
     double x0, cot, speed;
 };
 
+// value of a ghost leaf of kind COPY or a boundary state
+__device__ __forceinline__ double4 ghost_simple_value(const Tables &T, const double4 *buf, const GhostStates &GS,
+                                                      const DevScalars *__restrict__ sc, int j, int64_t gi,
+                                                      int kind) {
+    if (kind == GH_COPY) return buf[T.gh_a[gi]];
+    // boundary time of body_boundary_RK (src/solution.F90:320-326)
+    double t = sc->tt;
+    if (j == 2) t = sc->tt + sc->tstep;
+    else if (j == 3) t = sc->tt + 0.5 * sc->tstep;
+    int st = T.gh_a[gi];
+    if (kind == GH_DMR_TOP) {
+        const double xs = GS.x0 + T.gh_y[gi] * GS.cot + GS.speed * t;
+        st = T.gh_x[gi] < xs ? 4 : 5;
+    }
+    return make_double4(GS.s[st][0], GS.s[st][1], GS.s[st][2], GS.s[st][3]);
+}
+// mirror (wall) flip and store of a ghost value
+__device__ __forceinline__ void ghost_store(const Tables &T, double4 *buf, int64_t gi, double4 v) {
+    const int fl = T.gh_flip[gi];
+    if (fl == 1) v.y = -v.y;
+    else if (fl == 2) v.z = -v.z;
+    buf[T.NI + gi] = v;
+}
+
 // ghost leaf gi (whole warp: interpA images can span hundreds of leaves)
 __device__ __forceinline__ void ghost_warp(const Tables &T, double4 *buf, const GhostStates &GS,
                                            const DevScalars *__restrict__ sc, int j, int64_t gi, RestrictSmem &sm) {
@@ -256,27 +280,10 @@ __device__ __forceinline__ void ghost_warp(const Tables &T, double4 *buf, const 
     const int kind = T.gh_kind[gi];
     if (kind == GH_NONE) return;
     double4 v;
-    if (kind == GH_RESTRICT) {
-        v = restrict_warp(T, buf, T.gh_a[gi], T.gh_b[gi], sm);
-    } else if (kind == GH_COPY) {
-        v = buf[T.gh_a[gi]];
-    } else {
-        // boundary time of body_boundary_RK (src/solution.F90:320-326)
-        double t = sc->tt;
-        if (j == 2) t = sc->tt + sc->tstep;
-        else if (j == 3) t = sc->tt + 0.5 * sc->tstep;
-        int st = T.gh_a[gi];
-        if (kind == GH_DMR_TOP) {
-            const double xs = GS.x0 + T.gh_y[gi] * GS.cot + GS.speed * t;
-            st = T.gh_x[gi] < xs ? 4 : 5;
-        }
-        v = make_double4(GS.s[st][0], GS.s[st][1], GS.s[st][2], GS.s[st][3]);
-    }
+    if (kind == GH_RESTRICT) v = restrict_warp(T, buf, T.gh_a[gi], T.gh_b[gi], sm);
+    else v = ghost_simple_value(T, buf, GS, sc, j, gi, kind);
     if (lane != 0) return;
-    const int fl = T.gh_flip[gi];
-    if (fl == 1) v.y = -v.y;
-    else if (fl == 2) v.z = -v.z;
-    buf[T.NI + gi] = v;
+    ghost_store(T, buf, gi, v);
 }
 
 __host__ inline GhostStates ghost_states(const fdm_params &p) {

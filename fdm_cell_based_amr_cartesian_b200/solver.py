@@ -39,7 +39,7 @@ EXPORTS = [
     "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
     "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
     "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
-    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream",
+    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
 ]
 
 
@@ -120,6 +120,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_batch_set_blocks_per_sm.argtypes = [vp, i32]
     L.fdm_batch_info.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64)]
     L.fdm_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.fdm_batch_phase_us.argtypes = [vp, dp]
     _lib = L
     return L
 
@@ -423,6 +424,12 @@ class Batch:
         g, bps, sm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
         self._check(self.L.fdm_batch_info(self.b, ctypes.byref(g), ctypes.byref(bps), ctypes.byref(sm)))
         return {"grid": g.value, "blocks_per_sm": bps.value, "smem_bytes": sm.value}
+
+    def phase_us(self):
+        """Microseconds of each phase of the last step, shape (3 stages, 16)."""
+        a = np.zeros(48)
+        self._check(self.L.fdm_batch_phase_us(self.b, _dp(a)))
+        return a.reshape(3, 16)
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -304,6 +304,8 @@ int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t blocks_per_sm);
 int fdm_batch_info(const fdm_batch *b, int32_t *grid, int32_t *blocks_per_sm,
                    int64_t *smem_bytes);
 int fdm_batch_stream(const fdm_batch *b, void **stream);
+/* diagnostics: microseconds of each phase of the last step, [3 stages][16] */
+int fdm_batch_phase_us(fdm_batch *b, double us[48]);
 
 /* ------------------------------------------------- no-allocation entry point
  * One SSP-RK3 step (the three stages of Time_advance_RK with periodic ghost
