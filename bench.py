@@ -341,10 +341,15 @@ def ensemble_window(args, world):
             "gpu_launches_per_step": 3}
 
 
-def full_run(S, gate):
+def full_run(S, gate, ulp=False):
     import torch
     gf = S.Solver(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
     gf.creat_mesh_and_initial()
+    if ulp:
+        _, p0 = gf.leaves()
+        p0 = p0.copy()
+        p0[:, 0] = np.nextafter(p0[:, 0], np.inf)
+        gf.set_values(p0)
     if gate:
         from fdm_cell_based_amr_cartesian_b200 import learned as LG
         LG.enable(gf)
@@ -437,20 +442,26 @@ def run_ours(args):
     step_gbs = step_bytes / (ms / args.steps * 1e-3) / 1e9
     traffic = profile_traffic()
 
-    # end-to-end through the public API with host buffers
-    e2e = None
-    if True:
-        host_in = torch.empty((len(keys), 4), dtype=torch.float64, pin_memory=True)
-        host_in.numpy()[:] = g.leaves()[1]
-        t0 = time.perf_counter()
-        n_e2e = max(3, min(args.steps, 10))
-        for _ in range(n_e2e):
-            g.set_values(host_in.numpy())
-            g.advance(1)
-            _, out = g.leaves()
-        e2e_s = time.perf_counter() - t0
-        e2e = {"value": NI * world * n_e2e / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(len(keys) * 32), "d2h_bytes_per_step": int(len(keys) * 40)}
+    # end-to-end through the public API with host buffers: every step uploads
+    # its input state from pinned host memory (fdm_set_values), advances one
+    # step and reads the new state back into pinned host memory
+    host_in = torch.empty((len(keys), 4), dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty((len(keys), 4), dtype=torch.float64, pin_memory=True)
+    hin, hout = host_in.numpy(), host_out.numpy()
+    g.download_values(hin)
+    g.set_values(hin)          # first use of the staging buffers, untimed
+    g.advance(1)
+    g.download_values(hout)
+    n_e2e = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        g.set_values(hin)
+        g.advance(1)
+        g.download_values(hout)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, device="cuda")
+    e2e = {"value": NI * world * n_e2e / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(hin.nbytes), "d2h_bytes_per_step": int(hout.nbytes)}
 
     # step control, lambda reset, step end, residual reduction (stage 3) and,
     # per stage: 2 face kernels, the update, hanging nodes (+ interpA
@@ -474,12 +485,19 @@ def run_ours(args):
     # plain and learned-gated, and the gated run's density error at t = 0.3
     full = None
     if not args.no_full_run:
+        from fdm_cell_based_amr_cartesian_b200 import learned as LG
         full, leaves_plain = full_run(S, gate=False)
+        cfg_full = P.riemann4(base=128, lvl_amr=4)
         if gated is not None:
             full_g, leaves_gated = full_run(S, gate=True)
-            from fdm_cell_based_amr_cartesian_b200 import learned as LG
-            l1, linf = LG.density_errors(P.riemann4(base=128, lvl_amr=4), leaves_plain, leaves_gated)
+            l1, linf = LG.density_errors(cfg_full, leaves_plain, leaves_gated)
             full["gated"] = dict(full_g, l1_density_vs_plain=l1, linf_density_vs_plain=linf)
+        # the same plain run from an initial density one ulp higher: the spread
+        # that the regrid decisions alone give a whole run
+        full_u, leaves_ulp = full_run(S, gate=False, ulp=True)
+        l1, linf = LG.density_errors(cfg_full, leaves_plain, leaves_ulp)
+        full["one_ulp_initial_density"] = {"steps": full_u["steps"], "regrids": full_u["regrids"],
+                                           "l1_density_vs_plain": l1, "linf_density_vs_plain": linf}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1

@@ -97,6 +97,7 @@ struct fdm_handle {
     double amr_phase_ms[AMR_PHASES] = {};
 
     // learned gate of the face flux
+    fdm::DevBuf io;   // staging of fdm_set_values / fdm_download_leaves (grows, kept)
     fdm::DevBuf gate_params, gate_flag;   // gate_flag: per-stage hard-face lists
     float gate_logit_thr = 0.f;
     bool gate_on = false;

@@ -245,7 +245,7 @@ void fdm_destroy(fdm_handle *h) {
                       &h->ifxl, &h->ifyl, &h->uxl, &h->uyl, &h->rq_kind, &h->rq_m, &h->rq_mem, &h->rq_geo, &h->rq_node,
                       &h->gh_kind, &h->gh_a, &h->gh_b, &h->gh_flip, &h->gh_x, &h->gh_y, &h->B[0], &h->B[1],
                       &h->B[2], &h->Fx, &h->Fy, &h->Ut, &h->scal, &h->res_part, &h->cub_tmp, &h->flag,
-                      &h->gate_params, &h->gate_flag, &h->ikey, &h->ival};
+                      &h->gate_params, &h->gate_flag, &h->ikey, &h->ival, &h->io};
     for (DevBuf *b : bufs) b->release();
     for (auto &t : h->tmp) t.release();
     for (cudaEvent_t e : h->amr_ev)
@@ -288,13 +288,15 @@ int fdm_download_leaves(fdm_handle *h, int64_t cap, int64_t *n_out, uint64_t *ke
     CHECK_LOADED(h);
     if (n_out) *n_out = h->NL;
     if (cap < h->NL) return arg_fail(h, "capacity below the leaf count");
-    DevBuf dp;
+    DevBuf &dp = h->io;
     FDM_CK(h, dp.ensure(h->NL * 32));
-    k_out<<<nblk(h->NL, 256), 256, 0, h->s>>>(h->NL, h->lslot.as<int32_t>(), h->B[0].as<double4>(), dp.as<double>());
     if (keys) FDM_CK(h, cudaMemcpyAsync(keys, h->lkey.p, h->NL * 8, cudaMemcpyDeviceToHost, h->s));
-    if (prim) FDM_CK(h, cudaMemcpyAsync(prim, dp.p, h->NL * 32, cudaMemcpyDeviceToHost, h->s));
+    if (prim) {
+        k_out<<<nblk(h->NL, 256), 256, 0, h->s>>>(h->NL, h->lslot.as<int32_t>(), h->B[0].as<double4>(),
+                                                  dp.as<double>());
+        FDM_CK(h, cudaMemcpyAsync(prim, dp.p, h->NL * 32, cudaMemcpyDeviceToHost, h->s));
+    }
     FDM_CK(h, cudaStreamSynchronize(h->s));
-    dp.release();
     return FDM_OK;
 }
 
@@ -302,7 +304,7 @@ int fdm_set_values(fdm_handle *h, int64_t n, const double *prim) {
     CHECK_H(h);
     CHECK_LOADED(h);
     if (n != h->NL || !prim) return arg_fail(h, "value count differs from the leaf count");
-    DevBuf dp;
+    DevBuf &dp = h->io;
     FDM_CK(h, dp.ensure(n * 32));
     FDM_CK(h, cudaMemcpyAsync(dp.p, prim, n * 32, cudaMemcpyHostToDevice, h->s));
     k_in<<<nblk(n, 256), 256, 0, h->s>>>(n, h->lslot.as<int32_t>(), h->B[0].as<double4>(), dp.as<double>());
@@ -311,7 +313,6 @@ int fdm_set_values(fdm_handle *h, int64_t n, const double *prim) {
             FDM_CK(h, cudaMemcpyAsync(h->B[b].as<double4>() + h->NI + h->NG, h->B[0].as<double4>() + h->NI + h->NG,
                                       h->NC * 32, cudaMemcpyDeviceToDevice, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
-    dp.release();
     h->lam_fresh = false;
     return FDM_OK;
 }

@@ -255,6 +255,15 @@ class Solver:
         self._check(self.L.fdm_download_leaves(self.h, n, ctypes.byref(nout), _u64p(keys), _dp(prim)))
         return keys, prim
 
+    def download_values(self, out):
+        """Primitive values of all leaves, key order, into out (n x 4 float64,
+        C-contiguous; pinned host memory makes the copy direct)."""
+        n = self.num_leaves()
+        assert out.shape == (n, 4) and out.dtype == np.float64 and out.flags["C_CONTIGUOUS"]
+        nout = ctypes.c_int64()
+        self._check(self.L.fdm_download_leaves(self.h, n, ctypes.byref(nout), None, _dp(out)))
+        return out
+
     def scalars(self) -> dict:
         lx, ly, dt, tt = (ctypes.c_double() for _ in range(4))
         it = ctypes.c_int64()

@@ -146,7 +146,8 @@ int fdm_last_error(const fdm_handle *h, char *buf, size_t n);
 int fdm_upload_leaves(fdm_handle *h, int64_t n, const uint64_t *keys,
                       const double *prim);
 int64_t fdm_num_leaves(const fdm_handle *h);
-/* Download all leaves in key order; cap is the capacity of keys/prim. */
+/* Download all leaves in key order; cap is the capacity of keys/prim.
+ * keys or prim may be NULL (values only, or keys only). */
 int fdm_download_leaves(fdm_handle *h, int64_t cap, int64_t *n_out,
                         uint64_t *keys, double *prim);
 /* Overwrite the primitive values of the current leaf set (same keys as the
