@@ -619,7 +619,8 @@ struct Pool {
     uint64_t *hrank;     // heap of leaves to visit ahead of the traversal
     int32_t *hidx, *hgen;
     int64_t hcap;
-    int32_t *err;        // [0] capacity exceeded, [1] visits, [2] non-leaf refines, [3] step limit
+    int32_t *err;        // [0] capacity exceeded, [1] visits, [2] non-leaf refines, [3] step limit,
+                         // [4] refines, [5] replay steps
 };
 constexpr int32_t SLOT_DEL = 0x40000000;
 __device__ __forceinline__ uint64_t hmix(uint64_t k) {
@@ -689,6 +690,38 @@ __device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v) {
     }
     return -1;
 }
+// Insert or revive a leaf with value v from several lanes at once (distinct
+// keys): slots are claimed with atomicCAS, pool entries with atomicAdd.  An
+// empty slot's key is ~0 (never a node key), so a lane probing for its own
+// key passes a slot that another lane has claimed but not yet keyed.
+// Returns the pool index (or -1 when the pool is full) and its generation.
+__device__ int32_t hinsert_atomic(Pool &P, uint64_t k, const double4 &v, int32_t &gen) {
+    int32_t s;
+    const int64_t pos = hpos(P, k, s);
+    if (pos >= 0) {
+        const int32_t i = s & ~SLOT_DEL;
+        P.slot[pos] = i;
+        P.flags[i] = PF_LEAF;
+        gen = P.gen[i] + 1;
+        P.gen[i] = gen;
+        P.val[i] = v;
+        return i;
+    }
+    const int64_t i = (int64_t)atomicAdd((unsigned long long *)P.n, 1ull);
+    if (i >= P.cap) return -1;
+    P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
+    gen = 0;
+    uint64_t hsh = hmix(k) & P.mask;
+    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
+        if (atomicCAS(P.slot + hsh, -1, (int32_t)i) == -1) {
+            P.skey[hsh] = k;
+            return (int32_t)i;
+        }
+        hsh = (hsh + 1) & P.mask;
+    }
+    return -1;
+}
+
 // live neighbour in the pool: the same-level node, else the deepest existing
 // ancestor of it; its key in nk
 __device__ int32_t live_nb_pool(const Pool &P, const Geometry &G, uint64_t k, int dir, uint64_t &nk) {
@@ -701,39 +734,65 @@ __device__ int32_t live_nb_pool(const Pool &P, const Geometry &G, uint64_t k, in
         t = parent_key(t);
     }
 }
-__device__ void heap_push(Pool &P, int64_t &hn, uint64_t r, int32_t idx, int32_t gen) {
-    if (hn >= P.hcap) { P.err[0] = 1; return; }
-    int64_t i = hn++;
+// Leaves to visit ahead of the traversal: a binary min-heap on traversal
+// rank in shared memory, spilling into a second heap in global memory when
+// full.  One lane operates on it; the sizes are kept uniform by the caller.
+struct Heap {
+    uint64_t *rank;
+    int32_t *idx, *gen;
+    int64_t cap, n;
+};
+struct Queue {
+    Heap s, g;
+};
+__device__ bool hpush(Heap &H, uint64_t r, int32_t idx, int32_t gen) {
+    if (H.n >= H.cap) return false;
+    int64_t i = H.n++;
     while (i > 0) {
         const int64_t pa = (i - 1) >> 1;
-        if (P.hrank[pa] <= r) break;
-        P.hrank[i] = P.hrank[pa]; P.hidx[i] = P.hidx[pa]; P.hgen[i] = P.hgen[pa];
+        if (H.rank[pa] <= r) break;
+        H.rank[i] = H.rank[pa]; H.idx[i] = H.idx[pa]; H.gen[i] = H.gen[pa];
         i = pa;
     }
-    P.hrank[i] = r; P.hidx[i] = idx; P.hgen[i] = gen;
+    H.rank[i] = r; H.idx[i] = idx; H.gen[i] = gen;
+    return true;
 }
-__device__ void heap_pop(Pool &P, int64_t &hn, uint64_t &r, int32_t &idx, int32_t &gen) {
-    r = P.hrank[0]; idx = P.hidx[0]; gen = P.hgen[0];
-    --hn;
-    const uint64_t lr = P.hrank[hn];
-    const int32_t li = P.hidx[hn], lg = P.hgen[hn];
+__device__ void hpop(Heap &H, uint64_t &r, int32_t &idx, int32_t &gen) {
+    r = H.rank[0]; idx = H.idx[0]; gen = H.gen[0];
+    --H.n;
+    const int64_t hn = H.n;
+    const uint64_t lr = H.rank[hn];
+    const int32_t li = H.idx[hn], lg = H.gen[hn];
     int64_t i = 0;
     for (;;) {
         int64_t c = 2 * i + 1;
         if (c >= hn) break;
-        if (c + 1 < hn && P.hrank[c + 1] < P.hrank[c]) ++c;
-        if (P.hrank[c] >= lr) break;
-        P.hrank[i] = P.hrank[c]; P.hidx[i] = P.hidx[c]; P.hgen[i] = P.hgen[c];
+        if (c + 1 < hn && H.rank[c + 1] < H.rank[c]) ++c;
+        if (H.rank[c] >= lr) break;
+        H.rank[i] = H.rank[c]; H.idx[i] = H.idx[c]; H.gen[i] = H.gen[c];
         i = c;
     }
-    if (hn > 0) { P.hrank[i] = lr; P.hidx[i] = li; P.hgen[i] = lg; }
+    if (hn > 0) { H.rank[i] = lr; H.idx[i] = li; H.gen[i] = lg; }
 }
+__device__ __forceinline__ uint64_t qtop(const Queue &Q) {
+    const uint64_t a = Q.s.n > 0 ? Q.s.rank[0] : ~0ull, b = Q.g.n > 0 ? Q.g.rank[0] : ~0ull;
+    return a < b ? a : b;
+}
+__device__ void qpush(Pool &P, Queue &Q, uint64_t r, int32_t idx, int32_t gen) {
+    if (!hpush(Q.s, r, idx, gen) && !hpush(Q.g, r, idx, gen)) P.err[0] = 1;
+}
+__device__ void qpop(Queue &Q, uint64_t &r, int32_t &idx, int32_t &gen) {
+    const uint64_t a = Q.s.n > 0 ? Q.s.rank[0] : ~0ull, b = Q.g.n > 0 ? Q.g.rank[0] : ~0ull;
+    if (a <= b) hpop(Q.s, r, idx, gen);
+    else hpop(Q.g, r, idx, gen);
+}
+
 // After a non-leaf Refine_cell dropped a subtree two or more levels deep,
 // the region of pk (level l0) is coarser than before: leaves at level
 // >= l0 + 3 in the four edge-adjacent level-l0 cells can now find one of the
 // new sons as a neighbour (or neighbour's neighbour) two levels coarser.  The
 // reference visits every leaf, so those ahead of the traversal are queued.
-__device__ void push_ring(Pool &P, const Geometry &G, int64_t &hn, uint64_t pk, uint64_t cur_rank, int32_t &nl) {
+__device__ void push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uint64_t cur_rank) {
     const int l0 = (int)(pk & 15u);
     const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
     for (int d = 0; d < 4; ++d) {
@@ -752,7 +811,7 @@ __device__ void push_ring(Pool &P, const Geometry &G, int64_t &hn, uint64_t pk, 
                 if (c < 0) continue;
                 if (P.flags[c] & PF_LEAF) {
                     const uint64_t r = dfs_rank(ck);
-                    if ((int)(ck & 15u) >= l0 + 3 && r > cur_rank) heap_push(P, hn, r, c, P.gen[c]);
+                    if ((int)(ck & 15u) >= l0 + 3 && r > cur_rank) qpush(P, Q, r, c, P.gen[c]);
                 } else if (sp < 64) {
                     st[sp++] = ck;
                 } else {
@@ -764,7 +823,7 @@ __device__ void push_ring(Pool &P, const Geometry &G, int64_t &hn, uint64_t pk, 
 }
 // Refine_cell (src/mesh.F90:199-260) of a leaf, or of a non-leaf whose old
 // subtree is dropped and whose new sons copy its stale value (counted in nl)
-__device__ void refine_pool(Pool &P, const Geometry &G, int64_t &hn, int32_t p, uint64_t cur_rank, int32_t &nl) {
+__device__ void refine_pool(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t cur_rank, int32_t &nl) {
     const uint64_t pk = P.key[p];
     bool deep = false;
     if (!(P.flags[p] & PF_LEAF)) {
@@ -795,44 +854,150 @@ __device__ void refine_pool(Pool &P, const Geometry &G, int64_t &hn, int32_t p, 
         const int32_t c = hinsert(P, ck, v);
         if (c < 0) { P.err[0] = 1; return; }
         const uint64_t r = dfs_rank(ck);
-        if (r > cur_rank) heap_push(P, hn, r, c, P.gen[c]);
+        if (r > cur_rank) qpush(P, Q, r, c, P.gen[c]);
     }
-    if (deep) push_ring(P, G, hn, pk, cur_rank, nl);
+    if (deep) push_ring(P, G, Q, pk, cur_rank);
 }
+constexpr int GM4_BATCH = 8;
+constexpr int GM4_SHEAP = 8192;   // entries of the shared-memory heap (16 B each)
+
+// Is the node with key s (or the position s stands for) inside node r?
+__device__ __forceinline__ bool key_inside(uint64_t r, uint64_t s) {
+    const int lr = (int)(r & 15u), ls = (int)(s & 15u);
+    if (lr > ls || (r >> 34) != (s >> 34)) return false;
+    const uint64_t path_mask = (1ull << 30) - 1ull;
+    const uint64_t keep = lr == 0 ? 0ull : (path_mask & ~((1ull << (30 - 2 * lr)) - 1ull));
+    return (((s >> 4) & path_mask) & keep) == ((r >> 4) & path_mask);
+}
+
+// A lookup from key k towards d starts at the shifted key S and walks up to
+// the first existing node; refining or dropping node R changes it only when
+// S lies inside R.  sk = S (or ~0 when the shift leaves the grid).
+__device__ __forceinline__ int32_t lookup_from(const Pool &P, const Geometry &G, uint64_t k, int d, uint64_t &nk,
+                                               uint64_t &sk) {
+    uint64_t t;
+    if (!shift_key(G, k, d, t)) { sk = ~0ull; return -1; }
+    sk = t;
+    for (;;) {
+        const int32_t i = hfind(P, t);
+        if (i >= 0) { nk = t; return i; }
+        if ((t & 15u) == 0) return -1;
+        t = parent_key(t);
+    }
+}
+struct Look {
+    int32_t nb, nn;
+    uint64_t nbk, nnk, snb, snn;
+};
+// the reference's direction order of gridmodify4: right, left, up, down
+__device__ __forceinline__ int gm4_dir(int t) { return (t + DIR_RIGHT) & 3; }
+__device__ __forceinline__ void dir_lookups(const Pool &P, const Geometry &G, uint64_t k, int t, Look &L) {
+    L.nn = -1;
+    L.snn = ~0ull;
+    L.nb = lookup_from(P, G, k, gm4_dir(t), L.nbk, L.snb);
+    if (L.nb >= 0) L.nn = lookup_from(P, G, L.nbk, gm4_dir(t), L.nnk, L.snn);
+}
+__device__ __forceinline__ Look shfl_look(const Look &L, int src) {
+    const unsigned FULL = 0xffffffffu;
+    Look o;
+    o.nb = __shfl_sync(FULL, L.nb, src);
+    o.nn = __shfl_sync(FULL, L.nn, src);
+    o.nbk = __shfl_sync(FULL, L.nbk, src);
+    o.nnk = __shfl_sync(FULL, L.nnk, src);
+    o.snb = __shfl_sync(FULL, L.snb, src);
+    o.snn = __shfl_sync(FULL, L.snn, src);
+    return o;
+}
+
+// Refine_cell of pool node p by the warp: a leaf's four sons are inserted by
+// lanes 0..3 at once, a non-leaf (rare) by lane 0 alone.  Returns false when
+// the pool or the queue overflowed.
+__device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t pk, uint64_t cur_rank,
+                            int32_t &nonleaf) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint8_t fp = (uint8_t)__shfl_sync(FULL, lane == 0 ? (int)P.flags[p] : 0, 0);
+    if (!(fp & PF_LEAF)) {
+        if (lane == 0) refine_pool(P, G, Q, p, cur_rank, nonleaf);
+    } else {
+        int32_t c = -1, gen = 0;
+        uint64_t ck = 0;
+        if (lane < 4) {
+            const double4 v = P.val[p];
+            ck = child_key(pk, lane);
+            c = hinsert_atomic(P, ck, v, gen);
+        }
+        __syncwarp();
+        const unsigned bad = __ballot_sync(FULL, lane < 4 && c < 0);
+        if (lane == 0) {
+            P.flags[p] = 0;   // internal, value kept
+            if (bad) P.err[0] = 1;
+        }
+        for (int q = 0; q < 4 && !bad; ++q) {
+            const int32_t cq = __shfl_sync(FULL, c, q);
+            const int32_t gq = __shfl_sync(FULL, gen, q);
+            const uint64_t kq = __shfl_sync(FULL, ck, q);
+            const uint64_t r = dfs_rank(kq);
+            if (lane == 0 && r > cur_rank) qpush(P, Q, r, cq, gq);
+        }
+    }
+    Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
+    Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+    __syncwarp();
+    return __shfl_sync(FULL, lane == 0 ? P.err[0] : 0, 0) == 0;
+}
+
 // gridmodify4 (src/mesh.F90:355-395) over one pass of the tree, by one
 // warp.  The leaves that can act (the initial triggers, sorted by traversal
 // rank, and every leaf queued ahead of the traversal) are visited in
 // traversal order.  Up to 8 upcoming trigger leaves are looked at together:
 // 4 lanes per leaf find its right/left/up/down neighbour and that
-// neighbour's neighbour at once.  The decisions are then applied leaf by
-// leaf in order; the batch ends after a leaf that refined something, and
-// within that leaf every later lookup is repeated on lane 0 after the
-// refinement, so the result is the sequential traversal's.
-constexpr int GM4_BATCH = 8;
+// neighbour's neighbour at once, and each lane tells whether its direction
+// would refine something.  The leaves before the first one that refines
+// have no effect but being visited, so they are marked in parallel; the
+// first one that refines is then applied alone, in order, and the batch
+// ends there.  Within that leaf a lookup starts at a shifted key and walks
+// up to the first existing node, so a refinement (or a dropped subtree) of
+// node R can change a later lookup only when its start lies inside R: those
+// lookups, and only those, are repeated.  The queue of leaves ahead lives in
+// shared memory.
 __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint64_t *__restrict__ trank,
                                                  const int32_t *__restrict__ tidx, int64_t ntrig, int64_t max_steps) {
+    extern __shared__ __align__(16) unsigned char gm4_smem[];
     const int lane = threadIdx.x, grp = lane >> 2, tl = lane & 3;
     const unsigned FULL = 0xffffffffu;
-    const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
-    int64_t ti = 0, hn = 0;   // uniform
+    Queue Q;
+    Q.s.rank = reinterpret_cast<uint64_t *>(gm4_smem);
+    Q.s.idx = reinterpret_cast<int32_t *>(Q.s.rank + GM4_SHEAP);
+    Q.s.gen = Q.s.idx + GM4_SHEAP;
+    Q.s.cap = GM4_SHEAP;
+    Q.s.n = 0;
+    Q.g.rank = P.hrank;
+    Q.g.idx = P.hidx;
+    Q.g.gen = P.hgen;
+    Q.g.cap = P.hcap;
+    Q.g.n = 0;
+    int64_t ti = 0;   // uniform
     int64_t step = 0;
-    int32_t visits = 0, nonleaf = 0;   // lane 0's counts, stored at the end
+    int32_t visits = 0, nonleaf = 0, refines = 0;   // lane 0's counts, stored at the end
     for (;; ++step) {
         if (step >= max_steps) { if (lane == 0) P.err[3] = 1; break; }
         // the next items in traversal order
-        const uint64_t htop = hn > 0 ? P.hrank[0] : ~0ull;
+        const uint64_t htop = qtop(Q);
+        const bool queued = Q.s.n + Q.g.n > 0;
         int cnt = 0;
         bool from_heap = false;
         uint64_t r = 0;
         int32_t c = -1, gen = 0;
-        if (hn > 0 && (ti >= ntrig || htop < trank[ti])) {
+        if (queued && (ti >= ntrig || htop < trank[ti])) {
             from_heap = true;
             cnt = 1;
-            if (lane == 0) heap_pop(P, hn, r, c, gen);
+            if (lane == 0) qpop(Q, r, c, gen);
             r = __shfl_sync(FULL, r, 0);
             c = __shfl_sync(FULL, c, 0);
             gen = __shfl_sync(FULL, gen, 0);
-            hn = __shfl_sync(FULL, hn, 0);
+            Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
+            Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
             __syncwarp();
         } else if (ti < ntrig) {
             const int64_t j = ti + grp;
@@ -847,10 +1012,13 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
         } else {
             break;
         }
-        // speculative lookups: lane (grp, tl) handles direction tl of item grp
-        bool valid = false;
-        uint64_t ck = 0, nbk = 0, nnk = 0;
-        int32_t nb = -1, nn = -1;
+        // lookups and decisions: lane (grp, tl) handles direction tl of item grp
+        bool valid = false, acts = false;
+        uint64_t ck = 0;
+        Look L;
+        L.nb = L.nn = -1;
+        L.nbk = L.nnk = 0;
+        L.snb = L.snn = ~0ull;
         uint8_t fl = 0;
         if (grp < cnt) {
             fl = P.flags[c];
@@ -858,57 +1026,61 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
             ck = P.key[c];
             valid = gc == gen && (fl & (PF_LEAF | PF_DELETED | PF_VISITED)) == PF_LEAF;
             if (valid) {
-                nb = live_nb_pool(P, G, ck, dirs[tl], nbk);
-                if (nb >= 0) nn = live_nb_pool(P, G, nbk, dirs[tl], nnk);
+                dir_lookups(P, G, ck, tl, L);
+                const int lc = (int)(ck & 15u);
+                acts = (L.nb >= 0 && (int)(L.nbk & 15u) <= lc - 2) || (L.nn >= 0 && (int)(L.nnk & 15u) <= lc - 2);
             }
         }
-        int consumed = 0;
-        for (int b = 0; b < cnt; ++b) {
-            const bool vb = __shfl_sync(FULL, valid, b * 4);
-            const uint64_t rb = __shfl_sync(FULL, r, b * 4);
-            const int32_t cb = __shfl_sync(FULL, c, b * 4);
-            const uint64_t kb = __shfl_sync(FULL, ck, b * 4);
-            const uint8_t fb = (uint8_t)__shfl_sync(FULL, (int)fl, b * 4);
-            consumed = b + 1;
-            if (!vb) continue;
+        const unsigned am = __ballot_sync(FULL, acts);
+        const int fa = am ? (__ffs(am) - 1) >> 2 : cnt;   // first item that refines
+        // items before it: visited, nothing else
+        const unsigned vm = __ballot_sync(FULL, valid && tl == 0 && grp < fa);
+        if (valid && tl == 0 && grp < fa) P.flags[c] = fl | PF_VISITED;
+        if (lane == 0) visits += __popc(vm);
+        int consumed = fa;
+        if (fa < cnt) {
+            consumed = fa + 1;
+            const uint64_t rb = __shfl_sync(FULL, r, fa * 4);
+            const int32_t cb = __shfl_sync(FULL, c, fa * 4);
+            const uint64_t kb = __shfl_sync(FULL, ck, fa * 4);
+            const uint8_t fb = (uint8_t)__shfl_sync(FULL, (int)fl, fa * 4);
             const int lc = (int)(kb & 15u);
-            bool dirty = false;   // a refinement since the lookups were made
             if (lane == 0) {
                 P.flags[cb] = fb | PF_VISITED;
                 ++visits;
             }
+            uint64_t refined[8];   // uniform: nodes refined by this leaf
+            int nref = 0;
             for (int t = 0; t < 4; ++t) {
-                int32_t nbt = __shfl_sync(FULL, nb, b * 4 + t);
-                uint64_t nbkt = __shfl_sync(FULL, nbk, b * 4 + t);
-                int32_t nnt = __shfl_sync(FULL, nn, b * 4 + t);
-                uint64_t nnkt = __shfl_sync(FULL, nnk, b * 4 + t);
-                if (dirty) {   // repeat the lookup after a refinement (lane 0)
-                    if (lane == 0) nbt = live_nb_pool(P, G, kb, dirs[t], nbkt);
-                    nbt = __shfl_sync(FULL, nbt, 0);
-                    nbkt = __shfl_sync(FULL, nbkt, 0);
+                Look Lt = shfl_look(L, fa * 4 + t);
+                // repeat the lookups whose start lies inside a node refined earlier
+                bool re_nb = false, re_nn = false;
+                for (int k = 0; k < nref; ++k) {
+                    re_nb = re_nb || key_inside(refined[k], Lt.snb);
+                    re_nn = re_nn || key_inside(refined[k], Lt.snn);
                 }
-                if (nbt < 0) continue;
-                if ((int)(nbkt & 15u) <= lc - 2) {
-                    if (lane == 0) refine_pool(P, G, hn, nbt, rb, nonleaf);
-                    hn = __shfl_sync(FULL, hn, 0);
-                    __syncwarp();
-                    dirty = true;
-                    if (__shfl_sync(FULL, lane == 0 ? P.err[0] : 0, 0)) return;
+                if (re_nb || re_nn) {
+                    if (lane == 0) {
+                        if (re_nb) dir_lookups(P, G, kb, t, Lt);
+                        else Lt.nn = lookup_from(P, G, Lt.nbk, gm4_dir(t), Lt.nnk, Lt.snn);
+                    }
+                    Lt = shfl_look(Lt, 0);
                 }
-                if (dirty) {   // the neighbour's neighbour is looked up after Refine_cell(nbor)
-                    if (lane == 0) nnt = live_nb_pool(P, G, nbkt, dirs[t], nnkt);
-                    nnt = __shfl_sync(FULL, nnt, 0);
-                    nnkt = __shfl_sync(FULL, nnkt, 0);
+                if (Lt.nb < 0) continue;
+                // a neighbour two levels coarser is a leaf (every internal node
+                // has four sons), and refining it leaves the lookup of its own
+                // neighbour unchanged (that start lies outside it)
+                if ((int)(Lt.nbk & 15u) <= lc - 2) {
+                    if (!refine_warp(P, G, Q, Lt.nb, Lt.nbk, rb, nonleaf)) return;
+                    refined[nref++] = Lt.nbk;
+                    ++refines;
                 }
-                if (nnt >= 0 && (int)(nnkt & 15u) <= lc - 2) {
-                    if (lane == 0) refine_pool(P, G, hn, nnt, rb, nonleaf);
-                    hn = __shfl_sync(FULL, hn, 0);
-                    __syncwarp();
-                    dirty = true;
-                    if (__shfl_sync(FULL, lane == 0 ? P.err[0] : 0, 0)) return;
+                if (Lt.nn >= 0 && (int)(Lt.nnk & 15u) <= lc - 2) {
+                    if (!refine_warp(P, G, Q, Lt.nn, Lt.nnk, rb, nonleaf)) return;
+                    refined[nref++] = Lt.nnk;
+                    ++refines;
                 }
             }
-            if (dirty) break;   // later items are looked up again
         }
         if (!from_heap) ti += consumed;
         __syncwarp();
@@ -916,8 +1088,11 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
     if (lane == 0) {
         P.err[1] = visits;
         P.err[2] = nonleaf;
+        P.err[4] = refines;
+        P.err[5] = (int32_t)step;
     }
 }
+
 __global__ void k_pool_live(int64_t n, const uint8_t *flags, int32_t *live) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < n) live[i] = !(flags[i] & PF_DELETED);
@@ -1054,7 +1229,7 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     while (slots < (uint64_t)(2 * cap)) slots <<= 1;
     Carve cp;
     cp.add(cap * 8); cp.add(cap); cp.add(cap * 4); cp.add(cap * 32); cp.add(slots * 4); cp.add(16);
-    cp.add(cap * 8); cp.add(cap * 4); cp.add(cap * 4); cp.add(16); cp.add(slots * 8);
+    cp.add(cap * 8); cp.add(cap * 4); cp.add(cap * 4); cp.add(32); cp.add(slots * 8);
     FDM_CK(h, h->amr[16].ensure(cp.total));
     DevBuf &pb = h->amr[16];
     Pool P;
@@ -1067,20 +1242,26 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     P.cap = cap;
     P.hcap = cap;
     FDM_CK(h, cudaMemsetAsync(P.slot, 0xff, slots * 4, h->s));
-    FDM_CK(h, cudaMemsetAsync(P.err, 0, 16, h->s));
+    FDM_CK(h, cudaMemsetAsync(P.skey, 0xff, slots * 8, h->s));
+    FDM_CK(h, cudaMemsetAsync(P.err, 0, 32, h->s));
     FDM_CK(h, cudaMemcpyAsync(P.n, &n, 8, cudaMemcpyHostToDevice, h->s));
     k_pool_init<<<nblk(n, TB), TB, 0, h->s>>>(X.A, P);
     // every step consumes a trigger or a queued leaf, or ends the pass
-    k_gm4_warp<<<1, 32, 0, h->s>>>(P, h->G, rk, idx, ntrig, ntrig + P.hcap + 16);
-    int32_t herr[4] = {0, 0, 0, 0};
+    const size_t gm4_smem = (size_t)GM4_SHEAP * 16;
+    FDM_CK(h, cudaFuncSetAttribute(k_gm4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gm4_smem));
+    k_gm4_warp<<<1, 32, gm4_smem, h->s>>>(P, h->G, rk, idx, ntrig, ntrig + GM4_SHEAP + P.hcap + 16);
+    int32_t herr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t pn = 0;
-    FDM_CK(h, cudaMemcpyAsync(herr, P.err, 16, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaMemcpyAsync(herr, P.err, 32, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaMemcpyAsync(&pn, P.n, 8, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     if (herr[0]) { h->err = "gridmodify4 cascade exceeded its node pool"; return FDM_ERR_UNSUPPORTED; }
     if (herr[3]) { h->err = "gridmodify4 replay did not finish"; return FDM_ERR_UNSUPPORTED; }
     h->gm4_visits += herr[1];
     h->gm4_nonleaf += herr[2];
+    h->gm4_refines += herr[4];
+    h->gm4_steps += herr[5];
+    h->gm4_triggers += ntrig;
     // live nodes back into a sorted node set
     Carve ce;
     ce.add(pn * 4); ce.add(pn * 4);

@@ -90,7 +90,7 @@ struct fdm_handle {
     fdm::DevBuf ikey, ival;
     int64_t NInt = 0;
     fdm::DevBuf amr[20];     // regrid scratch
-    int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0;
+    int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0, gm4_triggers = 0, gm4_refines = 0, gm4_steps = 0;
     // device-timeline phases of the last regrid (events recorded on the stream)
     static constexpr int AMR_PHASES = 5;
     cudaEvent_t amr_ev[AMR_PHASES + 1] = {};

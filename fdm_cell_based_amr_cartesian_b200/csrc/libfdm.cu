@@ -494,6 +494,9 @@ int fdm_get_counters(fdm_handle *h, fdm_counters *c) {
     c->n_gm1_iterations = h->gm1_iters;
     c->n_gm4_visits = h->gm4_visits;
     c->n_gm4_nonleaf = h->gm4_nonleaf;
+    c->n_gm4_triggers = h->gm4_triggers;
+    c->n_gm4_refines = h->gm4_refines;
+    c->n_gm4_steps = h->gm4_steps;
     return FDM_OK;
 }
 

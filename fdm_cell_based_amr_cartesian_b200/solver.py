@@ -56,7 +56,9 @@ class FdmCounters(ctypes.Structure):
                 ("n_faces_y", ctypes.c_int64), ("n_singular", ctypes.c_int64),
                 ("n_regrids", ctypes.c_int64), ("n_internal", ctypes.c_int64),
                 ("n_gm1_iterations", ctypes.c_int64), ("n_gm4_visits", ctypes.c_int64),
-                ("n_gm4_nonleaf", ctypes.c_int64), ("reserved", ctypes.c_int64 * 4)]
+                ("n_gm4_nonleaf", ctypes.c_int64), ("n_gm4_triggers", ctypes.c_int64),
+                ("n_gm4_refines", ctypes.c_int64), ("n_gm4_steps", ctypes.c_int64),
+                ("reserved", ctypes.c_int64 * 1)]
 
 
 _lib = None

@@ -127,7 +127,10 @@ typedef struct fdm_counters {
     int64_t n_gm4_visits;      /* leaves gridmodify4 acted from               */
     int64_t n_gm4_nonleaf;     /* Refine_cell of a non-leaf by gridmodify4
                                   (src/mesh.F90:389-392)                      */
-    int64_t reserved[4];
+    int64_t n_gm4_triggers;    /* gridmodify4: leaves marked able to act at pass start */
+    int64_t n_gm4_refines;     /* gridmodify4: Refine_cell calls */
+    int64_t n_gm4_steps;       /* gridmodify4: replay iterations (batches and queued leaves) */
+    int64_t reserved[1];
 } fdm_counters;
 
 /* ------------------------------------------------------------- lifecycle */
