@@ -980,38 +980,68 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
     int64_t ti = 0;   // uniform
     int64_t step = 0;
     int32_t visits = 0, nonleaf = 0, refines = 0;   // lane 0's counts, stored at the end
+    __shared__ uint64_t it_rank[GM4_BATCH];
+    __shared__ int32_t it_idx[GM4_BATCH], it_gen[GM4_BATCH];
+    __shared__ int8_t it_heap[GM4_BATCH];
+    int tk_extra = 0;   // lane 0: triggers taken into the batch (duplicates included)
     for (;; ++step) {
         if (step >= max_steps) { if (lane == 0) P.err[3] = 1; break; }
-        // the next items in traversal order
-        const uint64_t htop = qtop(Q);
-        const bool queued = Q.s.n + Q.g.n > 0;
+        // the next items in traversal order: the queued leaves and the
+        // triggers merged by rank (lane 0), up to GM4_BATCH of them
+        uint64_t tr = ~0ull;
+        int32_t tx = -1;
+        {
+            const int64_t j = ti + lane;
+            if (lane < GM4_BATCH && j < ntrig) { tr = trank[j]; tx = tidx[j]; }
+        }
         int cnt = 0;
-        bool from_heap = false;
+        {
+            // lane 0 merges; the trigger window is broadcast lane by lane
+            uint64_t wr[GM4_BATCH];
+            int32_t wx[GM4_BATCH];
+#pragma unroll
+            for (int q = 0; q < GM4_BATCH; ++q) {
+                wr[q] = __shfl_sync(FULL, tr, q);
+                wx[q] = __shfl_sync(FULL, tx, q);
+            }
+            if (lane == 0) {
+                int k = 0;   // triggers taken
+                uint64_t last_r = ~0ull;
+                int32_t last_i = -1;
+                while (cnt < GM4_BATCH) {
+                    const uint64_t h = qtop(Q);
+                    const uint64_t t = k < GM4_BATCH ? wr[k] : ~0ull;
+                    if (h == ~0ull && t == ~0ull) break;
+                    uint64_t rr;
+                    int32_t ii, gg;
+                    int8_t fromq;
+                    if (t != ~0ull && t <= h) {   // on a tie the trigger comes first
+                        rr = t; ii = wx[k]; gg = 0; fromq = 0;
+                        ++k;
+                    } else {
+                        qpop(Q, rr, ii, gg);
+                        fromq = 1;
+                    }
+                    // the same leaf twice (queued and a trigger, or queued twice):
+                    // visited once, as in the reference's single traversal
+                    if (rr == last_r && ii == last_i) continue;
+                    last_r = rr;
+                    last_i = ii;
+                    it_rank[cnt] = rr; it_idx[cnt] = ii; it_gen[cnt] = gg; it_heap[cnt] = fromq;
+                    ++cnt;
+                }
+                // a skipped duplicate trigger still counts as taken
+                tk_extra = k;
+            }
+        }
+        cnt = __shfl_sync(FULL, cnt, 0);
+        Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
+        Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+        __syncwarp();
+        if (cnt == 0) break;
         uint64_t r = 0;
         int32_t c = -1, gen = 0;
-        if (queued && (ti >= ntrig || htop < trank[ti])) {
-            from_heap = true;
-            cnt = 1;
-            if (lane == 0) qpop(Q, r, c, gen);
-            r = __shfl_sync(FULL, r, 0);
-            c = __shfl_sync(FULL, c, 0);
-            gen = __shfl_sync(FULL, gen, 0);
-            Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
-            Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
-            __syncwarp();
-        } else if (ti < ntrig) {
-            const int64_t j = ti + grp;
-            bool ok = grp < GM4_BATCH && j < ntrig;
-            if (ok) {
-                r = trank[j];
-                c = tidx[j];
-                ok = r <= htop;   // a tie is the same leaf queued twice
-            }
-            const unsigned m = __ballot_sync(FULL, ok && tl == 0);
-            cnt = __popc(m);   // the ranks are sorted, so the ok items form a prefix
-        } else {
-            break;
-        }
+        if (grp < cnt) { r = it_rank[grp]; c = it_idx[grp]; gen = it_gen[grp]; }
         // lookups and decisions: lane (grp, tl) handles direction tl of item grp
         bool valid = false, acts = false;
         uint64_t ck = 0;
@@ -1082,7 +1112,20 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
                 }
             }
         }
-        if (!from_heap) ti += consumed;
+        // unconsumed queued leaves go back; consumed triggers advance ti.  When
+        // every item is consumed, so are the triggers that were skipped as
+        // duplicates; otherwise ti stops at the first unconsumed trigger
+        if (lane == 0) {
+            int ntr = 0;
+            for (int q = 0; q < cnt; ++q) {
+                if (q < consumed) ntr += it_heap[q] ? 0 : 1;
+                else if (it_heap[q]) qpush(P, Q, it_rank[q], it_idx[q], it_gen[q]);
+            }
+            ti += consumed == cnt ? tk_extra : ntr;
+        }
+        ti = __shfl_sync(FULL, ti, 0);
+        Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
+        Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
         __syncwarp();
     }
     if (lane == 0) {
@@ -1168,18 +1211,25 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X) {
     k_scatter_rank<<<nblk(n, TB), TB, 0, h->s>>>(n, pi2, L.rank);
     FDM_CK(h, cudaMemsetAsync(d0, 0, n, h->s));
     int8_t *cur = d0, *nxt = d1;
+    // Sweeps are enqueued GM1_SWEEPS at a time and the change flag of the
+    // last one is read: once the decisions are settled a sweep changes
+    // nothing, so the extra sweeps leave the fixpoint as it is.
+    constexpr int GM1_SWEEPS = 4;
     int64_t it = 0;
-    for (;; ++it) {
-        if (it > n + 2) { h->err = "gridmodify1 decisions did not settle"; return FDM_ERR_UNSUPPORTED; }
-        FDM_CK(h, cudaMemsetAsync(changed, 0, 4, h->s));
-        k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed);
+    for (;;) {
+        if (it > n + 2 + GM1_SWEEPS) { h->err = "gridmodify1 decisions did not settle"; return FDM_ERR_UNSUPPORTED; }
+        for (int k = 0; k < GM1_SWEEPS; ++k) {
+            if (k == GM1_SWEEPS - 1) FDM_CK(h, cudaMemsetAsync(changed, 0, 4, h->s));
+            k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed);
+            std::swap(cur, nxt);
+        }
+        it += GM1_SWEEPS;
         int32_t hc = 0;
         FDM_CK(h, cudaMemcpyAsync(&hc, changed, 4, cudaMemcpyDeviceToHost, h->s));
         FDM_CK(h, cudaStreamSynchronize(h->s));
-        std::swap(cur, nxt);
         if (!hc) break;
     }
-    h->gm1_iters += it + 1;
+    h->gm1_iters += it;
     for (int l = MAXLVL_TAB - 2; l >= 0; --l) k_gm1_vals<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, l);
     k_gm1_count<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, cnt);
     int64_t total = 0;
@@ -1339,7 +1389,7 @@ int run_amr(fdm_handle *h) {
     int64_t nleaf = 0, nint = 0;
     AMR_RC(scan_total32(h, fl, ol, n, nleaf));
     AMR_RC(scan_total32(h, fi, oi, n, nint));
-    DevBuf lk, lv;
+    DevBuf &lk = h->amr[20], &lv = h->amr[21];   // kept between regrids
     FDM_CK(h, lk.ensure(nleaf * 8 + 8));
     FDM_CK(h, lv.ensure(nleaf * 32 + 32));
     FDM_CK(h, h->ikey.ensure(nint * 8 + 8));
@@ -1357,6 +1407,7 @@ int run_amr(fdm_handle *h) {
         float t = 0.f;
         cudaEventElapsedTime(&t, h->amr_ev[k], h->amr_ev[k + 1]);
         h->amr_phase_ms[k] = t;
+        h->amr_phase_total_ms[k] += t;
     }
     h->n_regrids++;
     return FDM_OK;
@@ -1364,12 +1415,16 @@ int run_amr(fdm_handle *h) {
 
 }  // namespace fdm
 
-// Device-timeline milliseconds of the last regrid's phases: indicators and
+// Device-timeline milliseconds of the regrid phases: indicators and
 // ordered sums, refine/coarsen flags and the first node sort, the lvlAMR
-// gridmodify rounds, the leaf/internal split, the table rebuild.
+// gridmodify rounds, the leaf/internal split, the table rebuild; ms[0..4]
+// for the last regrid, ms[5..9] summed over all regrids of the handle.
 extern "C" int fdm_amr_phase_ms(const fdm_handle *h, double *ms) {
     if (!h || !ms) return FDM_ERR_ARG;
-    for (int k = 0; k < fdm_handle::AMR_PHASES; ++k) ms[k] = h->amr_phase_ms[k];
+    for (int k = 0; k < fdm_handle::AMR_PHASES; ++k) {
+        ms[k] = h->amr_phase_ms[k];
+        ms[fdm_handle::AMR_PHASES + k] = h->amr_phase_total_ms[k];
+    }
     return FDM_OK;
 }
 

@@ -17,13 +17,21 @@ struct DevBuf {
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
+    // At least nbytes; a buffer that has to grow takes 25 % + 1 MiB more, so
+    // that a mesh growing by a few cells per regrid does not reallocate (a
+    // cudaFree synchronises the device) at every regrid.
     cudaError_t ensure(size_t nbytes) {
         if (nbytes <= bytes && p) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
         size_t nb = nbytes ? nbytes : 16;
+        if (nbytes > 0) nb += nbytes / 4 + (1u << 20);
         cudaError_t e = cudaMalloc(&p, nb);
+        if (e != cudaSuccess && nb > nbytes) {   // no room for headroom
+            cudaGetLastError();
+            e = cudaMalloc(&p, nb = nbytes);
+        }
         if (e == cudaSuccess) bytes = nb;
         return e;
     }
@@ -89,12 +97,13 @@ struct fdm_handle {
     // stale U in every refined node; gridmodify4 can copy it back)
     fdm::DevBuf ikey, ival;
     int64_t NInt = 0;
-    fdm::DevBuf amr[20];     // regrid scratch
+    fdm::DevBuf amr[22];     // regrid scratch: [0..5] node sets, [6..19] work arrays, [20, 21] new leaves
     int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0, gm4_triggers = 0, gm4_refines = 0, gm4_steps = 0;
     // device-timeline phases of the last regrid (events recorded on the stream)
     static constexpr int AMR_PHASES = 5;
     cudaEvent_t amr_ev[AMR_PHASES + 1] = {};
     double amr_phase_ms[AMR_PHASES] = {};
+    double amr_phase_total_ms[AMR_PHASES] = {};   // summed over all regrids
 
     // learned gate of the face flux
     fdm::DevBuf io;   // staging of fdm_set_values / fdm_download_leaves (grows, kept)

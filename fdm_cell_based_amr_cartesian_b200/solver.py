@@ -357,11 +357,13 @@ class Solver:
         self._check(self.L.fdm_debug_rot_div(self.h, n, _dp(rot), _dp(div), _dp(sums)))
         return rot, div, sums
 
-    def amr_phase_ms(self) -> dict:
-        """Device-timeline ms of the last regrid's phases."""
-        a = np.zeros(5)
+    def amr_phase_ms(self, total: bool = False) -> dict:
+        """Device-timeline ms of the regrid phases: of the last regrid, or
+        summed over all regrids of this solver."""
+        a = np.zeros(10)
         self._check(self.L.fdm_amr_phase_ms(self.h, _dp(a)))
-        return dict(zip(("indicators", "flags", "gridmodify", "split", "tables"), a.tolist()))
+        v = a[5:] if total else a[:5]
+        return dict(zip(("indicators", "flags", "gridmodify", "split", "tables"), v.tolist()))
 
     def time_kernels(self, reps: int = 10):
         """Average ms per launch: faces (x+y), cells, hanging nodes, ghosts."""

@@ -275,10 +275,10 @@ int fdm_gate_eval(const float *X, int64_t n, const float *params, float *prob,
 int fdm_gate_stats(fdm_handle *h, int64_t *gated, int64_t *total);
 
 /* Diagnostics, no reference counterpart: device-timeline milliseconds of
- * the last regrid's five phases (indicators + ordered sums; flags + first
- * node sort; the lvlAMR gridmodify rounds; leaf/internal split; table
- * rebuild). */
-int fdm_amr_phase_ms(const fdm_handle *h, double ms[5]);
+ * the five regrid phases (indicators + ordered sums; flags + first node
+ * sort; the lvlAMR gridmodify rounds; leaf/internal split; table rebuild),
+ * ms[0..4] for the last regrid and ms[5..9] summed over all regrids. */
+int fdm_amr_phase_ms(const fdm_handle *h, double ms[10]);
 
 /* ------------------------------------------------------------ ensembles
  * No reference counterpart (the reference runs one mesh per process).  A
