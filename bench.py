@@ -197,6 +197,42 @@ def timed_window(g, steps, warmup, flush):
     return sum(a.elapsed_time(b) for a, b in ev)
 
 
+def fast_window(args, keys, prim, NI, flush, world):
+    """flux_variant 1 (FMA contraction, shared reciprocals) on the same mesh
+    and window: updates/s, and the difference after one step from the same
+    state against the exact path (relative to each field's magnitude)."""
+    import torch
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+    from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
+    cfg_f = P.riemann4(base=128, lvl_amr=4)
+    cfg_f.params.flux_variant = 1
+    gf = S.Solver(cfg_f)
+    gf.upload(keys, prim)
+    gf.body_boundary(1)
+    gf.step_control()
+    tuned, _ = gf.autotune(reps=5)
+    ms = max_over_ranks(timed_window(gf, args.steps, args.warmup, flush), device="cuda")
+    kt = gf.time_kernels(reps=9)
+    gf.close()
+    # one step from the initial state on fresh handles (scalars included),
+    # fast against exact
+    pair = []
+    for fv in (1, 0):
+        c = P.riemann4(base=128, lvl_amr=4)
+        c.params.flux_variant = fv
+        g = S.Solver(c)
+        g.upload(keys, prim)
+        g.body_boundary(1)
+        g.advance(1)
+        pair.append(g.leaves()[1])
+        g.close()
+    a, b = pair
+    dev = float(np.max(np.max(np.abs(a - b), axis=0) / np.max(np.abs(b), axis=0)))
+    return {"value": NI * world * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "face_variant": tuned, "kernel_ms": kt, "one_step_rel_diff_vs_exact": dev,
+            "note": "flux_variant 1: FMA contraction, shared reciprocals, one division per Z-weight pair"}
+
+
 def learned_window(args, cfg, keys, prim, NI, flush, world):
     """The learned-gated solver on the same mesh and window as the plain
     one: updates/s, the gated face share, and the density error against a
@@ -471,6 +507,9 @@ def run_ours(args):
         + (1 if cnt["n_restrict_requests"] else 0) + (1 if cnt["n_ghost"] else 0)
     launches_per_step = 4 + 3 * per_stage
 
+    # the fast face flux (flux_variant 1) on the same mesh and window
+    fastf = fast_window(args, keys, prim, NI, flush, world)
+
     # learned-gated path on the same workload and window
     gated = None
     if not args.no_learned:
@@ -524,7 +563,7 @@ def run_ours(args):
                 "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
                 "counters": cnt, "state_finite_after_timed_steps": finite, "cpu_baseline": cpu,
-                "learned": gated, "ensemble": ens, "full_run": full}
+                "fast_flux": fastf, "learned": gated, "ensemble": ens, "full_run": full}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -1,7 +1,8 @@
 """Build libfdm.so (sm_100a) in-tree with nvcc.
 
 The exact path is compiled with ``-fmad=false`` so that every FP64 product
-and sum is rounded as the reference's source order writes it.
+and sum is rounded as the reference's source order writes it; the fast face
+flux (flux_variant 1, fast_flux.cu) is built with FMA contraction.
 """
 from __future__ import annotations
 
@@ -15,8 +16,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfdm.so")
-SOURCES = ["build.cu", "stage.cu", "amr.cu", "libfdm.cu", "timing.cu", "static_uniform.cu", "gate.cu", "batch.cu"]
-HEADERS = ["fdm_common.cuh", "handle.cuh", "numerics.cuh", "topo.cuh"]
+SOURCES = ["build.cu", "stage.cu", "amr.cu", "libfdm.cu", "timing.cu", "static_uniform.cu", "gate.cu", "batch.cu",
+           "fast_flux.cu"]
+# fast_flux.cu is the one file built with FMA contraction (flux_variant 1)
+FMAD_TRUE = {"fast_flux.cu"}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
@@ -39,7 +42,7 @@ def _stale(target: str, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [
+    hdrs = [os.path.join(CSRC, h) for h in sorted(os.listdir(CSRC)) if h.endswith(".cuh")] + [
         os.path.join(HERE, "..", "include", "fdm.h")]
     objs = []
     jobs = []
@@ -48,7 +51,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", s, "-o", o]
+            flags = [f if not (src in FMAD_TRUE and f == "-fmad=false") else "-fmad=true" for f in NVCC_FLAGS]
+            cmd = [nvcc(), *ARCH, *flags, "-c", s, "-o", o]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             jobs.append(cmd)

@@ -569,6 +569,7 @@ int fdm_batch_create(fdm_handle *const *members, int32_t n, fdm_batch **out) {
     int dev = -1;
     for (int m = 0; m < n; ++m) {
         if (!members[m] || !members[m]->loaded) return FDM_ERR_STATE;
+        if (members[m]->p.flux_variant != 0) return FDM_ERR_UNSUPPORTED;   // the batch runs the exact flux
         if (dev < 0) dev = members[m]->device;
         if (members[m]->device != dev) return FDM_ERR_ARG;
         for (int k = 0; k < m; ++k)

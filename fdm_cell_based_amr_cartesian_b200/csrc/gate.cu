@@ -311,6 +311,10 @@ void launch_gated_faces(fdm_handle *h, const double4 *cur, int krk) {
         if (gx > 0) k_guard_linear<0><<<gx, 256, 0, h->s>>>(T, cur, h->Fx.as<double4>(), jx, sc, h->G.gama, hx, cnt);
         if (gy > 0) k_guard_linear<1><<<gy, 256, 0, h->s>>>(T, cur, h->Fy.as<double4>(), jy, sc, h->G.gama, hy, cnt + 1);
     }
+    if (h->p.flux_variant == 1) {
+        launch_faces_list_fast(h, cur, hx, hy, cnt, lx, ly);
+        return;
+    }
     if (lx > 0) k_faces_list<0><<<lx, 256, 0, h->s>>>(T, cur, h->Fx.as<double4>(), hx, cnt, sc, h->G.gama);
     if (ly > 0) k_faces_list<1><<<ly, 256, 0, h->s>>>(T, cur, h->Fy.as<double4>(), hy, cnt + 1, sc, h->G.gama);
 }

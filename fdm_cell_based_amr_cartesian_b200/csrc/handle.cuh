@@ -188,6 +188,10 @@ void launch_set_tstep(fdm_handle *h, double tstep);
 void launch_res_finalize(fdm_handle *h);
 int launch_stage(fdm_handle *h, int krk);
 void launch_gated_faces(fdm_handle *h, const double4 *cur, int krk);
+// flux_variant 1 (fast_flux.cu)
+void launch_faces_fast(fdm_handle *h, const double4 *cur);
+void launch_faces_list_fast(fdm_handle *h, const double4 *cur, const int32_t *hx, const int32_t *hy,
+                            const uint32_t *cnt, int lx, int ly);
 size_t gate_list_bytes(const fdm_handle *h);
 // AMR (amr.cu)
 int run_amr(fdm_handle *h);

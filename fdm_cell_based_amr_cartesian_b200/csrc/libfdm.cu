@@ -198,7 +198,7 @@ int fdm_create(const fdm_params *p, fdm_handle **out) {
     if (m != p->m || n != p->n) return FDM_ERR_ARG;
     if ((int64_t)p->m * p->n >= (1ll << 30)) return FDM_ERR_ARG;
     if (p->lvl_amr < 0 || p->lvl_amr > MAXLVL_TAB - 2) return FDM_ERR_ARG;
-    if (p->flux_variant != 0) return FDM_ERR_UNSUPPORTED;
+    if (p->flux_variant != 0 && p->flux_variant != 1) return FDM_ERR_UNSUPPORTED;
     fdm_handle *h = new (std::nothrow) fdm_handle();
     if (!h) return FDM_ERR_NOMEM;
     h->p = *p;

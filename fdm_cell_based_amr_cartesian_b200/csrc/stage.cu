@@ -208,6 +208,8 @@ const char *face_variant_name(int v) {
         case 2: return "1 thread/face, 64 threads, >=7 blocks/SM";
         case 3: return "1 thread/face, 256 threads, >=2 blocks/SM";
         case 4: return "4 threads/face, 256 threads";
+        case 5: return "1 thread/face, 128 threads, >=5 blocks/SM";
+        case 6: return "1 thread/face, 64 threads, >=10 blocks/SM";
         default: return "?";
     }
 }
@@ -217,11 +219,17 @@ void launch_faces(fdm_handle *h, const double4 *cur, int krk) {
         launch_gated_faces(h, cur, krk);
         return;
     }
+    if (h->p.flux_variant == 1) {
+        launch_faces_fast(h, cur);
+        return;
+    }
     switch (h->face_variant) {
         case 1: faces_1lane<128, 4>(h, cur); break;
         case 2: faces_1lane<64, 7>(h, cur); break;
         case 3: faces_1lane<256, 2>(h, cur); break;
         case 4: faces_4lane(h, cur); break;
+        case 5: faces_1lane<128, 5>(h, cur); break;
+        case 6: faces_1lane<64, 10>(h, cur); break;
         default: faces_1lane<128, 3>(h, cur); break;
     }
 }

@@ -49,7 +49,7 @@ extern "C" int fdm_time_kernels(fdm_handle *h, int32_t reps, double *ms) {
 
 namespace fdm {
 const char *face_variant_name(int v);
-constexpr int N_FACE_VARIANTS = 5;
+constexpr int N_FACE_VARIANTS = FDM_FACE_VARIANTS;
 }
 
 // Autotuner: times every launch shape of the face kernel on the current leaf

@@ -27,6 +27,8 @@ FDM_ERR_NAN = 3
 ERRORS = {1: "FDM_ERR_ARG", 2: "FDM_ERR_CUDA", 3: "FDM_ERR_NAN", 4: "FDM_ERR_TIMEOUT",
           5: "FDM_ERR_NOMEM", 6: "FDM_ERR_STATE", 7: "FDM_ERR_UNSUPPORTED"}
 
+FACE_VARIANTS = 7   # FDM_FACE_VARIANTS of include/fdm.h
+
 # every extern "C" symbol declared in include/fdm.h
 EXPORTS = [
     "fdm_create", "fdm_destroy", "fdm_last_error", "fdm_upload_leaves", "fdm_num_leaves",
@@ -374,7 +376,7 @@ class Solver:
     def autotune(self, reps: int = 5):
         """Pick the fastest face-kernel launch shape for this leaf set."""
         best = ctypes.c_int32()
-        ms = np.zeros(5)
+        ms = np.zeros(FACE_VARIANTS)
         self._check(self.L.fdm_autotune(self.h, int(reps), ctypes.byref(best), _dp(ms)))
         return best.value, ms
 

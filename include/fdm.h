@@ -237,9 +237,11 @@ int fdm_device_state(fdm_handle *h, void **stream, double **prim_dev,
  * counterpart. */
 int fdm_time_kernels(fdm_handle *h, int32_t reps, double *ms);
 int fdm_fp64_peak(double *tflops);
-/* Autotuner of the face-flux launch shape: times each of the 5 variants on
- * the current leaf set (ms[v] = ms per x+y launch pair), keeps the fastest
- * for this handle and reports it in *best.  fdm_set_variant forces one. */
+/* Autotuner of the face-flux launch shape: times each of the
+ * FDM_FACE_VARIANTS variants on the current leaf set (ms[v] = ms per x+y
+ * launch pair; ms holds FDM_FACE_VARIANTS doubles), keeps the fastest for
+ * this handle and reports it in *best.  fdm_set_variant forces one. */
+#define FDM_FACE_VARIANTS 7
 int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms);
 int fdm_set_variant(fdm_handle *h, int32_t face_variant);
 

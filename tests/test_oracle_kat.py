@@ -190,3 +190,23 @@ def test_leaf_order_is_reference_order(oracle_mod):
     keys, _, _ = o.leaves()
     assert np.all(np.diff(keys.astype(np.uint64)) > 0)
     assert o.num_interior() == int(_interior_mask(cfg, keys).sum())
+
+
+def test_wls_constant_error_grows_with_resolution(oracle_mod):
+    """The reference's hanging-node fit (src/XuanGua.F90:224-229: basis 1, x,
+    y, xy, x^2, y^2 in absolute coordinates, Gauss-Jordan inverse) loses
+    digits as the mesh spacing shrinks: on a band-refined 4-level mesh with a
+    constant state, the hanging-node values miss the constant by an amount
+    that grows with the background resolution.  The oracle (and the GPU,
+    bit for bit) reproduce this."""
+    from fdm_cell_based_amr_cartesian_b200.solver import distance_refined_keys
+    errs = []
+    for base in (16, 32):
+        cfg = P.riemann4(base=base, lvl_amr=4)
+        keys = distance_refined_keys(cfg, [("y", 0.5)], [0.2, 0.15, 0.1, 0.05])
+        prim = np.tile(np.array([1.5, 0.0, 0.0, 1.5]), (len(keys), 1))
+        o = oracle_mod.Oracle(cfg, initial=False)
+        o.set_leaves(keys, prim)
+        errs.append(float(np.abs(o.stencil()[:, :, 0] - 1.5).max()))
+        o.close()
+    assert 0.0 < errs[0] < errs[1] < 1e-3, errs
