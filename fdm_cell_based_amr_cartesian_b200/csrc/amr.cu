@@ -505,7 +505,7 @@ __device__ __forceinline__ bool gm1_has_son(const Links &L, const int8_t *d, int
 // gridmodify1 decision of one node (src/mesh.F90:305-353) given the current
 // estimate of all decisions; a decision only reads decisions of nodes that
 // are visited earlier, so iterating to a fixpoint gives the sequential result
-__global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, int32_t *changed) {
+__global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, int32_t *changed, int32_t *any) {
     const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (x >= n) return;
     int8_t r = D_NONE;
@@ -529,6 +529,7 @@ __global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, in
     }
     dn[x] = r;
     if (r != d[x]) atomicExch(changed, 1);
+    if (any && r != D_NONE) atomicExch(any, 1);
 }
 // values of coarsened nodes, deepest level first (interpA of the sons as they
 // are at the node's visit)
@@ -1186,7 +1187,9 @@ static int emit_buffers(fdm_handle *h, int64_t n, Emit &E) {
     } while (0)
 
 // one gridmodify1 pass over the node set A -> A
-static int gridmodify1_pass(fdm_handle *h, AmrCtx &X) {
+// One gridmodify1 pass over the node set A -> A; *did: a node was refined
+// or coarsened (otherwise A is left as it is).
+static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     const int TB = 256;
     const int64_t n = X.A.n;
     Carve cv;
@@ -1218,18 +1221,23 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X) {
     int64_t it = 0;
     for (;;) {
         if (it > n + 2 + GM1_SWEEPS) { h->err = "gridmodify1 decisions did not settle"; return FDM_ERR_UNSUPPORTED; }
+        int32_t hc[2] = {0, 0};   // last sweep: changed, any decision
         for (int k = 0; k < GM1_SWEEPS; ++k) {
-            if (k == GM1_SWEEPS - 1) FDM_CK(h, cudaMemsetAsync(changed, 0, 4, h->s));
-            k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed);
+            const bool last = k == GM1_SWEEPS - 1;
+            if (last) FDM_CK(h, cudaMemsetAsync(changed, 0, 8, h->s));
+            k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed, last ? changed + 1 : nullptr);
             std::swap(cur, nxt);
         }
         it += GM1_SWEEPS;
-        int32_t hc = 0;
-        FDM_CK(h, cudaMemcpyAsync(&hc, changed, 4, cudaMemcpyDeviceToHost, h->s));
+        FDM_CK(h, cudaMemcpyAsync(hc, changed, 8, cudaMemcpyDeviceToHost, h->s));
         FDM_CK(h, cudaStreamSynchronize(h->s));
-        if (!hc) break;
+        if (!hc[0]) {
+            *did = hc[1] != 0;
+            break;
+        }
     }
     h->gm1_iters += it;
+    if (!*did) return FDM_OK;   // every decision is "nothing": A stays
     for (int l = MAXLVL_TAB - 2; l >= 0; --l) k_gm1_vals<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, l);
     k_gm1_count<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, cnt);
     int64_t total = 0;
@@ -1243,8 +1251,9 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X) {
     return FDM_OK;
 }
 
-// one gridmodify4 pass over the node set A -> A
-static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
+// One gridmodify4 pass over the node set A -> A; *did: something was
+// refined (otherwise A is left as it is).
+static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     const int TB = 256;
     const int64_t n = X.A.n;
     Carve cv;
@@ -1267,6 +1276,7 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     int64_t ntrig = 0;
     FDM_CK(h, cudaMemcpyAsync(&ntrig, nsel, 8, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
+    *did = false;
     if (ntrig == 0) return FDM_OK;
     // key order is Morton order (son4 before son3); the traversal visits
     // son3 first, so sort the triggers by traversal rank
@@ -1312,6 +1322,8 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X) {
     h->gm4_refines += herr[4];
     h->gm4_steps += herr[5];
     h->gm4_triggers += ntrig;
+    *did = herr[4] != 0;
+    if (!*did) return FDM_OK;   // no Refine_cell: the pool holds A unchanged
     // live nodes back into a sorted node set
     Carve ce;
     ce.add(pn * 4); ce.add(pn * 4);
@@ -1373,9 +1385,13 @@ int run_amr(fdm_handle *h) {
     swap_sets(h, X);
     FDM_CK(h, cudaEventRecord(h->amr_ev[2], h->s));
     // 3. solute_gridmodify: lvlAMR rounds (src/solution.F90:537-556)
+    // A round that changes nothing leaves the node set as it found it, so
+    // the rounds after it would change nothing either.
     for (int k = 1; k <= h->p.lvl_amr; ++k) {
-        AMR_RC(gridmodify1_pass(h, X));
-        AMR_RC(gridmodify4_pass(h, X));
+        bool did1 = false, did4 = false;
+        AMR_RC(gridmodify1_pass(h, X, &did1));
+        AMR_RC(gridmodify4_pass(h, X, &did4));
+        if (!did1 && !did4) break;
     }
     FDM_CK(h, cudaEventRecord(h->amr_ev[3], h->s));
     // 4. split leaves / internal nodes, rebuild the tables (idneighbor + IDgrid)
