@@ -107,6 +107,13 @@ struct fdm_handle {
 
     // learned gate of the face flux
     fdm::DevBuf io;   // staging of fdm_set_values / fdm_download_leaves (grows, kept)
+    // asynchronous value transfers: a copy stream each way (uploads, read-
+    // backs), two staging buffers each way, and the events that order them
+    // with the compute stream
+    cudaStream_t cs = nullptr, cs_out = nullptr;
+    fdm::DevBuf in_stage[2], out_stage[2];
+    cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+    int in_b = 0, out_b = 0;
     fdm::DevBuf gate_params, gate_flag;   // gate_flag: per-stage hard-face lists
     float gate_logit_thr = 0.f;
     bool gate_on = false;

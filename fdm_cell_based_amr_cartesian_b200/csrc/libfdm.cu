@@ -250,6 +250,18 @@ void fdm_destroy(fdm_handle *h) {
     for (auto &t : h->tmp) t.release();
     for (cudaEvent_t e : h->amr_ev)
         if (e) cudaEventDestroy(e);
+    for (int b = 0; b < 2; ++b) {
+        cudaEvent_t ev[4] = {h->in_ready[b], h->in_free[b], h->out_ready[b], h->out_free[b]};
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        h->in_stage[b].release();
+        h->out_stage[b].release();
+    }
+    for (cudaStream_t cs : {h->cs, h->cs_out})
+        if (cs) {
+            cudaStreamSynchronize(cs);
+            cudaStreamDestroy(cs);
+        }
     if (h->hs) cudaFreeHost(h->hs);
     if (h->s) cudaStreamDestroy(h->s);
     delete h;
@@ -296,6 +308,78 @@ int fdm_download_leaves(fdm_handle *h, int64_t cap, int64_t *n_out, uint64_t *ke
                                                   dp.as<double>());
         FDM_CK(h, cudaMemcpyAsync(prim, dp.p, h->NL * 32, cudaMemcpyDeviceToHost, h->s));
     }
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+
+// Asynchronous value transfers (no reference counterpart): the copies run
+// on a copy stream with double-buffered device staging, so the upload of the
+// next step's input and the read-back of the last result overlap the steps
+// in between.  Host buffers must be pinned and stay untouched until
+// fdm_io_sync returns.
+static int io_setup(fdm_handle *h) {
+    if (h->cs) return FDM_OK;
+    FDM_CK(h, cudaStreamCreateWithFlags(&h->cs, cudaStreamNonBlocking));
+    FDM_CK(h, cudaStreamCreateWithFlags(&h->cs_out, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+        FDM_CK(h, cudaEventCreateWithFlags(&h->in_ready[b], cudaEventDisableTiming));
+        FDM_CK(h, cudaEventCreateWithFlags(&h->in_free[b], cudaEventDisableTiming));
+        FDM_CK(h, cudaEventCreateWithFlags(&h->out_ready[b], cudaEventDisableTiming));
+        FDM_CK(h, cudaEventCreateWithFlags(&h->out_free[b], cudaEventDisableTiming));
+    }
+    return FDM_OK;
+}
+
+int fdm_set_values_async(fdm_handle *h, int64_t n, const double *prim) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (n != h->NL || !prim) return arg_fail(h, "value count differs from the leaf count");
+    RC(io_setup(h));
+    const int b = h->in_b;
+    h->in_b ^= 1;
+    if (h->in_stage[b].bytes < (size_t)n * 32) {
+        FDM_CK(h, cudaStreamSynchronize(h->s));   // the buffer may still be read
+        FDM_CK(h, h->in_stage[b].ensure(n * 32));
+    }
+    FDM_CK(h, cudaStreamWaitEvent(h->cs, h->in_free[b], 0));
+    FDM_CK(h, cudaMemcpyAsync(h->in_stage[b].p, prim, n * 32, cudaMemcpyHostToDevice, h->cs));
+    FDM_CK(h, cudaEventRecord(h->in_ready[b], h->cs));
+    FDM_CK(h, cudaStreamWaitEvent(h->s, h->in_ready[b], 0));
+    k_in<<<nblk(n, 256), 256, 0, h->s>>>(n, h->lslot.as<int32_t>(), h->B[0].as<double4>(), h->in_stage[b].as<double>());
+    if (h->NC > 0)
+        for (int k = 1; k < 3; ++k)
+            FDM_CK(h, cudaMemcpyAsync(h->B[k].as<double4>() + h->NI + h->NG, h->B[0].as<double4>() + h->NI + h->NG,
+                                      h->NC * 32, cudaMemcpyDeviceToDevice, h->s));
+    FDM_CK(h, cudaEventRecord(h->in_free[b], h->s));
+    h->lam_fresh = false;
+    return FDM_OK;
+}
+
+int fdm_download_values_async(fdm_handle *h, int64_t cap, double *prim) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (cap < h->NL || !prim) return arg_fail(h, "capacity below the leaf count");
+    RC(io_setup(h));
+    const int b = h->out_b;
+    h->out_b ^= 1;
+    if (h->out_stage[b].bytes < (size_t)h->NL * 32) {
+        FDM_CK(h, cudaStreamSynchronize(h->cs_out));   // the buffer may still be copied out
+        FDM_CK(h, h->out_stage[b].ensure(h->NL * 32));
+    }
+    FDM_CK(h, cudaStreamWaitEvent(h->s, h->out_free[b], 0));
+    k_out<<<nblk(h->NL, 256), 256, 0, h->s>>>(h->NL, h->lslot.as<int32_t>(), h->B[0].as<double4>(),
+                                              h->out_stage[b].as<double>());
+    FDM_CK(h, cudaEventRecord(h->out_ready[b], h->s));
+    FDM_CK(h, cudaStreamWaitEvent(h->cs_out, h->out_ready[b], 0));
+    FDM_CK(h, cudaMemcpyAsync(prim, h->out_stage[b].p, h->NL * 32, cudaMemcpyDeviceToHost, h->cs_out));
+    FDM_CK(h, cudaEventRecord(h->out_free[b], h->cs_out));
+    return FDM_OK;
+}
+
+int fdm_io_sync(fdm_handle *h) {
+    CHECK_H(h);
+    if (h->cs) FDM_CK(h, cudaStreamSynchronize(h->cs));
+    if (h->cs_out) FDM_CK(h, cudaStreamSynchronize(h->cs_out));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     return FDM_OK;
 }

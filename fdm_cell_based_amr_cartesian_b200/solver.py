@@ -42,6 +42,7 @@ EXPORTS = [
     "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
     "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
     "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
+    "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
 ]
 
 
@@ -85,6 +86,9 @@ def load_library(path: str = LIB_PATH):
     L.fdm_num_leaves.restype = i64
     L.fdm_download_leaves.argtypes = [vp, i64, ctypes.POINTER(i64), u64p, dp]
     L.fdm_set_values.argtypes = [vp, i64, dp]
+    L.fdm_set_values_async.argtypes = [vp, i64, dp]
+    L.fdm_download_values_async.argtypes = [vp, i64, dp]
+    L.fdm_io_sync.argtypes = [vp]
     L.fdm_get_scalars.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(i64), ctypes.POINTER(i32)]
     L.fdm_set_scalars.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_double, i64]
@@ -267,6 +271,20 @@ class Solver:
         nout = ctypes.c_int64()
         self._check(self.L.fdm_download_leaves(self.h, n, ctypes.byref(nout), None, _dp(out)))
         return out
+
+    def set_values_async(self, prim):
+        """Asynchronous fdm_set_values: prim must be pinned host memory
+        (e.g. a torch pinned tensor's numpy view) kept until io_sync()."""
+        assert prim.dtype == np.float64 and prim.flags["C_CONTIGUOUS"]
+        self._check(self.L.fdm_set_values_async(self.h, len(prim), _dp(prim)))
+
+    def download_values_async(self, out):
+        """Asynchronous read-back of the current values into pinned out."""
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"]
+        self._check(self.L.fdm_download_values_async(self.h, len(out), _dp(out)))
+
+    def io_sync(self):
+        self._check(self.L.fdm_io_sync(self.h))
 
     def scalars(self) -> dict:
         lx, ly, dt, tt = (ctypes.c_double() for _ in range(4))

@@ -156,6 +156,17 @@ int fdm_download_leaves(fdm_handle *h, int64_t cap, int64_t *n_out,
 /* Overwrite the primitive values of the current leaf set (same keys as the
  * last upload/regrid, in key order).  No table rebuild. */
 int fdm_set_values(fdm_handle *h, int64_t n, const double *prim);
+/* Asynchronous forms (no reference counterpart): the copies run on copy
+ * streams (one for uploads, one for read-backs) with double-buffered device
+ * staging, ordered with the compute
+ * stream by events, so an upload of the next input and a read-back of the
+ * last result overlap the steps in between.  prim must be pinned host
+ * memory and stay untouched until fdm_io_sync returns; the values are those
+ * of the state at the point in the call sequence (uploads before the next
+ * step, read-backs after the previous one). */
+int fdm_set_values_async(fdm_handle *h, int64_t n, const double *prim);
+int fdm_download_values_async(fdm_handle *h, int64_t cap, double *prim);
+int fdm_io_sync(fdm_handle *h);
 
 /* Scalars of the time loop: lambda_x, lambda_y, tstep, tt, it, l_max. */
 int fdm_get_scalars(fdm_handle *h, double *lambda_x, double *lambda_y,

@@ -262,3 +262,29 @@ def test_fast_flux_within_per_step_bar(oracle_mod, name):
         worst = max(worst, err)
         assert err <= 1e-6, err
     assert worst > 0.0   # it is a different rounding, not the exact path
+
+
+def test_async_value_transfers_match_sync():
+    """fdm_set_values_async / fdm_download_values_async (copy stream, double-
+    buffered staging) give the same states as the synchronous calls, over
+    several pipelined steps."""
+    import torch
+    cfg = P.riemann4(base=32, lvl_amr=2)
+    a, b = Solver(cfg), Solver(cfg)
+    a.creat_mesh_and_initial()
+    b.creat_mesh_and_initial()
+    _, p0 = a.leaves()
+    hin = torch.empty(p0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hin[:] = p0
+    outs = [torch.empty(p0.shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+    ref = []
+    for k in range(4):
+        a.set_values_async(hin)
+        a.advance(1)
+        a.download_values_async(outs[k])
+        b.set_values(p0)
+        b.advance(1)
+        ref.append(b.leaves()[1])
+    a.io_sync()
+    for k in range(4):
+        assert np.array_equal(outs[k], ref[k]), k
