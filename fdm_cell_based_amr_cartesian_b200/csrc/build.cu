@@ -409,6 +409,7 @@ __global__ void k_gather(Tables T, Geometry G, ReqDesc D, ReqOut O, int32_t *err
 struct GhostOut {
     int32_t *kind, *a, *b, *flip;
     double *x, *y;
+    unsigned long long *n_restrict;   // ghosts imaged by a subtree restriction
 };
 
 __device__ __forceinline__ void ghost_from_ref(const Tables &T, const NodeRef &img, GhostOut &O, int64_t g) {
@@ -419,6 +420,7 @@ __device__ __forceinline__ void ghost_from_ref(const Tables &T, const NodeRef &i
     } else {
         const uint64_t p0 = node_pos(img.n);
         O.kind[g] = GH_RESTRICT;
+        atomicAdd(O.n_restrict, 1ull);
         O.a[g] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0);
         O.b[g] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(img.n.lvl));
     }
@@ -753,7 +755,8 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     if (NG > 0) {
         Tables T = h->tables();
         GhostOut O{h->gh_kind.as<int32_t>(), h->gh_a.as<int32_t>(), h->gh_b.as<int32_t>(),
-                   h->gh_flip.as<int32_t>(), h->gh_x.as<double>(), h->gh_y.as<double>()};
+                   h->gh_flip.as<int32_t>(), h->gh_x.as<double>(),  h->gh_y.as<double>(),
+                   h->tmp[5].as<unsigned long long>() + 4};
         k_ghosts<<<nblk(NG, 128), 128, 0, s>>>(T, h->G, h->p, O);
     }
     // 7. faces
@@ -805,7 +808,7 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     FDM_CK(h, cudaMemsetAsync(dl, 0, 4, s));
     k_lmax<<<nblk(NI, TB), TB, 0, s>>>(NI, h->ilvl.as<uint8_t>(), dl);
     int32_t he[8];
-    unsigned long long hc[4];
+    unsigned long long hc[5];
     FDM_CK(h, cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, s));
     FDM_CK(h, cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s));
     FDM_CK(h, cudaStreamSynchronize(s));
@@ -816,6 +819,7 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     FDM_CK(h, cudaMemcpy(&h->scal.as<DevScalars>()->l_max, &h->l_max, 4, cudaMemcpyHostToDevice));
     h->n_singular += (int64_t)hc[0];
     h->n_restrict = (int64_t)hc[2];
+    h->n_ghost_restrict = (int64_t)hc[4];
     h->table_version++;
     h->gate_stage1_valid = false;
     h->lam_fresh = false;

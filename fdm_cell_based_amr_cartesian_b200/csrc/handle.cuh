@@ -75,7 +75,7 @@ struct fdm_handle {
     bool lam_fresh = false;
     int cur_buf = 0;         // split API: buffer holding the latest interior values
     int face_variant = 0;    // 0: four lanes per face, 1: one thread per face
-    int64_t n_singular = 0, n_regrids = 0, n_restrict = 0;
+    int64_t n_singular = 0, n_regrids = 0, n_restrict = 0, n_ghost_restrict = 0;
 
     // tables
     fdm::DevBuf lkey, lslot, slot_leaf, lcx, lcy, lcross;

@@ -101,6 +101,27 @@ __device__ __forceinline__ void request_item(const Tables &T, double4 *cur, int6
     cur[out] = v;
 }
 
+// component v (0..3) of hanging-node request r of kind WLS or COPY: the
+// four components of a value are independent, so four threads can share a
+// request
+__device__ __forceinline__ void request_item_var(const Tables &T, double4 *cur, int64_t r, int v) {
+    const int64_t out = T.NI + T.NG + T.NC + r;
+    const int kind = T.rq_kind[r];
+    const int32_t *mem = T.rq_mem + r * WLS_MAXM;
+    double *o = reinterpret_cast<double *>(cur + out) + v;
+    if (kind == RQ_COPY) {
+        *o = reinterpret_cast<const double *>(cur + mem[0])[v];
+        return;
+    }
+    if (kind == RQ_RESTRICT) return;
+    const int m1 = T.rq_m[2 * r], m2 = T.rq_m[2 * r + 1];
+    const int m = m1 + m2;
+    const double *geo = T.rq_geo + r * RQ_GEO;
+    double ph[WLS_MAXM];
+    for (int i = 0; i < m; ++i) ph[i] = reinterpret_cast<const double *>(cur + mem[i])[v];
+    *o = wls_eval_var(geo, m1, m2, ph);
+}
+
 // interpA fallback of parent_value_weno for request r (whole warp)
 __device__ __forceinline__ void request_restrict_warp(const Tables &T, double4 *cur, int64_t r, RestrictSmem &sm) {
     if (T.rq_kind[r] != RQ_RESTRICT) return;

@@ -19,10 +19,12 @@ namespace fdm {
 
 static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
-__global__ void __launch_bounds__(64) k_requests(Tables T, double4 *cur) {
-    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// four threads per request, one per component
+__global__ void __launch_bounds__(256) k_requests4(Tables T, double4 *cur) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t r = g >> 2;
     if (r >= T.NR) return;
-    request_item(T, cur, r);
+    request_item_var(T, cur, r, (int)(g & 3));
 }
 
 // interpA fallbacks of parent_value_weno: one warp per request
@@ -129,12 +131,24 @@ __global__ void k_blend(int64_t NI, const double4 *__restrict__ un, const double
     cur[i] = make_double4(ra * a.x + rb * b.x, ra * a.y + rb * b.y, ra * a.z + rb * b.z, ra * a.w + rb * b.w);
 }
 
-// one warp per ghost leaf (interpA images can span hundreds of leaves)
+// ghost leaves imaged by a copy or a boundary state: one thread each
+__global__ void __launch_bounds__(256) k_ghost_simple(Tables T, double4 *buf, GhostStates GS,
+                                                      const DevScalars *__restrict__ sc, int j) {
+    const int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (gi >= T.NG) return;
+    const int kind = T.gh_kind[gi];
+    if (kind == GH_NONE || kind == GH_RESTRICT) return;
+    ghost_store(T, buf, gi, ghost_simple_value(T, buf, GS, sc, j, gi, kind));
+}
+
+// ghost leaves imaged by a subtree restriction (interpA images can span
+// hundreds of leaves): one warp each
 __global__ void __launch_bounds__(128) k_ghost(Tables T, double4 *buf, GhostStates GS,
                                                const DevScalars *__restrict__ sc, int j) {
     __shared__ RestrictSmem sm[4];
     const int64_t gi = blockIdx.x * 4 + (threadIdx.x >> 5);
     if (gi >= T.NG) return;
+    if (T.gh_kind[gi] != GH_RESTRICT) return;
     ghost_warp(T, buf, GS, sc, j, gi, sm[threadIdx.x >> 5]);
 }
 
@@ -183,7 +197,7 @@ __global__ void k_set_tstep(DevScalars *sc, double tstep) {
 // ------------------------------------------------------------ launchers
 void launch_requests(fdm_handle *h, const double4 *cur) {
     if (h->NR == 0) return;
-    k_requests<<<nblk(h->NR, 64), 64, 0, h->s>>>(h->tables(), (double4 *)cur);
+    k_requests4<<<nblk(4 * h->NR, 256), 256, 0, h->s>>>(h->tables(), (double4 *)cur);
     if (h->n_restrict > 0) k_requests_restrict<<<nblk(h->NR, 4), 128, 0, h->s>>>(h->tables(), (double4 *)cur);
 }
 // Launch shapes of the face kernel that the autotuner chooses from.
@@ -244,7 +258,10 @@ void launch_cells(fdm_handle *h, const double4 *cur, const double4 *un, double4 
 }
 void launch_ghosts(fdm_handle *h, double4 *next, int j) {
     if (h->NG == 0) return;
-    k_ghost<<<nblk(h->NG, 4), 128, 0, h->s>>>(h->tables(), next, ghost_states(h->p), h->scal.as<DevScalars>(), j);
+    const GhostStates GS = ghost_states(h->p);
+    k_ghost_simple<<<nblk(h->NG, 256), 256, 0, h->s>>>(h->tables(), next, GS, h->scal.as<DevScalars>(), j);
+    if (h->n_ghost_restrict > 0)
+        k_ghost<<<nblk(h->NG, 4), 128, 0, h->s>>>(h->tables(), next, GS, h->scal.as<DevScalars>(), j);
 }
 void launch_blend(fdm_handle *h, const double4 *un, double4 *cur, int krk) {
     k_blend<<<nblk(h->NI, 256), 256, 0, h->s>>>(h->NI, un, h->Ut.as<double4>(), cur, krk);
