@@ -223,10 +223,10 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
         const Member &M = A.mem[m];
         if (!A.act[m]) return;
         double4 *cur = const_cast<double4 *>(stage_cur(M, krk));
-        const int64_t nthr = cdiv(M.T.NR, BT);
+        const int64_t nthr = cdiv(4 * M.T.NR, BT);   // four threads per request, one per component
         if (t < nthr) {
-            const int64_t r = t * BT + threadIdx.x;
-            if (r < M.T.NR) request_item(M.T, cur, r);
+            const int64_t q = t * BT + threadIdx.x;
+            if ((q >> 2) < M.T.NR) request_item_var(M.T, cur, q >> 2, (int)(q & 3));
         } else {
             const int64_t r = (t - nthr) * BW + wid;
             if (r < M.T.NR) request_restrict_warp(M.T, cur, r, S.rs[wid]);
@@ -422,7 +422,7 @@ static int batch_refresh(fdm_batch *b) {
             d.GL = gate_lists(h->gate_flag.p, d.nfx, d.nfy);
         }
         const int64_t tiles[N_PHASE] = {
-            cdiv(h->NR, BT) + (d.has_restrict ? cdiv(h->NR, BW) : 0),   // PH_REQ
+            cdiv(4 * h->NR, BT) + (d.has_restrict ? cdiv(h->NR, BW) : 0),   // PH_REQ
             cdiv(d.nfx, BT) + cdiv(d.nfy, BT),                          // PH_FACE
             0,                                                          // PH_HARD (device)
             cdiv(h->NI, BT),                                            // PH_CELL
