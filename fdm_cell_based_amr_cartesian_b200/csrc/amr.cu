@@ -142,41 +142,62 @@ __device__ __forceinline__ int64_t find_key(const uint64_t *__restrict__ keys, i
     return (lo < n && keys[lo] == k) ? lo : -1;
 }
 
+// The helpers below work on the interleaved path bits directly.  Level j's
+// digit (x bit | y bit << 1) sits at key bit 4 + 2 (LMAX - j); the x bits of
+// the path occupy the even path positions and the y bits the odd ones.
+constexpr uint64_t KEY_PATH_X = 0x15555555ull << 4;   // x bits of the path
+constexpr uint64_t KEY_PATH_Y = 0x2AAAAAAAull << 4;   // y bits of the path
+constexpr uint64_t KEY_PATH = (KEY_PATH_X | KEY_PATH_Y);
+FDM_HD int key_digit_shift(int lvl) { return 4 + 2 * (LMAX - lvl); }
+
 FDM_HD uint64_t parent_key(uint64_t k) {
-    Node n = node_of_key(k);
-    n.lvl -= 1;
-    n.ix >>= 1;
-    n.iy >>= 1;
-    return node_key(n);
+    const int lvl = (int)(k & 15u);
+    return (k & ~(3ull << key_digit_shift(lvl))) - 1u;
 }
 FDM_HD uint64_t child_key(uint64_t k, int q) {
-    Node n = node_of_key(k);
-    n.lvl += 1;
-    n.ix = 2u * n.ix + (uint32_t)(q & 1);
-    n.iy = 2u * n.iy + (uint32_t)(q >> 1);
-    return node_key(n);
+    const int lvl = (int)(k & 15u);
+    return (k | ((uint64_t)q << key_digit_shift(lvl + 1))) + 1u;
 }
-// same-level neighbour node key across a face; false across the grid edge
+// same-level neighbour node key across a face; false across the grid edge.
+// A step along x (y) is a dilated increment or decrement of the x (y) bits
+// at the node's level; a carry out of the path moves to the next root.
 FDM_HD bool shift_key(const Geometry &G, uint64_t k, int dir, uint64_t &out) {
-    Node n = node_of_key(k);
-    int64_t row = n.root / G.m, col = n.root % G.m;
-    const uint32_t N = 1u << n.lvl;
-    switch (dir) {
-        case DIR_UP:
-            if (n.iy + 1 == N) { if (row + 1 >= G.n) return false; ++row; n.iy = 0; } else ++n.iy;
-            break;
-        case DIR_DOWN:
-            if (n.iy == 0) { if (row == 0) return false; --row; n.iy = N - 1; } else --n.iy;
-            break;
-        case DIR_RIGHT:
-            if (n.ix + 1 == N) { if (col + 1 >= G.m) return false; ++col; n.ix = 0; } else ++n.ix;
-            break;
-        default:
-            if (n.ix == 0) { if (col == 0) return false; --col; n.ix = N - 1; } else --n.ix;
-            break;
+    const int lvl = (int)(k & 15u);
+    const uint64_t unit = 1ull << key_digit_shift(lvl);
+    const bool alongx = dir == DIR_RIGHT || dir == DIR_LEFT;
+    const uint64_t mask = alongx ? KEY_PATH_X : KEY_PATH_Y;
+    const uint64_t u = alongx ? unit : unit << 1;
+    const uint64_t bits = k & mask;
+    const uint64_t rest = k & ~mask;
+    const uint32_t root = (uint32_t)(k >> 34);
+    const uint32_t m = (uint32_t)G.m;
+    if (dir == DIR_RIGHT || dir == DIR_UP) {
+        const uint64_t t = (bits | ~mask) + u;   // carries skip the other coordinate's bits
+        if (((bits | ~mask | (u - 1)) & KEY_PATH) == KEY_PATH) {   // last node of the root
+            if (alongx) {
+                if (root % m + 1 >= m) return false;
+            } else if (root / m + 1 >= (uint32_t)G.n) {
+                return false;
+            }
+            const uint64_t nroot = (uint64_t)(alongx ? root + 1u : root + m);
+            out = (nroot << 34) | (rest & ((1ull << 34) - 1ull));
+            return true;
+        }
+        out = rest | (t & mask);
+        return true;
     }
-    n.root = row * G.m + col;
-    out = node_key(n);
+    if (bits == 0) {   // first node of the root
+        if (alongx) {
+            if (root % m == 0) return false;
+        } else if (root < m) {
+            return false;
+        }
+        const uint64_t nroot = (uint64_t)(alongx ? root - 1u : root - m);
+        const uint64_t full = mask & ~(u - 1);   // all ones down to the node's level
+        out = (nroot << 34) | (rest & ((1ull << 34) - 1ull)) | full;
+        return true;
+    }
+    out = rest | ((bits - u) & mask);
     return true;
 }
 // traversal rank of gridmodify4 / solute_div_rot (sons 1,2,3,4): Morton path
