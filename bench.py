@@ -408,7 +408,8 @@ def full_run(S, gate, ulp=False):
     out = {"workload": "riemann4 128^2, 4 levels, t = 0 -> 0.3, regrid every 10 steps",
            "seconds": t_full, "steps": steps, "regrids": cf["n_regrids"],
            "mean_updates_per_s": upd / t_full, "leaves_at_end": cf["n_leaves"],
-           "regrid_device_ms_total": gf.amr_phase_ms(total=True)}
+           "regrid_device_ms_total": gf.amr_phase_ms(total=True),
+           "gridmodify_counters": {k: v for k, v in cf.items() if "gm" in k}}
     leaves = gf.leaves()
     gf.close()
     return out, leaves

@@ -206,6 +206,16 @@ FDM_HD uint64_t dfs_rank(uint64_t k) {
     const uint64_t path = key_pos(k) & ((1ull << 30) - 1ull);
     return ((k >> 34) << 30) | (path ^ ((path & 0x2AAAAAAAull) >> 1));
 }
+// Visit order of gridmodify4's traversal (sons 1,2,3,4 of every node): the
+// traversal rank of the node's position, then its level, so a node comes
+// before its first son, which starts at the same position.  The node's key
+// is recovered from it.  Below 2^53 for up to 2^19 background cells.
+FDM_HD uint64_t visit_rank(uint64_t k) { return (dfs_rank(k) << 4) | (k & 15u); }
+FDM_HD uint64_t key_of_visit_rank(uint64_t r) {
+    const uint64_t pr = r >> 4;
+    const uint64_t path = pr & ((1ull << 30) - 1ull);
+    return ((pr >> 30) << 34) | ((path ^ ((path & 0x2AAAAAAAull) >> 1)) << 4) | (r & 15u);
+}
 // post-order rank of gridmodify1 (a node after all of its descendants):
 // 3 bits per level, sons 1,2,3,4 -> 0,1,2,3 and 4 below the node's level
 FDM_HD uint64_t post_rank(uint64_t k) {
@@ -624,10 +634,17 @@ __global__ void k_gm4_triggers(NodeSet A, Geometry G, int32_t *flag, uint64_t *r
         }
     }
     flag[c] = f;
-    rank[c] = dfs_rank(A.key[c]);
+    rank[c] = visit_rank(A.key[c]);
     idx[c] = (int32_t)c;
 }
 
+// An item of the replay: mk = visit rank * 2, + 1 for a leaf queued ahead of
+// the traversal (so that on equal rank the initial trigger comes first), its
+// pool index and the generation it was queued with.
+struct __align__(16) HEnt {
+    uint64_t mk;
+    int32_t idx, gen;
+};
 struct Pool {
     uint64_t *key;
     uint8_t *flags;
@@ -638,8 +655,7 @@ struct Pool {
     uint64_t mask;       // slots - 1
     int64_t cap;         // pool capacity
     int64_t *n;          // pool size (device counter)
-    uint64_t *hrank;     // heap of leaves to visit ahead of the traversal
-    int32_t *hidx, *hgen;
+    HEnt *heap;          // heap of leaves to visit ahead of the traversal (spill)
     int64_t hcap;
     int32_t *err;        // [0] capacity exceeded, [1] visits, [2] non-leaf refines, [3] step limit,
                          // [4] refines, [5] replay steps
@@ -685,8 +701,9 @@ __device__ __forceinline__ int32_t hfind(const Pool &P, uint64_t k) {
     if (hpos(P, k, s) < 0) return -1;
     return (s & SLOT_DEL) ? -1 : s;
 }
-// insert or revive a leaf with value v; returns its pool index or -1
-__device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v) {
+// insert or revive a leaf with value v (one lane); pn is the pool size.
+// Returns its pool index or -1
+__device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v, int64_t &pn) {
     int32_t s;
     const int64_t pos = hpos(P, k, s);
     if (pos >= 0) {
@@ -700,9 +717,9 @@ __device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v) {
     uint64_t hsh = hmix(k) & P.mask;
     for (uint64_t probe = 0; probe <= P.mask; ++probe) {
         if (P.slot[hsh] == -1) {
-            const int64_t i = *P.n;
+            const int64_t i = pn;
             if (i >= P.cap) return -1;
-            *P.n = i + 1;
+            pn = i + 1;
             P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
             P.slot[hsh] = (int32_t)i;
             P.skey[hsh] = k;
@@ -712,101 +729,77 @@ __device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v) {
     }
     return -1;
 }
-// Insert or revive a leaf with value v from several lanes at once (distinct
-// keys): slots are claimed with atomicCAS, pool entries with atomicAdd.  An
-// empty slot's key is ~0 (never a node key), so a lane probing for its own
-// key passes a slot that another lane has claimed but not yet keyed.
-// Returns the pool index (or -1 when the pool is full) and its generation.
-__device__ int32_t hinsert_atomic(Pool &P, uint64_t k, const double4 &v, int32_t &gen) {
-    int32_t s;
-    const int64_t pos = hpos(P, k, s);
-    if (pos >= 0) {
-        const int32_t i = s & ~SLOT_DEL;
-        P.slot[pos] = i;
-        P.flags[i] = PF_LEAF;
-        gen = P.gen[i] + 1;
-        P.gen[i] = gen;
-        P.val[i] = v;
-        return i;
-    }
-    const int64_t i = (int64_t)atomicAdd((unsigned long long *)P.n, 1ull);
-    if (i >= P.cap) return -1;
-    P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
-    gen = 0;
-    uint64_t hsh = hmix(k) & P.mask;
+// the rest of key k's probe sequence, given its first probe (position h,
+// slot word s, slot key q): the live node's pool index, or -1
+__device__ __forceinline__ int32_t hfind_rest(const Pool &P, uint64_t k, uint64_t h, int32_t s, uint64_t q) {
     for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        if (atomicCAS(P.slot + hsh, -1, (int32_t)i) == -1) {
-            P.skey[hsh] = k;
-            return (int32_t)i;
-        }
-        hsh = (hsh + 1) & P.mask;
+        if (s == -1) return -1;
+        if (q == k) return (s & SLOT_DEL) ? -1 : s;
+        h = (h + 1) & P.mask;
+        s = P.slot[h];
+        q = P.skey[h];
     }
     return -1;
 }
 
-// live neighbour in the pool: the same-level node, else the deepest existing
-// ancestor of it; its key in nk
-__device__ int32_t live_nb_pool(const Pool &P, const Geometry &G, uint64_t k, int dir, uint64_t &nk) {
-    uint64_t t;
-    if (!shift_key(G, k, dir, t)) return -1;
-    for (;;) {
-        const int32_t i = hfind(P, t);
-        if (i >= 0) { nk = t; return i; }
-        if ((t & 15u) == 0) return -1;
-        t = parent_key(t);
-    }
-}
-// Leaves to visit ahead of the traversal: a binary min-heap on traversal
-// rank in shared memory, spilling into a second heap in global memory when
-// full.  One lane operates on it; the sizes are kept uniform by the caller.
+// Leaves to visit ahead of the traversal: a binary min-heap on mk in shared
+// memory, spilling into a second heap in global memory when full.  One lane
+// operates on it; the sizes are kept uniform by the caller.
 struct Heap {
-    uint64_t *rank;
-    int32_t *idx, *gen;
+    HEnt *e;
     int64_t cap, n;
 };
 struct Queue {
     Heap s, g;
 };
-__device__ bool hpush(Heap &H, uint64_t r, int32_t idx, int32_t gen) {
+__device__ bool hpush(Heap &H, const HEnt &x) {
     if (H.n >= H.cap) return false;
     int64_t i = H.n++;
     while (i > 0) {
         const int64_t pa = (i - 1) >> 1;
-        if (H.rank[pa] <= r) break;
-        H.rank[i] = H.rank[pa]; H.idx[i] = H.idx[pa]; H.gen[i] = H.gen[pa];
+        const HEnt p = H.e[pa];
+        if (p.mk <= x.mk) break;
+        H.e[i] = p;
         i = pa;
     }
-    H.rank[i] = r; H.idx[i] = idx; H.gen[i] = gen;
+    H.e[i] = x;
     return true;
 }
-__device__ void hpop(Heap &H, uint64_t &r, int32_t &idx, int32_t &gen) {
-    r = H.rank[0]; idx = H.idx[0]; gen = H.gen[0];
-    --H.n;
-    const int64_t hn = H.n;
-    const uint64_t lr = H.rank[hn];
-    const int32_t li = H.idx[hn], lg = H.gen[hn];
+__device__ HEnt hpop(Heap &H) {
+    const HEnt top = H.e[0];
+    const int64_t hn = --H.n;
+    const HEnt last = H.e[hn];
     int64_t i = 0;
     for (;;) {
         int64_t c = 2 * i + 1;
         if (c >= hn) break;
-        if (c + 1 < hn && H.rank[c + 1] < H.rank[c]) ++c;
-        if (H.rank[c] >= lr) break;
-        H.rank[i] = H.rank[c]; H.idx[i] = H.idx[c]; H.gen[i] = H.gen[c];
+        HEnt a = H.e[c];
+        if (c + 1 < hn) {
+            const HEnt b = H.e[c + 1];
+            if (b.mk < a.mk) { a = b; ++c; }
+        }
+        if (a.mk >= last.mk) break;
+        H.e[i] = a;
         i = c;
     }
-    if (hn > 0) { H.rank[i] = lr; H.idx[i] = li; H.gen[i] = lg; }
+    if (hn > 0) H.e[i] = last;
+    return top;
 }
 __device__ __forceinline__ uint64_t qtop(const Queue &Q) {
-    const uint64_t a = Q.s.n > 0 ? Q.s.rank[0] : ~0ull, b = Q.g.n > 0 ? Q.g.rank[0] : ~0ull;
+    const uint64_t a = Q.s.n > 0 ? Q.s.e[0].mk : ~0ull, b = Q.g.n > 0 ? Q.g.e[0].mk : ~0ull;
     return a < b ? a : b;
 }
-__device__ void qpush(Pool &P, Queue &Q, uint64_t r, int32_t idx, int32_t gen) {
-    if (!hpush(Q.s, r, idx, gen) && !hpush(Q.g, r, idx, gen)) P.err[0] = 1;
+__device__ bool qpush(Queue &Q, const HEnt &x) { return hpush(Q.s, x) || hpush(Q.g, x); }
+__device__ bool qpush_leaf(Queue &Q, uint64_t key, int32_t idx, int32_t gen) {
+    HEnt x;
+    x.mk = visit_rank(key) * 2 + 1;
+    x.idx = idx;
+    x.gen = gen;
+    return qpush(Q, x);
 }
-__device__ void qpop(Queue &Q, uint64_t &r, int32_t &idx, int32_t &gen) {
-    const uint64_t a = Q.s.n > 0 ? Q.s.rank[0] : ~0ull, b = Q.g.n > 0 ? Q.g.rank[0] : ~0ull;
-    if (a <= b) hpop(Q.s, r, idx, gen);
-    else hpop(Q.g, r, idx, gen);
+__device__ HEnt qpop(Queue &Q) {
+    const uint64_t a = Q.s.n > 0 ? Q.s.e[0].mk : ~0ull, b = Q.g.n > 0 ? Q.g.e[0].mk : ~0ull;
+    return a <= b ? hpop(Q.s) : hpop(Q.g);
 }
 
 // After a non-leaf Refine_cell dropped a subtree two or more levels deep,
@@ -814,9 +807,10 @@ __device__ void qpop(Queue &Q, uint64_t &r, int32_t &idx, int32_t &gen) {
 // >= l0 + 3 in the four edge-adjacent level-l0 cells can now find one of the
 // new sons as a neighbour (or neighbour's neighbour) two levels coarser.  The
 // reference visits every leaf, so those ahead of the traversal are queued.
-__device__ void push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uint64_t cur_rank) {
+__device__ bool push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uint64_t cur_rank) {
     const int l0 = (int)(pk & 15u);
     const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
+    bool ok = true;
     for (int d = 0; d < 4; ++d) {
         uint64_t t;
         if (!shift_key(G, pk, dirs[d], t)) continue;
@@ -832,55 +826,58 @@ __device__ void push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uin
                 const int32_t c = hfind(P, ck);
                 if (c < 0) continue;
                 if (P.flags[c] & PF_LEAF) {
-                    const uint64_t r = dfs_rank(ck);
-                    if ((int)(ck & 15u) >= l0 + 3 && r > cur_rank) qpush(P, Q, r, c, P.gen[c]);
+                    if ((int)(ck & 15u) >= l0 + 3 && visit_rank(ck) > cur_rank) ok = qpush_leaf(Q, ck, c, P.gen[c]) && ok;
                 } else if (sp < 64) {
                     st[sp++] = ck;
                 } else {
-                    P.err[0] = 1;
+                    ok = false;
                 }
             }
         }
     }
+    return ok;
 }
-// Refine_cell (src/mesh.F90:199-260) of a leaf, or of a non-leaf whose old
-// subtree is dropped and whose new sons copy its stale value (counted in nl)
-__device__ void refine_pool(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t cur_rank, int32_t &nl) {
+// Refine_cell (src/mesh.F90:199-260) of a non-leaf whose old subtree is
+// dropped and whose new sons copy its stale value (counted in nl); one lane.
+// cur_rank is the visit rank of the leaf being visited.
+__device__ bool refine_nonleaf(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t cur_rank, int32_t &nl,
+                               int64_t &pn) {
     const uint64_t pk = P.key[p];
-    bool deep = false;
-    if (!(P.flags[p] & PF_LEAF)) {
-        nl += 1;
-        uint64_t st[64];
-        int sp = 0;
-        st[sp++] = pk;
-        while (sp > 0) {
-            const uint64_t k = st[--sp];
-            for (int q = 0; q < 4; ++q) {
-                int32_t s;
-                const int64_t pos = hpos(P, child_key(k, q), s);
-                if (pos < 0 || (s & SLOT_DEL)) continue;
-                if (!(P.flags[s] & PF_LEAF)) {
-                    if (k != pk) deep = true;
-                    if (sp < 64) st[sp++] = P.key[s];
-                    else P.err[0] = 1;
-                }
-                P.flags[s] |= PF_DELETED;
-                P.slot[pos] = s | SLOT_DEL;
+    bool deep = false, ok = true;
+    nl += 1;
+    uint64_t st[64];
+    int sp = 0;
+    st[sp++] = pk;
+    while (sp > 0) {
+        const uint64_t k = st[--sp];
+        for (int q = 0; q < 4; ++q) {
+            int32_t s;
+            const int64_t pos = hpos(P, child_key(k, q), s);
+            if (pos < 0 || (s & SLOT_DEL)) continue;
+            if (!(P.flags[s] & PF_LEAF)) {
+                if (k != pk) deep = true;
+                if (sp < 64) st[sp++] = P.key[s];
+                else ok = false;
             }
+            P.flags[s] |= PF_DELETED;
+            P.slot[pos] = s | SLOT_DEL;
         }
     }
     P.flags[p] = 0;   // internal, value kept
     const double4 v = P.val[p];
     for (int q = 0; q < 4; ++q) {
         const uint64_t ck = child_key(pk, q);
-        const int32_t c = hinsert(P, ck, v);
-        if (c < 0) { P.err[0] = 1; return; }
-        const uint64_t r = dfs_rank(ck);
-        if (r > cur_rank) qpush(P, Q, r, c, P.gen[c]);
+        const int32_t c = hinsert(P, ck, v, pn);
+        if (c < 0) return false;
+        if (visit_rank(ck) > cur_rank) ok = qpush_leaf(Q, ck, c, P.gen[c]) && ok;
     }
-    if (deep) push_ring(P, G, Q, pk, cur_rank);
+    if (deep) ok = push_ring(P, G, Q, pk, cur_rank) && ok;
+    return ok;
 }
-constexpr int GM4_BATCH = 8;
+constexpr int GM4_BATCH = 8;      // items looked at together
+constexpr int GM4_STAGE = 16;     // items merged but not consumed yet
+constexpr int GM4_TWIN = 64;      // trigger window in shared memory
+constexpr int GM4_UP = 4;         // ancestors probed at once by a lookup
 constexpr int GM4_SHEAP = 8192;   // entries of the shared-memory heap (16 B each)
 
 // Is the node with key s (or the position s stands for) inside node r?
@@ -894,17 +891,40 @@ __device__ __forceinline__ bool key_inside(uint64_t r, uint64_t s) {
 
 // A lookup from key k towards d starts at the shifted key S and walks up to
 // the first existing node; refining or dropping node R changes it only when
-// S lies inside R.  sk = S (or ~0 when the shift leaves the grid).
+// S lies inside R.  sk = S (or ~0 when the shift leaves the grid).  S and its
+// next GM4_UP - 1 ancestors are probed at once (their first probes are
+// independent loads), then the walk goes on from there if none exists.
 __device__ __forceinline__ int32_t lookup_from(const Pool &P, const Geometry &G, uint64_t k, int d, uint64_t &nk,
                                                uint64_t &sk) {
     uint64_t t;
     if (!shift_key(G, k, d, t)) { sk = ~0ull; return -1; }
     sk = t;
     for (;;) {
-        const int32_t i = hfind(P, t);
-        if (i >= 0) { nk = t; return i; }
-        if ((t & 15u) == 0) return -1;
-        t = parent_key(t);
+        const int lt = (int)(t & 15u);
+        uint64_t c[GM4_UP], h[GM4_UP], q[GM4_UP];
+        int32_t s[GM4_UP];
+#pragma unroll
+        for (int j = 0; j < GM4_UP; ++j) {
+            c[j] = j == 0 ? t : (j <= lt ? parent_key(c[j - 1]) : c[j - 1]);
+            h[j] = hmix(c[j]) & P.mask;
+        }
+#pragma unroll
+        for (int j = 0; j < GM4_UP; ++j) {
+            s[j] = -1;
+            q[j] = 0;
+            if (j <= lt) {
+                s[j] = P.slot[h[j]];
+                q[j] = P.skey[h[j]];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < GM4_UP; ++j) {
+            if (j > lt) return -1;
+            const int32_t i = hfind_rest(P, c[j], h[j], s[j], q[j]);
+            if (i >= 0) { nk = c[j]; return i; }
+        }
+        if (lt < GM4_UP) return -1;   // level 0 was probed
+        t = parent_key(c[GM4_UP - 1]);
     }
 }
 struct Look {
@@ -931,169 +951,234 @@ __device__ __forceinline__ Look shfl_look(const Look &L, int src) {
     return o;
 }
 
-// Refine_cell of pool node p by the warp: a leaf's four sons are inserted by
-// lanes 0..3 at once, a non-leaf (rare) by lane 0 alone.  Returns false when
-// the pool or the queue overflowed.
+// Refine_cell of pool node p (key pk) by the warp.  Lanes 0..3 read the
+// node's flags and value and make the first probe for their son's key at
+// once.  A leaf's sons are then stored by those lanes: a son found in the
+// table (dropped earlier) is revived, the others take new pool entries and
+// the first empty slot of their probe sequence.  Sons whose sequences share
+// that slot take it one at a time, lowest lane first, the others probing on
+// past it.  A non-leaf (rare) is refined by lane 0 alone.  pn (the pool
+// size) is uniform.  Returns false when the pool or the queue overflowed.
 __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t pk, uint64_t cur_rank,
-                            int32_t &nonleaf) {
+                            int32_t &nonleaf, int64_t &pn) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const uint8_t fp = (uint8_t)__shfl_sync(FULL, lane == 0 ? (int)P.flags[p] : 0, 0);
+    const bool son = lane < 4;
+    int fp = 0;
+    double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+    uint64_t ck = 0, h = 0, q = 0;
+    int32_t s = -1;
+    if (son) {
+        fp = P.flags[p];
+        v = P.val[p];
+        ck = child_key(pk, lane);
+        h = hmix(ck) & P.mask;
+        s = P.slot[h];
+        q = P.skey[h];
+    }
+    fp = __shfl_sync(FULL, fp, 0);
+    bool ok = true;
     if (!(fp & PF_LEAF)) {
-        if (lane == 0) refine_pool(P, G, Q, p, cur_rank, nonleaf);
+        int e = 0;
+        if (lane == 0) e = refine_nonleaf(P, G, Q, p, cur_rank, nonleaf, pn) ? 0 : 1;
+        ok = __shfl_sync(FULL, e, 0) == 0;
+        pn = __shfl_sync(FULL, pn, 0);
     } else {
-        int32_t c = -1, gen = 0;
-        uint64_t ck = 0;
-        if (lane < 4) {
-            const double4 v = P.val[p];
-            ck = child_key(pk, lane);
-            c = hinsert_atomic(P, ck, v, gen);
+        // the son's own slot (a dropped node), or the first empty slot
+        bool found = false;
+        if (son) {
+            for (uint64_t probe = 0; probe <= P.mask; ++probe) {
+                if (s == -1) break;
+                if (q == ck) { found = true; break; }
+                h = (h + 1) & P.mask;
+                s = P.slot[h];
+                q = P.skey[h];
+            }
         }
-        __syncwarp();
-        const unsigned bad = __ballot_sync(FULL, lane < 4 && c < 0);
-        if (lane == 0) {
-            P.flags[p] = 0;   // internal, value kept
-            if (bad) P.err[0] = 1;
+        const unsigned nm = __ballot_sync(FULL, son && !found);
+        int32_t i = -1, gen = 0;
+        if (found) {
+            i = s & ~SLOT_DEL;
+            gen = P.gen[i] + 1;
+        } else if (son) {
+            i = (int32_t)(pn + __popc(nm & ((1u << lane) - 1u)));
         }
-        for (int q = 0; q < 4 && !bad; ++q) {
-            const int32_t cq = __shfl_sync(FULL, c, q);
-            const int32_t gq = __shfl_sync(FULL, gen, q);
-            const uint64_t kq = __shfl_sync(FULL, ck, q);
-            const uint64_t r = dfs_rank(kq);
-            if (lane == 0 && r > cur_rank) qpush(P, Q, r, cq, gq);
+        pn += __popc(nm);
+        ok = pn <= P.cap;
+        if (ok) {
+            bool need = son && !found;
+            for (;;) {
+                const unsigned pend = __ballot_sync(FULL, need);
+                if (!pend) break;
+                if (need) {
+                    const unsigned peers = __match_any_sync(pend, h);
+                    if (__ffs(peers) - 1 == lane) {
+                        P.slot[h] = i;
+                        P.skey[h] = ck;
+                        need = false;
+                    }
+                }
+                __syncwarp();
+                if (need) {   // a lower lane took the slot: probe on to the next empty one
+                    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
+                        h = (h + 1) & P.mask;
+                        if (P.slot[h] == -1) break;
+                    }
+                }
+            }
+            if (son) {
+                if (found) P.slot[h] = i;
+                else P.key[i] = ck;
+                P.flags[i] = PF_LEAF;
+                P.gen[i] = gen;
+                P.val[i] = v;
+            }
+            if (lane == 0) P.flags[p] = 0;   // internal, value kept
+            // the sons ahead of the traversal are queued
+            const bool ahead = son && visit_rank(ck) > cur_rank;
+            int e = 0;
+            for (int k = 0; k < 4; ++k) {
+                const int32_t ik = __shfl_sync(FULL, i, k);
+                const int32_t gk = __shfl_sync(FULL, gen, k);
+                const uint64_t kk = __shfl_sync(FULL, ck, k);
+                const bool ak = __shfl_sync(FULL, (int)ahead, k) != 0;
+                if (lane == 0 && ak && !qpush_leaf(Q, kk, ik, gk)) e = 1;
+            }
+            ok = __shfl_sync(FULL, e, 0) == 0;
         }
     }
     Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
     Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+    if (!ok && lane == 0) P.err[0] = 1;
     __syncwarp();
-    return __shfl_sync(FULL, lane == 0 ? P.err[0] : 0, 0) == 0;
+    return ok;
 }
 
 // gridmodify4 (src/mesh.F90:355-395) over one pass of the tree, by one
-// warp.  The leaves that can act (the initial triggers, sorted by traversal
+// warp.  The leaves that can act (the initial triggers, sorted by visit
 // rank, and every leaf queued ahead of the traversal) are visited in
-// traversal order.  Up to 8 upcoming trigger leaves are looked at together:
-// 4 lanes per leaf find its right/left/up/down neighbour and that
-// neighbour's neighbour at once, and each lane tells whether its direction
-// would refine something.  The leaves before the first one that refines
-// have no effect but being visited, so they are marked in parallel; the
-// first one that refines is then applied alone, in order, and the batch
-// ends there.  Within that leaf a lookup starts at a shifted key and walks
-// up to the first existing node, so a refinement (or a dropped subtree) of
-// node R can change a later lookup only when its start lies inside R: those
-// lookups, and only those, are repeated.  The queue of leaves ahead lives in
-// shared memory.
+// traversal order.  Up to 8 upcoming leaves are looked at together: 4 lanes
+// per leaf find its right/left/up/down neighbour and that neighbour's
+// neighbour at once, and each lane tells whether its direction would refine
+// something.  The leaves before the first one that refines have no effect
+// but being visited, so they are marked in parallel; the first one that
+// refines is then applied alone, in order, and the batch ends there; the
+// leaves after it stay staged for the next batch.  Within that leaf a
+// lookup starts at a shifted key and walks up to the first existing node,
+// so a refinement (or a dropped subtree) of node R can change a later lookup
+// only when its start lies inside R: those lookups, and only those, are
+// repeated.  The queue of leaves ahead, the staged leaves and a window of
+// the triggers live in shared memory.
 __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint64_t *__restrict__ trank,
                                                  const int32_t *__restrict__ tidx, int64_t ntrig, int64_t max_steps) {
     extern __shared__ __align__(16) unsigned char gm4_smem[];
+    __shared__ HEnt items[GM4_BATCH];
+    __shared__ HEnt stg[2][GM4_STAGE];
+    __shared__ uint64_t twr[GM4_TWIN];
+    __shared__ int32_t twx[GM4_TWIN];
     const int lane = threadIdx.x, grp = lane >> 2, tl = lane & 3;
     const unsigned FULL = 0xffffffffu;
     Queue Q;
-    Q.s.rank = reinterpret_cast<uint64_t *>(gm4_smem);
-    Q.s.idx = reinterpret_cast<int32_t *>(Q.s.rank + GM4_SHEAP);
-    Q.s.gen = Q.s.idx + GM4_SHEAP;
+    Q.s.e = reinterpret_cast<HEnt *>(gm4_smem);
     Q.s.cap = GM4_SHEAP;
     Q.s.n = 0;
-    Q.g.rank = P.hrank;
-    Q.g.idx = P.hidx;
-    Q.g.gen = P.hgen;
+    Q.g.e = P.heap;
     Q.g.cap = P.hcap;
     Q.g.n = 0;
-    int64_t ti = 0;   // uniform
+    int64_t pn = *P.n;     // pool size (uniform; stored at the end)
+    int64_t tg = 0;        // next trigger to bring into the window
+    int tw_n = 0, tp = 0;  // triggers in the window, next one to merge
+    int ns = 0, sb = 0;    // staged items, staging buffer in use
     int64_t step = 0;
     int32_t visits = 0, nonleaf = 0, refines = 0;   // lane 0's counts, stored at the end
-    __shared__ uint64_t it_rank[GM4_BATCH];
-    __shared__ int32_t it_idx[GM4_BATCH], it_gen[GM4_BATCH];
-    __shared__ int8_t it_heap[GM4_BATCH];
-    int tk_extra = 0;   // lane 0: triggers taken into the batch (duplicates included)
+    bool ok = true;
     for (;; ++step) {
         if (step >= max_steps) { if (lane == 0) P.err[3] = 1; break; }
-        // the next items in traversal order: the queued leaves and the
-        // triggers merged by rank (lane 0), up to GM4_BATCH of them
-        uint64_t tr = ~0ull;
-        int32_t tx = -1;
-        {
-            const int64_t j = ti + lane;
-            if (lane < GM4_BATCH && j < ntrig) { tr = trank[j]; tx = tidx[j]; }
+        // keep at least a batch of triggers in the window
+        if (tw_n - tp < GM4_BATCH && tg < ntrig) {
+            const int rem = tw_n - tp;
+            uint64_t rr = 0;
+            int32_t rx = 0;
+            if (lane < rem) { rr = twr[tp + lane]; rx = twx[tp + lane]; }
+            __syncwarp();
+            if (lane < rem) { twr[lane] = rr; twx[lane] = rx; }
+            const int nl = (int)min((int64_t)(GM4_TWIN - rem), ntrig - tg);
+            for (int j = lane; j < nl; j += 32) { twr[rem + j] = trank[tg + j]; twx[rem + j] = tidx[tg + j]; }
+            tg += nl;
+            tw_n = rem + nl;
+            tp = 0;
+            __syncwarp();
         }
-        int cnt = 0;
-        {
-            // lane 0 merges; the trigger window is broadcast lane by lane
-            uint64_t wr[GM4_BATCH];
-            int32_t wx[GM4_BATCH];
-#pragma unroll
-            for (int q = 0; q < GM4_BATCH; ++q) {
-                wr[q] = __shfl_sync(FULL, tr, q);
-                wx[q] = __shfl_sync(FULL, tx, q);
-            }
-            if (lane == 0) {
-                int k = 0;   // triggers taken
-                uint64_t last_r = ~0ull;
-                int32_t last_i = -1;
-                while (cnt < GM4_BATCH) {
-                    const uint64_t h = qtop(Q);
-                    const uint64_t t = k < GM4_BATCH ? wr[k] : ~0ull;
-                    if (h == ~0ull && t == ~0ull) break;
-                    uint64_t rr;
-                    int32_t ii, gg;
-                    int8_t fromq;
-                    if (t != ~0ull && t <= h) {   // on a tie the trigger comes first
-                        rr = t; ii = wx[k]; gg = 0; fromq = 0;
-                        ++k;
-                    } else {
-                        qpop(Q, rr, ii, gg);
-                        fromq = 1;
-                    }
-                    // the same leaf twice (queued and a trigger, or queued twice):
-                    // visited once, as in the reference's single traversal
-                    if (rr == last_r && ii == last_i) continue;
-                    last_r = rr;
-                    last_i = ii;
-                    it_rank[cnt] = rr; it_idx[cnt] = ii; it_gen[cnt] = gg; it_heap[cnt] = fromq;
-                    ++cnt;
+        // the next items in traversal order: staged items, queued leaves and
+        // triggers merged by lane 0, up to GM4_BATCH of them
+        int cnt = 0, sp = 0;
+        if (lane == 0) {
+            const HEnt *so = stg[sb];
+            uint64_t last_r = ~0ull;
+            int32_t last_i = -1;
+            while (cnt < GM4_BATCH) {
+                const uint64_t a = sp < ns ? so[sp].mk : ~0ull;
+                const uint64_t b = qtop(Q);
+                const uint64_t c = tp < tw_n ? twr[tp] * 2 : ~0ull;
+                HEnt x;
+                if (c <= a && c <= b) {
+                    if (c == ~0ull) break;
+                    x.mk = c; x.idx = twx[tp]; x.gen = 0;
+                    ++tp;
+                } else if (a <= b) {
+                    x = so[sp++];
+                } else {
+                    x = qpop(Q);
                 }
-                // a skipped duplicate trigger still counts as taken
-                tk_extra = k;
+                // the same leaf twice (queued and a trigger, or queued twice):
+                // visited once, as in the reference's single traversal
+                if ((x.mk >> 1) == last_r && x.idx == last_i) continue;
+                last_r = x.mk >> 1;
+                last_i = x.idx;
+                items[cnt++] = x;
             }
         }
         cnt = __shfl_sync(FULL, cnt, 0);
+        sp = __shfl_sync(FULL, sp, 0);
+        tp = __shfl_sync(FULL, tp, 0);
         Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
         Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
         __syncwarp();
         if (cnt == 0) break;
-        uint64_t r = 0;
-        int32_t c = -1, gen = 0;
-        if (grp < cnt) { r = it_rank[grp]; c = it_idx[grp]; gen = it_gen[grp]; }
-        // lookups and decisions: lane (grp, tl) handles direction tl of item grp
+        // lookups and decisions: lane (grp, tl) handles direction tl of item
+        // grp; the item's key comes from its rank, so its flags and
+        // generation load while the lookups run
+        HEnt it;
+        it.mk = 0; it.idx = -1; it.gen = 0;
+        if (grp < cnt) it = items[grp];
+        const uint64_t vr = it.mk >> 1;
+        const uint64_t ck = key_of_visit_rank(vr);
         bool valid = false, acts = false;
-        uint64_t ck = 0;
+        uint8_t fl = 0;
         Look L;
         L.nb = L.nn = -1;
         L.nbk = L.nnk = 0;
         L.snb = L.snn = ~0ull;
-        uint8_t fl = 0;
         if (grp < cnt) {
-            fl = P.flags[c];
-            const int32_t gc = P.gen[c];
-            ck = P.key[c];
-            valid = gc == gen && (fl & (PF_LEAF | PF_DELETED | PF_VISITED)) == PF_LEAF;
-            if (valid) {
-                dir_lookups(P, G, ck, tl, L);
-                const int lc = (int)(ck & 15u);
-                acts = (L.nb >= 0 && (int)(L.nbk & 15u) <= lc - 2) || (L.nn >= 0 && (int)(L.nnk & 15u) <= lc - 2);
-            }
+            fl = P.flags[it.idx];
+            const int32_t gc = P.gen[it.idx];
+            dir_lookups(P, G, ck, tl, L);
+            valid = gc == it.gen && (fl & (PF_LEAF | PF_DELETED | PF_VISITED)) == PF_LEAF;
+            const int lc = (int)(ck & 15u);
+            acts = valid &&
+                   ((L.nb >= 0 && (int)(L.nbk & 15u) <= lc - 2) || (L.nn >= 0 && (int)(L.nnk & 15u) <= lc - 2));
         }
         const unsigned am = __ballot_sync(FULL, acts);
         const int fa = am ? (__ffs(am) - 1) >> 2 : cnt;   // first item that refines
         // items before it: visited, nothing else
         const unsigned vm = __ballot_sync(FULL, valid && tl == 0 && grp < fa);
-        if (valid && tl == 0 && grp < fa) P.flags[c] = fl | PF_VISITED;
+        if (valid && tl == 0 && grp < fa) P.flags[it.idx] = fl | PF_VISITED;
         if (lane == 0) visits += __popc(vm);
         int consumed = fa;
         if (fa < cnt) {
             consumed = fa + 1;
-            const uint64_t rb = __shfl_sync(FULL, r, fa * 4);
-            const int32_t cb = __shfl_sync(FULL, c, fa * 4);
+            const uint64_t rb = __shfl_sync(FULL, vr, fa * 4);
+            const int32_t cb = __shfl_sync(FULL, it.idx, fa * 4);
             const uint64_t kb = __shfl_sync(FULL, ck, fa * 4);
             const uint8_t fb = (uint8_t)__shfl_sync(FULL, (int)fl, fa * 4);
             const int lc = (int)(kb & 15u);
@@ -1103,7 +1188,7 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
             }
             uint64_t refined[8];   // uniform: nodes refined by this leaf
             int nref = 0;
-            for (int t = 0; t < 4; ++t) {
+            for (int t = 0; t < 4 && ok; ++t) {
                 Look Lt = shfl_look(L, fa * 4 + t);
                 // repeat the lookups whose start lies inside a node refined earlier
                 bool re_nb = false, re_nn = false;
@@ -1123,34 +1208,45 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
                 // has four sons), and refining it leaves the lookup of its own
                 // neighbour unchanged (that start lies outside it)
                 if ((int)(Lt.nbk & 15u) <= lc - 2) {
-                    if (!refine_warp(P, G, Q, Lt.nb, Lt.nbk, rb, nonleaf)) return;
+                    ok = refine_warp(P, G, Q, Lt.nb, Lt.nbk, rb, nonleaf, pn);
                     refined[nref++] = Lt.nbk;
                     ++refines;
                 }
-                if (Lt.nn >= 0 && (int)(Lt.nnk & 15u) <= lc - 2) {
-                    if (!refine_warp(P, G, Q, Lt.nn, Lt.nnk, rb, nonleaf)) return;
+                if (ok && Lt.nn >= 0 && (int)(Lt.nnk & 15u) <= lc - 2) {
+                    ok = refine_warp(P, G, Q, Lt.nn, Lt.nnk, rb, nonleaf, pn);
                     refined[nref++] = Lt.nnk;
                     ++refines;
                 }
             }
+            if (!ok) break;
         }
-        // unconsumed queued leaves go back; consumed triggers advance ti.  When
-        // every item is consumed, so are the triggers that were skipped as
-        // duplicates; otherwise ti stops at the first unconsumed trigger
-        if (lane == 0) {
-            int ntr = 0;
-            for (int q = 0; q < cnt; ++q) {
-                if (q < consumed) ntr += it_heap[q] ? 0 : 1;
-                else if (it_heap[q]) qpush(P, Q, it_rank[q], it_idx[q], it_gen[q]);
+        // the items not consumed stay staged, followed by the staged items
+        // that were not merged (all of them later in traversal order); what
+        // does not fit goes back to the queue
+        {
+            const HEnt *so = stg[sb];
+            HEnt *sn = stg[sb ^ 1];
+            const int nu = cnt - consumed, tot = nu + ns - sp;
+            if (lane < nu) sn[lane] = items[consumed + lane];
+            else if (lane < tot && lane < GM4_STAGE) sn[lane] = so[sp + lane - nu];
+            __syncwarp();
+            int e = 0;
+            if (lane == 0)
+                for (int j = GM4_STAGE; j < tot; ++j)
+                    if (!qpush(Q, so[sp + j - nu])) e = 1;
+            if (__shfl_sync(FULL, e, 0)) {
+                if (lane == 0) P.err[0] = 1;
+                break;
             }
-            ti += consumed == cnt ? tk_extra : ntr;
+            ns = tot < GM4_STAGE ? tot : GM4_STAGE;
+            sb ^= 1;
+            Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
+            Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+            __syncwarp();
         }
-        ti = __shfl_sync(FULL, ti, 0);
-        Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
-        Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
-        __syncwarp();
     }
     if (lane == 0) {
+        *P.n = pn;
         P.err[1] = visits;
         P.err[2] = nonleaf;
         P.err[4] = refines;
@@ -1301,24 +1397,24 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     if (ntrig == 0) return FDM_OK;
     // key order is Morton order (son4 before son3); the traversal visits
     // son3 first, so sort the triggers by traversal rank
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, srk, rk, sidx, idx, (int)ntrig, 0, 64, h->s));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, srk, rk, sidx, idx, (int)ntrig, 0, 56, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, srk, rk, sidx, idx, (int)ntrig, 0, 64, h->s));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, srk, rk, sidx, idx, (int)ntrig, 0, 56, h->s));
     // pool + hash of all nodes, room for new ones
     const int64_t cap = 2 * n + 4096;
     uint64_t slots = 1;
     while (slots < (uint64_t)(2 * cap)) slots <<= 1;
     Carve cp;
     cp.add(cap * 8); cp.add(cap); cp.add(cap * 4); cp.add(cap * 32); cp.add(slots * 4); cp.add(16);
-    cp.add(cap * 8); cp.add(cap * 4); cp.add(cap * 4); cp.add(32); cp.add(slots * 8);
+    cp.add(cap * sizeof(HEnt)); cp.add(32); cp.add(slots * 8);
     FDM_CK(h, h->amr[16].ensure(cp.total));
     DevBuf &pb = h->amr[16];
     Pool P;
     P.key = cp.at<uint64_t>(pb, 0); P.flags = cp.at<uint8_t>(pb, 1); P.gen = cp.at<int32_t>(pb, 2);
     P.val = cp.at<double4>(pb, 3); P.slot = cp.at<int32_t>(pb, 4); P.n = cp.at<int64_t>(pb, 5);
-    P.hrank = cp.at<uint64_t>(pb, 6); P.hidx = cp.at<int32_t>(pb, 7); P.hgen = cp.at<int32_t>(pb, 8);
-    P.err = cp.at<int32_t>(pb, 9);
-    P.skey = cp.at<uint64_t>(pb, 10);
+    P.heap = cp.at<HEnt>(pb, 6);
+    P.err = cp.at<int32_t>(pb, 7);
+    P.skey = cp.at<uint64_t>(pb, 8);
     P.mask = slots - 1;
     P.cap = cap;
     P.hcap = cap;
@@ -1330,12 +1426,18 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     // every step consumes a trigger or a queued leaf, or ends the pass
     const size_t gm4_smem = (size_t)GM4_SHEAP * 16;
     FDM_CK(h, cudaFuncSetAttribute(k_gm4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gm4_smem));
+    for (cudaEvent_t &e : h->gm4_ev)
+        if (!e) FDM_CK(h, cudaEventCreate(&e));
+    FDM_CK(h, cudaEventRecord(h->gm4_ev[0], h->s));
     k_gm4_warp<<<1, 32, gm4_smem, h->s>>>(P, h->G, rk, idx, ntrig, ntrig + GM4_SHEAP + P.hcap + 16);
+    FDM_CK(h, cudaEventRecord(h->gm4_ev[1], h->s));
     int32_t herr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t pn = 0;
     FDM_CK(h, cudaMemcpyAsync(herr, P.err, 32, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaMemcpyAsync(&pn, P.n, 8, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
+    float gm4_t = 0.f;
+    if (cudaEventElapsedTime(&gm4_t, h->gm4_ev[0], h->gm4_ev[1]) == cudaSuccess) h->gm4_ms += gm4_t;
     if (herr[0]) { h->err = "gridmodify4 cascade exceeded its node pool"; return FDM_ERR_UNSUPPORTED; }
     if (herr[3]) { h->err = "gridmodify4 replay did not finish"; return FDM_ERR_UNSUPPORTED; }
     h->gm4_visits += herr[1];

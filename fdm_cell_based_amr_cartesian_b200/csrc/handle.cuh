@@ -102,6 +102,8 @@ struct fdm_handle {
     // device-timeline phases of the last regrid (events recorded on the stream)
     static constexpr int AMR_PHASES = 5;
     cudaEvent_t amr_ev[AMR_PHASES + 1] = {};
+    cudaEvent_t gm4_ev[2] = {};   // around the gridmodify4 replay kernel
+    double gm4_ms = 0.0;          // its device time, summed over all passes
     double amr_phase_ms[AMR_PHASES] = {};
     double amr_phase_total_ms[AMR_PHASES] = {};   // summed over all regrids
 

@@ -250,6 +250,8 @@ void fdm_destroy(fdm_handle *h) {
     for (auto &t : h->tmp) t.release();
     for (cudaEvent_t e : h->amr_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->gm4_ev)
+        if (e) cudaEventDestroy(e);
     for (int b = 0; b < 2; ++b) {
         cudaEvent_t ev[4] = {h->in_ready[b], h->in_free[b], h->out_ready[b], h->out_free[b]};
         for (cudaEvent_t e : ev)
@@ -581,6 +583,7 @@ int fdm_get_counters(fdm_handle *h, fdm_counters *c) {
     c->n_gm4_triggers = h->gm4_triggers;
     c->n_gm4_refines = h->gm4_refines;
     c->n_gm4_steps = h->gm4_steps;
+    c->gm4_replay_us = (int64_t)(h->gm4_ms * 1e3);
     return FDM_OK;
 }
 

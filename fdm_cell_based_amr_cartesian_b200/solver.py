@@ -61,7 +61,7 @@ class FdmCounters(ctypes.Structure):
                 ("n_gm1_iterations", ctypes.c_int64), ("n_gm4_visits", ctypes.c_int64),
                 ("n_gm4_nonleaf", ctypes.c_int64), ("n_gm4_triggers", ctypes.c_int64),
                 ("n_gm4_refines", ctypes.c_int64), ("n_gm4_steps", ctypes.c_int64),
-                ("reserved", ctypes.c_int64 * 1)]
+                ("gm4_replay_us", ctypes.c_int64)]
 
 
 _lib = None

@@ -130,7 +130,7 @@ typedef struct fdm_counters {
     int64_t n_gm4_triggers;    /* gridmodify4: leaves marked able to act at pass start */
     int64_t n_gm4_refines;     /* gridmodify4: Refine_cell calls */
     int64_t n_gm4_steps;       /* gridmodify4: replay iterations (batches and queued leaves) */
-    int64_t reserved[1];
+    int64_t gm4_replay_us;     /* gridmodify4: device time of the replay kernel, microseconds */
 } fdm_counters;
 
 /* ------------------------------------------------------------- lifecycle */
