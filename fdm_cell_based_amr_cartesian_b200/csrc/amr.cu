@@ -742,15 +742,24 @@ __device__ __forceinline__ int32_t hfind_rest(const Pool &P, uint64_t k, uint64_
     return -1;
 }
 
-// Leaves to visit ahead of the traversal: a binary min-heap on mk in shared
-// memory, spilling into a second heap in global memory when full.  One lane
-// operates on it; the sizes are kept uniform by the caller.
+constexpr int GM4_BATCH = 8;      // items looked at together
+constexpr int GM4_TWIN = 64;      // trigger window in shared memory
+constexpr int GM4_UP = 4;         // ancestors probed at once by a lookup
+constexpr int GM4_SQ = 4096;      // sorted queue in shared memory (16 B entries)
+
+// Leaves to visit ahead of the traversal, ordered by mk: a sorted array
+// q[head, tail) in shared memory that the warp inserts into and consumes
+// from the front, and a binary min-heap in global memory for what does not
+// fit there and for the (rare) entries that one lane queues alone.  The
+// sizes are kept uniform across the warp.
 struct Heap {
     HEnt *e;
     int64_t cap, n;
 };
 struct Queue {
-    Heap s, g;
+    HEnt *q;
+    int head, tail;
+    Heap g;
 };
 __device__ bool hpush(Heap &H, const HEnt &x) {
     if (H.n >= H.cap) return false;
@@ -785,21 +794,109 @@ __device__ HEnt hpop(Heap &H) {
     if (hn > 0) H.e[i] = last;
     return top;
 }
-__device__ __forceinline__ uint64_t qtop(const Queue &Q) {
-    const uint64_t a = Q.s.n > 0 ? Q.s.e[0].mk : ~0ull, b = Q.g.n > 0 ? Q.g.e[0].mk : ~0ull;
-    return a < b ? a : b;
-}
-__device__ bool qpush(Queue &Q, const HEnt &x) { return hpush(Q.s, x) || hpush(Q.g, x); }
-__device__ bool qpush_leaf(Queue &Q, uint64_t key, int32_t idx, int32_t gen) {
+__device__ __forceinline__ HEnt queued_leaf(uint64_t key, int32_t idx, int32_t gen) {
     HEnt x;
     x.mk = visit_rank(key) * 2 + 1;
     x.idx = idx;
     x.gen = gen;
-    return qpush(Q, x);
+    return x;
 }
-__device__ HEnt qpop(Queue &Q) {
-    const uint64_t a = Q.s.n > 0 ? Q.s.e[0].mk : ~0ull, b = Q.g.n > 0 ? Q.g.e[0].mk : ~0ull;
-    return a <= b ? hpop(Q.s) : hpop(Q.g);
+// one lane: into the global heap
+__device__ bool gpush_leaf(Queue &Q, uint64_t key, int32_t idx, int32_t gen) {
+    return hpush(Q.g, queued_leaf(key, idx, gen));
+}
+
+// The warp inserts the entries x of the lanes with has (at most 4, lanes
+// 0..3) into the sorted array: entries at or above each new one move up by
+// the number of new ones below them, top chunk first; each new entry lands
+// after the old entries with mk not above its own.  When the array is full
+// its upper half moves to the global heap first.  Returns false when the
+// global heap overflowed.
+__device__ bool sq_insert(Queue &Q, const HEnt &x, bool has) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned hm = __ballot_sync(FULL, has);
+    const int k = __popc(hm);
+    if (k == 0) return true;
+    bool ok = true;
+    if (Q.tail + k > GM4_SQ) {
+        // move [head, tail) down to 0, ascending chunks (the target lies below the source)
+        const int n = Q.tail - Q.head;
+        if (Q.head > 0) {
+            for (int b = 0; b < n; b += 32) {
+                HEnt y;
+                if (b + lane < n) y = Q.q[Q.head + b + lane];
+                __syncwarp();
+                if (b + lane < n) Q.q[b + lane] = y;
+                __syncwarp();
+            }
+            Q.head = 0;
+            Q.tail = n;
+        }
+        if (Q.tail + k > GM4_SQ) {   // the upper half goes to the global heap
+            int e = 0;
+            if (lane == 0)
+                for (int j = n / 2; j < n; ++j)
+                    if (!hpush(Q.g, Q.q[j])) e = 1;
+            Q.tail = n / 2;
+            Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+            ok = __shfl_sync(FULL, e, 0) == 0;
+            __syncwarp();
+        }
+    }
+    uint64_t m[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) m[j] = __shfl_sync(FULL, x.mk, j);
+    // rank among the new entries (equal keys by lane) and place among the old ones
+    int rank = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        rank += ((hm >> j) & 1u) && (m[j] < x.mk || (m[j] == x.mk && j < lane)) ? 1 : 0;
+    int ub = Q.head;
+    if (has) {
+        int hi = Q.tail;
+        while (ub < hi) {
+            const int mid = (ub + hi) >> 1;
+            if (Q.q[mid].mk <= x.mk) ub = mid + 1;
+            else hi = mid;
+        }
+    }
+    for (int b = Q.tail - 32;; b -= 32) {
+        const int p = b + lane;
+        const bool in = p >= Q.head;
+        HEnt y;
+        int s = 0;
+        if (in) {
+            y = Q.q[p];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) s += ((hm >> j) & 1u) && m[j] < y.mk ? 1 : 0;
+        }
+        __syncwarp();
+        if (in && s > 0) Q.q[p + s] = y;
+        __syncwarp();
+        if (b <= Q.head || __any_sync(FULL, in && s == 0)) break;
+    }
+    if (has) Q.q[ub + rank] = x;
+    Q.tail += k;
+    __syncwarp();
+    return ok;
+}
+// Entries of the global heap that belong among the first GM4_BATCH come
+// into the sorted array before a merge
+__device__ bool sq_pull(Queue &Q) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    bool ok = true;
+    while (Q.g.n > 0 && ok) {
+        const uint64_t kth = Q.tail - Q.head >= GM4_BATCH ? Q.q[Q.head + GM4_BATCH - 1].mk : ~0ull;
+        if (Q.g.e[0].mk >= kth) break;
+        HEnt x;
+        if (lane == 0) x = hpop(Q.g);
+        Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+        __syncwarp();
+        ok = sq_insert(Q, x, lane == 0);
+    }
+    return ok;
 }
 
 // After a non-leaf Refine_cell dropped a subtree two or more levels deep,
@@ -826,7 +923,7 @@ __device__ bool push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uin
                 const int32_t c = hfind(P, ck);
                 if (c < 0) continue;
                 if (P.flags[c] & PF_LEAF) {
-                    if ((int)(ck & 15u) >= l0 + 3 && visit_rank(ck) > cur_rank) ok = qpush_leaf(Q, ck, c, P.gen[c]) && ok;
+                    if ((int)(ck & 15u) >= l0 + 3 && visit_rank(ck) > cur_rank) ok = gpush_leaf(Q, ck, c, P.gen[c]) && ok;
                 } else if (sp < 64) {
                     st[sp++] = ck;
                 } else {
@@ -869,17 +966,11 @@ __device__ bool refine_nonleaf(Pool &P, const Geometry &G, Queue &Q, int32_t p, 
         const uint64_t ck = child_key(pk, q);
         const int32_t c = hinsert(P, ck, v, pn);
         if (c < 0) return false;
-        if (visit_rank(ck) > cur_rank) ok = qpush_leaf(Q, ck, c, P.gen[c]) && ok;
+        if (visit_rank(ck) > cur_rank) ok = gpush_leaf(Q, ck, c, P.gen[c]) && ok;
     }
     if (deep) ok = push_ring(P, G, Q, pk, cur_rank) && ok;
     return ok;
 }
-constexpr int GM4_BATCH = 8;      // items looked at together
-constexpr int GM4_STAGE = 16;     // items merged but not consumed yet
-constexpr int GM4_TWIN = 64;      // trigger window in shared memory
-constexpr int GM4_UP = 4;         // ancestors probed at once by a lookup
-constexpr int GM4_SHEAP = 8192;   // entries of the shared-memory heap (16 B each)
-
 // Is the node with key s (or the position s stands for) inside node r?
 __device__ __forceinline__ bool key_inside(uint64_t r, uint64_t s) {
     const int lr = (int)(r & 15u), ls = (int)(s & 15u);
@@ -1035,19 +1126,9 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
             }
             if (lane == 0) P.flags[p] = 0;   // internal, value kept
             // the sons ahead of the traversal are queued
-            const bool ahead = son && visit_rank(ck) > cur_rank;
-            int e = 0;
-            for (int k = 0; k < 4; ++k) {
-                const int32_t ik = __shfl_sync(FULL, i, k);
-                const int32_t gk = __shfl_sync(FULL, gen, k);
-                const uint64_t kk = __shfl_sync(FULL, ck, k);
-                const bool ak = __shfl_sync(FULL, (int)ahead, k) != 0;
-                if (lane == 0 && ak && !qpush_leaf(Q, kk, ik, gk)) e = 1;
-            }
-            ok = __shfl_sync(FULL, e, 0) == 0;
+            ok = sq_insert(Q, queued_leaf(ck, i, gen), son && visit_rank(ck) > cur_rank);
         }
     }
-    Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
     Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
     if (!ok && lane == 0) P.err[0] = 1;
     __syncwarp();
@@ -1057,38 +1138,36 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
 // gridmodify4 (src/mesh.F90:355-395) over one pass of the tree, by one
 // warp.  The leaves that can act (the initial triggers, sorted by visit
 // rank, and every leaf queued ahead of the traversal) are visited in
-// traversal order.  Up to 8 upcoming leaves are looked at together: 4 lanes
-// per leaf find its right/left/up/down neighbour and that neighbour's
-// neighbour at once, and each lane tells whether its direction would refine
+// traversal order.  The next 8 of them (from the sorted queue and the
+// trigger window, merged by the lanes at once) are looked at together: 4
+// lanes per leaf find its right/left/up/down neighbour and that neighbour's
+// neighbour, and each lane tells whether its direction would refine
 // something.  The leaves before the first one that refines have no effect
 // but being visited, so they are marked in parallel; the first one that
-// refines is then applied alone, in order, and the batch ends there; the
-// leaves after it stay staged for the next batch.  Within that leaf a
-// lookup starts at a shifted key and walks up to the first existing node,
-// so a refinement (or a dropped subtree) of node R can change a later lookup
-// only when its start lies inside R: those lookups, and only those, are
-// repeated.  The queue of leaves ahead, the staged leaves and a window of
-// the triggers live in shared memory.
+// refines is then applied alone, in order, and the batch ends there (the
+// leaves after it stay where they are for the next batch).  Within that
+// leaf a lookup starts at a shifted key and walks up to the first existing
+// node, so a refinement (or a dropped subtree) of node R can change a later
+// lookup only when its start lies inside R: those lookups, and only those,
+// are repeated.  A leaf that is both a trigger and queued is looked at
+// twice; the second look finds it visited.
 __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint64_t *__restrict__ trank,
                                                  const int32_t *__restrict__ tidx, int64_t ntrig, int64_t max_steps) {
     extern __shared__ __align__(16) unsigned char gm4_smem[];
     __shared__ HEnt items[GM4_BATCH];
-    __shared__ HEnt stg[2][GM4_STAGE];
     __shared__ uint64_t twr[GM4_TWIN];
     __shared__ int32_t twx[GM4_TWIN];
     const int lane = threadIdx.x, grp = lane >> 2, tl = lane & 3;
     const unsigned FULL = 0xffffffffu;
     Queue Q;
-    Q.s.e = reinterpret_cast<HEnt *>(gm4_smem);
-    Q.s.cap = GM4_SHEAP;
-    Q.s.n = 0;
+    Q.q = reinterpret_cast<HEnt *>(gm4_smem);
+    Q.head = Q.tail = 0;
     Q.g.e = P.heap;
     Q.g.cap = P.hcap;
     Q.g.n = 0;
     int64_t pn = *P.n;     // pool size (uniform; stored at the end)
     int64_t tg = 0;        // next trigger to bring into the window
     int tw_n = 0, tp = 0;  // triggers in the window, next one to merge
-    int ns = 0, sb = 0;    // staged items, staging buffer in use
     int64_t step = 0;
     int32_t visits = 0, nonleaf = 0, refines = 0;   // lane 0's counts, stored at the end
     bool ok = true;
@@ -1109,40 +1188,30 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
             tp = 0;
             __syncwarp();
         }
-        // the next items in traversal order: staged items, queued leaves and
-        // triggers merged by lane 0, up to GM4_BATCH of them
-        int cnt = 0, sp = 0;
-        if (lane == 0) {
-            const HEnt *so = stg[sb];
-            uint64_t last_r = ~0ull;
-            int32_t last_i = -1;
-            while (cnt < GM4_BATCH) {
-                const uint64_t a = sp < ns ? so[sp].mk : ~0ull;
-                const uint64_t b = qtop(Q);
-                const uint64_t c = tp < tw_n ? twr[tp] * 2 : ~0ull;
-                HEnt x;
-                if (c <= a && c <= b) {
-                    if (c == ~0ull) break;
-                    x.mk = c; x.idx = twx[tp]; x.gen = 0;
-                    ++tp;
-                } else if (a <= b) {
-                    x = so[sp++];
-                } else {
-                    x = qpop(Q);
-                }
-                // the same leaf twice (queued and a trigger, or queued twice):
-                // visited once, as in the reference's single traversal
-                if ((x.mk >> 1) == last_r && x.idx == last_i) continue;
-                last_r = x.mk >> 1;
-                last_i = x.idx;
-                items[cnt++] = x;
-            }
+        if (Q.g.n > 0 && !sq_pull(Q)) { ok = false; break; }
+        // the next items in traversal order: lanes 0..7 hold the first
+        // queued leaves, lanes 8..15 the first triggers; each finds its
+        // place among the other list's eight (a trigger's mk is even, a
+        // queued leaf's odd: no ties)
+        HEnt x;
+        x.mk = ~0ull; x.idx = -1; x.gen = 0;
+        if (lane < GM4_BATCH) {
+            if (Q.head + lane < Q.tail) x = Q.q[Q.head + lane];
+        } else if (lane < 2 * GM4_BATCH) {
+            const int j = tp + lane - GM4_BATCH;
+            if (j < tw_n) { x.mk = twr[j] * 2; x.idx = twx[j]; }
         }
-        cnt = __shfl_sync(FULL, cnt, 0);
-        sp = __shfl_sync(FULL, sp, 0);
-        tp = __shfl_sync(FULL, tp, 0);
-        Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
-        Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
+        int pos = lane & (GM4_BATCH - 1);
+        const int other = lane < GM4_BATCH ? GM4_BATCH : 0;
+#pragma unroll
+        for (int j = 0; j < GM4_BATCH; ++j) {
+            const uint64_t o = __shfl_sync(FULL, x.mk, other + j);
+            pos += o < x.mk ? 1 : 0;
+        }
+        const bool take = lane < 2 * GM4_BATCH && x.mk != ~0ull && pos < GM4_BATCH;
+        if (take) items[pos] = x;
+        const unsigned tm = __ballot_sync(FULL, take);
+        const int cnt = __popc(tm);
         __syncwarp();
         if (cnt == 0) break;
         // lookups and decisions: lane (grp, tl) handles direction tl of item
@@ -1174,9 +1243,13 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
         const unsigned vm = __ballot_sync(FULL, valid && tl == 0 && grp < fa);
         if (valid && tl == 0 && grp < fa) P.flags[it.idx] = fl | PF_VISITED;
         if (lane == 0) visits += __popc(vm);
-        int consumed = fa;
+        const int consumed = fa < cnt ? fa + 1 : cnt;
+        // the consumed items leave the front of their lists (the sons queued
+        // below all rank after the item being visited)
+        const int cq = __popc(__ballot_sync(FULL, take && lane < GM4_BATCH && pos < consumed));
+        Q.head += cq;
+        tp += consumed - cq;
         if (fa < cnt) {
-            consumed = fa + 1;
             const uint64_t rb = __shfl_sync(FULL, vr, fa * 4);
             const int32_t cb = __shfl_sync(FULL, it.idx, fa * 4);
             const uint64_t kb = __shfl_sync(FULL, ck, fa * 4);
@@ -1220,32 +1293,9 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
             }
             if (!ok) break;
         }
-        // the items not consumed stay staged, followed by the staged items
-        // that were not merged (all of them later in traversal order); what
-        // does not fit goes back to the queue
-        {
-            const HEnt *so = stg[sb];
-            HEnt *sn = stg[sb ^ 1];
-            const int nu = cnt - consumed, tot = nu + ns - sp;
-            if (lane < nu) sn[lane] = items[consumed + lane];
-            else if (lane < tot && lane < GM4_STAGE) sn[lane] = so[sp + lane - nu];
-            __syncwarp();
-            int e = 0;
-            if (lane == 0)
-                for (int j = GM4_STAGE; j < tot; ++j)
-                    if (!qpush(Q, so[sp + j - nu])) e = 1;
-            if (__shfl_sync(FULL, e, 0)) {
-                if (lane == 0) P.err[0] = 1;
-                break;
-            }
-            ns = tot < GM4_STAGE ? tot : GM4_STAGE;
-            sb ^= 1;
-            Q.s.n = __shfl_sync(FULL, Q.s.n, 0);
-            Q.g.n = __shfl_sync(FULL, Q.g.n, 0);
-            __syncwarp();
-        }
     }
     if (lane == 0) {
+        if (!ok) P.err[0] = 1;
         *P.n = pn;
         P.err[1] = visits;
         P.err[2] = nonleaf;
@@ -1424,12 +1474,12 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     FDM_CK(h, cudaMemcpyAsync(P.n, &n, 8, cudaMemcpyHostToDevice, h->s));
     k_pool_init<<<nblk(n, TB), TB, 0, h->s>>>(X.A, P);
     // every step consumes a trigger or a queued leaf, or ends the pass
-    const size_t gm4_smem = (size_t)GM4_SHEAP * 16;
+    const size_t gm4_smem = (size_t)GM4_SQ * sizeof(HEnt);
     FDM_CK(h, cudaFuncSetAttribute(k_gm4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gm4_smem));
     for (cudaEvent_t &e : h->gm4_ev)
         if (!e) FDM_CK(h, cudaEventCreate(&e));
     FDM_CK(h, cudaEventRecord(h->gm4_ev[0], h->s));
-    k_gm4_warp<<<1, 32, gm4_smem, h->s>>>(P, h->G, rk, idx, ntrig, ntrig + GM4_SHEAP + P.hcap + 16);
+    k_gm4_warp<<<1, 32, gm4_smem, h->s>>>(P, h->G, rk, idx, ntrig, 2 * ntrig + 2 * P.hcap + 16);
     FDM_CK(h, cudaEventRecord(h->gm4_ev[1], h->s));
     int32_t herr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t pn = 0;
