@@ -645,14 +645,25 @@ struct __align__(16) HEnt {
     uint64_t mk;
     int32_t idx, gen;
 };
+// Hash table of the pool: open addressing over buckets of 8 entries, one
+// 128-byte line each (8 keys, then 8 slot words).  A key's probe sequence is
+// its home bucket's entries in order, then the next buckets' (linear
+// probing from a bucket boundary), so at the table's load (a quarter or
+// less) one bucket read settles a lookup but about once in a thousand.
+constexpr int HB = 8;
+struct __align__(128) HBucket {
+    uint64_t key[HB];
+    int32_t slot[HB];    // pool index (| SLOT_DEL when deleted), -1 empty
+    int32_t pad[HB];
+};
+constexpr int HB_COPY = 96;   // the bytes of a bucket that a probe reads (keys and slots)
 struct Pool {
     uint64_t *key;
     uint8_t *flags;
     int32_t *gen;
     double4 *val;
-    int32_t *slot;       // hash slots -> pool index (| SLOT_DEL when deleted), -1 empty
-    uint64_t *skey;      // the key held by each slot
-    uint64_t mask;       // slots - 1
+    HBucket *tab;
+    uint64_t bmask;      // buckets - 1
     int64_t cap;         // pool capacity
     int64_t *n;          // pool size (device counter)
     HEnt *heap;          // heap of leaves to visit ahead of the traversal (spill)
@@ -665,35 +676,85 @@ __device__ __forceinline__ uint64_t hmix(uint64_t k) {
     k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
     return k;
 }
+__device__ __forceinline__ uint64_t hhome(const Pool &P, uint64_t k) { return hmix(k) & P.bmask; }
+__device__ __forceinline__ int32_t *hslot(const Pool &P, uint64_t pos) { return &P.tab[pos >> 3].slot[pos & 7]; }
+__device__ __forceinline__ uint64_t *hkey(const Pool &P, uint64_t pos) { return &P.tab[pos >> 3].key[pos & 7]; }
+// the entry after pos in every probe sequence through it
+__device__ __forceinline__ uint64_t hnext(const Pool &P, uint64_t pos) {
+    return (pos & 7) == 7 ? (((pos >> 3) + 1) & P.bmask) << 3 : pos + 1;
+}
+// key k in bucket b, read from memory: 1 found at entry e (slot word s),
+// 0 absent (e = the first empty entry), -1 every entry holds another key
+__device__ __forceinline__ int hscan_mem(const Pool &P, uint64_t b, uint64_t k, int &e, int32_t &s) {
+    for (int j = 0; j < HB; ++j) {
+        s = P.tab[b].slot[j];
+        if (s == -1) { e = j; return 0; }
+        if (P.tab[b].key[j] == k) { e = j; return 1; }
+    }
+    return -1;
+}
+// the same on the copy of a bucket in shared memory
+__device__ __forceinline__ int hscan_copy(const unsigned char *c, uint64_t k, int &e, int32_t &s) {
+    const uint64_t *key = reinterpret_cast<const uint64_t *>(c);
+    const int32_t *slot = reinterpret_cast<const int32_t *>(c + HB * 8);
+#pragma unroll
+    for (int j = 0; j < HB; ++j) {
+        const int32_t sj = slot[j];
+        if (sj == -1) { e = j; s = -1; return 0; }
+        if (key[j] == k) { e = j; s = sj; return 1; }
+    }
+    return -1;
+}
+// key k's entry from bucket b on: 1 found at pos (slot word s), 0 absent
+// (pos = the first empty entry of its sequence), -1 the table is full
+__device__ __forceinline__ int hlocate_from(const Pool &P, uint64_t k, uint64_t b, uint64_t &pos, int32_t &s) {
+    for (uint64_t probe = 0; probe <= P.bmask; ++probe) {
+        int e = 0;
+        const int r = hscan_mem(P, b, k, e, s);
+        if (r >= 0) { pos = b * HB + (uint64_t)e; return r; }
+        b = (b + 1) & P.bmask;
+    }
+    return -1;
+}
+__device__ __forceinline__ int hlocate(const Pool &P, uint64_t k, uint64_t &pos, int32_t &s) {
+    return hlocate_from(P, k, hhome(P, k), pos, s);
+}
+// asynchronous copy of a bucket's keys and slot words into shared memory
+__device__ __forceinline__ void hfetch(const Pool &P, uint64_t b, unsigned char *dst) {
+    const unsigned char *src = reinterpret_cast<const unsigned char *>(&P.tab[b]);
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+#pragma unroll
+    for (int q = 0; q < HB_COPY / 16; ++q)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d + 16 * q), "l"(src + 16 * q) : "memory");
+}
+__device__ __forceinline__ void hfetch_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __global__ void k_pool_init(NodeSet A, Pool P) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= A.n) return;
-    P.key[i] = A.key[i];
+    const uint64_t k = A.key[i];
+    P.key[i] = k;
     P.flags[i] = A.leaf[i] ? PF_LEAF : 0;
     P.gen[i] = 0;
     P.val[i] = A.val[i];
-    uint64_t hsh = hmix(A.key[i]) & P.mask;
-    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        const int32_t old = atomicCAS(P.slot + hsh, -1, (int32_t)i);
-        if (old == -1) {
-            P.skey[hsh] = A.key[i];
-            return;
+    // claim the first free entry of the sequence (entries only fill up here)
+    uint64_t b = hhome(P, k);
+    for (uint64_t probe = 0; probe <= P.bmask; ++probe) {
+        for (int j = 0; j < HB; ++j) {
+            if (P.tab[b].slot[j] != -1) continue;
+            if (atomicCAS(&P.tab[b].slot[j], -1, (int32_t)i) == -1) {
+                P.tab[b].key[j] = k;
+                return;
+            }
         }
-        hsh = (hsh + 1) & P.mask;
+        b = (b + 1) & P.bmask;
     }
 }
-// slot position of key k (live or deleted), or -1; the slot word and the
-// slot key are independent loads, so a probe costs one memory round trip
+// entry position of key k (live or deleted), or -1
 __device__ __forceinline__ int64_t hpos(const Pool &P, uint64_t k, int32_t &s) {
-    uint64_t hsh = hmix(k) & P.mask;
-    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        s = P.slot[hsh];
-        const uint64_t sk = P.skey[hsh];
-        if (s == -1) return -1;
-        if (sk == k) return (int64_t)hsh;
-        hsh = (hsh + 1) & P.mask;
-    }
-    return -1;
+    uint64_t pos = 0;
+    s = -1;
+    return hlocate(P, k, pos, s) == 1 ? (int64_t)pos : -1;
 }
 // pool index of the live node with key k, or -1
 __device__ __forceinline__ int32_t hfind(const Pool &P, uint64_t k) {
@@ -705,46 +766,28 @@ __device__ __forceinline__ int32_t hfind(const Pool &P, uint64_t k) {
 // Returns its pool index or -1
 __device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v, int64_t &pn) {
     int32_t s;
-    const int64_t pos = hpos(P, k, s);
-    if (pos >= 0) {
+    uint64_t pos;
+    const int r = hlocate(P, k, pos, s);
+    if (r < 0) return -1;
+    if (r == 1) {
         const int32_t i = s & ~SLOT_DEL;
-        P.slot[pos] = i;
+        *hslot(P, pos) = i;
         P.flags[i] = PF_LEAF;
         P.gen[i] = P.gen[i] + 1;
         P.val[i] = v;
         return i;
     }
-    uint64_t hsh = hmix(k) & P.mask;
-    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        if (P.slot[hsh] == -1) {
-            const int64_t i = pn;
-            if (i >= P.cap) return -1;
-            pn = i + 1;
-            P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
-            P.slot[hsh] = (int32_t)i;
-            P.skey[hsh] = k;
-            return (int32_t)i;
-        }
-        hsh = (hsh + 1) & P.mask;
-    }
-    return -1;
-}
-// the rest of key k's probe sequence, given its first probe (position h,
-// slot word s, slot key q): the live node's pool index, or -1
-__device__ __forceinline__ int32_t hfind_rest(const Pool &P, uint64_t k, uint64_t h, int32_t s, uint64_t q) {
-    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-        if (s == -1) return -1;
-        if (q == k) return (s & SLOT_DEL) ? -1 : s;
-        h = (h + 1) & P.mask;
-        s = P.slot[h];
-        q = P.skey[h];
-    }
-    return -1;
+    const int64_t i = pn;
+    if (i >= P.cap) return -1;
+    pn = i + 1;
+    P.key[i] = k; P.flags[i] = PF_LEAF; P.gen[i] = 0; P.val[i] = v;
+    *hslot(P, pos) = (int32_t)i;
+    *hkey(P, pos) = k;
+    return (int32_t)i;
 }
 
 constexpr int GM4_BATCH = 8;      // items looked at together
 constexpr int GM4_TWIN = 64;      // trigger window in shared memory
-constexpr int GM4_UP = 4;         // ancestors probed at once by a lookup
 constexpr int GM4_SQ = 4096;      // sorted queue in shared memory (16 B entries)
 
 // Leaves to visit ahead of the traversal, ordered by mk: a sorted array
@@ -957,7 +1000,7 @@ __device__ bool refine_nonleaf(Pool &P, const Geometry &G, Queue &Q, int32_t p, 
                 else ok = false;
             }
             P.flags[s] |= PF_DELETED;
-            P.slot[pos] = s | SLOT_DEL;
+            *hslot(P, (uint64_t)pos) = s | SLOT_DEL;
         }
     }
     P.flags[p] = 0;   // internal, value kept
@@ -982,64 +1025,61 @@ __device__ __forceinline__ bool key_inside(uint64_t r, uint64_t s) {
 
 // A lookup from key k towards d starts at the shifted key S and walks up to
 // the first existing node; refining or dropping node R changes it only when
-// S lies inside R.  sk = S (or ~0 when the shift leaves the grid).  S and its
-// next GM4_UP - 1 ancestors are probed at once (their first probes are
-// independent loads), then the walk goes on from there if none exists.
-__device__ __forceinline__ int32_t lookup_from(const Pool &P, const Geometry &G, uint64_t k, int d, uint64_t &nk,
-                                               uint64_t &sk) {
+// S lies inside R.  sk = S (or ~0 when the shift leaves the grid).  It is
+// made by a group of 4 consecutive lanes (mask gm, first lane g0): lane
+// g0 + j probes the j-th ancestor of the walk's current start, copying its
+// home bucket into the lane's shared-memory area lk (HB_COPY bytes), and
+// the deepest node found ends the walk; otherwise the walk moves up 4
+// levels.  Every lane of the group returns the result.
+__device__ __forceinline__ int32_t group_lookup(const Pool &P, const Geometry &G, uint64_t k, int d, uint64_t &nk,
+                                                uint64_t &sk, unsigned char *lk, unsigned gm, int g0) {
+    const int j = (int)(threadIdx.x & 3);
     uint64_t t;
     if (!shift_key(G, k, d, t)) { sk = ~0ull; return -1; }
     sk = t;
     for (;;) {
         const int lt = (int)(t & 15u);
-        uint64_t c[GM4_UP], h[GM4_UP], q[GM4_UP];
-        int32_t s[GM4_UP];
-#pragma unroll
-        for (int j = 0; j < GM4_UP; ++j) {
-            c[j] = j == 0 ? t : (j <= lt ? parent_key(c[j - 1]) : c[j - 1]);
-            h[j] = hmix(c[j]) & P.mask;
-        }
-#pragma unroll
-        for (int j = 0; j < GM4_UP; ++j) {
-            s[j] = -1;
-            q[j] = 0;
-            if (j <= lt) {
-                s[j] = P.slot[h[j]];
-                q[j] = P.skey[h[j]];
+        uint64_t c = t;
+        for (int a = 0; a < j && a < lt; ++a) c = parent_key(c);
+        bool found = false;
+        int32_t s = -1;
+        if (j <= lt) {
+            const uint64_t b = hhome(P, c);
+            hfetch(P, b, lk);
+            hfetch_wait();
+            int e = 0;
+            int r = hscan_copy(lk, c, e, s);
+            if (r < 0) {   // a full bucket: the sequence goes on in the next ones
+                uint64_t pos;
+                r = hlocate_from(P, c, (b + 1) & P.bmask, pos, s);
             }
+            found = r == 1 && !(s & SLOT_DEL);
         }
-#pragma unroll
-        for (int j = 0; j < GM4_UP; ++j) {
-            if (j > lt) return -1;
-            const int32_t i = hfind_rest(P, c[j], h[j], s[j], q[j]);
-            if (i >= 0) { nk = c[j]; return i; }
+        const unsigned fm = (__ballot_sync(gm, found) >> g0) & 0xFu;
+        if (fm) {
+            const int w = g0 + __ffs(fm) - 1;
+            nk = __shfl_sync(gm, c, w);
+            return __shfl_sync(gm, s, w);
         }
-        if (lt < GM4_UP) return -1;   // level 0 was probed
-        t = parent_key(c[GM4_UP - 1]);
+        if (lt < 4) return -1;   // level 0 was probed
+        t = parent_key(parent_key(parent_key(parent_key(t))));
     }
 }
+// the reference's direction order of gridmodify4: right, left, up, down
+__device__ __forceinline__ int gm4_dir(int t) { return (t + DIR_RIGHT) & 3; }
+// the neighbour of leaf k in direction t of that order and the neighbour's
+// neighbour, by a group of 4 lanes
 struct Look {
     int32_t nb, nn;
     uint64_t nbk, nnk, snb, snn;
 };
-// the reference's direction order of gridmodify4: right, left, up, down
-__device__ __forceinline__ int gm4_dir(int t) { return (t + DIR_RIGHT) & 3; }
-__device__ __forceinline__ void dir_lookups(const Pool &P, const Geometry &G, uint64_t k, int t, Look &L) {
+__device__ __forceinline__ void group_dir_lookups(const Pool &P, const Geometry &G, uint64_t k, int t, Look &L,
+                                                  unsigned char *lk, unsigned gm, int g0) {
     L.nn = -1;
     L.snn = ~0ull;
-    L.nb = lookup_from(P, G, k, gm4_dir(t), L.nbk, L.snb);
-    if (L.nb >= 0) L.nn = lookup_from(P, G, L.nbk, gm4_dir(t), L.nnk, L.snn);
-}
-__device__ __forceinline__ Look shfl_look(const Look &L, int src) {
-    const unsigned FULL = 0xffffffffu;
-    Look o;
-    o.nb = __shfl_sync(FULL, L.nb, src);
-    o.nn = __shfl_sync(FULL, L.nn, src);
-    o.nbk = __shfl_sync(FULL, L.nbk, src);
-    o.nnk = __shfl_sync(FULL, L.nnk, src);
-    o.snb = __shfl_sync(FULL, L.snb, src);
-    o.snn = __shfl_sync(FULL, L.snn, src);
-    return o;
+    L.nnk = 0;
+    L.nb = group_lookup(P, G, k, gm4_dir(t), L.nbk, L.snb, lk, gm, g0);
+    if (L.nb >= 0) L.nn = group_lookup(P, G, L.nbk, gm4_dir(t), L.nnk, L.snn, lk, gm, g0);
 }
 
 // Refine_cell of pool node p (key pk) by the warp.  Lanes 0..3 read the
@@ -1051,21 +1091,20 @@ __device__ __forceinline__ Look shfl_look(const Look &L, int src) {
 // past it.  A non-leaf (rare) is refined by lane 0 alone.  pn (the pool
 // size) is uniform.  Returns false when the pool or the queue overflowed.
 __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t pk, uint64_t cur_rank,
-                            int32_t &nonleaf, int64_t &pn) {
+                            int32_t &nonleaf, int64_t &pn, unsigned char *lk) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const bool son = lane < 4;
     int fp = 0;
     double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
-    uint64_t ck = 0, h = 0, q = 0;
-    int32_t s = -1;
+    uint64_t ck = 0, b = 0;
     if (son) {
+        ck = child_key(pk, lane);
+        b = hhome(P, ck);
+        hfetch(P, b, lk);
         fp = P.flags[p];
         v = P.val[p];
-        ck = child_key(pk, lane);
-        h = hmix(ck) & P.mask;
-        s = P.slot[h];
-        q = P.skey[h];
+        hfetch_wait();
     }
     fp = __shfl_sync(FULL, fp, 0);
     bool ok = true;
@@ -1075,16 +1114,17 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
         ok = __shfl_sync(FULL, e, 0) == 0;
         pn = __shfl_sync(FULL, pn, 0);
     } else {
-        // the son's own slot (a dropped node), or the first empty slot
+        // the son's own entry (a dropped node), or the first empty entry
         bool found = false;
+        uint64_t h = 0;
+        int32_t s = -1;
+        int r = 0;
         if (son) {
-            for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-                if (s == -1) break;
-                if (q == ck) { found = true; break; }
-                h = (h + 1) & P.mask;
-                s = P.slot[h];
-                q = P.skey[h];
-            }
+            int e = 0;
+            r = hscan_copy(lk, ck, e, s);
+            if (r >= 0) h = b * HB + (uint64_t)e;
+            else r = hlocate_from(P, ck, (b + 1) & P.bmask, h, s);
+            found = r == 1;
         }
         const unsigned nm = __ballot_sync(FULL, son && !found);
         int32_t i = -1, gen = 0;
@@ -1095,7 +1135,7 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
             i = (int32_t)(pn + __popc(nm & ((1u << lane) - 1u)));
         }
         pn += __popc(nm);
-        ok = pn <= P.cap;
+        ok = pn <= P.cap && !__any_sync(FULL, r < 0);   // the pool, or the table, is full
         if (ok) {
             bool need = son && !found;
             for (;;) {
@@ -1104,21 +1144,26 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
                 if (need) {
                     const unsigned peers = __match_any_sync(pend, h);
                     if (__ffs(peers) - 1 == lane) {
-                        P.slot[h] = i;
-                        P.skey[h] = ck;
+                        *hslot(P, h) = i;
+                        *hkey(P, h) = ck;
                         need = false;
                     }
                 }
                 __syncwarp();
-                if (need) {   // a lower lane took the slot: probe on to the next empty one
-                    for (uint64_t probe = 0; probe <= P.mask; ++probe) {
-                        h = (h + 1) & P.mask;
-                        if (P.slot[h] == -1) break;
+                bool lost = false;
+                if (need) {   // a lower lane took the entry: probe on to the next empty one
+                    lost = true;
+                    for (uint64_t probe = 0; probe <= P.bmask * HB && lost; ++probe) {
+                        h = hnext(P, h);
+                        lost = *hslot(P, h) != -1;
                     }
                 }
+                if (__any_sync(FULL, lost)) { ok = false; break; }
             }
+        }
+        if (ok) {
             if (son) {
-                if (found) P.slot[h] = i;
+                if (found) *hslot(P, h) = i;
                 else P.key[i] = ck;
                 P.flags[i] = PF_LEAF;
                 P.gen[i] = gen;
@@ -1135,105 +1180,152 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
     return ok;
 }
 
+__device__ __forceinline__ Look shfl_look(const Look &L, int src) {
+    const unsigned FULL = 0xffffffffu;
+    Look o;
+    o.nb = __shfl_sync(FULL, L.nb, src);
+    o.nn = __shfl_sync(FULL, L.nn, src);
+    o.nbk = __shfl_sync(FULL, L.nbk, src);
+    o.nnk = __shfl_sync(FULL, L.nnk, src);
+    o.snb = __shfl_sync(FULL, L.snb, src);
+    o.snn = __shfl_sync(FULL, L.snn, src);
+    return o;
+}
+
+constexpr int GM4_THREADS = 128;   // 8 leaves x 4 directions x 4 probing lanes
+
 // gridmodify4 (src/mesh.F90:355-395) over one pass of the tree, by one
-// warp.  The leaves that can act (the initial triggers, sorted by visit
+// block.  The leaves that can act (the initial triggers, sorted by visit
 // rank, and every leaf queued ahead of the traversal) are visited in
-// traversal order.  The next 8 of them (from the sorted queue and the
-// trigger window, merged by the lanes at once) are looked at together: 4
-// lanes per leaf find its right/left/up/down neighbour and that neighbour's
-// neighbour, and each lane tells whether its direction would refine
-// something.  The leaves before the first one that refines have no effect
-// but being visited, so they are marked in parallel; the first one that
-// refines is then applied alone, in order, and the batch ends there (the
-// leaves after it stay where they are for the next batch).  Within that
-// leaf a lookup starts at a shifted key and walks up to the first existing
-// node, so a refinement (or a dropped subtree) of node R can change a later
-// lookup only when its start lies inside R: those lookups, and only those,
-// are repeated.  A leaf that is both a trigger and queued is looked at
-// twice; the second look finds it visited.
-__global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint64_t *__restrict__ trank,
-                                                 const int32_t *__restrict__ tidx, int64_t ntrig, int64_t max_steps) {
+// traversal order.  Warp 0 merges the next 8 of them from the sorted queue
+// and the trigger window (its lanes at once); then the whole block looks at
+// them together: 16 threads per leaf find its right/left/up/down neighbour
+// and that neighbour's neighbour, 4 per direction.  Warp 0 then tells which
+// directions would refine something.  The leaves before the first one that
+// refines have no effect but being visited, so they are marked in
+// parallel; the first one that refines is then applied alone, in order, by
+// warp 0, and the batch ends there (the leaves after it stay where they are
+// for the next batch).  Within that leaf a lookup starts at a shifted key
+// and walks up to the first existing node, so a refinement (or a dropped
+// subtree) of node R can change a later lookup only when its start lies
+// inside R: those lookups, and only those, are repeated.  A leaf that is
+// both a trigger and queued is looked at twice; the second look finds it
+// visited.
+__global__ void __launch_bounds__(GM4_THREADS) k_gm4_block(Pool P, Geometry G, const uint64_t *__restrict__ trank,
+                                                           const int32_t *__restrict__ tidx, int64_t ntrig,
+                                                           int64_t max_steps) {
     extern __shared__ __align__(16) unsigned char gm4_smem[];
     __shared__ HEnt items[GM4_BATCH];
     __shared__ uint64_t twr[GM4_TWIN];
     __shared__ int32_t twx[GM4_TWIN];
-    const int lane = threadIdx.x, grp = lane >> 2, tl = lane & 3;
+    __shared__ __align__(16) unsigned char lkbuf[GM4_THREADS][HB_COPY];   // each thread's bucket copy
+    __shared__ Look looks[GM4_BATCH][4];
+    __shared__ uint8_t s_fl[GM4_BATCH], s_valid[GM4_BATCH];
+    __shared__ int s_cnt;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned char *lk = lkbuf[tid];
     const unsigned FULL = 0xffffffffu;
+    // this thread's part of the block-wide lookups
+    const int bi = tid >> 4, bd = (tid >> 2) & 3, g0 = lane & ~3;
+    const unsigned gmask = 0xFu << g0;
+    // warp 0's state (uniform in warp 0)
     Queue Q;
     Q.q = reinterpret_cast<HEnt *>(gm4_smem);
     Q.head = Q.tail = 0;
     Q.g.e = P.heap;
     Q.g.cap = P.hcap;
     Q.g.n = 0;
-    int64_t pn = *P.n;     // pool size (uniform; stored at the end)
+    int64_t pn = *P.n;     // pool size (stored at the end)
     int64_t tg = 0;        // next trigger to bring into the window
     int tw_n = 0, tp = 0;  // triggers in the window, next one to merge
     int64_t step = 0;
     int32_t visits = 0, nonleaf = 0, refines = 0;   // lane 0's counts, stored at the end
     bool ok = true;
+    bool take = false;     // warp 0: this lane's merged entry is an item ...
+    int pos = 0;           // ... at this place
     for (;; ++step) {
-        if (step >= max_steps) { if (lane == 0) P.err[3] = 1; break; }
-        // keep at least a batch of triggers in the window
-        if (tw_n - tp < GM4_BATCH && tg < ntrig) {
-            const int rem = tw_n - tp;
-            uint64_t rr = 0;
-            int32_t rx = 0;
-            if (lane < rem) { rr = twr[tp + lane]; rx = twx[tp + lane]; }
-            __syncwarp();
-            if (lane < rem) { twr[lane] = rr; twx[lane] = rx; }
-            const int nl = (int)min((int64_t)(GM4_TWIN - rem), ntrig - tg);
-            for (int j = lane; j < nl; j += 32) { twr[rem + j] = trank[tg + j]; twx[rem + j] = tidx[tg + j]; }
-            tg += nl;
-            tw_n = rem + nl;
-            tp = 0;
-            __syncwarp();
-        }
-        if (Q.g.n > 0 && !sq_pull(Q)) { ok = false; break; }
-        // the next items in traversal order: lanes 0..7 hold the first
-        // queued leaves, lanes 8..15 the first triggers; each finds its
-        // place among the other list's eight (a trigger's mk is even, a
-        // queued leaf's odd: no ties)
-        HEnt x;
-        x.mk = ~0ull; x.idx = -1; x.gen = 0;
-        if (lane < GM4_BATCH) {
-            if (Q.head + lane < Q.tail) x = Q.q[Q.head + lane];
-        } else if (lane < 2 * GM4_BATCH) {
-            const int j = tp + lane - GM4_BATCH;
-            if (j < tw_n) { x.mk = twr[j] * 2; x.idx = twx[j]; }
-        }
-        int pos = lane & (GM4_BATCH - 1);
-        const int other = lane < GM4_BATCH ? GM4_BATCH : 0;
+        if (warp == 0) {
+            int c = 0;
+            if (step >= max_steps) {
+                if (lane == 0) P.err[3] = 1;
+            } else if (ok) {
+                // keep at least a batch of triggers in the window
+                if (tw_n - tp < GM4_BATCH && tg < ntrig) {
+                    const int rem = tw_n - tp;
+                    uint64_t rr = 0;
+                    int32_t rx = 0;
+                    if (lane < rem) { rr = twr[tp + lane]; rx = twx[tp + lane]; }
+                    __syncwarp();
+                    if (lane < rem) { twr[lane] = rr; twx[lane] = rx; }
+                    const int nl = (int)min((int64_t)(GM4_TWIN - rem), ntrig - tg);
+                    for (int j = lane; j < nl; j += 32) { twr[rem + j] = trank[tg + j]; twx[rem + j] = tidx[tg + j]; }
+                    tg += nl;
+                    tw_n = rem + nl;
+                    tp = 0;
+                    __syncwarp();
+                }
+                if (Q.g.n > 0 && !sq_pull(Q)) ok = false;
+            }
+            if (step < max_steps && ok) {
+                // the next items in traversal order: lanes 0..7 hold the first
+                // queued leaves, lanes 8..15 the first triggers; each finds its
+                // place among the other list's eight (a trigger's mk is even, a
+                // queued leaf's odd: no ties)
+                HEnt x;
+                x.mk = ~0ull; x.idx = -1; x.gen = 0;
+                if (lane < GM4_BATCH) {
+                    if (Q.head + lane < Q.tail) x = Q.q[Q.head + lane];
+                } else if (lane < 2 * GM4_BATCH) {
+                    const int j = tp + lane - GM4_BATCH;
+                    if (j < tw_n) { x.mk = twr[j] * 2; x.idx = twx[j]; }
+                }
+                pos = lane & (GM4_BATCH - 1);
+                const int other = lane < GM4_BATCH ? GM4_BATCH : 0;
 #pragma unroll
-        for (int j = 0; j < GM4_BATCH; ++j) {
-            const uint64_t o = __shfl_sync(FULL, x.mk, other + j);
-            pos += o < x.mk ? 1 : 0;
+                for (int j = 0; j < GM4_BATCH; ++j) {
+                    const uint64_t o = __shfl_sync(FULL, x.mk, other + j);
+                    pos += o < x.mk ? 1 : 0;
+                }
+                take = lane < 2 * GM4_BATCH && x.mk != ~0ull && pos < GM4_BATCH;
+                if (take) items[pos] = x;
+                c = __popc(__ballot_sync(FULL, take));
+            }
+            if (lane == 0) s_cnt = c;
         }
-        const bool take = lane < 2 * GM4_BATCH && x.mk != ~0ull && pos < GM4_BATCH;
-        if (take) items[pos] = x;
-        const unsigned tm = __ballot_sync(FULL, take);
-        const int cnt = __popc(tm);
-        __syncwarp();
+        __syncthreads();
+        const int cnt = s_cnt;
         if (cnt == 0) break;
-        // lookups and decisions: lane (grp, tl) handles direction tl of item
-        // grp; the item's key comes from its rank, so its flags and
-        // generation load while the lookups run
-        HEnt it;
-        it.mk = 0; it.idx = -1; it.gen = 0;
-        if (grp < cnt) it = items[grp];
-        const uint64_t vr = it.mk >> 1;
-        const uint64_t ck = key_of_visit_rank(vr);
+        // lookups: 16 threads per item, 4 per direction; the item's key comes
+        // from its rank, so its flags and generation load meanwhile
+        if (bi < cnt) {
+            const HEnt it = items[bi];
+            const uint64_t ck = key_of_visit_rank(it.mk >> 1);
+            uint8_t fl = 0;
+            int32_t gc = 0;
+            const bool lead = (tid & 15) == 0;
+            if (lead) { fl = P.flags[it.idx]; gc = P.gen[it.idx]; }
+            Look L;
+            group_dir_lookups(P, G, ck, bd, L, lk, gmask, g0);
+            if ((tid & 3) == 0) looks[bi][bd] = L;
+            if (lead) {
+                s_fl[bi] = fl;
+                s_valid[bi] = gc == it.gen && (fl & (PF_LEAF | PF_DELETED | PF_VISITED)) == PF_LEAF;
+            }
+        }
+        __syncthreads();
+        if (warp != 0) continue;
+        // decisions: lane (grp, tl) tells whether direction tl of item grp refines
+        const int grp = lane >> 2, tl = lane & 3;
         bool valid = false, acts = false;
         uint8_t fl = 0;
-        Look L;
-        L.nb = L.nn = -1;
-        L.nbk = L.nnk = 0;
-        L.snb = L.snn = ~0ull;
+        HEnt it;
+        it.mk = 0; it.idx = -1; it.gen = 0;
         if (grp < cnt) {
-            fl = P.flags[it.idx];
-            const int32_t gc = P.gen[it.idx];
-            dir_lookups(P, G, ck, tl, L);
-            valid = gc == it.gen && (fl & (PF_LEAF | PF_DELETED | PF_VISITED)) == PF_LEAF;
-            const int lc = (int)(ck & 15u);
+            it = items[grp];
+            valid = s_valid[grp] != 0;
+            fl = s_fl[grp];
+            const Look L = looks[grp][tl];
+            const int lc = (int)(it.mk >> 1) & 15;
             acts = valid &&
                    ((L.nb >= 0 && (int)(L.nbk & 15u) <= lc - 2) || (L.nn >= 0 && (int)(L.nnk & 15u) <= lc - 2));
         }
@@ -1250,19 +1342,18 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
         Q.head += cq;
         tp += consumed - cq;
         if (fa < cnt) {
-            const uint64_t rb = __shfl_sync(FULL, vr, fa * 4);
-            const int32_t cb = __shfl_sync(FULL, it.idx, fa * 4);
-            const uint64_t kb = __shfl_sync(FULL, ck, fa * 4);
-            const uint8_t fb = (uint8_t)__shfl_sync(FULL, (int)fl, fa * 4);
+            const HEnt ib = items[fa];
+            const uint64_t rb = ib.mk >> 1;
+            const uint64_t kb = key_of_visit_rank(rb);
             const int lc = (int)(kb & 15u);
             if (lane == 0) {
-                P.flags[cb] = fb | PF_VISITED;
+                P.flags[ib.idx] = s_fl[fa] | PF_VISITED;
                 ++visits;
             }
             uint64_t refined[8];   // uniform: nodes refined by this leaf
             int nref = 0;
             for (int t = 0; t < 4 && ok; ++t) {
-                Look Lt = shfl_look(L, fa * 4 + t);
+                Look Lt = looks[fa][t];
                 // repeat the lookups whose start lies inside a node refined earlier
                 bool re_nb = false, re_nn = false;
                 for (int k = 0; k < nref; ++k) {
@@ -1270,9 +1361,9 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
                     re_nn = re_nn || key_inside(refined[k], Lt.snn);
                 }
                 if (re_nb || re_nn) {
-                    if (lane == 0) {
-                        if (re_nb) dir_lookups(P, G, kb, t, Lt);
-                        else Lt.nn = lookup_from(P, G, Lt.nbk, gm4_dir(t), Lt.nnk, Lt.snn);
+                    if (lane < 4) {
+                        if (re_nb) group_dir_lookups(P, G, kb, t, Lt, lk, 0xFu, 0);
+                        else Lt.nn = group_lookup(P, G, Lt.nbk, gm4_dir(t), Lt.nnk, Lt.snn, lk, 0xFu, 0);
                     }
                     Lt = shfl_look(Lt, 0);
                 }
@@ -1281,20 +1372,19 @@ __global__ void __launch_bounds__(32) k_gm4_warp(Pool P, Geometry G, const uint6
                 // has four sons), and refining it leaves the lookup of its own
                 // neighbour unchanged (that start lies outside it)
                 if ((int)(Lt.nbk & 15u) <= lc - 2) {
-                    ok = refine_warp(P, G, Q, Lt.nb, Lt.nbk, rb, nonleaf, pn);
+                    ok = refine_warp(P, G, Q, Lt.nb, Lt.nbk, rb, nonleaf, pn, lk);
                     refined[nref++] = Lt.nbk;
                     ++refines;
                 }
                 if (ok && Lt.nn >= 0 && (int)(Lt.nnk & 15u) <= lc - 2) {
-                    ok = refine_warp(P, G, Q, Lt.nn, Lt.nnk, rb, nonleaf, pn);
+                    ok = refine_warp(P, G, Q, Lt.nn, Lt.nnk, rb, nonleaf, pn, lk);
                     refined[nref++] = Lt.nnk;
                     ++refines;
                 }
             }
-            if (!ok) break;
         }
     }
-    if (lane == 0) {
+    if (tid == 0) {
         if (!ok) P.err[0] = 1;
         *P.n = pn;
         P.err[1] = visits;
@@ -1455,31 +1545,29 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     uint64_t slots = 1;
     while (slots < (uint64_t)(2 * cap)) slots <<= 1;
     Carve cp;
-    cp.add(cap * 8); cp.add(cap); cp.add(cap * 4); cp.add(cap * 32); cp.add(slots * 4); cp.add(16);
-    cp.add(cap * sizeof(HEnt)); cp.add(32); cp.add(slots * 8);
+    cp.add(cap * 8); cp.add(cap); cp.add(cap * 4); cp.add(cap * 32); cp.add(slots / HB * sizeof(HBucket)); cp.add(16);
+    cp.add(cap * sizeof(HEnt)); cp.add(32);
     FDM_CK(h, h->amr[16].ensure(cp.total));
     DevBuf &pb = h->amr[16];
     Pool P;
     P.key = cp.at<uint64_t>(pb, 0); P.flags = cp.at<uint8_t>(pb, 1); P.gen = cp.at<int32_t>(pb, 2);
-    P.val = cp.at<double4>(pb, 3); P.slot = cp.at<int32_t>(pb, 4); P.n = cp.at<int64_t>(pb, 5);
+    P.val = cp.at<double4>(pb, 3); P.tab = cp.at<HBucket>(pb, 4); P.n = cp.at<int64_t>(pb, 5);
     P.heap = cp.at<HEnt>(pb, 6);
     P.err = cp.at<int32_t>(pb, 7);
-    P.skey = cp.at<uint64_t>(pb, 8);
-    P.mask = slots - 1;
+    P.bmask = slots / HB - 1;
     P.cap = cap;
     P.hcap = cap;
-    FDM_CK(h, cudaMemsetAsync(P.slot, 0xff, slots * 4, h->s));
-    FDM_CK(h, cudaMemsetAsync(P.skey, 0xff, slots * 8, h->s));
+    FDM_CK(h, cudaMemsetAsync(P.tab, 0xff, slots / HB * sizeof(HBucket), h->s));
     FDM_CK(h, cudaMemsetAsync(P.err, 0, 32, h->s));
     FDM_CK(h, cudaMemcpyAsync(P.n, &n, 8, cudaMemcpyHostToDevice, h->s));
     k_pool_init<<<nblk(n, TB), TB, 0, h->s>>>(X.A, P);
     // every step consumes a trigger or a queued leaf, or ends the pass
     const size_t gm4_smem = (size_t)GM4_SQ * sizeof(HEnt);
-    FDM_CK(h, cudaFuncSetAttribute(k_gm4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gm4_smem));
+    FDM_CK(h, cudaFuncSetAttribute(k_gm4_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gm4_smem));
     for (cudaEvent_t &e : h->gm4_ev)
         if (!e) FDM_CK(h, cudaEventCreate(&e));
     FDM_CK(h, cudaEventRecord(h->gm4_ev[0], h->s));
-    k_gm4_warp<<<1, 32, gm4_smem, h->s>>>(P, h->G, rk, idx, ntrig, 2 * ntrig + 2 * P.hcap + 16);
+    k_gm4_block<<<1, GM4_THREADS, gm4_smem, h->s>>>(P, h->G, rk, idx, ntrig, 2 * ntrig + 2 * P.hcap + 16);
     FDM_CK(h, cudaEventRecord(h->gm4_ev[1], h->s));
     int32_t herr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t pn = 0;
