@@ -1,0 +1,71 @@
+"""Command-line run of one configuration, in the place of the reference's
+main program (src/MAIN.F90:1-25: set_parameter, creat_mesh, idneighbor,
+initial, solute), without its file output.
+
+    python -m fdm_cell_based_amr_cartesian_b200 --case riemann4 --base 128 --lvl-amr 4 --steps 200
+
+runs the four-quadrant problem on a 128^2 background with 4 levels for 200
+steps (or to t_end when --steps is 0) with device regrids every nstep_adapt
+steps, and prints one JSON line: steps, seconds, the solver's counters and
+the device time of each regrid phase, summed over the run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+
+from . import params as P
+from .solver import Solver
+
+
+def config(args) -> P.Config:
+    if args.case == "riemann4":
+        return P.riemann4(base=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.3)
+    if args.case == "vortex":
+        return P.vortex(base=args.base, lvl_amr=args.lvl_amr)
+    if args.case == "double_mach":
+        return P.double_mach(base_y=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.2)
+    if args.case == "reference":
+        return P.reference_default()
+    raise SystemExit(f"unknown case {args.case}")
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m fdm_cell_based_amr_cartesian_b200")
+    ap.add_argument("--case", default="riemann4", choices=["riemann4", "vortex", "double_mach", "reference"])
+    ap.add_argument("--base", type=int, default=128, help="background cells (per side; rows for double_mach)")
+    ap.add_argument("--lvl-amr", type=int, default=4)
+    ap.add_argument("--t-end", type=float, default=0.0, help="end time (0: the case's own)")
+    ap.add_argument("--steps", type=int, default=0, help="steps to run (0: run to t_end)")
+    ap.add_argument("--gate", action="store_true", help="learned face gate on")
+    args = ap.parse_args(argv)
+
+    cfg = config(args)
+    g = Solver(cfg)
+    g.creat_mesh_and_initial()
+    if args.gate:
+        from . import learned
+        learned.enable(g)
+    t0 = time.perf_counter()
+    n = 0
+    if args.steps > 0:
+        n = g.solute(args.steps)
+    else:
+        while g.scalars()["tt"] < cfg.params.t_end:
+            k = g.solute(100)
+            n += k
+            if k == 0:
+                break
+    tt = g.scalars()["tt"]   # waits for the device
+    seconds = time.perf_counter() - t0
+    out = {"case": args.case, "steps": n, "seconds": seconds, "tt": tt,
+           "counters": g.counters(), "regrid_device_ms_total": g.amr_phase_ms(total=True)}
+    g.close()
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
