@@ -158,47 +158,49 @@ FDM_HD uint64_t child_key(uint64_t k, int q) {
     const int lvl = (int)(k & 15u);
     return (k | ((uint64_t)q << key_digit_shift(lvl + 1))) + 1u;
 }
+// The ancestor of key k at level la (0 <= la <= k's level): the path digits
+// below level la cleared
+FDM_HD uint64_t ancestor_key(uint64_t k, int la) {
+    const uint64_t below = ((1ull << (2 * (LMAX - la))) - 1ull) << 4;
+    return (k & ~below & ~15ull) | (uint64_t)la;
+}
+// Row and column of a background cell: q = root / m from a float reciprocal
+// (root < 2^24, so the estimate is off by at most one) and one correction
+FDM_HD void root_row_col(uint32_t root, uint32_t m, uint32_t &row, uint32_t &col) {
+    uint32_t q = (uint32_t)((float)root * (1.0f / (float)m));
+    int64_t r = (int64_t)root - (int64_t)q * m;
+    q = r < 0 ? q - 1u : (r >= (int64_t)m ? q + 1u : q);
+    r = r < 0 ? r + m : (r >= (int64_t)m ? r - m : r);
+    row = q;
+    col = (uint32_t)r;
+}
 // same-level neighbour node key across a face; false across the grid edge.
 // A step along x (y) is a dilated increment or decrement of the x (y) bits
-// at the node's level; a carry out of the path moves to the next root.
+// at the node's level; a carry out of the path (or a borrow) moves to the
+// next root.  Written without branches: the lanes of a warp step in
+// different directions.
 FDM_HD bool shift_key(const Geometry &G, uint64_t k, int dir, uint64_t &out) {
     const int lvl = (int)(k & 15u);
     const uint64_t unit = 1ull << key_digit_shift(lvl);
     const bool alongx = dir == DIR_RIGHT || dir == DIR_LEFT;
+    const bool inc = dir == DIR_RIGHT || dir == DIR_UP;
     const uint64_t mask = alongx ? KEY_PATH_X : KEY_PATH_Y;
     const uint64_t u = alongx ? unit : unit << 1;
     const uint64_t bits = k & mask;
-    const uint64_t rest = k & ~mask;
+    // carries skip the other coordinate's bits; a borrow from zero leaves all
+    // ones down to the node's level, the first node of the next root back
+    const uint64_t path = inc ? (((bits | ~mask) + u) & mask) : ((bits - u) & mask);
+    const bool wrap = inc ? (((bits | ~mask | (u - 1)) & KEY_PATH) == KEY_PATH) : bits == 0;
     const uint32_t root = (uint32_t)(k >> 34);
     const uint32_t m = (uint32_t)G.m;
-    if (dir == DIR_RIGHT || dir == DIR_UP) {
-        const uint64_t t = (bits | ~mask) + u;   // carries skip the other coordinate's bits
-        if (((bits | ~mask | (u - 1)) & KEY_PATH) == KEY_PATH) {   // last node of the root
-            if (alongx) {
-                if (root % m + 1 >= m) return false;
-            } else if (root / m + 1 >= (uint32_t)G.n) {
-                return false;
-            }
-            const uint64_t nroot = (uint64_t)(alongx ? root + 1u : root + m);
-            out = (nroot << 34) | (rest & ((1ull << 34) - 1ull));
-            return true;
-        }
-        out = rest | (t & mask);
-        return true;
-    }
-    if (bits == 0) {   // first node of the root
-        if (alongx) {
-            if (root % m == 0) return false;
-        } else if (root < m) {
-            return false;
-        }
-        const uint64_t nroot = (uint64_t)(alongx ? root - 1u : root - m);
-        const uint64_t full = mask & ~(u - 1);   // all ones down to the node's level
-        out = (nroot << 34) | (rest & ((1ull << 34) - 1ull)) | full;
-        return true;
-    }
-    out = rest | ((bits - u) & mask);
-    return true;
+    uint32_t row, col;
+    root_row_col(root, m, row, col);
+    const uint32_t rc = alongx ? col : row, lim = alongx ? m : (uint32_t)G.n;
+    const bool edge = inc ? rc + 1u >= lim : rc == 0u;
+    const uint32_t step = alongx ? 1u : m;
+    const uint32_t nroot = wrap ? (inc ? root + step : root - step) : root;
+    out = ((uint64_t)nroot << 34) | (k & ~mask & ((1ull << 34) - 1ull)) | path;
+    return !(wrap && edge);
 }
 // traversal rank of gridmodify4 / solute_div_rot (sons 1,2,3,4): Morton path
 // with the digits of son3 and son4 swapped
@@ -672,9 +674,12 @@ struct Pool {
                          // [4] refines, [5] replay steps
 };
 constexpr int32_t SLOT_DEL = 0x40000000;
+// Home bucket hash: the key folded to 32 bits, then MurmurHash3's 32-bit
+// finaliser (A. Appleby, public domain); 32-bit multiplies only
 __device__ __forceinline__ uint64_t hmix(uint64_t k) {
-    k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
-    return k;
+    uint32_t x = (uint32_t)k ^ ((uint32_t)(k >> 32) * 0x9E3779B1u);
+    x ^= x >> 16; x *= 0x85EBCA6Bu; x ^= x >> 13; x *= 0xC2B2AE35u; x ^= x >> 16;
+    return x;
 }
 __device__ __forceinline__ uint64_t hhome(const Pool &P, uint64_t k) { return hmix(k) & P.bmask; }
 __device__ __forceinline__ int32_t *hslot(const Pool &P, uint64_t pos) { return &P.tab[pos >> 3].slot[pos & 7]; }
@@ -693,17 +698,34 @@ __device__ __forceinline__ int hscan_mem(const Pool &P, uint64_t b, uint64_t k, 
     }
     return -1;
 }
-// the same on the copy of a bucket in shared memory
+// the same on the copy of a bucket in shared memory, without branches: bit
+// masks of the empty entries and of the entries holding k, then the first of
+// each
 __device__ __forceinline__ int hscan_copy(const unsigned char *c, uint64_t k, int &e, int32_t &s) {
-    const uint64_t *key = reinterpret_cast<const uint64_t *>(c);
-    const int32_t *slot = reinterpret_cast<const int32_t *>(c + HB * 8);
+    const ulonglong2 *kp = reinterpret_cast<const ulonglong2 *>(c);
+    const int4 *sp = reinterpret_cast<const int4 *>(c + HB * 8);
+    unsigned em = 0, mm = 0;
 #pragma unroll
-    for (int j = 0; j < HB; ++j) {
-        const int32_t sj = slot[j];
-        if (sj == -1) { e = j; s = -1; return 0; }
-        if (key[j] == k) { e = j; s = sj; return 1; }
+    for (int j = 0; j < HB / 2; ++j) {
+        const ulonglong2 v = kp[j];
+        mm |= (v.x == k ? 1u : 0u) << (2 * j);
+        mm |= (v.y == k ? 1u : 0u) << (2 * j + 1);
     }
-    return -1;
+#pragma unroll
+    for (int j = 0; j < HB / 4; ++j) {
+        const int4 v = sp[j];
+        em |= (v.x == -1 ? 1u : 0u) << (4 * j);
+        em |= (v.y == -1 ? 1u : 0u) << (4 * j + 1);
+        em |= (v.z == -1 ? 1u : 0u) << (4 * j + 2);
+        em |= (v.w == -1 ? 1u : 0u) << (4 * j + 3);
+    }
+    // entries fill in order, so the key can only sit before the first empty one
+    const unsigned live = em ? (em & (0u - em)) - 1u : 0xFFu;   // entries before the first empty
+    mm &= live;
+    const int fe = em ? __ffs(em) - 1 : HB, fm = mm ? __ffs(mm) - 1 : HB;
+    e = mm ? fm : fe;
+    s = mm ? reinterpret_cast<const int32_t *>(c + HB * 8)[fm] : -1;
+    return mm ? 1 : (em ? 0 : -1);
 }
 // key k's entry from bucket b on: 1 found at pos (slot word s), 0 absent
 // (pos = the first empty entry of its sequence), -1 the table is full
@@ -1039,8 +1061,7 @@ __device__ __forceinline__ int32_t group_lookup(const Pool &P, const Geometry &G
     sk = t;
     for (;;) {
         const int lt = (int)(t & 15u);
-        uint64_t c = t;
-        for (int a = 0; a < j && a < lt; ++a) c = parent_key(c);
+        const uint64_t c = ancestor_key(t, lt > j ? lt - j : 0);
         bool found = false;
         int32_t s = -1;
         if (j <= lt) {
@@ -1062,7 +1083,7 @@ __device__ __forceinline__ int32_t group_lookup(const Pool &P, const Geometry &G
             return __shfl_sync(gm, s, w);
         }
         if (lt < 4) return -1;   // level 0 was probed
-        t = parent_key(parent_key(parent_key(parent_key(t))));
+        t = ancestor_key(t, lt - 4);
     }
 }
 // the reference's direction order of gridmodify4: right, left, up, down
