@@ -122,7 +122,8 @@ struct fdm_handle {
     bool gate_stage1_valid = false;   // stage-1 decisions exist for the current tables
 
     // CUDA graph of one RK3 step (captured lazily, dropped at regrid)
-    cudaGraphExec_t step_graph = nullptr;
+    cudaGraphExec_t step_graph = nullptr;     // one solute iteration
+    cudaGraphExec_t step_graph_g = nullptr;   // the same followed by the j = 1 ghost refresh
     int64_t graph_version = -1;
     int64_t table_version = 0;
 

@@ -367,7 +367,9 @@ __device__ __forceinline__ void step_end_item(DevScalars *sc, int64_t NI) {
         sc->res_rms[n] = sqrt(sc->res_rms[n] / (1.0 * (double)NI));
         if (isnan(sc->res_rms[n])) sc->status = FDM_ERR_NAN;
     }
-    if (!(sc->tt < sc->t_end)) sc->done = 1;
+    // the reference stops at t_end and at a NaN residual: later iterations
+    // are no-ops
+    if (!(sc->tt < sc->t_end) || sc->status == FDM_ERR_NAN) sc->done = 1;
 }
 
 }  // namespace fdm

@@ -138,31 +138,36 @@ static int prepare_buffers(fdm_handle *h) {
 
 static void drop_graph(fdm_handle *h) {
     if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
-    h->step_graph = nullptr;
+    if (h->step_graph_g) cudaGraphExecDestroy(h->step_graph_g);
+    h->step_graph = h->step_graph_g = nullptr;
     h->graph_version = -1;
 }
 
-// CUDA graph of one solute iteration; re-captured after every rebuild of the
-// tables (upload / regrid), replayed otherwise.
-static int step_graph(fdm_handle *h, cudaGraphExec_t *out) {
-    if (h->step_graph && h->graph_version == h->table_version) {
-        *out = h->step_graph;
+// CUDA graph of one solute iteration (ghosts: followed by the j = 1 ghost
+// refresh that solute does after an iteration without regrid); both are
+// re-captured after every rebuild of the tables (upload / regrid), replayed
+// otherwise.
+static int step_graph(fdm_handle *h, cudaGraphExec_t *out, bool ghosts = false) {
+    if (h->graph_version != h->table_version) drop_graph(h);
+    cudaGraphExec_t &slot = ghosts ? h->step_graph_g : h->step_graph;
+    if (slot) {
+        *out = slot;
         return FDM_OK;
     }
-    drop_graph(h);
     cudaGraph_t g = nullptr;
     FDM_CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
     enqueue_solute_iteration(h);
+    if (ghosts) launch_ghosts(h, h->B[0].as<double4>(), 1);
     cudaError_t e = cudaStreamEndCapture(h->s, &g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    e = cudaGraphInstantiate(&slot, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
-        h->step_graph = nullptr;
+        slot = nullptr;
         return cuda_fail(h, e, "cudaGraphInstantiate");
     }
     h->graph_version = h->table_version;
-    *out = h->step_graph;
+    *out = slot;
     return FDM_OK;
 }
 
@@ -526,16 +531,51 @@ int fdm_solute_step(fdm_handle *h) {
     return FDM_OK;
 }
 
+// nsteps iterations of solute_step, run as chunks that end at the next
+// regrid: the iterations of a chunk are replays of the step graph (with the
+// ghost refresh after each, as solute_step does, when AMR is on) and the host
+// reads the scalars once per chunk.  The device makes an iteration after
+// t_end or after a NaN residual a no-op, so the steps counted are the
+// device's own; after a NaN the ghost cells may have been refreshed once more
+// than solute_step leaves them.
 int fdm_solute(fdm_handle *h, int64_t nsteps, int64_t *steps_done) {
     CHECK_H(h);
     CHECK_LOADED(h);
     int64_t k = 0;
     int rc = FDM_OK;
     RC(sync_scalars_from_device(h));
+    if (h->hs->status == FDM_ERR_NAN) {
+        if (steps_done) *steps_done = 0;
+        h->err = "NaN in the residual RMS (the reference stops here)";
+        return FDM_ERR_NAN;
+    }
     while (k < nsteps && h->hs->tt < h->p.t_end) {
-        rc = fdm_solute_step(h);
-        ++k;
-        if (rc) break;
+        const int64_t it0 = h->hs->it;
+        int64_t j = 1;
+        while (k + j < nsteps && j < 64 && !amr_due(h, it0 + j)) ++j;   // at most 64 before a look at tt
+        const bool regrid = amr_due(h, it0 + j);
+        RC(ensure_lambda(h));
+        cudaGraphExec_t gs = nullptr, gl = nullptr;   // iterations before the last, the last
+        RC(step_graph(h, &gs, h->p.iflag_amr != 0));
+        gl = gs;
+        if (regrid) RC(step_graph(h, &gl, false));
+        for (int64_t s = 0; s < j; ++s) FDM_CK(h, cudaGraphLaunch(s + 1 < j ? gs : gl, h->s));
+        h->lam_fresh = true;
+        RC(sync_scalars_from_device(h));
+        FDM_CK(h, cudaGetLastError());
+        const int64_t taken = h->hs->it - it0;
+        k += taken;
+        if (h->hs->status == FDM_ERR_NAN) {
+            h->err = "NaN in the residual RMS (the reference stops here)";
+            rc = FDM_ERR_NAN;
+            break;
+        }
+        if (taken < j) break;   // t_end came inside the chunk
+        if (regrid) {
+            RC(fdm_amr(h));
+            launch_ghosts(h, h->B[0].as<double4>(), 1);
+            FDM_CK(h, cudaStreamSynchronize(h->s));
+        }
     }
     if (steps_done) *steps_done = k;
     return rc;

@@ -117,7 +117,9 @@ __global__ void __launch_bounds__(256) k_cells(Tables T, LevelTab LT, const doub
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     double rm[4] = {0.0, 0.0, 0.0, 0.0}, rs[4] = {0.0, 0.0, 0.0, 0.0};
     double lx = 0.0, ly = 0.0;
-    if (i < T.NI) cell_item(T, LT, cur, un, next, Fx, Fy, sc->tstep, krk, mode, g, i, rm, rs, lx, ly);
+    // an iteration after t_end (or after a NaN residual) leaves the state as it is
+    if (i < T.NI && !(mode == 0 && sc->done))
+        cell_item(T, LT, cur, un, next, Fx, Fy, sc->tstep, krk, mode, g, i, rm, rs, lx, ly);
     cells_block_reduce(rm, rs, lx, ly, res_part + blockIdx.x * 8, sc, krk == 3 && mode == 0, S);
 }
 
@@ -178,8 +180,10 @@ __global__ void k_step_control(DevScalars *sc, fdm_params P, int use_dt) {
 }
 
 // residual partials -> Res_max / Res_rms sums
-__global__ void __launch_bounds__(256) k_res_finalize(const double *__restrict__ res_part, int nb, DevScalars *sc) {
+__global__ void __launch_bounds__(256) k_res_finalize(const double *__restrict__ res_part, int nb, DevScalars *sc,
+                                                      int keep_when_done) {
     __shared__ double sh[256][8];
+    if (keep_when_done && sc->done) return;   // a no-op iteration keeps the last residual
     res_finalize_block(res_part, nb, sc, sh);
 }
 
@@ -254,7 +258,8 @@ void launch_cells(fdm_handle *h, const double4 *cur, const double4 *un, double4 
                                   h->scal.as<DevScalars>(), h->res_part.as<double>(), krk, mode, h->G.gama);
     // Res_max / Res_rms are reset every stage and read after the last one
     // (src/solution.F90:276-277, 209-210): reduce them once, after stage 3
-    if (krk == 3 || mode == 1) k_res_finalize<<<1, 256, 0, h->s>>>(h->res_part.as<double>(), nb, h->scal.as<DevScalars>());
+    if (krk == 3 || mode == 1)
+        k_res_finalize<<<1, 256, 0, h->s>>>(h->res_part.as<double>(), nb, h->scal.as<DevScalars>(), mode == 0);
 }
 void launch_ghosts(fdm_handle *h, double4 *next, int j) {
     if (h->NG == 0) return;
