@@ -24,19 +24,90 @@ namespace fdm {
 // interpA over a subtree whose leaves are [lo, hi) of the sorted array
 // (src/XuanGua.F90:359-398): children combined as
 // 0.25*(son1 + son2 + son3 + son4) = 0.25*(((q0 + q1) + q3) + q2).
-// One warp: the lanes stage the subtree's leaves in shared memory, lane 0
-// folds them in key order with a stack of pending sibling groups.
+// One warp: the lanes stage the subtree's leaves in shared memory.  A
+// subtree of up to RW_CAP leaves is folded level by level by all lanes; a
+// larger one is folded by lane 0 in key order with a stack of pending
+// sibling groups.  Every father is formed from the same four values in the
+// same order either way.
 constexpr int RW_CAP = 256;     // leaves staged per pass
 constexpr int RW_STACK = 48;    // >= 3 pending siblings x 15 levels + 1
 struct RestrictSmem {
     double4 v[RW_CAP];
     int8_t l[RW_CAP];
-    double4 st[RW_STACK];
-    int8_t sl[RW_STACK];
+    union {
+        struct {
+            double4 st[RW_STACK];
+            int8_t sl[RW_STACK];
+        } s;                   // the stack of the lane-0 fold
+        uint32_t p[RW_CAP];    // path bits of the staged entries (level fold)
+    } u;
 };
+
+// the fold of n <= RW_CAP leaves from lo: at the deepest level present,
+// every group of four siblings (consecutive in key order, the first with
+// digit 0) becomes its father; the list is compacted and the next level up
+// follows
+__device__ __forceinline__ double4 restrict_warp_levels(const Tables &T, const double4 *__restrict__ buf,
+                                                        int64_t lo, int n, RestrictSmem &sm) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int lmax = 0;
+    for (int k = lane; k < n; k += 32) {
+        const uint64_t key = __ldg(T.lkey + lo + k);
+        sm.v[k] = buf[__ldg(T.lslot + lo + k)];
+        sm.l[k] = (int8_t)(key & 15u);
+        sm.u.p[k] = (uint32_t)((key >> 4) & ((1ull << 30) - 1ull));
+        lmax = max(lmax, (int)(key & 15u));
+    }
+    lmax = __reduce_max_sync(FULL, lmax);
+    __syncwarp();
+    while (n > 1 && lmax > 0) {
+        const int sh = 2 * (LMAX - lmax);
+        int off = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
+            int8_t li = 0;
+            uint32_t pi = 0;
+            bool keep = false;
+            if (i < n) {
+                vi = sm.v[i];
+                li = sm.l[i];
+                pi = sm.u.p[i];
+                const bool deep = li == lmax;
+                const bool first = deep && ((pi >> sh) & 3u) == 0u && i + 3 < n;
+                keep = !deep || first;
+                if (first) {   // the father (its path: the first son's, digit 0)
+                    const double4 e0 = vi, e1 = sm.v[i + 1], e2 = sm.v[i + 2], e3 = sm.v[i + 3];
+                    vi.x = 0.25 * (e0.x + e1.x + e3.x + e2.x);
+                    vi.y = 0.25 * (e0.y + e1.y + e3.y + e2.y);
+                    vi.z = 0.25 * (e0.z + e1.z + e3.z + e2.z);
+                    vi.w = 0.25 * (e0.w + e1.w + e3.w + e2.w);
+                    li = (int8_t)(lmax - 1);
+                }
+            }
+            const unsigned km = __ballot_sync(FULL, keep);
+            const int pos = off + __popc(km & ((1u << lane) - 1u));
+            off += __popc(km);
+            __syncwarp();
+            if (keep) {   // positions only move down, below what later chunks read
+                sm.v[pos] = vi;
+                sm.l[pos] = li;
+                sm.u.p[pos] = pi;
+            }
+            __syncwarp();
+        }
+        n = off;
+        --lmax;
+    }
+    const double4 r = sm.v[0];
+    __syncwarp();
+    return r;
+}
 
 __device__ __forceinline__ double4 restrict_warp(const Tables &T, const double4 *__restrict__ buf, int64_t lo,
                                                  int64_t hi, RestrictSmem &sm) {
+    if (hi - lo <= RW_CAP) return restrict_warp_levels(T, buf, lo, (int)(hi - lo), sm);
     const int lane = threadIdx.x & 31;
     int top = 0;
     for (int64_t base = lo; base < hi; base += RW_CAP) {
@@ -49,28 +120,28 @@ __device__ __forceinline__ double4 restrict_warp(const Tables &T, const double4 
         if (lane == 0) {
             for (int k = 0; k < n; ++k) {
                 if (top >= RW_STACK) break;  // cannot happen for a valid subtree
-                sm.st[top] = sm.v[k];
-                sm.sl[top] = sm.l[k];
+                sm.u.s.st[top] = sm.v[k];
+                sm.u.s.sl[top] = sm.l[k];
                 ++top;
-                while (top >= 4 && sm.sl[top - 1] == sm.sl[top - 2] && sm.sl[top - 1] == sm.sl[top - 3] &&
-                       sm.sl[top - 1] == sm.sl[top - 4]) {
-                    const double4 e0 = sm.st[top - 4], e1 = sm.st[top - 3], e2 = sm.st[top - 2], e3 = sm.st[top - 1];
+                while (top >= 4 && sm.u.s.sl[top - 1] == sm.u.s.sl[top - 2] && sm.u.s.sl[top - 1] == sm.u.s.sl[top - 3] &&
+                       sm.u.s.sl[top - 1] == sm.u.s.sl[top - 4]) {
+                    const double4 e0 = sm.u.s.st[top - 4], e1 = sm.u.s.st[top - 3], e2 = sm.u.s.st[top - 2], e3 = sm.u.s.st[top - 1];
                     double4 v;
                     v.x = 0.25 * (e0.x + e1.x + e3.x + e2.x);
                     v.y = 0.25 * (e0.y + e1.y + e3.y + e2.y);
                     v.z = 0.25 * (e0.z + e1.z + e3.z + e2.z);
                     v.w = 0.25 * (e0.w + e1.w + e3.w + e2.w);
-                    const int8_t l = (int8_t)(sm.sl[top - 1] - 1);
+                    const int8_t l = (int8_t)(sm.u.s.sl[top - 1] - 1);
                     top -= 4;
-                    sm.st[top] = v;
-                    sm.sl[top] = l;
+                    sm.u.s.st[top] = v;
+                    sm.u.s.sl[top] = l;
                     ++top;
                 }
             }
         }
         __syncwarp();
     }
-    double4 r = sm.st[0];
+    double4 r = sm.u.s.st[0];
     __syncwarp();
     return r;
 }
