@@ -160,8 +160,9 @@ __device__ __forceinline__ void request_item(const Tables &T, double4 *cur, int6
     const int m = m1 + m2;
     const double *geo = T.rq_geo + r * RQ_GEO;
     double ph[4][WLS_MAXM];
-    for (int i = 0; i < m; ++i) {
-        const double4 q = cur[mem[i]];
+#pragma unroll
+    for (int i = 0; i < WLS_MAXM; ++i) {
+        const double4 q = i < m ? cur[mem[i]] : make_double4(0.0, 0.0, 0.0, 0.0);
         ph[0][i] = q.x; ph[1][i] = q.y; ph[2][i] = q.z; ph[3][i] = q.w;
     }
     double4 v;
@@ -189,7 +190,8 @@ __device__ __forceinline__ void request_item_var(const Tables &T, double4 *cur, 
     const int m = m1 + m2;
     const double *geo = T.rq_geo + r * RQ_GEO;
     double ph[WLS_MAXM];
-    for (int i = 0; i < m; ++i) ph[i] = reinterpret_cast<const double *>(cur + mem[i])[v];
+#pragma unroll
+    for (int i = 0; i < WLS_MAXM; ++i) ph[i] = i < m ? reinterpret_cast<const double *>(cur + mem[i])[v] : 0.0;
     *o = wls_eval_var(geo, m1, m2, ph);
 }
 

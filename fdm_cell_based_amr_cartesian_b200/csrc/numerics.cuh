@@ -309,12 +309,17 @@ __device__ __forceinline__ double wls_eval_var(const double *__restrict__ geo, i
     const double *x = geo + G_X, *y = geo + G_Y, *w = geo + G_W;
     const double xx = geo[G_XX], yy = geo[G_YY];
     const double *box = geo + G_BOX;
+    // the loops run over the fixed WLS_MAXM slots with the members' count as a
+    // predicate, so the arrays stay in registers (the sums keep their order)
     double wphi[WLS_MAXM];
-    for (int i = 0; i < m; ++i) wphi[i] = w[i] * phi[i];
+#pragma unroll
+    for (int i = 0; i < WLS_MAXM; ++i) wphi[i] = i < m ? w[i] * phi[i] : 0.0;
     double pt[6];
     {
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0, s5 = 0.0;
-        for (int i = 0; i < m; ++i) {
+#pragma unroll
+        for (int i = 0; i < WLS_MAXM; ++i) {
+            if (i >= m) continue;
             const double xi = x[i], yi = y[i], wp = wphi[i];
             s0 = s0 + 1.0 * wp;
             s1 = s1 + xi * wp;
@@ -338,12 +343,16 @@ __device__ __forceinline__ double wls_eval_var(const double *__restrict__ geo, i
                              xx * xx * arr[4] + yy * yy * arr[5];
     const double sm_large = smooth2(arr, box);
     double p1[3] = {0.0, 0.0, 0.0}, p2[3] = {0.0, 0.0, 0.0};
-    for (int i = 0; i < m1; ++i) {
+#pragma unroll
+    for (int i = 0; i < WLS_MAXM; ++i) {
+        if (i >= m1) continue;
         p1[0] = p1[0] + 1.0 * wphi[i];
         p1[1] = p1[1] + x[i] * wphi[i];
         p1[2] = p1[2] + y[i] * wphi[i];
     }
-    for (int i = m1; i < m; ++i) {
+#pragma unroll
+    for (int i = 0; i < WLS_MAXM; ++i) {
+        if (i < m1 || i >= m) continue;
         p2[0] = p2[0] + 1.0 * wphi[i];
         p2[1] = p2[1] + x[i] * wphi[i];
         p2[2] = p2[2] + y[i] * wphi[i];
