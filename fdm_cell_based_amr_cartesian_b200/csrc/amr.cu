@@ -366,6 +366,15 @@ static int scan_total32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t 
     return FDM_OK;
 }
 
+// exclusive scan without reading the total back
+static int scan_i32_only(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n) {
+    size_t bytes = 0;
+    FDM_CK(h, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, h->s));
+    FDM_CK(h, h->cub_tmp.ensure(bytes));
+    FDM_CK(h, cub::DeviceScan::ExclusiveSum(h->cub_tmp.p, bytes, in, out, (int)n, h->s));
+    return FDM_OK;
+}
+
 // internal nodes and their interpA values from the current leaf set
 // (values as the reference's import of a leaf set would give them)
 int init_internal(fdm_handle *h) {
@@ -1685,8 +1694,9 @@ int run_amr(fdm_handle *h) {
     int32_t *ol = cs.at<int32_t>(h->amr[8], 2), *oi = cs.at<int32_t>(h->amr[8], 3);
     k_split_count<<<nblk(n, TB), TB, 0, h->s>>>(n, X.A.leaf, fl, fi);
     int64_t nleaf = 0, nint = 0;
+    AMR_RC(scan_i32_only(h, fi, oi, n));
     AMR_RC(scan_total32(h, fl, ol, n, nleaf));
-    AMR_RC(scan_total32(h, fi, oi, n, nint));
+    nint = n - nleaf;   // every node is one or the other
     DevBuf &lk = h->amr[20], &lv = h->amr[21];   // kept between regrids
     FDM_CK(h, lk.ensure(nleaf * 8 + 8));
     FDM_CK(h, lv.ensure(nleaf * 32 + 32));

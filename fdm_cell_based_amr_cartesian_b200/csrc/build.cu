@@ -614,14 +614,23 @@ static int scan_i32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n) {
     FDM_CK(h, cub::DeviceScan::ExclusiveSum(h->cub_tmp.p, bytes, in, out, (int)n, h->s));
     return FDM_OK;
 }
-// total of an exclusive scan: last scan value + last flag
-static int scan_total(fdm_handle *h, const int32_t *flags, const int32_t *scan, int64_t n, int64_t &total) {
-    if (n == 0) { total = 0; return FDM_OK; }
-    int32_t a = 0, b = 0;
-    FDM_CK(h, cudaMemcpyAsync(&a, flags + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
-    FDM_CK(h, cudaMemcpyAsync(&b, scan + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
+// totals of exclusive scans, written on the device (read back later in one copy)
+static __global__ void k_scan_total(const int32_t *__restrict__ flags, const int32_t *__restrict__ scan, int64_t n,
+                             int64_t *out) {
+    if (threadIdx.x == 0) *out = n > 0 ? (int64_t)flags[n - 1] + scan[n - 1] : 0;
+}
+static __global__ void k_iota_b(int64_t n, int32_t *a) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (int32_t)i;
+}
+static __global__ void k_set_lmax(const int32_t *lmax, DevScalars *sc) {
+    if (threadIdx.x == 0) sc->l_max = *lmax;
+}
+// the error flags and up to 6 totals in one read-back
+static int read_back(fdm_handle *h, int32_t he[8], int64_t *tot, int nt) {
+    FDM_CK(h, cudaMemcpyAsync(he, h->flag.p, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
+    if (nt > 0) FDM_CK(h, cudaMemcpyAsync(tot, h->tmp[7].p, nt * sizeof(int64_t), cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
-    total = (int64_t)a + b;
     return FDM_OK;
 }
 
@@ -642,18 +651,17 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     FDM_CK(h, h->lkey.ensure(n * 8));
     FDM_CK(h, h->tmp[0].ensure(n * 4));   // iota
     FDM_CK(h, h->tmp[1].ensure(n * 4));   // perm
+    FDM_CK(h, h->tmp[7].ensure(6 * sizeof(int64_t)));
+    int64_t *dtot = h->tmp[7].as<int64_t>();
     {
         int32_t *iota = h->tmp[0].as<int32_t>();
-        std::vector<int32_t> hi((size_t)n);
-        for (int64_t k = 0; k < n; ++k) hi[(size_t)k] = (int32_t)k;
-        FDM_CK(h, cudaMemcpyAsync(iota, hi.data(), n * 4, cudaMemcpyHostToDevice, s));
+        k_iota_b<<<nblk(n, TB), TB, 0, s>>>(n, iota);
         size_t bytes = 0;
         FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
                                                   h->tmp[1].as<int32_t>(), (int)n, 0, 64, s));
         FDM_CK(h, h->cub_tmp.ensure(bytes));
         FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
                                                   h->tmp[1].as<int32_t>(), (int)n, 0, 64, s));
-        FDM_CK(h, cudaStreamSynchronize(s));   // host iota buffer
     }
     const uint64_t *lkey = h->lkey.as<uint64_t>();
     const int32_t *perm = h->tmp[1].as<int32_t>();
@@ -669,12 +677,14 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     FDM_RC(scan_i32(h, fG, sG, n));
     FDM_RC(scan_i32(h, fC, sC, n));
     int64_t NI, NG, NC;
-    FDM_RC(scan_total(h, fI, sI, n, NI));
-    FDM_RC(scan_total(h, fG, sG, n, NG));
-    FDM_RC(scan_total(h, fC, sC, n, NC));
     {
+        k_scan_total<<<1, 32, 0, s>>>(fI, sI, n, dtot);
+        k_scan_total<<<1, 32, 0, s>>>(fG, sG, n, dtot + 1);
+        k_scan_total<<<1, 32, 0, s>>>(fC, sC, n, dtot + 2);
         int32_t he[8];
-        FDM_CK(h, cudaMemcpy(he, err, sizeof(he), cudaMemcpyDeviceToHost));
+        int64_t tot[3];
+        FDM_RC(read_back(h, he, tot, 3));
+        NI = tot[0]; NG = tot[1]; NC = tot[2];
         if (he[BE_ROOT]) return arg_fail(h, "leaf key names a background cell outside the m x n grid");
         if (he[BE_PARTITION]) return arg_fail(h, "leaf set does not partition the background grid (gap, overlap or duplicate)");
         if (he[BE_LEVEL]) return arg_fail(h, "leaf level above the supported maximum (14)");
@@ -710,10 +720,10 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     k_req_flags<<<nblk(ne, TB), TB, 0, s>>>(ne, RO.slot, rflag);
     FDM_RC(scan_i32(h, rflag, ridx, ne));
     int64_t NR;
-    FDM_RC(scan_total(h, rflag, ridx, ne, NR));
     {
+        k_scan_total<<<1, 32, 0, s>>>(rflag, ridx, ne, dtot);
         int32_t he[8];
-        FDM_CK(h, cudaMemcpy(he, err, sizeof(he), cudaMemcpyDeviceToHost));
+        FDM_RC(read_back(h, he, &NR, 1));
         if (he[BE_NULLNB]) return arg_fail(h, "an interior leaf has a null stencil neighbour (fewer than 3 ghost layers?)");
     }
     h->NR = NR;
@@ -772,8 +782,15 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     FDM_RC(scan_i32(h, ux, sx, NI));
     FDM_RC(scan_i32(h, uy, sy, NI));
     int64_t nux, nuy;
-    FDM_RC(scan_total(h, ux, sx, NI, nux));
-    FDM_RC(scan_total(h, uy, sy, NI, nuy));
+    {
+        k_scan_total<<<1, 32, 0, s>>>(ux, sx, NI, dtot);
+        k_scan_total<<<1, 32, 0, s>>>(uy, sy, NI, dtot + 1);
+        int32_t he[8];
+        int64_t tot[2];
+        FDM_RC(read_back(h, he, tot, 2));
+        nux = tot[0];
+        nuy = tot[1];
+    }
     h->nux = nux; h->nuy = nuy;
     FDM_CK(h, h->ifxl.ensure(NI * 4));
     FDM_CK(h, h->ifyl.ensure(NI * 4));
@@ -807,6 +824,7 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     int32_t *dl = err + 7;
     FDM_CK(h, cudaMemsetAsync(dl, 0, 4, s));
     k_lmax<<<nblk(NI, TB), TB, 0, s>>>(NI, h->ilvl.as<uint8_t>(), dl);
+    k_set_lmax<<<1, 32, 0, s>>>(dl, h->scal.as<DevScalars>());
     int32_t he[8];
     unsigned long long hc[5];
     FDM_CK(h, cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, s));
@@ -816,7 +834,6 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     if (he[BE_OVERFLOW]) return arg_fail(h, "hanging-node stencil larger than supported");
     if (he[BE_INDEX]) return arg_fail(h, "internal table check failed: an index is out of range");
     h->l_max = he[7];
-    FDM_CK(h, cudaMemcpy(&h->scal.as<DevScalars>()->l_max, &h->l_max, 4, cudaMemcpyHostToDevice));
     h->n_singular += (int64_t)hc[0];
     h->n_restrict = (int64_t)hc[2];
     h->n_ghost_restrict = (int64_t)hc[4];
