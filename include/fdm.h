@@ -195,7 +195,12 @@ int fdm_residual(fdm_handle *h, double res_max[4], double res_rms[4]);
  * output: step control, Time_advance_RK, tt update, NaN check, and AMR +
  * boundary refill when iflag_amr.  Returns FDM_ERR_NAN on a NaN residual. */
 int fdm_solute_step(fdm_handle *h);
-/* Run solute steps until tt >= t_end or nsteps were taken. */
+/* Run solute steps until tt >= t_end or nsteps were taken: the same
+ * iterations as fdm_solute_step, replayed as a CUDA graph in chunks that end
+ * at the next regrid, with the scalars read once per chunk.  On the device an
+ * iteration after t_end or after a NaN residual changes nothing, so
+ * *steps_done counts the iterations actually taken; returns FDM_ERR_NAN
+ * after the iteration whose residual is NaN. */
 int fdm_solute(fdm_handle *h, int64_t nsteps, int64_t *steps_done);
 
 /* Run nsteps solute iterations on the device (step control, RK3 step,
