@@ -205,6 +205,29 @@ def test_nan_state_stops(oracle_mod):
     assert e.value.code == 3
 
 
+def test_nan_state_stops_the_chunked_solute(oracle_mod):
+    """fdm_solute replays the step graph in chunks: the iteration with the
+    NaN residual is the last one that changes anything (the reference stops
+    there), so the device's step counter ends one past where it started and
+    the state stays as that iteration left it."""
+    cfg = P.vortex(lvl_amr=0)
+    o = oracle_mod.Oracle(cfg)
+    keys, prim, s = snapshot(o)
+    prim[(cfg.n // 2) * cfg.m + cfg.m // 2, 0] = np.nan
+    g = gpu_from(cfg, keys, prim, s)
+    it0 = g.scalars()["it"]
+    with pytest.raises(FdmError) as e:
+        g.solute(7)
+    assert e.value.code == 3
+    assert g.scalars()["it"] == it0 + 1
+    _, after = g.leaves()
+    g.advance(3)   # further iterations are no-ops
+    _, later = g.leaves()
+    assert np.array_equal(np.isnan(after), np.isnan(later))
+    assert np.array_equal(np.nan_to_num(after), np.nan_to_num(later))
+    assert g.scalars()["it"] == it0 + 1
+
+
 def test_distance_refined_mesh_steps(oracle_mod):
     """The benchmark's kind of mesh (statically refined bands, 4 levels,
     ghost cells refined with the interior) uploaded to both sides."""
