@@ -228,6 +228,29 @@ def test_nan_state_stops_the_chunked_solute(oracle_mod):
     assert g.scalars()["it"] == it0 + 1
 
 
+def test_face_launch_shapes_agree(oracle_mod):
+    """Every launch shape of the face kernel that the autotuner chooses from
+    (one or four threads per face, block sizes) gives
+    the same bits after two steps on a refined mesh with hanging nodes."""
+    from fdm_cell_based_amr_cartesian_b200.solver import FACE_VARIANTS, distance_refined_keys, initial_state
+    cfg = P.riemann4(base=32, lvl_amr=3, pstep_adapt=1000)
+    keys = distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], [0.2, 0.1, 0.05])
+    prim = initial_state(cfg, keys)
+    ref = None
+    for v in range(FACE_VARIANTS):
+        g = Solver(cfg)
+        g.upload(keys, prim)
+        g.set_variant(v)
+        for _ in range(2):
+            g.time_advance_rk(g.step_control())
+        out = g.leaves()[1]
+        g.close()
+        if ref is None:
+            ref = out
+        else:
+            assert np.array_equal(out, ref), f"face variant {v}"
+
+
 def test_distance_refined_mesh_steps(oracle_mod):
     """The benchmark's kind of mesh (statically refined bands, 4 levels,
     ghost cells refined with the interior) uploaded to both sides."""
