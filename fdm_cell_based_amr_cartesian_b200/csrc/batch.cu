@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
         if (!M.gate_on) {
             const int64_t f = lt * BT + threadIdx.x;
             if (f < nf) {
-                if (dir == 0) face_item<0>(M.T, cur, M.Fx, lam, M.gama, f);
-                else face_item<1>(M.T, cur, M.Fy, lam, M.gama, f);
+                if (dir == 0) face_item<0, false>(M.T, cur, M.Fx, lam, M.gama, f);
+                else face_item<1, false>(M.T, cur, M.Fy, lam, M.gama, f);
             }
             return;
         }
@@ -301,10 +301,10 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
             const int64_t tx = cdiv(M.GL.cnt[0], BT);
             if (t < tx) {
                 const int64_t i = t * BT + threadIdx.x;
-                if (i < M.GL.cnt[0]) face_item<0>(M.T, cur, M.Fx, M.sc->lambda_x, M.gama, M.GL.hx[i]);
+                if (i < M.GL.cnt[0]) face_item<0, false>(M.T, cur, M.Fx, M.sc->lambda_x, M.gama, M.GL.hx[i]);
             } else {
                 const int64_t i = (t - tx) * BT + threadIdx.x;
-                if (i < M.GL.cnt[1]) face_item<1>(M.T, cur, M.Fy, M.sc->lambda_y, M.gama, M.GL.hy[i]);
+                if (i < M.GL.cnt[1]) face_item<1, false>(M.T, cur, M.Fy, M.sc->lambda_y, M.gama, M.GL.hy[i]);
             }
         });
         BAR_STAMP(5);

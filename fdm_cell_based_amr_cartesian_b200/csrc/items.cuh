@@ -220,14 +220,14 @@ __device__ __forceinline__ void face_slots(const Tables &T, int64_t f, int32_t &
     }
 }
 
-template <int DIR>
+template <int DIR, bool SPLIT = true>
 __device__ __forceinline__ void face_item(const Tables &T, const double4 *__restrict__ cur, double4 *F, double lam,
                                           double g, int64_t f) {
     int32_t a, b, c, d;
     face_slots<DIR>(T, f, a, b, c, d);
     const Prim p0 = load_prim(cur, a), p1 = load_prim(cur, b), p2 = load_prim(cur, c), p3 = load_prim(cur, d);
     double out[4];
-    face_flux<DIR>(p0, p1, p2, p3, g, lam, out);
+    face_flux<DIR, SPLIT>(p0, p1, p2, p3, g, lam, out);
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 

@@ -163,46 +163,103 @@ __device__ __forceinline__ double wcns_z3(double u1, double u2, double u3) {
     return w1 * p1 + w2 * p2;
 }
 
+// the conserved state of cons_flux alone (the same operations)
+template <int DIR>
+__device__ __forceinline__ void cons_state(const Prim &q, double g, double U[4]) {
+    const double ke = q.u * q.u + q.v * q.v;
+    U[0] = q.r;
+    U[1] = q.r * q.u;
+    U[2] = q.r * q.v;
+    U[3] = q.p / (g - 1.0) + 0.5 * q.r * ke;
+}
 // Numerical flux at the face between s1 and s2 from the 4-point stencil
 // s0..s3 (one half of LXL_X_wcns3 / LXL_Y_wcns3, src/nnd_center_RK.F90:84-106,
 // 205-227): characteristic projection at the face mean, four WCNS_Z3
 // reconstructions and the global Lax-Friedrichs split.
-template <int DIR>
+template <int DIR, bool SPLIT = true>
 __device__ __forceinline__ void face_flux(const Prim &s0, const Prim &s1, const Prim &s2,
                                           const Prim &s3, double g, double lam, double out[4]) {
-    double U0[4], U1[4], U2[4], U3[4], F0[4], F1[4], F2[4], F3[4];
-    cons_flux<DIR>(s0, g, U0, F0);
-    cons_flux<DIR>(s1, g, U1, F1);
-    cons_flux<DIR>(s2, g, U2, F2);
-    cons_flux<DIR>(s3, g, U3, F3);
-    double Um[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
-    Eig E;
-    eigen<DIR>(Um, g, E);
-    double w0[4], w1[4], w2[4], w3[4];
-    double uwL[4], uwR[4], ugL[4], ugR[4];
-    project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
-    project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        uwL[r] = wcns_z3(w0[r], w1[r], w2[r]);
-        uwR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+    if constexpr (SPLIT) {
+        // The state half (U, its projections and reconstructions, back-projected)
+        // is finished before the flux half starts, so the four conserved states
+        // and the four fluxes are never held at once (fewer registers); every
+        // value is formed by the same operations as in the reference's order.
+        double wL[4], wR[4];
+        Eig E;
+        {
+            double U0[4], U1[4], U2[4], U3[4];
+            cons_state<DIR>(s1, g, U1);
+            cons_state<DIR>(s2, g, U2);
+            double Um[4];
+    #pragma unroll
+            for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
+            eigen<DIR>(Um, g, E);
+            cons_state<DIR>(s0, g, U0);
+            cons_state<DIR>(s3, g, U3);
+            double w0[4], w1[4], w2[4], w3[4], uwL[4], uwR[4];
+            project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
+            project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
+    #pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                uwL[r] = wcns_z3(w0[r], w1[r], w2[r]);
+                uwR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+            }
+            back_project<DIR>(E, uwL, wL);
+            back_project<DIR>(E, uwR, wR);
+        }
+        double F0[4], F1[4], F2[4], F3[4];
+        phys_flux<DIR>(s0, g, F0); phys_flux<DIR>(s1, g, F1);
+        phys_flux<DIR>(s2, g, F2); phys_flux<DIR>(s3, g, F3);
+        double w0[4], w1[4], w2[4], w3[4], ugL[4], ugR[4];
+        project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
+        project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
+    #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            ugL[r] = wcns_z3(w0[r], w1[r], w2[r]);
+            ugR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+        }
+        double gL[4], gR[4];
+        back_project<DIR>(E, ugL, gL);
+        back_project<DIR>(E, ugR, gR);
+    #pragma unroll
+        for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
+    } else {
+        // the same values with the four states and fluxes formed first (for
+        // the batched kernel, whose register budget this order suits better)
+        double U0[4], U1[4], U2[4], U3[4], F0[4], F1[4], F2[4], F3[4];
+        cons_flux<DIR>(s0, g, U0, F0);
+        cons_flux<DIR>(s1, g, U1, F1);
+        cons_flux<DIR>(s2, g, U2, F2);
+        cons_flux<DIR>(s3, g, U3, F3);
+        double Um[4];
+    #pragma unroll
+        for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
+        Eig E;
+        eigen<DIR>(Um, g, E);
+        double w0[4], w1[4], w2[4], w3[4];
+        double uwL[4], uwR[4], ugL[4], ugR[4];
+        project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
+        project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
+    #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            uwL[r] = wcns_z3(w0[r], w1[r], w2[r]);
+            uwR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+        }
+        project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
+        project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
+    #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            ugL[r] = wcns_z3(w0[r], w1[r], w2[r]);
+            ugR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+        }
+        double wL[4], wR[4], gL[4], gR[4];
+        back_project<DIR>(E, uwL, wL);
+        back_project<DIR>(E, uwR, wR);
+        back_project<DIR>(E, ugL, gL);
+        back_project<DIR>(E, ugR, gR);
+    #pragma unroll
+        for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
     }
-    project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
-    project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        ugL[r] = wcns_z3(w0[r], w1[r], w2[r]);
-        ugR[r] = wcns_z3(w3[r], w2[r], w1[r]);
-    }
-    double wL[4], wR[4], gL[4], gR[4];
-    back_project<DIR>(E, uwL, wL);
-    back_project<DIR>(E, uwR, wR);
-    back_project<DIR>(E, ugL, gL);
-    back_project<DIR>(E, ugR, gR);
-#pragma unroll
-    for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
 }
 
 // ------------------------------------------------ face flux, 4 lanes/face
