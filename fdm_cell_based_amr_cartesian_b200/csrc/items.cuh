@@ -225,9 +225,13 @@ __device__ __forceinline__ void face_item(const Tables &T, const double4 *__rest
                                           double g, int64_t f) {
     int32_t a, b, c, d;
     face_slots<DIR>(T, f, a, b, c, d);
-    const Prim p0 = load_prim(cur, a), p1 = load_prim(cur, b), p2 = load_prim(cur, c), p3 = load_prim(cur, d);
     double out[4];
-    face_flux<DIR, SPLIT>(p0, p1, p2, p3, g, lam, out);
+    if constexpr (SPLIT) {   // the records read again for the flux half: fewer live registers
+        face_flux_slots<DIR>(cur, a, b, c, d, g, lam, out);
+    } else {
+        const Prim p0 = load_prim(cur, a), p1 = load_prim(cur, b), p2 = load_prim(cur, c), p3 = load_prim(cur, d);
+        face_flux<DIR, false>(p0, p1, p2, p3, g, lam, out);
+    }
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 

@@ -163,6 +163,17 @@ __device__ __forceinline__ double wcns_z3(double u1, double u2, double u3) {
     return w1 * p1 + w2 * p2;
 }
 
+// the record of slot i read again through the non-coherent path, as an
+// opaque load (the optimiser may not replace it by an earlier read, so the
+// earlier values need not stay in registers)
+__device__ __forceinline__ Prim load_prim_again(const double4 *s, int64_t i) {
+    const double *p = reinterpret_cast<const double *>(s + i);
+    double a, b, c, d;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%4];\n\tld.global.nc.v2.f64 {%2, %3}, [%4+16];"
+                 : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+                 : "l"(p));
+    return Prim{a, b, c, d};
+}
 // the conserved state of cons_flux alone (the same operations)
 template <int DIR>
 __device__ __forceinline__ void cons_state(const Prim &q, double g, double U[4]) {
@@ -260,6 +271,55 @@ __device__ __forceinline__ void face_flux(const Prim &s0, const Prim &s1, const 
     #pragma unroll
         for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
     }
+}
+
+// face_flux in the split order, reading the stencil records (slots a..d of
+// cur) once for the state half and again for the flux half
+template <int DIR>
+__device__ __forceinline__ void face_flux_slots(const double4 *__restrict__ cur, int32_t ia, int32_t ib,
+                                                int32_t ic, int32_t id, double g, double lam, double out[4]) {
+    double wL[4], wR[4];
+    Eig E;
+    {
+        const Prim s0 = load_prim(cur, ia), s1 = load_prim(cur, ib), s2 = load_prim(cur, ic), s3 = load_prim(cur, id);
+        double U0[4], U1[4], U2[4], U3[4];
+        cons_state<DIR>(s1, g, U1);
+        cons_state<DIR>(s2, g, U2);
+        double Um[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
+        eigen<DIR>(Um, g, E);
+        cons_state<DIR>(s0, g, U0);
+        cons_state<DIR>(s3, g, U3);
+        double w0[4], w1[4], w2[4], w3[4], uwL[4], uwR[4];
+        project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
+        project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            uwL[r] = wcns_z3(w0[r], w1[r], w2[r]);
+            uwR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+        }
+        back_project<DIR>(E, uwL, wL);
+        back_project<DIR>(E, uwR, wR);
+    }
+    double F0[4], F1[4], F2[4], F3[4];
+    phys_flux<DIR>(load_prim_again(cur, ia), g, F0);
+    phys_flux<DIR>(load_prim_again(cur, ib), g, F1);
+    phys_flux<DIR>(load_prim_again(cur, ic), g, F2);
+    phys_flux<DIR>(load_prim_again(cur, id), g, F3);
+    double w0[4], w1[4], w2[4], w3[4], ugL[4], ugR[4];
+    project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
+    project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        ugL[r] = wcns_z3(w0[r], w1[r], w2[r]);
+        ugR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+    }
+    double gL[4], gR[4];
+    back_project<DIR>(E, ugL, gL);
+    back_project<DIR>(E, ugR, gR);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
 }
 
 // ------------------------------------------------ face flux, 4 lanes/face
