@@ -140,13 +140,62 @@ __device__ __forceinline__ void face_flux_f(const Prim &s0, const Prim &s1, cons
     for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
 }
 
+// the same flux with the state half finished before the flux half, and the
+// stencil records read again for the flux half (fewer live registers)
+template <int DIR>
+__device__ __forceinline__ void face_flux_f_slots(const double4 *__restrict__ cur, int32_t ia, int32_t ib,
+                                                  int32_t ic, int32_t id, double g, double ig1, double lam,
+                                                  double out[4]) {
+    double wL[4], wR[4];
+    Eig E;
+    {
+        double U0[4], U1[4], U2[4], U3[4], Fd[4];
+        cons_flux_f<DIR>(load_prim(cur, ib), ig1, U1, Fd);
+        cons_flux_f<DIR>(load_prim(cur, ic), ig1, U2, Fd);
+        double Um[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) Um[r] = 0.5 * (U1[r] + U2[r]);
+        eigen_f<DIR>(Um, g, ig1, E);
+        cons_flux_f<DIR>(load_prim(cur, ia), ig1, U0, Fd);
+        cons_flux_f<DIR>(load_prim(cur, id), ig1, U3, Fd);
+        double w0[4], w1[4], w2[4], w3[4], uwL[4], uwR[4];
+        project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
+        project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            uwL[r] = wcns_z3_f(w0[r], w1[r], w2[r]);
+            uwR[r] = wcns_z3_f(w3[r], w2[r], w1[r]);
+        }
+        back_project<DIR>(E, uwL, wL);
+        back_project<DIR>(E, uwR, wR);
+    }
+    double F0[4], F1[4], F2[4], F3[4], Ud[4];
+    cons_flux_f<DIR>(load_prim_again(cur, ia), ig1, Ud, F0);
+    cons_flux_f<DIR>(load_prim_again(cur, ib), ig1, Ud, F1);
+    cons_flux_f<DIR>(load_prim_again(cur, ic), ig1, Ud, F2);
+    cons_flux_f<DIR>(load_prim_again(cur, id), ig1, Ud, F3);
+    double w0[4], w1[4], w2[4], w3[4], ugL[4], ugR[4];
+    project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
+    project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        ugL[r] = wcns_z3_f(w0[r], w1[r], w2[r]);
+        ugR[r] = wcns_z3_f(w3[r], w2[r], w1[r]);
+    }
+    double gL[4], gR[4];
+    back_project<DIR>(E, ugL, gL);
+    back_project<DIR>(E, ugR, gR);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
+}
+
 template <int DIR>
 __device__ __forceinline__ void face_item(const Tables &T, const double4 *__restrict__ cur, double4 *F, double lam,
                                           double g, double ig1, int64_t f) {
     int32_t a, b, c, d;
     face_slots<DIR>(T, f, a, b, c, d);
     double out[4];
-    face_flux_f<DIR>(load_prim(cur, a), load_prim(cur, b), load_prim(cur, c), load_prim(cur, d), g, ig1, lam, out);
+    face_flux_f_slots<DIR>(cur, a, b, c, d, g, ig1, lam, out);
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 
