@@ -361,7 +361,7 @@ struct fdm_batch {
     cudaStream_t s = nullptr;
     DevBuf d_mem, d_off, d_ctr, d_bar, d_act, d_skip, d_stamp;
     std::vector<int32_t> h_skip;
-    int grid = 0, blocks_per_sm = 0, want_bps = 2;
+    int grid = 0, blocks_per_sm = 0, want_bps = 2;   // want_bps 0: the members' own step graphs
     size_t smem = 0;
     bool any_gate = false;
     cudaGraphExec_t graph = nullptr;
@@ -456,6 +456,10 @@ static bool batch_stale(const fdm_batch *b) {
 }
 
 static int batch_grid(fdm_batch *b) {
+    if (b->want_bps == 0) {   // no persistent kernel
+        b->blocks_per_sm = 0;
+        return FDM_OK;
+    }
     int sms = 0, bps = 0;
     BCK(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
     if (b->want_bps == 1) {
@@ -553,7 +557,30 @@ static int release_members(fdm_batch *b) {
     return FDM_OK;
 }
 
+// the streams strategy: each active member's step graph on its own stream,
+// after the batch stream's queued work and before the batch stream's next
+static int launch_member_steps(fdm_batch *b, int64_t nsteps, const std::vector<int32_t> *regrid_next,
+                               const std::vector<bool> *active) {
+    int rc = release_members(b);
+    if (rc) return rc;
+    for (size_t m = 0; m < b->mem.size(); ++m) {
+        if (active && !(*active)[m]) continue;
+        fdm_handle *h = b->mem[m];
+        for (int64_t k = 0; k < nsteps; ++k) {
+            rc = member_launch_step(h, regrid_next && (*regrid_next)[m] != 0 && k + 1 == nsteps);
+            if (rc) { b->err = "member " + std::to_string(m) + ": " + h->err; return rc; }
+        }
+    }
+    return join_members(b);
+}
+
 static int check_barrier(fdm_batch *b) {
+    if (b->want_bps == 0) {   // no grid barrier: the members' streams
+        int rc = join_members(b);
+        if (rc) return rc;
+        BCK(b, cudaStreamSynchronize(b->s));
+        return FDM_OK;
+    }
     GridBar gb;
     BCK(b, cudaMemcpyAsync(&gb, b->d_bar.p, sizeof gb, cudaMemcpyDeviceToHost, b->s));
     BCK(b, cudaStreamSynchronize(b->s));
@@ -633,6 +660,12 @@ int fdm_batch_advance(fdm_batch *b, int64_t nsteps) {
         int rc = member_ready(h);
         if (rc) { b->err = "member: " + h->err; return rc; }
     }
+    if (b->want_bps == 0) {
+        int rc = launch_member_steps(b, nsteps, nullptr, nullptr);
+        if (rc) return rc;
+        for (fdm_handle *h : b->mem) member_stepped(h);
+        return FDM_OK;
+    }
     std::fill(b->h_skip.begin(), b->h_skip.end(), 0);
     int rc = join_members(b);
     if (rc) return rc;
@@ -672,17 +705,24 @@ int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done) {
             BCK(b, cudaMemcpyAsync(&hs[m], b->mem[m]->scal.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, b->s));
         BCK(b, cudaStreamSynchronize(b->s));
         bool any = false;
+        std::vector<bool> act(n, false);
         for (int m = 0; m < n; ++m) {
             const bool active = !hs[m].done && hs[m].tt < b->mem[m]->p.t_end;
+            act[m] = active;
             any = any || active;
             b->h_skip[m] = active && member_amr_due(b->mem[m], hs[m].it + 1) ? 1 : 0;
         }
         if (!any) break;
-        BCK(b, cudaMemcpyAsync(b->d_skip.p, b->h_skip.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, b->s));
-        rc = batch_graph(b);
-        if (rc) break;
-        rc = launch_step(b);
-        if (rc) break;
+        if (b->want_bps == 0) {
+            rc = launch_member_steps(b, 1, &b->h_skip, &act);
+            if (rc) break;
+        } else {
+            BCK(b, cudaMemcpyAsync(b->d_skip.p, b->h_skip.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, b->s));
+            rc = batch_graph(b);
+            if (rc) break;
+            rc = launch_step(b);
+            if (rc) break;
+        }
         rc = check_barrier(b);
         if (rc) break;
         for (int m = 0; m < n; ++m)
@@ -714,10 +754,12 @@ int fdm_batch_sync(fdm_batch *b) {
     return check_barrier(b);
 }
 
-// 1 or 2 resident blocks per SM for the persistent kernel; the next graph
-// uses the new grid.
+// 1 or 2 resident blocks per SM for the persistent kernel (the next graph
+// uses the new grid), or 0: no persistent kernel, each member's own step
+// graph on its own stream (faster when the members are large enough to fill
+// the GPU between them).
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t bps) {
-    if (!b || bps < 1 || bps > 2) return FDM_ERR_ARG;
+    if (!b || bps < 0 || bps > 2) return FDM_ERR_ARG;
     b->want_bps = bps;
     int rc = batch_grid(b);
     if (rc) return rc;

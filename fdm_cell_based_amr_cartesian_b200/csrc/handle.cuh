@@ -192,6 +192,7 @@ int member_ready(fdm_handle *h);
 void member_stepped(fdm_handle *h);
 bool member_amr_due(const fdm_handle *h, int64_t it);
 int member_regrid(fdm_handle *h);
+int member_launch_step(fdm_handle *h, bool regrid_next);
 void launch_step_control(fdm_handle *h);
 void launch_step_end(fdm_handle *h);
 void launch_set_tstep(fdm_handle *h, double tstep);

@@ -704,6 +704,17 @@ void member_stepped(fdm_handle *h) {
     if (h->gate_on) h->gate_stage1_valid = true;
 }
 bool member_amr_due(const fdm_handle *h, int64_t it) { return amr_due(h, it); }
+// One solute iteration of member h on its own stream, through its step
+// graph: followed by the j = 1 ghost refresh unless a regrid comes next
+// (member_regrid refreshes after it), as fdm_solute does.
+int member_launch_step(fdm_handle *h, bool regrid_next) {
+    RC(ensure_lambda(h));
+    cudaGraphExec_t g = nullptr;
+    RC(step_graph(h, &g, h->p.iflag_amr != 0 && !regrid_next));
+    FDM_CK(h, cudaGraphLaunch(g, h->s));
+    h->lam_fresh = true;
+    return FDM_OK;
+}
 int member_regrid(fdm_handle *h) {
     int rc = fdm_amr(h);
     if (rc) return rc;

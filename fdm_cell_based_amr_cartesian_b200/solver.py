@@ -451,6 +451,8 @@ class Batch:
         self._check(self.L.fdm_batch_sync(self.b))
 
     def set_blocks_per_sm(self, k: int):
+        """1 or 2 resident blocks per SM for the persistent kernel, or 0: each
+        member's own step graph on its own stream."""
         self._check(self.L.fdm_batch_set_blocks_per_sm(self.b, int(k)))
 
     def info(self) -> dict:

@@ -105,3 +105,31 @@ def test_one_and_two_blocks_per_sm_agree():
     b2.sync()
     for (x, y) in pa:
         _assert_same(x, y)
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+def test_streams_strategy_matches_single():
+    """blocks_per_sm 0: no persistent kernel, each member's own step graph
+    on its own stream; regrids, the gate and t_end as in the kernel path."""
+    cfgs = _cfgs() + [P.riemann4(base=32, lvl_amr=2, t_end=0.004)]
+    pairs = [_pair(c, gate=(k % 2 == 1)) for k, c in enumerate(cfgs)]
+    batch = Batch([p[0] for p in pairs])
+    batch.set_blocks_per_sm(0)
+    assert batch.info()["blocks_per_sm"] == 0
+    assert batch.solute(25) == 25
+    for (bm, solo) in pairs:
+        solo.solute(25)
+        _assert_same(bm, solo)
+    assert pairs[0][0].counters()["n_regrids"] >= 2
+
+
+def test_streams_strategy_advance_matches_single_steps():
+    cfgs = _cfgs(no_regrid=True)
+    pairs = [_pair(c) for c in cfgs]
+    batch = Batch([p[0] for p in pairs])
+    batch.set_blocks_per_sm(0)
+    batch.advance(6)
+    batch.sync()
+    for (bm, solo) in pairs:
+        solo.solute(6)
+        _assert_same(bm, solo)
