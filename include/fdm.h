@@ -322,6 +322,12 @@ int fdm_batch_last_error(const fdm_batch *b, char *buf, size_t n);
 int fdm_batch_advance(fdm_batch *b, int64_t nsteps);
 int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done);
 int fdm_batch_sync(fdm_batch *b);
+/* blocks_per_sm 1 or 2: resident blocks of the persistent kernel per SM;
+ * 0: no persistent kernel, each member's own step graph on its own stream
+ * (the batch stream is joined to the members' streams around every call,
+ * so ordering and event timing on the batch stream are unchanged).  Results
+ * are the same bits either way; which is faster depends on the members'
+ * sizes (measure both). */
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t blocks_per_sm);
 int fdm_batch_info(const fdm_batch *b, int32_t *grid, int32_t *blocks_per_sm,
                    int64_t *smem_bytes);
