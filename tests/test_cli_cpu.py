@@ -1,0 +1,24 @@
+"""The command-line run's options map to the reference's configurations (no
+GPU needed: only the parameter sets are built)."""
+import argparse
+
+from fdm_cell_based_amr_cartesian_b200.__main__ import config
+
+
+def _args(**kw):
+    base = dict(case="riemann4", base=128, lvl_amr=4, t_end=0.0, steps=0, gate=False)
+    base.update(kw)
+    return argparse.Namespace(**base)
+
+
+def test_cli_configurations():
+    c = config(_args())
+    assert c.params.t_end == 0.3 and int(c.params.lvl_amr) == 4
+    c = config(_args(case="riemann4", base=64, lvl_amr=3, t_end=0.1))
+    assert c.params.t_end == 0.1 and int(c.params.lvl_amr) == 3
+    c = config(_args(case="vortex", base=32, lvl_amr=2))
+    assert int(c.params.lvl_amr) == 2
+    c = config(_args(case="double_mach", base=16, lvl_amr=2))
+    assert c.params.t_end == 0.2
+    c = config(_args(case="reference"))
+    assert c.name == "reference_default"
