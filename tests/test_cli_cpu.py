@@ -13,6 +13,7 @@ def _args(**kw):
 
 def test_cli_configurations():
     c = config(_args())
+    assert (c.m, c.n) == (134, 134)   # 128 + 3 ghost layers each side
     assert c.params.t_end == 0.3 and int(c.params.lvl_amr) == 4
     c = config(_args(case="riemann4", base=64, lvl_amr=3, t_end=0.1))
     assert c.params.t_end == 0.1 and int(c.params.lvl_amr) == 3
