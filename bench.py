@@ -106,16 +106,21 @@ def measured_peaks():
         return None
 
 
-def profile_traffic():
-    """DRAM bytes per face-kernel launch from the committed ncu summary."""
+def profile_figure(name):
+    """A figure of the committed ncu summary of the face kernel (a line
+    'name: value'): DRAM bytes per x+y launch pair, FP64 pipe activity."""
     path = os.path.join(ROOT, "profiles", "face_flux_riemann4.md")
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(name + ":"):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
+
+
+def profile_traffic():
+    return profile_figure("traffic_bytes_per_launch")
 
 
 # ------------------------------------------------------------ CPU legs
@@ -567,7 +572,10 @@ def run_ours(args):
                              "peak_source": "measured" if peaks else "fallback"},
                 "roofline_fp64": {"achieved": face_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                                   "frac": face_tflops / fp64_peak, "flops_per_face": FLOPS_PER_FACE,
-                                  "peak_source": "measured DFMA probe"},
+                                  "peak_source": "measured DFMA probe",
+                                  "fp64_pipe_active_pct_ncu": profile_figure("fp64_pipe_active_pct"),
+                                  "note": "a correctly rounded division is one flop here but several FP64-pipe "
+                                          "instructions; the pipe figure is ncu's, from profiles/"},
                 "step_hbm": {"algorithmic_bytes_per_update": BYTES_PER_UPDATE, "achieved_gbs": step_gbs,
                              "frac": step_gbs / hbm_peak},
                 "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
