@@ -1,7 +1,7 @@
 """Golden final states of the oracle (the CPU restatement of the reference's
 solver) for whole runs with regrids, stored as digests in oracle_runs.json.
 
-    python tests/golden/make_golden.py            # the short cases
+    python tests/golden/make_golden.py            # the short cases (about 2 min on 8 cores)
     python tests/golden/make_golden.py --long     # also the four-quadrant
                                                   # problem at 128^2, 4 levels
                                                   # (about 25 min on 8 cores)
@@ -34,6 +34,10 @@ def cases(long=False):
     c = {
         "vortex_200_steps": (lambda: P.vortex(), 200),
         "riemann4_32_l2_to_t0.3": (lambda: P.riemann4(base=32, lvl_amr=2, t_end=0.3), None),
+        # the Mach-10 reflection: time-dependent top boundary, wall, inflow,
+        # a regrid every 5 steps (the larger one has non-leaf refinements)
+        "double_mach_64x16_l2_to_t0.2": (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), None),
+        "double_mach_128x32_l3_to_t0.2": (lambda: P.double_mach(base_y=32, lvl_amr=3, t_end=0.2), None),
     }
     if long:
         c["riemann4_128_l4_to_t0.3"] = (lambda: P.riemann4(base=128, lvl_amr=4, t_end=0.3), None)

@@ -16,7 +16,7 @@ import make_golden  # noqa: E402
 GOLDEN = json.load(open(os.path.join(HERE, "golden", "oracle_runs.json")))
 
 
-@pytest.mark.parametrize("name", ["vortex_200_steps", "riemann4_32_l2_to_t0.3"])
+@pytest.mark.parametrize("name", ["vortex_200_steps", "riemann4_32_l2_to_t0.3", "double_mach_64x16_l2_to_t0.2"])
 def test_oracle_reproduces_golden_run(oracle_mod, name):
     make, steps = make_golden.cases()[name]
     rec = make_golden.run(make, steps)

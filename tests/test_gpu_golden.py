@@ -1,8 +1,10 @@
 """The GPU solver (libfdm through the C-ABI) against the oracle's golden final
 states of whole runs with regrids: bit-identical leaf sets and states after
 the configuration-1 vortex (200 steps, 20 regrids), the four-quadrant
-problem at 32^2 / 2 levels, and (when recorded) the four-quadrant problem at
-128^2 / 4 levels to t = 0.3 (6032 steps, 604 regrids)."""
+problem at 32^2 / 2 levels, the double Mach reflection at 64x16 / 2 levels
+and 128x32 / 3 levels to t = 0.2 (698 steps with 140 regrids, 3011 steps with
+603 regrids), and (when recorded) the four-quadrant problem at 128^2 / 4
+levels to t = 0.3 (6032 steps, 604 regrids)."""
 import json
 import os
 import sys
