@@ -386,9 +386,42 @@ def ensemble_window(args, world):
             "gpu_launches_per_step": 3 if best_bps else None}
 
 
-def full_run(S, gate, ulp=False):
+GOLDEN_RUNS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "oracle_runs.json")
+
+
+def matches_golden(name, keys, prim, steps, regrids):
+    """True when the run ends on the oracle's recorded final leaf set and
+    states bit for bit (SHA-256 of the uint64 keys and the float64 states in
+    key order), False when it does not, None when the run is not recorded."""
+    import hashlib
+    if not os.path.exists(GOLDEN_RUNS):
+        return None
+    want = json.load(open(GOLDEN_RUNS)).get(name)
+    if want is None:
+        return None
+    hk = hashlib.sha256(np.ascontiguousarray(keys, dtype=np.uint64).tobytes()).hexdigest()
+    hp = hashlib.sha256(np.ascontiguousarray(prim, dtype=np.float64).tobytes()).hexdigest()
+    return bool(hk == want["sha256_keys"] and hp == want["sha256_prim"]
+                and steps == want["steps"] and regrids == want["regrids"])
+
+
+FULL_RUNS = {
+    # name: (configuration, description, golden record)
+    "riemann4": (lambda: P.riemann4(base=128, lvl_amr=4, t_end=0.3),
+                 "riemann4 128^2, 4 levels, t = 0 -> 0.3, regrid every 10 steps", "riemann4_128_l4_to_t0.3"),
+    "double_mach": (lambda: P.double_mach(base_y=64, lvl_amr=4, t_end=0.2),
+                    "double Mach reflection (Mach-10 shock, reflecting wall) 256x64, 4 levels, "
+                    "t = 0 -> 0.2, regrid every 5 steps", "double_mach_256x64_l4_to_t0.2"),
+}
+
+
+def full_run(S, gate, ulp=False, case="riemann4"):
     import torch
-    gf = S.Solver(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
+    make, desc, golden = FULL_RUNS[case]
+    cfg = make()
+    t_end = cfg.params.t_end
+    chunk = cfg.params.pstep_adapt
+    gf = S.Solver(cfg)
     gf.creat_mesh_and_initial()
     if ulp:
         _, p0 = gf.leaves()
@@ -404,22 +437,24 @@ def full_run(S, gate, ulp=False):
     upd = 0
     while True:
         before = gf.scalars()["tt"]
-        if before >= 0.3:
+        if before >= t_end:
             break
         ni = gf.counters()["n_interior"]
-        n = gf.solute(10)
+        n = gf.solute(chunk)
         steps += n
         upd += n * ni
         if n == 0:
             break
     t_full = time.perf_counter() - t0
     cf = gf.counters()
-    out = {"workload": "riemann4 128^2, 4 levels, t = 0 -> 0.3, regrid every 10 steps",
+    leaves = gf.leaves()
+    out = {"workload": desc,
            "seconds": t_full, "steps": steps, "regrids": cf["n_regrids"],
            "mean_updates_per_s": upd / t_full, "leaves_at_end": cf["n_leaves"],
            "regrid_device_ms_total": gf.amr_phase_ms(total=True),
            "gridmodify_counters": {k: v for k, v in cf.items() if "gm" in k}}
-    leaves = gf.leaves()
+    if not gate and not ulp:
+        out["bit_identical_to_oracle_run"] = matches_golden(golden, leaves[0], leaves[1], steps, cf["n_regrids"])
     gf.close()
     return out, leaves
 
@@ -553,6 +588,8 @@ def run_ours(args):
         l1, linf = LG.density_errors(cfg_full, leaves_plain, leaves_ulp)
         full["one_ulp_initial_density"] = {"steps": full_u["steps"], "regrids": full_u["regrids"],
                                            "l1_density_vs_plain": l1, "linf_density_vs_plain": linf}
+        # configuration 3: the Mach-10 reflection to t = 0.2, a regrid every 5 steps
+        full["double_mach"] = full_run(S, gate=False, case="double_mach")[0]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1

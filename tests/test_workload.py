@@ -42,3 +42,29 @@ def test_distance_refined_mesh_stays_finite(oracle_mod):
     _, p, _ = o.leaves()
     assert np.isfinite(p).all()
     assert p[:, 0].min() > 0.1 and p[:, 3].min() > 0.02
+
+
+def test_bench_golden_check(tmp_path, monkeypatch):
+    """bench.matches_golden: True on the recorded digest, False on one flipped
+    bit or another step count, None for an unrecorded run."""
+    import hashlib
+    import json
+    import bench
+    rng = np.random.default_rng(3)
+    keys = np.sort(rng.integers(0, 1 << 40, 50, dtype=np.uint64))
+    prim = rng.random((50, 4))
+    rec = {"steps": 7, "regrids": 1,
+           "sha256_keys": hashlib.sha256(keys.tobytes()).hexdigest(),
+           "sha256_prim": hashlib.sha256(prim.tobytes()).hexdigest()}
+    path = tmp_path / "runs.json"
+    path.write_text(json.dumps({"case": rec}))
+    monkeypatch.setattr(bench, "GOLDEN_RUNS", str(path))
+    assert bench.matches_golden("case", keys, prim, 7, 1) is True
+    bad = prim.copy()
+    bad.view(np.uint64)[3, 2] ^= np.uint64(1)
+    assert bench.matches_golden("case", keys, bad, 7, 1) is False
+    assert bench.matches_golden("case", keys, prim, 8, 1) is False
+    assert bench.matches_golden("other", keys, prim, 7, 1) is None
+    # every full run names its configuration and golden record
+    for name, (make, desc, golden) in bench.FULL_RUNS.items():
+        assert make().params.t_end > 0 and desc and golden
