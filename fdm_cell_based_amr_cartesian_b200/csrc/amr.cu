@@ -1637,6 +1637,10 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
 int run_amr(fdm_handle *h) {
     const int TB = 256;
     const int64_t NL = h->NL, NI = h->NI, NInt = h->NInt;
+    if (h->p.window_rows != 0) {
+        h->err = "a strip of a mesh takes no regrid: regrid the whole mesh";
+        return FDM_ERR_UNSUPPORTED;
+    }
     if ((int64_t)h->p.m * h->p.n >= (1ll << 19)) {
         h->err = "device regrid supports up to 2^19 background cells";
         return FDM_ERR_UNSUPPORTED;

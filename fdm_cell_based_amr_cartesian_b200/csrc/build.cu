@@ -49,9 +49,11 @@ __global__ void k_classify(const uint64_t *__restrict__ lkey, int64_t NL, Geomet
     if (k == NL - 1 && pos + span_of_level(lvl) != ((uint64_t)total << 30)) atomicExch(err + BE_PARTITION, 1);
     const int c = root_cross(G, root);
     cross[k] = (int8_t)c;
-    fI[k] = c == 0;
-    fC[k] = c == -5;
-    fG[k] = (c != 0 && c != -5);
+    // halo leaves of a strip take ghost slots (not advanced, not filled)
+    const bool halo = root_in_halo(G, root);
+    fI[k] = c == 0 && !halo;
+    fC[k] = c == -5 && !halo;
+    fG[k] = !fI[k] && !fC[k];
 }
 
 __global__ void k_slots(int64_t NL, int64_t NI, int64_t NG, const int32_t *fI, const int32_t *fG,
@@ -452,6 +454,11 @@ __global__ void k_ghosts(Tables T, Geometry G, fdm_params P, GhostOut O) {
     if (g >= T.NG) return;
     const int32_t k = T.slot_leaf[T.NI + g];
     const Node gn = node_of_key(T.lkey[k]);
+    if (root_in_halo(G, gn.root)) {   // written by the strip's caller
+        O.kind[g] = GH_NONE; O.a[g] = 0; O.b[g] = 0; O.flip[g] = 0;
+        O.x[g] = T.lcx[k]; O.y[g] = T.lcy[k];
+        return;
+    }
     const int a = root_cross(G, gn.root);
     const int row = (int)(gn.root / G.m) + 1, col = (int)(gn.root % G.m) + 1;
     const int m = G.m, n = G.n;
@@ -840,6 +847,7 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     h->table_version++;
     h->gate_stage1_valid = false;
     h->lam_fresh = false;
+    h->cur_buf = 0;
     h->loaded = true;
     return FDM_OK;
 }

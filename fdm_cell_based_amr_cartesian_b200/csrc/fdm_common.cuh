@@ -44,7 +44,9 @@ struct LevelTab {
 
 struct Geometry {
     double xmin, ymin, h, xf, gama, cv;
-    int32_t m, n;
+    int32_t m, n;              // root columns / rows held (n = the strip's rows)
+    int32_t row0, nglob;       // global row of local row 0; rows of the whole mesh
+    int32_t halo_lo, halo_hi;  // the strip's bottom / top three rows are a halo
 };
 
 // All device pointers of the current leaf set.  Passed by value to kernels.

@@ -29,6 +29,33 @@ __global__ void k_in(int64_t NL, const int32_t *lslot, double4 *B0, const double
     if (k >= NL) return;
     B0[lslot[k]] = make_double4(prim[4 * k], prim[4 * k + 1], prim[4 * k + 2], prim[4 * k + 3]);
 }
+// halo records of a strip: gather / scatter at caller-given slots; a slot
+// outside the leaf slots is skipped and flagged
+__global__ void k_pack_slots(int64_t n, const int32_t *__restrict__ slots, int64_t ns, const double4 *B,
+                             double *buf, int32_t *bad) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t s = slots[i];
+    if (s < 0 || s >= ns) { atomicExch(bad, 1); return; }
+    const double4 v = B[s];
+    buf[4 * i] = v.x; buf[4 * i + 1] = v.y; buf[4 * i + 2] = v.z; buf[4 * i + 3] = v.w;
+}
+__global__ void k_unpack_slots(int64_t n, const int32_t *__restrict__ slots, int64_t ns, double4 *B,
+                               const double *buf, int32_t *bad) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t s = slots[i];
+    if (s < 0 || s >= ns) { atomicExch(bad, 1); return; }
+    B[s] = make_double4(buf[4 * i], buf[4 * i + 1], buf[4 * i + 2], buf[4 * i + 3]);
+}
+__global__ void k_set_global_lambda(DevScalars *sc, double lx, double ly, int32_t l_max) {
+    if (threadIdx.x || blockIdx.x) return;
+    sc->lambda_x = lx;
+    sc->lambda_y = ly;
+    sc->lam_next_x = 0.0;
+    sc->lam_next_y = 0.0;
+    sc->l_max = l_max;
+}
 __global__ void k_stencil_out(Tables T, const double4 *B, double *out) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= T.NI) return;
@@ -204,11 +231,31 @@ int fdm_create(const fdm_params *p, fdm_handle **out) {
     if ((int64_t)p->m * p->n >= (1ll << 30)) return FDM_ERR_ARG;
     if (p->lvl_amr < 0 || p->lvl_amr > MAXLVL_TAB - 2) return FDM_ERR_ARG;
     if (p->flux_variant != 0 && p->flux_variant != 1) return FDM_ERR_UNSUPPORTED;
+    // a strip: rows [row0, row0 + rows) of the n padded rows, at least three
+    // owned rows between its two three-row margins; a side where the mesh is
+    // cut is an exchange side, and only there
+    const bool strip = p->window_rows != 0;
+    if (strip) {
+        if (p->window_row0 < 0 || p->window_rows < 9 || p->window_row0 + p->window_rows > p->n) return FDM_ERR_ARG;
+        const bool cut_lo = p->window_row0 > 0, cut_hi = p->window_row0 + p->window_rows < p->n;
+        if (cut_lo != (p->kind_ymbc == FDM_BC_EXCHANGE) || cut_hi != (p->kind_ypbc == FDM_BC_EXCHANGE))
+            return FDM_ERR_ARG;
+        if ((cut_lo || cut_hi) && (p->kind_ymbc == FDM_BC_PERIODIC || p->kind_ypbc == FDM_BC_PERIODIC))
+            return FDM_ERR_UNSUPPORTED;   // the periodic image lies in another strip
+    } else if (p->window_row0 != 0 || p->kind_ymbc == FDM_BC_EXCHANGE || p->kind_ypbc == FDM_BC_EXCHANGE) {
+        return FDM_ERR_ARG;
+    }
+    if (p->kind_xmbc == FDM_BC_EXCHANGE || p->kind_xpbc == FDM_BC_EXCHANGE) return FDM_ERR_ARG;
     fdm_handle *h = new (std::nothrow) fdm_handle();
     if (!h) return FDM_ERR_NOMEM;
     h->p = *p;
     h->G.xmin = p->xmin; h->G.ymin = p->ymin; h->G.h = p->h; h->G.xf = p->x_factor;
-    h->G.gama = p->gama; h->G.cv = p->cv; h->G.m = p->m; h->G.n = p->n;
+    h->G.gama = p->gama; h->G.cv = p->cv; h->G.m = p->m;
+    h->G.n = strip ? p->window_rows : p->n;
+    h->G.row0 = strip ? p->window_row0 : 0;
+    h->G.nglob = p->n;
+    h->G.halo_lo = p->kind_ymbc == FDM_BC_EXCHANGE;
+    h->G.halo_hi = p->kind_ypbc == FDM_BC_EXCHANGE;
     for (int l = 0; l < MAXLVL_TAB; ++l) {
         const double dy = p->h / (double)(1ll << l);
         const double dx = p->x_factor * dy;
@@ -677,6 +724,58 @@ int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out) {
     FDM_CK(h, cudaMemcpyAsync(out, d.p, h->NL * 64, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     d.release();
+    return FDM_OK;
+}
+
+// ------------------------------------------------------ strips of one mesh
+int fdm_leaf_slots(fdm_handle *h, int64_t cap, int32_t *slot) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (cap < h->NL || !slot) return arg_fail(h, "capacity below the leaf count");
+    FDM_CK(h, cudaMemcpyAsync(slot, h->lslot.p, h->NL * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+
+static int pack_common(fdm_handle *h, int64_t n, const int32_t *slots, const double *buf, bool unpack) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (n < 0 || (n > 0 && (!slots || !buf))) return arg_fail(h, "bad slot list");
+    if (n == 0) return FDM_OK;
+    int32_t *bad = h->flag.as<int32_t>() + 6;
+    FDM_CK(h, cudaMemsetAsync(bad, 0, sizeof(int32_t), h->s));
+    const int64_t ns = h->NI + h->NG + h->NC;
+    double4 *B = h->B[h->cur_buf].as<double4>();
+    if (unpack)
+        k_unpack_slots<<<nblk(n, 256), 256, 0, h->s>>>(n, slots, ns, B, buf, bad);
+    else
+        k_pack_slots<<<nblk(n, 256), 256, 0, h->s>>>(n, slots, ns, B, const_cast<double *>(buf), bad);
+    FDM_CK(h, cudaGetLastError());
+    int32_t hb = 0;
+    FDM_CK(h, cudaMemcpyAsync(&hb, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    if (hb) return arg_fail(h, "a slot is outside the leaf slots");
+    return FDM_OK;
+}
+int fdm_pack_slots(fdm_handle *h, int64_t n, const int32_t *slots, double *buf) {
+    return pack_common(h, n, slots, buf, false);
+}
+int fdm_unpack_slots(fdm_handle *h, int64_t n, const int32_t *slots, const double *buf) {
+    return pack_common(h, n, slots, buf, true);
+}
+
+int fdm_step_control_global(fdm_handle *h, double lambda_x, double lambda_y, int32_t l_max, double *tstep) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (l_max < 0 || l_max > FDM_LMAX) return arg_fail(h, "l_max out of range");
+    if (!(lambda_x >= 0.0) || !(lambda_y >= 0.0)) return arg_fail(h, "lambda must be >= 0");
+    k_set_global_lambda<<<1, 32, 0, h->s>>>(h->scal.as<DevScalars>(), lambda_x, lambda_y, l_max);
+    h->l_max = l_max;
+    h->lam_fresh = true;
+    launch_step_control(h);
+    RC(sync_scalars_from_device(h));
+    FDM_CK(h, cudaGetLastError());
+    if (tstep) *tstep = h->hs->tstep;
     return FDM_OK;
 }
 

@@ -198,9 +198,11 @@ __device__ inline NodeRef downleft_nb(const Tables &T, const Geometry &G, const 
 }
 
 // gridcross (src/mesh.F90:89-142) from the background cell of a node
+// The class is that of the root in the whole mesh (global row), also for a
+// strip of it.
 FDM_HD int root_cross(const Geometry &G, int64_t root) {
-    const int r = (int)(root / G.m) + 1, q = (int)(root % G.m) + 1;
-    const int m = G.m, n = G.n;
+    const int r = (int)(root / G.m) + 1 + G.row0, q = (int)(root % G.m) + 1;
+    const int m = G.m, n = G.nglob;
     if ((r < 4 && q < 4) || (r < 4 && q > m - 3) || (r > n - 3 && q > m - 3) || (r > n - 3 && q < 4))
         return -5;
     if (r < 4) return -1;
@@ -210,12 +212,18 @@ FDM_HD int root_cross(const Geometry &G, int64_t root) {
     return 0;
 }
 
+// A root in one of the three halo rows of a strip (filled by the caller).
+FDM_HD bool root_in_halo(const Geometry &G, int64_t root) {
+    const int r = (int)(root / G.m);
+    return (G.halo_lo && r < 3) || (G.halo_hi && r >= G.n - 3);
+}
+
 FDM_HD double ipow2d(int l) { return (double)(1ll << l); }
 
 // Node centre by the same chain of operations as creat_mesh + Refine_cell
 // (src/mesh.F90:25-26, 205-248).
 FDM_HD void node_center(const Geometry &G, const Node &n, double &cx, double &cy) {
-    const int64_t row = n.root / G.m, col = n.root % G.m;
+    const int64_t row = n.root / G.m + G.row0, col = n.root % G.m;
     const double nj = (double)(col + 1), ni = (double)(row + 1);
     cx = 0.5 * (2.0 * nj - 1.0) * G.xf * G.h + G.xmin;
     cy = (ni - 0.5) * G.h + G.ymin;

@@ -22,6 +22,7 @@ BC_WALL = 3           # extension
 BC_INFLOW = 4         # extension
 BC_DMR_BOTTOM = 5     # extension
 BC_DMR_TOP = 7        # extension
+BC_EXCHANGE = 8       # y side of a strip of the mesh: halo rows written by the caller
 
 IC_VORTEX = 0         # src/solution.F90:31-69
 IC_QUADRANTS = 1      # extension: four-quadrant Riemann problem
@@ -56,7 +57,8 @@ class FdmParams(ctypes.Structure):
         ("dmr_post", ctypes.c_double * 4), ("dmr_pre", ctypes.c_double * 4),
         ("dmr_shock_speed", ctypes.c_double), ("dmr_angle_cot", ctypes.c_double),
         ("flux_variant", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("window_row0", ctypes.c_int32), ("window_rows", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 

@@ -43,6 +43,7 @@ EXPORTS = [
     "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
     "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
     "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
+    "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
 ]
 
 
@@ -129,6 +130,10 @@ def load_library(path: str = LIB_PATH):
     L.fdm_batch_info.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64)]
     L.fdm_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.fdm_batch_phase_us.argtypes = [vp, dp]
+    L.fdm_leaf_slots.argtypes = [vp, i64, i32p]
+    L.fdm_pack_slots.argtypes = [vp, i64, vp, vp]
+    L.fdm_unpack_slots.argtypes = [vp, i64, vp, vp]
+    L.fdm_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32, dp]
     _lib = L
     return L
 
@@ -157,7 +162,7 @@ def node_centers(cfg: P.Config, keys: np.ndarray):
     lvl = (keys & np.uint64(15)).astype(np.int64)
     path = ((keys >> np.uint64(4)) & np.uint64((1 << 30) - 1)).astype(np.int64)
     nj = (root % p.m + 1).astype(np.float64)
-    ni = (root // p.m + 1).astype(np.float64)
+    ni = (root // p.m + 1 + p.window_row0).astype(np.float64)   # global row of a strip
     cx = 0.5 * (2.0 * nj - 1.0) * p.x_factor * p.h + p.xmin
     cy = (ni - 0.5) * p.h + p.ymin
     for k in range(1, int(lvl.max(initial=0)) + 1):
@@ -310,6 +315,37 @@ class Solver:
         self._check(self.L.fdm_step_control(self.h, ctypes.byref(dt), ctypes.byref(lx), ctypes.byref(ly),
                                             ctypes.byref(lm)))
         return dt.value
+
+    def step_control_info(self):
+        """fdm_step_control: (tstep, lambda_x, lambda_y, l_max)."""
+        dt, lx, ly = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        lm = ctypes.c_int32()
+        self._check(self.L.fdm_step_control(self.h, ctypes.byref(dt), ctypes.byref(lx), ctypes.byref(ly),
+                                            ctypes.byref(lm)))
+        return dt.value, lx.value, ly.value, lm.value
+
+    # ---- strips of one mesh (halo exchange)
+    def step_control_global(self, lambda_x: float, lambda_y: float, l_max: int) -> float:
+        """The time step from maxima taken over all strips of the mesh."""
+        dt = ctypes.c_double()
+        self._check(self.L.fdm_step_control_global(self.h, float(lambda_x), float(lambda_y), int(l_max),
+                                                   ctypes.byref(dt)))
+        return dt.value
+
+    def leaf_slots(self) -> np.ndarray:
+        """State slot of every leaf, key order."""
+        n = self.num_leaves()
+        out = np.zeros(n, np.int32)
+        self._check(self.L.fdm_leaf_slots(self.h, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return out
+
+    def pack_slots(self, slots_dev: int, n: int, buf_dev: int):
+        """Gather the latest stage's records at n slots (device int32 array)
+        into a device buffer of n x 4 float64."""
+        self._check(self.L.fdm_pack_slots(self.h, int(n), ctypes.c_void_p(slots_dev), ctypes.c_void_p(buf_dev)))
+
+    def unpack_slots(self, slots_dev: int, n: int, buf_dev: int):
+        self._check(self.L.fdm_unpack_slots(self.h, int(n), ctypes.c_void_p(slots_dev), ctypes.c_void_p(buf_dev)))
 
     def time_advance_rk(self, tstep: float):
         self._check(self.L.fdm_time_advance_rk(self.h, float(tstep)))

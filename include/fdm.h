@@ -46,6 +46,8 @@ extern "C" {
 #define FDM_BC_INFLOW        4   /* fixed state bc_state[side]                        */
 #define FDM_BC_DMR_BOTTOM    5   /* inflow for x <= dmr_x0, reflecting wall beyond    */
 #define FDM_BC_DMR_TOP       7   /* exact moving oblique shock (post/pre states)      */
+#define FDM_BC_EXCHANGE      8   /* y side of a strip: halo rows written by the caller
+                                    (see "strips of one mesh" below)                  */
 
 /* sides for bc_state[] */
 #define FDM_SIDE_XM 0
@@ -106,7 +108,11 @@ typedef struct fdm_params {
     double dmr_angle_cot;            /* cot(angle) of the shock                 */
     int32_t flux_variant;            /* 0 = exact (reference op order, no FMA),
                                         1 = fast (FMA contraction)              */
-    int32_t reserved[7];
+    /* strip of the mesh held by this handle: root rows
+     * [window_row0, window_row0 + window_rows) of the n padded rows above;
+     * window_rows = 0 holds the whole mesh (see "strips of one mesh") */
+    int32_t window_row0, window_rows;
+    int32_t reserved[5];
 } fdm_params;
 
 typedef struct fdm_handle fdm_handle;
@@ -369,6 +375,45 @@ int fdm_time_advance_rk_uniform_static(const double *prim_in, double *prim_out,
                                        int32_t nx, int32_t ny, double h, double x_factor,
                                        double gama, double lambda_x, double lambda_y,
                                        double tstep, void *stream);
+
+/* ----------------------------------------------------- strips of one mesh
+ * No reference counterpart (the reference runs one OpenMP process).  One
+ * mesh is split into horizontal strips of background rows, one handle per
+ * strip (per GPU), exchanging halo rows after every stage.
+ *
+ * A strip handle is created with fdm_params.window_rows > 0: it holds the
+ * root rows [window_row0, window_row0 + window_rows) of the padded root grid
+ * that xmin..ymax, m and n describe.  Its leaf keys name roots relative to
+ * the strip (root - window_row0 * m).  A y side of kind FDM_BC_EXCHANGE makes
+ * the strip's three outer rows on that side a halo: their leaves are neither
+ * advanced nor filled by fdm_body_boundary; the caller writes them after
+ * every stage with the values of the strip that owns those rows.  Cell
+ * centres and the neighbour classification use the global row, so a leaf
+ * the strip owns is advanced by exactly the arithmetic the whole mesh gives
+ * it.  Strips need non-periodic y sides where they are cut, at least three
+ * owned rows each, and take no regrid (fdm_amr returns
+ * FDM_ERR_UNSUPPORTED): the caller regrids the whole mesh.
+ *
+ * One step of a strip (every strip the same calls in the same order):
+ *   fdm_step_control            local lambda, l_max
+ *   (max of lambda_x, lambda_y, l_max over the strips)
+ *   fdm_step_control_global     the step from the global maxima
+ *   for krk = 1..3: fdm_solution_cells, fdm_update_rk, fdm_body_boundary(3),
+ *                   fdm_pack_slots -> exchange -> fdm_unpack_slots
+ *   fdm_set_scalars             tt + tstep, it + 1
+ *
+ * fdm_leaf_slots: the state slot of every leaf in key order (cap entries).
+ * fdm_pack_slots / fdm_unpack_slots: gather the (rho,u,v,p) records of the
+ * latest stage at the given slots into buf[4*i..4*i+3] / scatter them back;
+ * slots and buf are DEVICE pointers (for NCCL or peer copies), the calls
+ * return when the copy is complete.
+ * fdm_step_control_global: sets lambda_x, lambda_y (monotone maxima) and
+ * l_max and forms the time step of src/solution.F90:195-201 from them. */
+int fdm_leaf_slots(fdm_handle *h, int64_t cap, int32_t *slot);
+int fdm_pack_slots(fdm_handle *h, int64_t n, const int32_t *slots, double *buf);
+int fdm_unpack_slots(fdm_handle *h, int64_t n, const int32_t *slots, const double *buf);
+int fdm_step_control_global(fdm_handle *h, double lambda_x, double lambda_y,
+                            int32_t l_max, double *tstep);
 
 #ifdef __cplusplus
 }

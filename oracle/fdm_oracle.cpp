@@ -85,6 +85,11 @@ struct Solver {
     fdm_params p{};
     double Xmin, Xmax, Ymin, Ymax, h, xf, gama, cv, Ma;
     int m = 0, n = 0, total = 0;
+    // strip of a mesh (no reference counterpart): local row 1 is global row
+    // row0 + 1 of nglob rows; halo_lo / halo_hi: the three outer rows on that
+    // side are a halo (neither advanced nor filled here)
+    int row0 = 0, nglob = 0;
+    bool halo_lo = false, halo_hi = false;
     std::vector<Grid> cell;  // cell(i) == cell[i-1]
     std::vector<Grid *> cell_NS, cell_BC;
     std::vector<double> fu_buf;  // per-leaf fu*dx*dy of the last stage (4 each)
@@ -839,7 +844,8 @@ static void solution_cell(Solver &S, Grid *c, double fu_out[4]) {
 
 // ====================================================== src/mesh.F90
 static int gridcross(const Solver &S, const Grid *c) {          // :89-142
-    const int r = c->num[0], q = c->num[1], m = S.m, n = S.n;
+    // the class in the whole mesh (global row), also for a strip of it
+    const int r = c->num[0] + S.row0, q = c->num[1], m = S.m, n = S.nglob;
     if (r < 4 && q < 4) return BCcorner;
     if (r < 4 && q > m - 3) return BCcorner;
     if (r > n - 3 && q > m - 3) return BCcorner;
@@ -849,6 +855,11 @@ static int gridcross(const Solver &S, const Grid *c) {          // :89-142
     if (q > m - 3) return -2;
     if (q < 4) return -4;
     return 0;  // gridsort is identically 0 (src/mesh.F90:81-87)
+}
+
+// a node in the halo rows of a strip
+static bool in_halo(const Solver &S, const Grid *c) {
+    return (S.halo_lo && c->num[0] <= 3) || (S.halo_hi && c->num[0] > S.n - 3);
 }
 
 static const int SP_TO_Q[5] = {0, 0, 1, 3, 2};  // sp -> Morton quadrant
@@ -940,7 +951,7 @@ static void IDNS(Solver &S, Grid *c) {                          // :655-670
     if (c->son1) {
         IDNS(S, c->son1); IDNS(S, c->son2); IDNS(S, c->son4); IDNS(S, c->son3);
     } else if (c->sort == 0) {
-        if (c->cross < 0) return;
+        if (c->cross < 0 || in_halo(S, c)) return;
         S.cell_NS.push_back(c);
     }
 }
@@ -948,7 +959,7 @@ static void IDBC(Solver &S, Grid *c) {                          // :672-693
     if (c->son1) {
         IDBC(S, c->son1); IDBC(S, c->son2); IDBC(S, c->son3); IDBC(S, c->son4);
     } else if (c->sort == 0) {
-        if (c->cross == BCcorner) return;
+        if (c->cross == BCcorner || in_halo(S, c)) return;
         if (c->cross < 0) S.cell_BC.push_back(c);
     }
 }
@@ -1010,7 +1021,7 @@ static void set_state(Solver &S, Grid *c, const double st[4]) {
 // One ghost leaf (body_boundary_RK / initial_boundary, src/solution.F90:71-107,
 // 314-356) at boundary time t.
 static void fill_ghost(Solver &S, Grid *c, double t) {
-    if (c->sort != 0) return;
+    if (c->sort != 0 || in_halo(S, c)) return;
     int a = c->cross;
     int kind;
     if (a == -4) kind = S.p.kind_xmbc;
@@ -1119,6 +1130,13 @@ static void ic_tree(Solver &S, Grid *c) {
 static void creat_mesh(Solver &S) {                             // src/mesh.F90:9-47
     S.m = (int)((S.Xmax - S.Xmin) / (S.xf * S.h));
     S.n = (int)((S.Ymax - S.Ymin) / S.h);
+    S.nglob = S.n;
+    if (S.p.window_rows > 0) {
+        S.row0 = S.p.window_row0;
+        S.n = S.p.window_rows;
+        S.halo_lo = S.p.kind_ymbc == FDM_BC_EXCHANGE;
+        S.halo_hi = S.p.kind_ypbc == FDM_BC_EXCHANGE;
+    }
     S.total = S.m * S.n;
     S.cell.assign((size_t)S.total, Grid{});
     for (int i = 1; i <= S.total; ++i) {
@@ -1128,7 +1146,7 @@ static void creat_mesh(Solver &S) {                             // src/mesh.F90:
         c->num[0] = ni; c->num[1] = nj;
         c->lvl = 0;
         c->cx = 0.5 * (2.0 * nj - 1.0) * S.xf * S.h + S.Xmin;
-        c->cy = (ni - 0.5) * S.h + S.Ymin;
+        c->cy = ((ni + S.row0) - 0.5) * S.h + S.Ymin;
         c->sp = 0;
         c->sort = 0;
         c->father = nullptr;
@@ -1429,6 +1447,36 @@ int orc_set_scalars(void *h, double lx, double ly, double tstep, double tt, int6
     return 0;
 }
 int orc_step_control(void *h) { step_control(*(Solver *)h); return 0; }
+// the step of src/solution.F90:195-201 from maxima taken over all strips
+int orc_step_control_global(void *h, double lx, double ly, int l_max) {
+    Solver &S = *(Solver *)h;
+    S.lambda_x = lx; S.lambda_y = ly; S.l_max = l_max;
+    if (S.p.iflag_localdt)
+        S.tstep = S.p.cfl / (S.lambda_x / (S.xf * S.h / ipow2(S.l_max)) + S.lambda_y / (S.h / ipow2(S.l_max)));
+    if (S.tt + S.tstep > S.p.t_end) S.tstep = S.p.t_end - S.tt;
+    return 0;
+}
+// U(1:7) of the leaves idx[] (key order) out / in: the halo exchange of strips
+int orc_get_U(void *h, int64_t n, const int64_t *idx, double *out) {
+    Solver &S = *(Solver *)h;
+    std::vector<Grid *> v;
+    all_leaves(S, v);
+    for (int64_t i = 0; i < n; ++i) {
+        if (idx[i] < 0 || idx[i] >= (int64_t)v.size()) return FDM_ERR_ARG;
+        for (int k = 0; k < 7; ++k) out[7 * i + k] = v[(size_t)idx[i]]->U[k];
+    }
+    return 0;
+}
+int orc_set_U(void *h, int64_t n, const int64_t *idx, const double *in) {
+    Solver &S = *(Solver *)h;
+    std::vector<Grid *> v;
+    all_leaves(S, v);
+    for (int64_t i = 0; i < n; ++i) {
+        if (idx[i] < 0 || idx[i] >= (int64_t)v.size()) return FDM_ERR_ARG;
+        for (int k = 0; k < 7; ++k) v[(size_t)idx[i]]->U[k] = in[7 * i + k];
+    }
+    return 0;
+}
 int orc_time_advance_rk(void *h) { time_advance_rk(*(Solver *)h); return 0; }
 int orc_stage(void *h, int krk) {
     Solver *S = (Solver *)h;
@@ -1453,6 +1501,7 @@ int orc_solute(void *h, int64_t nsteps, int64_t *done) {
 }
 int orc_amr(void *h) {
     Solver *S = (Solver *)h;
+    if (S->p.window_rows > 0) return FDM_ERR_UNSUPPORTED;
     amr_core(*S);
     body_boundary(*S, 1);
     return 0;

@@ -55,6 +55,9 @@ def lib():
                      "orc_rot_div"):
             getattr(L, name).argtypes = [vp]
         L.orc_stage.argtypes = [vp, i32]
+        L.orc_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32]
+        L.orc_get_U.argtypes = [vp, i64, i64p, dp]
+        L.orc_set_U.argtypes = [vp, i64, i64p, dp]
         L.orc_solute.argtypes = [vp, i64, i64p]
         L.orc_export_rot_div.argtypes = [vp, i64, dp, dp]
         L.orc_export_stencil.argtypes = [vp, i64, dp]
@@ -159,6 +162,28 @@ class Oracle:
 
     def stage(self, krk: int):
         self.L.orc_stage(self.h, krk)
+
+    # ---- strips of one mesh (halo exchange)
+    def step_control_global(self, lambda_x, lambda_y, l_max):
+        self.L.orc_step_control_global(self.h, float(lambda_x), float(lambda_y), int(l_max))
+        return self.scalars()["tstep"]
+
+    def get_U(self, idx):
+        """U(1:7) of the leaves idx (positions in key order), shape (n, 7)."""
+        idx = np.ascontiguousarray(idx, np.int64)
+        out = np.zeros((len(idx), 7), np.float64)
+        rc = self.L.orc_get_U(self.h, len(idx), idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _dp(out))
+        if rc:
+            raise IndexError("leaf index out of range")
+        return out
+
+    def set_U(self, idx, U):
+        idx = np.ascontiguousarray(idx, np.int64)
+        U = np.ascontiguousarray(U, np.float64)
+        assert U.shape == (len(idx), 7)
+        rc = self.L.orc_set_U(self.h, len(idx), idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _dp(U))
+        if rc:
+            raise IndexError("leaf index out of range")
 
     def solute_step(self) -> int:
         return int(self.L.orc_solute_step(self.h))
