@@ -14,12 +14,16 @@ Per step every strip makes the same calls in the same order:
   step_control (local lambda, l_max) -> max over strips -> step_control_global
   for krk = 1..3: solution_cells, update_rk, body_boundary(3), halo exchange
   tt + tstep, it + 1
-The y sides that are cut must not be periodic, each strip owns at least
-three rows, and the mesh is fixed while split (regrid the gathered mesh and
-split it again).
+The y sides that are cut must not be periodic and each strip owns at least
+three rows.  With AMR on, the ghosts are refreshed after every step (and the
+halos exchanged again), and a due regrid runs on a whole-mesh regrid host:
+the strips' leaf values are gathered into it (without a table rebuild, so its
+internal nodes keep the values the whole run gives them: they change only at
+regrids), it regrids, and its new leaf set is split again (``StripRun``).
 
 Engines: ``GpuStrip`` (a libfdm strip handle) and ``OracleStrip`` (the CPU
-restatement, for tests).  Transports: ``LocalExchange`` (all strips in this
+restatement, for tests), with the regrid hosts ``GpuRegridHost`` and
+``OracleRegridHost``.  Transports: ``LocalExchange`` (all strips in this
 process, e.g. on one GPU) and ``DistExchange`` (one strip per rank over
 torch.distributed: NCCL between GPUs, gloo on CPU).
 """
@@ -196,8 +200,14 @@ class GpuStrip:
     def end_step(self, lx, ly, tstep, tt, it):
         self.g.set_scalars(lx, ly, tstep, tt, it)
 
+    def body_boundary(self, j: int):
+        self.g.body_boundary(j)
+
     def leaves(self):
         return self.g.leaves()
+
+    def values(self):
+        return self.g.leaves()[1]
 
     def close(self):
         self.g.close()
@@ -208,11 +218,11 @@ class OracleStrip:
 
     width = 7   # U(1:7) per leaf
 
-    def __init__(self, plan: StripPlan, s: int, values: np.ndarray, oracle_mod, T=None, threads=1):
+    def __init__(self, plan: StripPlan, s: int, values: np.ndarray, oracle_mod, threads=1):
         st = plan.strips[s]
         self.strip = st
         self.o = oracle_mod.Oracle(plan.config(s), threads=threads, initial=False)
-        self.o.set_leaves(st.keys, values[st.sel], None if T is None else T[st.sel])
+        set_oracle_leaves(self.o, st.keys, values[st.sel])
         self._idx = {name: np.arange(*r, dtype=np.int64)
                      for name, r in (("send_down", st.send_down), ("send_up", st.send_up),
                                      ("recv_down", st.recv_down), ("recv_up", st.recv_up))}
@@ -242,9 +252,73 @@ class OracleStrip:
     def end_step(self, lx, ly, tstep, tt, it):
         self.o.set_scalars(lx, ly, tstep, tt, it)
 
+    def body_boundary(self, j: int):
+        self.o.body_boundary(j)
+
     def leaves(self):
         k, v, _ = self.o.leaves()
         return k, v
+
+    def values(self):
+        return self.o.get_U(np.arange(self.o.num_leaves()))
+
+    def close(self):
+        self.o.close()
+
+
+def set_oracle_leaves(o, keys, values):
+    """Leaves into an oracle instance from (rho, u, v, p) rows, or from full
+    U(1:7) rows (which also carry T and the two unused slots)."""
+    values = np.asarray(values, np.float64)
+    if values.shape[1] == 7:
+        o.set_leaves(keys, values[:, [0, 1, 2, 4]], values[:, 3])
+        o.set_U(np.arange(len(keys)), values)
+    else:
+        o.set_leaves(keys, values)
+
+
+class GpuRegridHost:
+    """The whole mesh in one libfdm handle, used only at regrids.  It holds
+    the mesh from the start of the run, so its internal nodes carry the
+    values the whole run gives them (set at refinement / coarsening,
+    src/mesh.F90:199-260, 397-408)."""
+
+    def __init__(self, cfg: P.Config, keys: np.ndarray, values: np.ndarray):
+        from .solver import Solver
+        self.g = Solver(cfg)
+        self.g.upload(keys, values)
+        self.keys = np.asarray(keys, np.uint64)
+
+    def regrid(self, keys, values, lx, ly, tstep, tt, it):
+        if not np.array_equal(keys, self.keys):
+            raise RuntimeError("the strips' leaf set differs from the regrid host's")
+        self.g.set_values(values)                  # leaves only: no table rebuild
+        self.g.set_scalars(lx, ly, tstep, tt, it)
+        self.g.amr()
+        self.g.body_boundary(1)
+        self.keys, v = self.g.leaves()
+        return self.keys, v
+
+    def close(self):
+        self.g.close()
+
+
+class OracleRegridHost:
+    """The CPU restatement's whole mesh, used only at regrids (tests)."""
+
+    def __init__(self, cfg: P.Config, keys, values, oracle_mod, threads=1):
+        self.o = oracle_mod.Oracle(cfg, threads=threads, initial=False)
+        set_oracle_leaves(self.o, keys, values)
+        self.keys = np.asarray(keys, np.uint64)
+
+    def regrid(self, keys, values, lx, ly, tstep, tt, it):
+        if not np.array_equal(keys, self.keys):
+            raise RuntimeError("the strips' leaf set differs from the regrid host's")
+        self.o.set_U(np.arange(len(keys)), values)  # leaves only
+        self.o.set_scalars(lx, ly, tstep, tt, it)
+        self.o.amr()                                # amr_core + body_boundary(1)
+        self.keys = self.o.leaves()[0]
+        return self.keys, self.o.get_U(np.arange(len(self.keys)))
 
     def close(self):
         self.o.close()
@@ -320,14 +394,11 @@ class DistExchange:
             e.unpack(name, buf)
 
 
-def check_fixed_mesh(cfg: P.Config):
-    if cfg.params.iflag_amr:
-        raise ValueError("strips advance a fixed mesh: set iflag_amr = 0 (regrid the gathered mesh)")
-
-
 def step(engines, xchg, tt: float, it: int):
-    """One solute iteration of the strips (without regrid); returns the new
-    (tt, it, tstep).  ``engines`` are this process's strips."""
+    """The RK3 step of one solute iteration on the strips (step control,
+    three stages with the halo exchange, tt and it); returns the new
+    (tt, it, tstep, lambda_x, lambda_y).  ``engines`` are this process's
+    strips."""
     lx, ly, lm = xchg.max3([e.step_control() for e in engines])
     dts = [e.step_control_global(lx, ly, lm) for e in engines]
     tstep = dts[0]
@@ -340,13 +411,116 @@ def step(engines, xchg, tt: float, it: int):
     it = it + 1
     for e in engines:
         e.end_step(lx, ly, tstep, tt, it)
-    return tt, it, tstep
+    return tt, it, tstep, lx, ly
 
 
 def run(engines, xchg, nsteps: int, t_end: float, tt: float = 0.0, it: int = 0):
-    """Up to nsteps iterations, stopping at t_end (src/solution.F90:182)."""
+    """Up to nsteps RK3 steps on a fixed mesh, stopping at t_end
+    (src/solution.F90:182); no ghost refresh or regrid between steps."""
     k = 0
     while k < nsteps and tt < t_end:
-        tt, it, _ = step(engines, xchg, tt, it)
+        tt, it, *_ = step(engines, xchg, tt, it)
         k += 1
     return tt, it, k
+
+
+def amr_due(p: P.FdmParams, it: int) -> bool:
+    """The regrid trigger of solute (it >= Nstep_Adapt, mod(it, Pstep_Adapt) == 1)."""
+    return bool(p.iflag_amr) and it >= p.nstep_adapt and p.pstep_adapt != 0 and it % p.pstep_adapt == 1
+
+
+class StripRun:
+    """The time loop of solute (src/solution.F90:182-236, without file
+    output) on strips: the RK3 step with halo exchanges, then with AMR on the
+    ghost refresh of body_boundary_RK(1) and, when due, the regrid on the
+    regrid host and a new split.
+
+    make_engine(plan, s, values) builds strip s; make_host(keys, values)
+    builds the regrid host (called on rank 0 only when ``comm`` is a
+    torch.distributed world of one strip per rank; ``rank`` then names this
+    process's strip)."""
+
+    def __init__(self, cfg, keys, values, nstrips, make_engine, make_host=None, rank=None, device=None):
+        self.cfg = cfg
+        self.nstrips = nstrips
+        self.make_engine = make_engine
+        self.rank = rank                 # None: every strip in this process
+        self.device = device
+        self.tt, self.it = 0.0, 0
+        self.steps = 0
+        self.regrids = 0
+        self.host = None
+        if cfg.params.iflag_amr and (rank is None or rank == 0):
+            if make_host is None:
+                raise ValueError("AMR is on: a regrid host is needed")
+            self.host = make_host(keys, values)
+        self._split(keys, values)
+
+    def _split(self, keys, values, scalars=None):
+        self.plan = StripPlan(self.cfg, keys, self.nstrips)
+        mine = range(self.nstrips) if self.rank is None else [self.rank]
+        self.engines = [self.make_engine(self.plan, s, values) for s in mine]
+        if scalars is not None:
+            for e in self.engines:
+                e.end_step(*scalars)
+        if self.rank is None:
+            self.xchg = LocalExchange(self.engines)
+        else:
+            self.xchg = DistExchange(self.engines[0], self.rank, self.nstrips, self.device)
+
+    def _regrid(self, lx, ly, tstep):
+        parts = [(e.strip.keys, e.values()) for e in self.engines]
+        scal = (lx, ly, tstep, self.tt, self.it)
+        if self.rank is None:
+            keys, vals = self.plan.gather(parts)
+            nk, nv = self.host.regrid(keys, vals, *scal)
+        else:
+            import torch.distributed as dist
+            got = [None] * self.nstrips if self.rank == 0 else None
+            dist.gather_object(parts[0], got, dst=0)
+            box = [None]
+            if self.rank == 0:
+                keys, vals = self.plan.gather(got)
+                box = [self.host.regrid(keys, vals, *scal)]
+            dist.broadcast_object_list(box, src=0)
+            nk, nv = box[0]
+        for e in self.engines:
+            e.close()
+        self._split(nk, nv, scal)
+        self.regrids += 1
+
+    def solute_step(self):
+        self.tt, self.it, tstep, lx, ly = step(self.engines, self.xchg, self.tt, self.it)
+        self.steps += 1
+        if self.cfg.params.iflag_amr:
+            if amr_due(self.cfg.params, self.it):
+                self._regrid(lx, ly, tstep)
+            else:
+                for e in self.engines:
+                    e.body_boundary(1)
+                self.xchg.halos()
+
+    def solute(self, nsteps: int) -> int:
+        k = 0
+        while k < nsteps and self.tt < self.cfg.params.t_end:
+            self.solute_step()
+            k += 1
+        return k
+
+    def gather(self):
+        """The whole mesh's (keys, values) from this process's strips (all
+        strips of a LocalExchange run; rank 0 gets them in a distributed run,
+        the other ranks None)."""
+        parts = [(e.strip.keys, e.values()) for e in self.engines]
+        if self.rank is None:
+            return self.plan.gather(parts)
+        import torch.distributed as dist
+        got = [None] * self.nstrips if self.rank == 0 else None
+        dist.gather_object(parts[0], got, dst=0)
+        return self.plan.gather(got) if self.rank == 0 else None
+
+    def close(self):
+        for e in self.engines:
+            e.close()
+        if self.host is not None:
+            self.host.close()

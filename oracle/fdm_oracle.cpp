@@ -1487,6 +1487,7 @@ int orc_stage(void *h, int krk) {
     return 0;
 }
 int orc_solute_step(void *h) { return solute_step(*(Solver *)h); }
+int orc_body_boundary(void *h, int j) { body_boundary(*(Solver *)h, j); return 0; }
 int orc_solute(void *h, int64_t nsteps, int64_t *done) {
     Solver *S = (Solver *)h;
     int64_t k = 0;

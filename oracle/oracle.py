@@ -55,6 +55,7 @@ def lib():
                      "orc_rot_div"):
             getattr(L, name).argtypes = [vp]
         L.orc_stage.argtypes = [vp, i32]
+        L.orc_body_boundary.argtypes = [vp, i32]
         L.orc_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32]
         L.orc_get_U.argtypes = [vp, i64, i64p, dp]
         L.orc_set_U.argtypes = [vp, i64, i64p, dp]
@@ -162,6 +163,9 @@ class Oracle:
 
     def stage(self, krk: int):
         self.L.orc_stage(self.h, krk)
+
+    def body_boundary(self, j: int):
+        self.L.orc_body_boundary(self.h, j)
 
     # ---- strips of one mesh (halo exchange)
     def step_control_global(self, lambda_x, lambda_y, l_max):

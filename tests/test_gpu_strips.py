@@ -80,3 +80,28 @@ def test_gpu_strip_errors():
     with pytest.raises(FdmError):
         e.g.step_control_global(1.0, 1.0, 99)
     e.close()
+
+
+@pytest.mark.parametrize("make,nstrips,nsteps", [
+    (lambda: P.riemann4(base=32, lvl_amr=2), 3, 25),
+    (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), 2, 12),
+    (lambda: P.riemann4(base=128, lvl_amr=4), 4, 31),      # configuration 2, 4 regrids
+])
+def test_gpu_strip_run_with_regrids(make, nstrips, nsteps):
+    """The time loop with AMR on, strips on one GPU and the regrid host
+    beside them: the same leaf sets and states as the whole handle."""
+    cfg = make()
+    g = Solver(cfg)
+    g.creat_mesh_and_initial()
+    keys, prim = g.leaves()
+    run = SP.StripRun(cfg, keys, prim, nstrips, lambda plan, s, v: SP.GpuStrip(plan, s, v),
+                      lambda k, v: SP.GpuRegridHost(cfg, k, v))
+    for _ in range(nsteps):
+        g.solute_step()
+        run.solute_step()
+    assert run.regrids >= 3 and run.tt == g.scalars()["tt"]
+    kw, pw = g.leaves()
+    ks, ps = run.gather()
+    run.close()
+    g.close()
+    assert np.array_equal(ks, kw) and np.array_equal(ps, pw)

@@ -166,3 +166,86 @@ def test_strip_parameters_validated_before_any_device_call():
     whole = P.FdmParams.from_buffer_copy(cfg.params)
     whole.kind_ypbc = P.BC_EXCHANGE
     assert create(whole) == 1                                           # exchange without a strip
+
+
+def oracle_start(oracle_mod, cfg):
+    """The whole mesh after creat_mesh + initial (roots, ghosts filled) as
+    (keys, U(1:7)), and the oracle holding it."""
+    o = oracle_mod.Oracle(cfg, threads=2)
+    k, _, _ = o.leaves()
+    return o, k, o.get_U(np.arange(len(k)))
+
+
+@pytest.mark.parametrize("make,nstrips,nsteps", [
+    (lambda: P.riemann4(base=32, lvl_amr=2), 3, 25),
+    (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), 2, 12),
+])
+def test_oracle_strip_run_with_regrids(oracle_mod, make, nstrips, nsteps):
+    """The time loop with AMR on: ghost refresh after every step, regrids on
+    the regrid host and a new split; leaf sets and states after every regrid
+    equal the whole run's."""
+    cfg = make()
+    whole, keys, U = oracle_start(oracle_mod, cfg)
+    run = SP.StripRun(cfg, keys, U, nstrips,
+                      lambda plan, s, v: SP.OracleStrip(plan, s, v, oracle_mod),
+                      lambda k, v: SP.OracleRegridHost(cfg, k, v, oracle_mod, threads=2))
+    for _ in range(nsteps):
+        assert whole.solute_step() == 0
+        run.solute_step()
+    assert run.regrids >= 2 and run.tt == whole.scalars()["tt"]
+    kw, pw, Tw = whole.leaves()
+    ks, Us = run.gather()
+    run.close()
+    whole.close()
+    assert np.array_equal(ks, kw)
+    assert np.array_equal(Us[:, [0, 1, 2, 4]], pw) and np.array_equal(Us[:, 3], Tw)
+
+
+def _rank_amr(rank, world, port, q):
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "oracle"))
+    import datetime
+    import oracle as oracle_mod
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        cfg = P.riemann4(base=32, lvl_amr=2)
+        o, keys, U = oracle_start(oracle_mod, cfg)
+        o.close()
+        run = SP.StripRun(cfg, keys, U, world,
+                          lambda plan, s, v: SP.OracleStrip(plan, s, v, oracle_mod),
+                          lambda k, v: SP.OracleRegridHost(cfg, k, v, oracle_mod), rank=rank)
+        run.solute(22)
+        out = run.gather()
+        q.put((rank, run.tt, run.regrids, out))
+        run.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_strip_run_with_regrids(oracle_mod):
+    import torch.multiprocessing as mp
+    cfg = P.riemann4(base=32, lvl_amr=2)
+    whole, _, _ = oracle_start(oracle_mod, cfg)
+    for _ in range(22):
+        whole.solute_step()
+    kw, pw, _ = whole.leaves()
+    tt = whole.scalars()["tt"]
+    whole.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_amr, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=240) for _ in range(2)], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out[0][1] == out[1][1] == tt and out[0][2] == 3
+    ks, Us = out[0][3]
+    assert out[1][3] is None
+    assert np.array_equal(ks, kw) and np.array_equal(Us[:, [0, 1, 2, 4]], pw)
