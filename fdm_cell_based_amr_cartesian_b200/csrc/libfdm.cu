@@ -1,7 +1,9 @@
 // libfdm.cu — the extern "C" boundary (include/fdm.h).
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <new>
+#include <vector>
 
 #include "handle.cuh"
 #include "topo.cuh"
@@ -724,6 +726,35 @@ int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out) {
     FDM_CK(h, cudaMemcpyAsync(out, d.p, h->NL * 64, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     d.release();
+    return FDM_OK;
+}
+
+// ------------------------------------------------------ checkpoint/restart
+int fdm_download_internal(fdm_handle *h, int64_t cap, int64_t *n_out, uint64_t *keys, double *vals) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (n_out) *n_out = h->NInt;
+    if (cap < h->NInt) return arg_fail(h, "capacity below the internal node count");
+    if (h->NInt == 0) return FDM_OK;
+    if (keys) FDM_CK(h, cudaMemcpyAsync(keys, h->ikey.p, h->NInt * 8, cudaMemcpyDeviceToHost, h->s));
+    if (vals) FDM_CK(h, cudaMemcpyAsync(vals, h->ival.p, h->NInt * 32, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    return FDM_OK;
+}
+
+int fdm_set_internal(fdm_handle *h, int64_t n, const uint64_t *keys, const double *vals) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (n != h->NInt) return arg_fail(h, "internal node count differs from the leaf set's");
+    if (n == 0) return FDM_OK;
+    if (!keys || !vals) return arg_fail(h, "null keys or values");
+    std::vector<uint64_t> cur((size_t)n);
+    FDM_CK(h, cudaMemcpyAsync(cur.data(), h->ikey.p, n * 8, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    if (std::memcmp(cur.data(), keys, (size_t)n * 8) != 0)
+        return arg_fail(h, "internal node keys differ from the leaf set's");
+    FDM_CK(h, cudaMemcpyAsync(h->ival.p, vals, n * 32, cudaMemcpyHostToDevice, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
     return FDM_OK;
 }
 

@@ -44,6 +44,7 @@ EXPORTS = [
     "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
     "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
     "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
+    "fdm_download_internal", "fdm_set_internal",
 ]
 
 
@@ -131,6 +132,8 @@ def load_library(path: str = LIB_PATH):
     L.fdm_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.fdm_batch_phase_us.argtypes = [vp, dp]
     L.fdm_leaf_slots.argtypes = [vp, i64, i32p]
+    L.fdm_download_internal.argtypes = [vp, i64, ctypes.POINTER(i64), u64p, dp]
+    L.fdm_set_internal.argtypes = [vp, i64, u64p, dp]
     L.fdm_pack_slots.argtypes = [vp, i64, vp, vp]
     L.fdm_unpack_slots.argtypes = [vp, i64, vp, vp]
     L.fdm_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32, dp]
@@ -315,6 +318,43 @@ class Solver:
         self._check(self.L.fdm_step_control(self.h, ctypes.byref(dt), ctypes.byref(lx), ctypes.byref(ly),
                                             ctypes.byref(lm)))
         return dt.value
+
+    # ---- checkpoint/restart
+    def internal_nodes(self):
+        """Keys (sorted) and (rho,u,v,p) values of the internal nodes."""
+        n = ctypes.c_int64()
+        cnt = self.counters()["n_internal"]
+        keys = np.zeros(cnt, np.uint64)
+        vals = np.zeros((cnt, 4))
+        self._check(self.L.fdm_download_internal(self.h, cnt, ctypes.byref(n), _u64p(keys), _dp(vals)))
+        return keys, vals
+
+    def set_internal(self, keys, vals):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        vals = np.ascontiguousarray(vals, np.float64)
+        self._check(self.L.fdm_set_internal(self.h, len(keys), _u64p(keys), _dp(vals)))
+
+    def save_checkpoint(self, path: str):
+        """The handle's whole state (leaves, internal-node values, scalars,
+        and the parameters it runs with) into one .npz file."""
+        keys, prim = self.leaves()
+        ikeys, ivals = self.internal_nodes()
+        sc = self.scalars()
+        np.savez(path, params=np.frombuffer(bytes(self.cfg.params), np.uint8), keys=keys, prim=prim,
+                 ikeys=ikeys, ivals=ivals,
+                 scalars=np.array([sc["lambda_x"], sc["lambda_y"], sc["tstep"], sc["tt"]]),
+                 it=np.array([sc["it"]], np.int64))
+
+    def load_checkpoint(self, path: str):
+        """Restore a state written by save_checkpoint into this handle (same
+        parameters); the run then continues bit for bit."""
+        with np.load(path) as z:
+            if bytes(z["params"]) != bytes(self.cfg.params):
+                raise ValueError("the checkpoint was written with other parameters")
+            self.upload(z["keys"], z["prim"])
+            self.set_internal(z["ikeys"], z["ivals"])
+            lx, ly, dt, tt = (float(v) for v in z["scalars"])
+            self.set_scalars(lx, ly, dt, tt, int(z["it"][0]))
 
     def step_control_info(self):
         """fdm_step_control: (tstep, lambda_x, lambda_y, l_max)."""

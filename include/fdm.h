@@ -376,6 +376,23 @@ int fdm_time_advance_rk_uniform_static(const double *prim_in, double *prim_out,
                                        double gama, double lambda_x, double lambda_y,
                                        double tstep, void *stream);
 
+/* ------------------------------------------------------ checkpoint/restart
+ * No reference counterpart (the reference writes only output files).  A
+ * handle's state is its leaves (fdm_download_leaves), the scalars
+ * (fdm_get_scalars) and the values of its internal nodes: every refined cell
+ * keeps a value (its U when refined, the interpA mean when coarsened,
+ * src/mesh.F90:199-260, 397-408) that a later gridmodify4 refinement of a
+ * non-leaf copies into new sons (src/mesh.F90:389-392), while an upload
+ * starts them as interpA means.  fdm_download_internal gives the internal
+ * nodes (keys sorted, the ancestors of the leaves) and their (rho,u,v,p);
+ * fdm_set_internal writes them back after an upload of the same leaf set
+ * (FDM_ERR_ARG when the keys differ).  Upload + fdm_set_internal +
+ * fdm_set_scalars restores a run that continues bit for bit. */
+int fdm_download_internal(fdm_handle *h, int64_t cap, int64_t *n_out,
+                          uint64_t *keys, double *vals);
+int fdm_set_internal(fdm_handle *h, int64_t n, const uint64_t *keys,
+                     const double *vals);
+
 /* ----------------------------------------------------- strips of one mesh
  * No reference counterpart (the reference runs one OpenMP process).  One
  * mesh is split into horizontal strips of background rows, one handle per
