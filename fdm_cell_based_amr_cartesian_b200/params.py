@@ -71,6 +71,9 @@ class Config:
     ic_kind: int
     ic_params: list = field(default_factory=list)
     max_steps: int = 10 ** 9
+    # static block refinement of creat_mesh (src/mesh.F90:41-44):
+    # (lvlBlock, Block_size(1:4) as set_parameter leaves it, BufferLayerLVL)
+    block: tuple | None = None
 
     @property
     def m(self) -> int:
@@ -123,6 +126,20 @@ def set_parameter(xmin: float, xmax: float, ymin: float, ymax: float, h: float, 
     p.t_end = t_end
     p.flux_variant = 0
     return p
+
+
+def with_block(cfg: Config, lvlblock: int, block_size, buffer_layer_lvl: int = 0) -> Config:
+    """The configuration with creat_mesh's static block refinement
+    (Block_refine, src/mesh.F90:49-79): cells inside the box
+    Block_size = (x1, x2, y1, y2) refined to lvlBlock, cells within
+    BufferLayerLVL*h/2**(i-1) of it to level i, then lvlBlock-1 passes of the
+    2:1 gridmodify.  set_parameter adds 1e-10 to the upper bounds
+    (src/MAIN.F90:57)."""
+    b = [float(v) for v in block_size]
+    b[1] = b[1] + 1.0e-10
+    b[3] = b[3] + 1.0e-10
+    cfg.block = (int(lvlblock), tuple(b), int(buffer_layer_lvl))
+    return cfg
 
 
 def reference_default() -> Config:

@@ -244,8 +244,14 @@ class Solver:
     # ---- mesh + state
     def creat_mesh_and_initial(self):
         """creat_mesh + initial (src/mesh.F90:9-47, src/solution.F90:9-29):
-        background grid, initial state, periodic/extension ghost fill."""
-        keys = root_keys(self.cfg.m, self.cfg.n)
+        background grid (with the static block refinement when the
+        configuration has one), initial state, periodic/extension ghost
+        fill."""
+        if self.cfg.block:
+            from .mesh import block_refined_keys
+            keys = block_refined_keys(self.cfg)
+        else:
+            keys = root_keys(self.cfg.m, self.cfg.n)
         prim = initial_state(self.cfg, keys)
         self.upload(keys, prim)
         self.body_boundary(1)

@@ -909,6 +909,85 @@ static void Coarse_cell(Solver &, Grid *c) {                    // :397-408
     c->son1 = c->son2 = c->son3 = c->son4 = nullptr;
 }
 
+// ---- static block refinement, run by creat_mesh when lvlBlock > 0
+// (src/mesh.F90:41-44, 49-197, 262-303, 421-461).  box = Block_size(1:4)
+// as set_parameter leaves it (+1e-10 on the upper bounds, src/MAIN.F90:57);
+// refinesize(i) = BufferLayerLVL*h/2**(i-1) (src/MAIN.F90:63-66); sort is
+// identically 0 (gridsort, src/mesh.F90:81-87).
+struct BlockSpec {
+    int lvlblock = 0;
+    double box[4] = {0, 0, 0, 0};
+    double refinesize[FDM_LMAX + 2] = {0};
+};
+static double miblock(const BlockSpec &B, const Grid *c) {      // :421-461
+    const double xo = c->cx, yo = c->cy;
+    const double *bs = B.box;
+    if (xo > bs[1]) {
+        if (yo > bs[3]) return std::sqrt((xo - bs[1]) * (xo - bs[1]) + (yo - bs[3]) * (yo - bs[3]));
+        if (yo < bs[2]) return std::sqrt((xo - bs[1]) * (xo - bs[1]) + (yo - bs[2]) * (yo - bs[2]));
+        return xo - bs[1];
+    }
+    if (xo < bs[0]) {
+        if (yo > bs[3]) return std::sqrt((xo - bs[0]) * (xo - bs[0]) + (yo - bs[3]) * (yo - bs[3]));
+        if (yo < bs[2]) return std::sqrt((xo - bs[0]) * (xo - bs[0]) + (yo - bs[2]) * (yo - bs[2]));
+        return bs[0] - xo;
+    }
+    if (yo > bs[3]) return yo - bs[3];
+    if (yo < bs[2]) return bs[2] - yo;
+    return 0.0;
+}
+static void Block_refi(Solver &S, const BlockSpec &B, Grid *c) {   // :176-197
+    if (c->lvl >= B.lvlblock) return;
+    if (c->son1) {
+        Block_refi(S, B, c->son1); Block_refi(S, B, c->son2);
+        Block_refi(S, B, c->son3); Block_refi(S, B, c->son4);
+        return;
+    }
+    if (c->sort == 1) return;
+    if (c->cx < B.box[0] || c->cx > B.box[1] || c->cy < B.box[2] || c->cy > B.box[3]) return;
+    Refine_cell(S, c);
+    Block_refi(S, B, c->son1); Block_refi(S, B, c->son2);
+    Block_refi(S, B, c->son3); Block_refi(S, B, c->son4);
+}
+static void BlockDis_refi(Solver &S, const BlockSpec &B, Grid *c) {  // :144-174
+    if (c->lvl >= B.lvlblock) return;
+    if (c->son1) {
+        BlockDis_refi(S, B, c->son1); BlockDis_refi(S, B, c->son2);
+        BlockDis_refi(S, B, c->son3); BlockDis_refi(S, B, c->son4);
+        return;
+    }
+    if (c->sort == 1) return;
+    const double dis = miblock(B, c);
+    for (int i = 1; i <= B.lvlblock; ++i) {
+        if (dis <= B.refinesize[i] && c->sort == 0 && c->lvl < i) {
+            Refine_cell(S, c);
+            BlockDis_refi(S, B, c->son1); BlockDis_refi(S, B, c->son2);
+            BlockDis_refi(S, B, c->son3); BlockDis_refi(S, B, c->son4);
+            break;
+        }
+    }
+}
+static void gridmodify0(Solver &S, Grid *c) {                   // gridmodify, :262-303
+    if (c->son1) {
+        gridmodify0(S, c->son1); gridmodify0(S, c->son2);
+        gridmodify0(S, c->son3); gridmodify0(S, c->son4);
+        return;
+    }
+    Grid *cjp = up_neighbor(S, c), *cjm = down_neighbor(S, c);
+    Grid *cim = left_neighbor(S, c), *cip = right_neighbor(S, c);
+    if (cjp && c->lvl - cjp->lvl > 1) Refine_cell(S, cjp);
+    if (cjm && c->lvl - cjm->lvl > 1) Refine_cell(S, cjm);
+    if (cim && c->lvl - cim->lvl > 1) Refine_cell(S, cim);
+    if (cip && c->lvl - cip->lvl > 1) Refine_cell(S, cip);
+}
+static void Block_refine(Solver &S, const BlockSpec &B) {        // :49-79
+    for (int i = 1; i <= S.total; ++i) Block_refi(S, B, S.C(i));
+    for (int i = 1; i <= S.total; ++i) BlockDis_refi(S, B, S.C(i));
+    for (int j = 1; j <= B.lvlblock - 1; ++j)
+        for (int i = 1; i <= S.total; ++i)
+            if (S.C(i)->son1) gridmodify0(S, S.C(i));
+}
+
 static void gridmodify1(Solver &S, Grid *c) {                   // :305-353
     if (c->son1) {
         gridmodify1(S, c->son1); gridmodify1(S, c->son2);
@@ -1363,12 +1442,28 @@ int orc_mesh_dims(void *h, int *m, int *n) {
     *m = S->m; *n = S->n;
     return 0;
 }
-// initial (src/solution.F90:9-29) + IDgrid; kind 0 vortex, 1 quadrants, 2 oblique shock
+// creat_mesh's Block_refine (src/mesh.F90:41-44), before initial
+int orc_block_refine(void *h, int lvlblock, const double *box, int buffer_layer_lvl) {
+    Solver *S = (Solver *)h;
+    if (lvlblock < 0 || lvlblock > FDM_LMAX) return FDM_ERR_ARG;
+    BlockSpec B;
+    B.lvlblock = lvlblock;
+    for (int k = 0; k < 4; ++k) B.box[k] = box[k];
+    for (int i = 1; i <= lvlblock; ++i) B.refinesize[i] = (double)buffer_layer_lvl * S->h / (double)(1LL << (i - 1));
+    Block_refine(*S, B);
+    idneighbor(*S);
+    return 0;
+}
+// initial (src/solution.F90:9-29) + IDgrid; kind 0 vortex, 1 quadrants, 2
+// oblique shock.  Internal nodes of a
+// block-refined mesh are left unset by the reference (allocated, never
+// assigned); here they take the interpA mean, as after an upload.
 int orc_initial(void *h, int kind, const double *icp, int nicp) {
     Solver *S = (Solver *)h;
     S->ic_kind = kind;
     for (int i = 0; i < nicp && i < 32; ++i) S->icp[i] = icp[i];
     for (int i = 1; i <= S->total; ++i) ic_tree(*S, S->C(i));
+    for (int i = 1; i <= S->total; ++i) set_internal_means(S->C(i));
     for (int i = 1; i <= S->total; ++i) initial_boundary(*S, S->C(i), S->tt);
     IDgrid(*S);
     return 0;

@@ -41,6 +41,7 @@ def lib():
         L.orc_destroy.argtypes = [vp]
         L.orc_set_threads.argtypes = [vp, i32]
         L.orc_initial.argtypes = [vp, i32, dp, i32]
+        L.orc_block_refine.argtypes = [vp, i32, dp, i32]
         L.orc_num_leaves.restype = i64
         L.orc_num_leaves.argtypes = [vp]
         L.orc_num_interior.restype = i64
@@ -98,6 +99,11 @@ class Oracle:
         if threads:
             self.L.orc_set_threads(self.h, threads)
         if initial:
+            if getattr(cfg, "block", None):
+                lvl, box, buf = cfg.block
+                bx = np.asarray(box, dtype=np.float64)
+                if self.L.orc_block_refine(self.h, lvl, _dp(bx), buf):
+                    raise ValueError("bad block refinement parameters")
             icp = np.asarray(cfg.ic_params if cfg.ic_params else [0.0], dtype=np.float64)
             self.L.orc_initial(self.h, cfg.ic_kind, _dp(icp), len(cfg.ic_params))
 
