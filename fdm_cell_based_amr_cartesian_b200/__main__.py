@@ -8,6 +8,11 @@ runs the four-quadrant problem on a 128^2 background with 4 levels for 200
 steps (or to t_end when --steps is 0) with device regrids every nstep_adapt
 steps, and prints one JSON line: steps, seconds, the solver's counters and
 the device time of each regrid phase, summed over the run.
+
+    --block LVL X1 X2 Y1 Y2 BUF
+
+adds creat_mesh's static block refinement (lvlBlock, Block_size,
+BufferLayerLVL of src/MAIN.F90:42-45) to the initial mesh.
 """
 from __future__ import annotations
 
@@ -22,14 +27,20 @@ from .solver import Solver
 
 def config(args) -> P.Config:
     if args.case == "riemann4":
-        return P.riemann4(base=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.3)
-    if args.case == "vortex":
-        return P.vortex(base=args.base, lvl_amr=args.lvl_amr)
-    if args.case == "double_mach":
-        return P.double_mach(base_y=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.2)
-    if args.case == "reference":
-        return P.reference_default()
-    raise SystemExit(f"unknown case {args.case}")
+        cfg = P.riemann4(base=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.3)
+    elif args.case == "vortex":
+        cfg = P.vortex(base=args.base, lvl_amr=args.lvl_amr)
+    elif args.case == "double_mach":
+        cfg = P.double_mach(base_y=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.2)
+    elif args.case == "reference":
+        cfg = P.reference_default()
+    else:
+        raise SystemExit(f"unknown case {args.case}")
+    block = getattr(args, "block", None)
+    if block:
+        lvl, x1, x2, y1, y2, buf = block
+        P.with_block(cfg, int(lvl), (float(x1), float(x2), float(y1), float(y2)), int(buf))
+    return cfg
 
 
 def main(argv=None) -> int:
@@ -40,6 +51,8 @@ def main(argv=None) -> int:
     ap.add_argument("--t-end", type=float, default=0.0, help="end time (0: the case's own)")
     ap.add_argument("--steps", type=int, default=0, help="steps to run (0: run to t_end)")
     ap.add_argument("--gate", action="store_true", help="learned face gate on")
+    ap.add_argument("--block", nargs=6, metavar=("LVL", "X1", "X2", "Y1", "Y2", "BUF"), default=None,
+                    help="static block refinement of the initial mesh (lvlBlock, Block_size, BufferLayerLVL)")
     args = ap.parse_args(argv)
 
     cfg = config(args)

@@ -6,7 +6,7 @@ from fdm_cell_based_amr_cartesian_b200.__main__ import config
 
 
 def _args(**kw):
-    base = dict(case="riemann4", base=128, lvl_amr=4, t_end=0.0, steps=0, gate=False)
+    base = dict(case="riemann4", base=128, lvl_amr=4, t_end=0.0, steps=0, gate=False, block=None)
     base.update(kw)
     return argparse.Namespace(**base)
 
@@ -23,3 +23,9 @@ def test_cli_configurations():
     assert c.params.t_end == 0.2
     c = config(_args(case="reference"))
     assert c.name == "reference_default"
+
+
+def test_cli_block_option():
+    c = config(_args(case="vortex", base=32, lvl_amr=2, block=["2", "2.5", "7.5", "2.5", "7.5", "2"]))
+    assert c.block == (2, (2.5, 7.5 + 1e-10, 2.5, 7.5 + 1e-10), 2)
+    assert config(_args()).block is None
