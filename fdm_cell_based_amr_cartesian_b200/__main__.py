@@ -12,7 +12,12 @@ the device time of each regrid phase, summed over the run.
     --block LVL X1 X2 Y1 Y2 BUF
 
 adds creat_mesh's static block refinement (lvlBlock, Block_size,
-BufferLayerLVL of src/MAIN.F90:42-45) to the initial mesh.
+BufferLayerLVL of src/MAIN.F90:42-45) to the initial mesh, and
+
+    --output DIR
+
+writes the reference's diagnostic files there (Residual.dat every 100 steps
+and at t_end, accuracy_error.dat at t_end; src/solution.F90:217-234).
 """
 from __future__ import annotations
 
@@ -30,6 +35,8 @@ def config(args) -> P.Config:
         cfg = P.riemann4(base=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.3)
     elif args.case == "vortex":
         cfg = P.vortex(base=args.base, lvl_amr=args.lvl_amr)
+        if args.t_end:
+            cfg.params.t_end = args.t_end
     elif args.case == "double_mach":
         cfg = P.double_mach(base_y=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.2)
     elif args.case == "reference":
@@ -51,6 +58,7 @@ def main(argv=None) -> int:
     ap.add_argument("--t-end", type=float, default=0.0, help="end time (0: the case's own)")
     ap.add_argument("--steps", type=int, default=0, help="steps to run (0: run to t_end)")
     ap.add_argument("--gate", action="store_true", help="learned face gate on")
+    ap.add_argument("--output", default=None, help="directory for Residual.dat / accuracy_error.dat")
     ap.add_argument("--block", nargs=6, metavar=("LVL", "X1", "X2", "Y1", "Y2", "BUF"), default=None,
                     help="static block refinement of the initial mesh (lvlBlock, Block_size, BufferLayerLVL)")
     args = ap.parse_args(argv)
@@ -61,18 +69,26 @@ def main(argv=None) -> int:
     if args.gate:
         from . import learned
         learned.enable(g)
+    diag = None
+    if args.output:
+        from .output import PSTEP_RES, Output
+        diag = Output(args.output)
     t0 = time.perf_counter()
     n = 0
-    if args.steps > 0:
-        n = g.solute(args.steps)
-    else:
-        while g.scalars()["tt"] < cfg.params.t_end:
-            k = g.solute(100)
-            n += k
-            if k == 0:
-                break
+    target = args.steps if args.steps > 0 else None
+    while (target is None or n < target) and g.scalars()["tt"] < cfg.params.t_end:
+        # chunks end on multiples of Pstep_Res = 100, where output_Res writes
+        k = g.solute(min(100, target - n) if target is not None else 100)
+        n += k
+        sc = g.scalars()
+        if diag is not None and (sc["it"] % PSTEP_RES == 0 or sc["tt"] == cfg.params.t_end):
+            print(diag.res(g), file=sys.stderr)
+        if k == 0:
+            break
     tt = g.scalars()["tt"]   # waits for the device
     seconds = time.perf_counter() - t0
+    if diag is not None and tt == cfg.params.t_end:
+        diag.error(g)
     out = {"case": args.case, "steps": n, "seconds": seconds, "tt": tt,
            "counters": g.counters(), "regrid_device_ms_total": g.amr_phase_ms(total=True)}
     g.close()

@@ -29,3 +29,7 @@ def test_cli_block_option():
     c = config(_args(case="vortex", base=32, lvl_amr=2, block=["2", "2.5", "7.5", "2.5", "7.5", "2"]))
     assert c.block == (2, (2.5, 7.5 + 1e-10, 2.5, 7.5 + 1e-10), 2)
     assert config(_args()).block is None
+
+
+def test_cli_vortex_end_time():
+    assert config(_args(case="vortex", base=32, lvl_amr=2, t_end=0.5)).params.t_end == 0.5

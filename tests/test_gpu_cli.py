@@ -15,3 +15,16 @@ def test_cli_short_vortex_run(capsys):
     assert out["steps"] == 25
     assert out["counters"]["n_regrids"] >= 2
     assert out["tt"] > 0
+
+
+def test_cli_writes_the_reference_diagnostics(tmp_path, capsys):
+    d = str(tmp_path / "Output")
+    assert main(["--case", "vortex", "--base", "32", "--lvl-amr", "2", "--t-end", "0.5", "--output", d]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["tt"] == 0.5
+    res = open(f"{d}/Residual.dat").read().splitlines()
+    assert len(res) >= 1 and all(len(r) == 16 + 10 * 24 for r in res)
+    err = open(f"{d}/accuracy_error.dat").read().splitlines()
+    assert err[0].split()[0] == "nstep" and len(err) == 3
+    l1 = float(err[1][16:30])
+    assert 0.0 < l1 < 1e-2
