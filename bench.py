@@ -386,6 +386,47 @@ def ensemble_window(args, world):
             "gpu_launches_per_step": 3 if best_bps else None}
 
 
+def strips_window(keys, prim, nstrips=4, steps=3):
+    """One mesh as strips of background rows with the halo exchange after
+    every stage, all strips on this GPU: time per step and bit-identity with
+    the whole mesh after the same steps."""
+    import torch
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+    from fdm_cell_based_amr_cartesian_b200 import strips as SP
+    cfg = P.riemann4(base=128, lvl_amr=4)
+    cfg.params.iflag_amr = 0
+    t_end = cfg.params.t_end
+    plan = SP.StripPlan(cfg, keys, nstrips)
+    engines = [SP.GpuStrip(plan, s, prim) for s in range(nstrips)]
+    xchg = SP.LocalExchange(engines)
+    tt, it, _ = SP.run(engines, xchg, 1, t_end)          # warm-up step
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tt, it, k = SP.run(engines, xchg, steps, t_end, tt, it)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    ks, ps = plan.gather([e.leaves() for e in engines])
+    for e in engines:
+        e.close()
+    whole = S.Solver(cfg)
+    whole.upload(keys, prim)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(1 + steps):
+        whole.solute_step()
+    torch.cuda.synchronize()
+    dt_whole = (time.perf_counter() - t1) / (1 + steps)
+    kw, pw = whole.leaves()
+    ni = whole.counters()["n_interior"]
+    whole.close()
+    return {"strips": nstrips, "rows": [list(st.own) for st in plan.strips], "steps": k,
+            "ms_per_step": dt / k * 1e3, "value": ni * k / dt, "unit": UNIT,
+            "whole_mesh_ms_per_step": dt_whole * 1e3,
+            "bit_identical_to_whole_mesh": bool(np.array_equal(ks, kw) and np.array_equal(ps, pw)),
+            "note": "all strips on one GPU with the host-driven exchange (every split-API call synchronises): "
+                    "the cost of the protocol, not a multi-GPU scaling figure; host-timed"}
+
+
 GOLDEN_RUNS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "oracle_runs.json")
 
 
@@ -565,6 +606,11 @@ def run_ours(args):
     if not args.no_learned:
         gated = learned_window(args, cfg, keys, prim, NI, flush, world)
 
+    # one mesh as 4 strips with the halo exchange (all on this GPU)
+    strips = None
+    if not args.no_strips:
+        strips = strips_window(keys, prim)
+
     # the batched ensemble (configuration 5)
     ens = None
     if not args.no_ensemble:
@@ -618,7 +664,7 @@ def run_ours(args):
                 "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
                 "counters": cnt, "state_finite_after_timed_steps": finite, "cpu_baseline": cpu,
-                "fast_flux": fastf, "learned": gated, "ensemble": ens, "full_run": full}
+                "fast_flux": fastf, "learned": gated, "ensemble": ens, "full_run": full, "strips": strips}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -637,6 +683,7 @@ def main():
     ap.add_argument("--no-full-run", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-strips", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
