@@ -386,7 +386,7 @@ def ensemble_window(args, world):
             "gpu_launches_per_step": 3 if best_bps else None}
 
 
-def strips_window(keys, prim, nstrips=4, steps=3):
+def strips_window(keys, prim, nstrips=4, steps=3, asynchronous=False):
     """One mesh as strips of background rows with the halo exchange after
     every stage, all strips on this GPU: time per step and bit-identity with
     the whole mesh after the same steps."""
@@ -397,7 +397,7 @@ def strips_window(keys, prim, nstrips=4, steps=3):
     cfg.params.iflag_amr = 0
     t_end = cfg.params.t_end
     plan = SP.StripPlan(cfg, keys, nstrips)
-    engines = [SP.GpuStrip(plan, s, prim) for s in range(nstrips)]
+    engines = [SP.GpuStrip(plan, s, prim, asynchronous) for s in range(nstrips)]
     xchg = SP.LocalExchange(engines)
     tt, it, _ = SP.run(engines, xchg, 1, t_end)          # warm-up step
     torch.cuda.synchronize()
@@ -419,12 +419,14 @@ def strips_window(keys, prim, nstrips=4, steps=3):
     kw, pw = whole.leaves()
     ni = whole.counters()["n_interior"]
     whole.close()
-    return {"strips": nstrips, "rows": [list(st.own) for st in plan.strips], "steps": k,
+    return {"strips": nstrips, "asynchronous": asynchronous, "rows": [list(st.own) for st in plan.strips],
+            "steps": k,
             "ms_per_step": dt / k * 1e3, "value": ni * k / dt, "unit": UNIT,
             "whole_mesh_ms_per_step": dt_whole * 1e3,
             "bit_identical_to_whole_mesh": bool(np.array_equal(ks, kw) and np.array_equal(ps, pw)),
-            "note": "all strips on one GPU with the host-driven exchange (every split-API call synchronises): "
-                    "the cost of the protocol, not a multi-GPU scaling figure; host-timed"}
+            "note": "all strips on one GPU (synchronous: every split-API call waits; asynchronous: each strip "
+                    "on its own stream, ordered by events, one host wait per strip at step control and step "
+                    "end): the cost of the protocol, not a multi-GPU scaling figure; host-timed"}
 
 
 GOLDEN_RUNS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "oracle_runs.json")
@@ -609,7 +611,8 @@ def run_ours(args):
     # one mesh as 4 strips with the halo exchange (all on this GPU)
     strips = None
     if not args.no_strips:
-        strips = strips_window(keys, prim)
+        strips = strips_window(keys, prim, asynchronous=True)
+        strips["synchronous"] = strips_window(keys, prim, asynchronous=False)
 
     # the batched ensemble (configuration 5)
     ens = None

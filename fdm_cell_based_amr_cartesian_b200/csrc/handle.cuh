@@ -74,6 +74,7 @@ struct fdm_handle {
     bool loaded = false;
     bool lam_fresh = false;
     int cur_buf = 0;         // split API: buffer holding the latest interior values
+    bool split_async = false;  // split API and halo copies return after enqueuing
     int face_variant = 0;    // 0: four lanes per face, 1: one thread per face
     int64_t n_singular = 0, n_regrids = 0, n_restrict = 0, n_ghost_restrict = 0;
 

@@ -143,6 +143,17 @@ static int ensure_lambda(fdm_handle *h) {
     return FDM_OK;
 }
 
+// end of a split-API call: wait for it, or (asynchronous mode) only check
+// that the launches were accepted
+static int split_done(fdm_handle *h) {
+    if (h->split_async) {
+        FDM_CK(h, cudaGetLastError());
+    } else {
+        FDM_CK(h, cudaStreamSynchronize(h->s));
+    }
+    return FDM_OK;
+}
+
 // getRKn + 3 x (solution_cell, updateRK, body_boundary_RK)
 static void enqueue_rk(fdm_handle *h) {
     launch_stage(h, 1);
@@ -526,8 +537,7 @@ int fdm_solution_cells(fdm_handle *h, int32_t krk) {
     launch_requests(h, cur);
     launch_faces(h, cur, krk);
     launch_cells(h, cur, h->B[0].as<double4>(), h->Ut.as<double4>(), krk, 1);
-    FDM_CK(h, cudaStreamSynchronize(h->s));
-    return FDM_OK;
+    return split_done(h);
 }
 int fdm_update_rk(fdm_handle *h, int32_t krk) {
     CHECK_H(h);
@@ -536,16 +546,14 @@ int fdm_update_rk(fdm_handle *h, int32_t krk) {
     launch_blend(h, h->B[0].as<double4>(), h->B[krk % 3].as<double4>(), krk);
     h->cur_buf = krk % 3;
     h->lam_fresh = false;
-    FDM_CK(h, cudaStreamSynchronize(h->s));
-    return FDM_OK;
+    return split_done(h);
 }
 int fdm_body_boundary(fdm_handle *h, int32_t j) {
     CHECK_H(h);
     CHECK_LOADED(h);
     // ghosts of the buffer that holds the latest interior values
     launch_ghosts(h, h->B[h->cur_buf].as<double4>(), j);
-    FDM_CK(h, cudaStreamSynchronize(h->s));
-    return FDM_OK;
+    return split_done(h);
 }
 
 int fdm_residual(fdm_handle *h, double res_max[4], double res_rms[4]) {
@@ -773,8 +781,10 @@ static int pack_common(fdm_handle *h, int64_t n, const int32_t *slots, const dou
     CHECK_LOADED(h);
     if (n < 0 || (n > 0 && (!slots || !buf))) return arg_fail(h, "bad slot list");
     if (n == 0) return FDM_OK;
+    // flag word 6: a slot outside the leaf slots (sticky in asynchronous
+    // mode, where fdm_step_control_global reports it)
     int32_t *bad = h->flag.as<int32_t>() + 6;
-    FDM_CK(h, cudaMemsetAsync(bad, 0, sizeof(int32_t), h->s));
+    if (!h->split_async) FDM_CK(h, cudaMemsetAsync(bad, 0, sizeof(int32_t), h->s));
     const int64_t ns = h->NI + h->NG + h->NC;
     double4 *B = h->B[h->cur_buf].as<double4>();
     if (unpack)
@@ -782,10 +792,21 @@ static int pack_common(fdm_handle *h, int64_t n, const int32_t *slots, const dou
     else
         k_pack_slots<<<nblk(n, 256), 256, 0, h->s>>>(n, slots, ns, B, const_cast<double *>(buf), bad);
     FDM_CK(h, cudaGetLastError());
+    if (h->split_async) return FDM_OK;
     int32_t hb = 0;
     FDM_CK(h, cudaMemcpyAsync(&hb, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     if (hb) return arg_fail(h, "a slot is outside the leaf slots");
+    return FDM_OK;
+}
+
+int fdm_set_async(fdm_handle *h, int32_t on) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    FDM_CK(h, cudaMemsetAsync(h->flag.as<int32_t>() + 6, 0, sizeof(int32_t), h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    h->split_async = on != 0;
     return FDM_OK;
 }
 int fdm_pack_slots(fdm_handle *h, int64_t n, const int32_t *slots, double *buf) {
@@ -806,6 +827,11 @@ int fdm_step_control_global(fdm_handle *h, double lambda_x, double lambda_y, int
     launch_step_control(h);
     RC(sync_scalars_from_device(h));
     FDM_CK(h, cudaGetLastError());
+    if (h->split_async) {   // sticky halo-slot error of the previous step's copies
+        int32_t hb = 0;
+        FDM_CK(h, cudaMemcpy(&hb, h->flag.as<int32_t>() + 6, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (hb) return arg_fail(h, "a halo copy named a slot outside the leaf slots");
+    }
     if (tstep) *tstep = h->hs->tstep;
     return FDM_OK;
 }

@@ -44,7 +44,7 @@ EXPORTS = [
     "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
     "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
     "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
-    "fdm_download_internal", "fdm_set_internal",
+    "fdm_download_internal", "fdm_set_internal", "fdm_set_async",
 ]
 
 
@@ -137,6 +137,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_pack_slots.argtypes = [vp, i64, vp, vp]
     L.fdm_unpack_slots.argtypes = [vp, i64, vp, vp]
     L.fdm_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32, dp]
+    L.fdm_set_async.argtypes = [vp, i32]
     _lib = L
     return L
 
@@ -377,6 +378,11 @@ class Solver:
         self._check(self.L.fdm_step_control_global(self.h, float(lambda_x), float(lambda_y), int(l_max),
                                                    ctypes.byref(dt)))
         return dt.value
+
+    def set_async(self, on: bool):
+        """Split-API calls and halo copies return once enqueued on the
+        handle's stream (device_state()[0]) instead of waiting."""
+        self._check(self.L.fdm_set_async(self.h, 1 if on else 0))
 
     def leaf_slots(self) -> np.ndarray:
         """State slot of every leaf, key order."""

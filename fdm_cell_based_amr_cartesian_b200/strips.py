@@ -153,11 +153,16 @@ class StripPlan:
 
 # ------------------------------------------------------------------ engines
 class GpuStrip:
-    """A libfdm handle holding one strip on the current CUDA device."""
+    """A libfdm handle holding one strip on the current CUDA device.
+
+    asynchronous=True: the stage calls and halo copies only enqueue on the
+    handle's stream (``self.stream``); the exchange orders the strips with
+    CUDA events.  The halo buffers live as long as the strip, so no copy in
+    flight ever reads memory that was handed back."""
 
     width = 4   # (rho, u, v, p) per leaf
 
-    def __init__(self, plan: StripPlan, s: int, values: np.ndarray):
+    def __init__(self, plan: StripPlan, s: int, values: np.ndarray, asynchronous: bool = False):
         import torch
         from .solver import Solver
         st = plan.strips[s]
@@ -169,7 +174,14 @@ class GpuStrip:
         self._slots = {name: torch.from_numpy(slots[r[0]:r[1]].copy()).to(dev)
                        for name, r in (("send_down", st.send_down), ("send_up", st.send_up),
                                        ("recv_down", st.recv_down), ("recv_up", st.recv_up))}
+        self._bufs = {name: torch.empty((len(sl), 4), dtype=torch.float64, device=dev)
+                      for name, sl in self._slots.items()}
+        torch.cuda.synchronize(dev)
         self.device = dev
+        self.stream = None
+        if asynchronous:
+            self.g.set_async(True)
+            self.stream = torch.cuda.ExternalStream(self.g.device_state()[0], device=dev)
 
     def step_control(self):
         _, lx, ly, lm = self.g.step_control_info()
@@ -184,8 +196,7 @@ class GpuStrip:
         self.g.body_boundary(3)
 
     def buffer(self, name: str):
-        import torch
-        return torch.empty((len(self._slots[name]), 4), dtype=torch.float64, device=self.device)
+        return self._bufs[name]
 
     def pack(self, name: str, buf):
         sl = self._slots[name]
@@ -338,6 +349,8 @@ class LocalExchange:
 
     def halos(self):
         e = self.engines
+        if e and getattr(e[0], "stream", None) is not None:
+            return self._halos_async()
         for lo, hi in zip(e[:-1], e[1:]):
             up = lo.buffer("send_up")
             lo.pack("send_up", up)
@@ -345,6 +358,35 @@ class LocalExchange:
             down = hi.buffer("send_down")
             hi.pack("send_down", down)
             lo.unpack("recv_up", down)
+
+    def _halos_async(self):
+        """Every strip on its own stream: packs, an event per strip, the
+        neighbours' unpacks after it, and a strip's next pack after the
+        neighbours have read its buffers."""
+        import torch
+        e = self.engines
+        pairs = list(zip(e[:-1], e[1:]))
+        for lo, hi in pairs:
+            lo.pack("send_up", lo.buffer("send_up"))
+            hi.pack("send_down", hi.buffer("send_down"))
+        packed = []
+        for x in e:
+            ev = torch.cuda.Event()
+            ev.record(x.stream)
+            packed.append(ev)
+        for i, (lo, hi) in enumerate(pairs):
+            hi.stream.wait_event(packed[i])
+            hi.unpack("recv_down", lo.buffer("send_up"))
+            lo.stream.wait_event(packed[i + 1])
+            lo.unpack("recv_up", hi.buffer("send_down"))
+        read = []
+        for x in e:
+            ev = torch.cuda.Event()
+            ev.record(x.stream)
+            read.append(ev)
+        for i, (lo, hi) in enumerate(pairs):
+            lo.stream.wait_event(read[i + 1])
+            hi.stream.wait_event(read[i])
 
 
 class DistExchange:

@@ -425,12 +425,19 @@ int fdm_set_internal(fdm_handle *h, int64_t n, const uint64_t *keys,
  * slots and buf are DEVICE pointers (for NCCL or peer copies), the calls
  * return when the copy is complete.
  * fdm_step_control_global: sets lambda_x, lambda_y (monotone maxima) and
- * l_max and forms the time step of src/solution.F90:195-201 from them. */
+ * l_max and forms the time step of src/solution.F90:195-201 from them.
+ * fdm_set_async(h, 1): fdm_solution_cells, fdm_update_rk, fdm_body_boundary
+ * and the two halo copies return once enqueued on the handle's stream
+ * (fdm_device_state), so the caller orders strips and transfers with CUDA
+ * events instead of host waits; a slot error of a halo copy is then reported
+ * by the next fdm_step_control_global.  fdm_set_async(h, 0) restores the
+ * synchronous calls. */
 int fdm_leaf_slots(fdm_handle *h, int64_t cap, int32_t *slot);
 int fdm_pack_slots(fdm_handle *h, int64_t n, const int32_t *slots, double *buf);
 int fdm_unpack_slots(fdm_handle *h, int64_t n, const int32_t *slots, const double *buf);
 int fdm_step_control_global(fdm_handle *h, double lambda_x, double lambda_y,
                             int32_t l_max, double *tstep);
+int fdm_set_async(fdm_handle *h, int32_t on);
 
 #ifdef __cplusplus
 }

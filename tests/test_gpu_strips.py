@@ -24,9 +24,9 @@ def whole_gpu(cfg, keys, prim, nsteps):
     return k, v, sc
 
 
-def strips_gpu(cfg, keys, prim, nstrips, nsteps):
+def strips_gpu(cfg, keys, prim, nstrips, nsteps, asynchronous=False):
     plan = SP.StripPlan(cfg, keys, nstrips)
-    engines = [SP.GpuStrip(plan, s, prim) for s in range(nstrips)]
+    engines = [SP.GpuStrip(plan, s, prim, asynchronous) for s in range(nstrips)]
     tt, it, k = SP.run(engines, SP.LocalExchange(engines), nsteps, cfg.params.t_end)
     parts = [e.leaves() for e in engines]
     for st, (lk, _) in zip(plan.strips, parts):
@@ -37,26 +37,28 @@ def strips_gpu(cfg, keys, prim, nstrips, nsteps):
     return kg, vg, tt, k
 
 
+@pytest.mark.parametrize("asynchronous", [False, True])
 @pytest.mark.parametrize("mesh,nstrips", [(riemann_mesh, 3), (dmr_mesh, 2), (dmr_mesh, 4)])
-def test_gpu_strips_equal_whole_mesh(oracle_mod, mesh, nstrips):
+def test_gpu_strips_equal_whole_mesh(oracle_mod, mesh, nstrips, asynchronous):
     cfg, keys, prim = mesh()
     nsteps = 5
     k0, v0, sc0 = whole_gpu(cfg, keys, prim, nsteps)
     ko, vo, _ = whole_run(oracle_mod, cfg, keys, prim, nsteps)
     assert np.array_equal(v0, vo)
-    kg, vg, tt, k = strips_gpu(cfg, keys, prim, nstrips, nsteps)
+    kg, vg, tt, k = strips_gpu(cfg, keys, prim, nstrips, nsteps, asynchronous)
     assert k == nsteps and tt == sc0["tt"]
     assert np.array_equal(kg, k0)
     assert np.array_equal(vg, v0)
 
 
-def test_gpu_strips_benchmark_mesh():
+@pytest.mark.parametrize("asynchronous", [False, True])
+def test_gpu_strips_benchmark_mesh(asynchronous):
     cfg = P.riemann4(base=128, lvl_amr=4)
     cfg.params.iflag_amr = 0
     keys = distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], [0.2, 0.15, 0.1, 0.05])
     prim = initial_state(cfg, keys)
     k0, v0, sc0 = whole_gpu(cfg, keys, prim, 3)
-    kg, vg, tt, k = strips_gpu(cfg, keys, prim, 4, 3)
+    kg, vg, tt, k = strips_gpu(cfg, keys, prim, 4, 3, asynchronous)
     assert len(keys) > 1_000_000
     assert tt == sc0["tt"]
     assert np.array_equal(kg, k0) and np.array_equal(vg, v0)
@@ -82,19 +84,20 @@ def test_gpu_strip_errors():
     e.close()
 
 
-@pytest.mark.parametrize("make,nstrips,nsteps", [
-    (lambda: P.riemann4(base=32, lvl_amr=2), 3, 25),
-    (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), 2, 12),
-    (lambda: P.riemann4(base=128, lvl_amr=4), 4, 31),      # configuration 2, 4 regrids
+@pytest.mark.parametrize("make,nstrips,nsteps,asynchronous", [
+    (lambda: P.riemann4(base=32, lvl_amr=2), 3, 25, False),
+    (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), 2, 12, False),
+    (lambda: P.riemann4(base=128, lvl_amr=4), 4, 31, False),      # configuration 2, 4 regrids
+    (lambda: P.riemann4(base=128, lvl_amr=4), 4, 31, True),
 ])
-def test_gpu_strip_run_with_regrids(make, nstrips, nsteps):
+def test_gpu_strip_run_with_regrids(make, nstrips, nsteps, asynchronous):
     """The time loop with AMR on, strips on one GPU and the regrid host
     beside them: the same leaf sets and states as the whole handle."""
     cfg = make()
     g = Solver(cfg)
     g.creat_mesh_and_initial()
     keys, prim = g.leaves()
-    run = SP.StripRun(cfg, keys, prim, nstrips, lambda plan, s, v: SP.GpuStrip(plan, s, v),
+    run = SP.StripRun(cfg, keys, prim, nstrips, lambda plan, s, v: SP.GpuStrip(plan, s, v, asynchronous),
                       lambda k, v: SP.GpuRegridHost(cfg, k, v))
     for _ in range(nsteps):
         g.solute_step()
