@@ -414,6 +414,16 @@ class DistExchange:
         return a if isinstance(a, torch.Tensor) else torch.from_numpy(a)
 
     def halos(self):
+        import contextlib
+        import torch
+        # an asynchronous strip's copies are ordered on its own stream: the
+        # transfers are issued on it and the waits make it (not the host)
+        # wait for them, so its next pack cannot overwrite a buffer in flight
+        st = getattr(self.e, "stream", None)
+        with torch.cuda.stream(st) if st is not None else contextlib.nullcontext():
+            self._halos()
+
+    def _halos(self):
         import torch.distributed as dist
         e, r = self.e, self.rank
         ops, recvs = [], []
