@@ -5,6 +5,9 @@ solver) for whole runs with regrids, stored as digests in oracle_runs.json.
     python tests/golden/make_golden.py --long     # also the four-quadrant
                                                   # problem at 128^2, 4 levels
                                                   # (about 25 min on 8 cores)
+                                                  # and the double Mach
+                                                  # reflection at 256x64, 4 levels
+    python tests/golden/make_golden.py --long --only NAME   # one case
 
 A case is a configuration run with Oracle.solute from its initial condition
 until t_end (or for a number of steps); the record holds the step count,
@@ -41,6 +44,7 @@ def cases(long=False):
     }
     if long:
         c["riemann4_128_l4_to_t0.3"] = (lambda: P.riemann4(base=128, lvl_amr=4, t_end=0.3), None)
+        c["double_mach_256x64_l4_to_t0.2"] = (lambda: P.double_mach(base_y=64, lvl_amr=4, t_end=0.2), None)
     return c
 
 
@@ -79,9 +83,12 @@ def run(make, steps, threads=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--long", action="store_true")
+    ap.add_argument("--only", default=None, help="run this case alone")
     args = ap.parse_args()
     out = json.load(open(OUT)) if os.path.exists(OUT) else {}
     for name, (make, steps) in cases(args.long).items():
+        if args.only and name != args.only:
+            continue
         t0 = time.time()
         out[name] = run(make, steps)
         print(name, out[name], f"{time.time() - t0:.1f}s", flush=True)
