@@ -4,7 +4,8 @@ the configuration-1 vortex (200 steps, 20 regrids), the four-quadrant
 problem at 32^2 / 2 levels, the double Mach reflection at 64x16 / 2 levels
 and 128x32 / 3 levels to t = 0.2 (698 steps with 140 regrids, 3011 steps with
 603 regrids), and (when recorded) the four-quadrant problem at 128^2 / 4
-levels to t = 0.3 (6032 steps, 604 regrids)."""
+levels to t = 0.3 (6032 steps, 604 regrids) and the Mach-10 reflection at
+256x64 / 4 levels to t = 0.2 (12939 steps, 2588 regrids)."""
 import json
 import os
 import sys
