@@ -29,7 +29,6 @@ torch.distributed: NCCL between GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
-import ctypes
 from dataclasses import dataclass
 
 import numpy as np
