@@ -351,6 +351,11 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
     });
 }
 
+// Test of the bounded waits: a grid barrier that waits for one block more
+// than the launch has, so every wait runs into its iteration limit, sets the
+// error word and returns.
+__global__ void k_barrier_timeout(GridBar *b, unsigned expected) { grid_bar(b, expected); }
+
 }  // namespace fdm
 
 using namespace fdm;
@@ -797,6 +802,36 @@ int fdm_batch_stream(const fdm_batch *b, void **stream) {
     if (!b || !stream) return FDM_ERR_ARG;
     *stream = (void *)b->s;
     return FDM_OK;
+}
+
+// 2 blocks in a grid barrier that expects 3: returns FDM_ERR_TIMEOUT when
+// the waits gave up (the expected outcome) and their device time in
+// *seconds; the context stays usable.
+int fdm_debug_barrier_timeout(double *seconds) {
+    fdm::GridBar *d = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    fdm::GridBar hb{};
+    int rc = FDM_ERR_CUDA;
+    if (cudaMalloc((void **)&d, sizeof(fdm::GridBar)) != cudaSuccess) return FDM_ERR_NOMEM;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+        cudaEventCreate(&e1) == cudaSuccess && cudaMemsetAsync(d, 0, sizeof(fdm::GridBar), s) == cudaSuccess &&
+        cudaEventRecord(e0, s) == cudaSuccess) {
+        fdm::k_barrier_timeout<<<2, 32, 0, s>>>(d, 3u);
+        if (cudaGetLastError() == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
+            cudaMemcpyAsync(&hb, d, sizeof hb, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+            cudaStreamSynchronize(s) == cudaSuccess) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (seconds) *seconds = ms * 1e-3;
+            rc = hb.err ? FDM_ERR_TIMEOUT : FDM_OK;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+    cudaFree(d);
+    return rc;
 }
 
 }  // extern "C"

@@ -44,7 +44,7 @@ EXPORTS = [
     "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
     "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
     "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
-    "fdm_download_internal", "fdm_set_internal", "fdm_set_async",
+    "fdm_download_internal", "fdm_set_internal", "fdm_set_async", "fdm_debug_barrier_timeout",
 ]
 
 
@@ -138,6 +138,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_unpack_slots.argtypes = [vp, i64, vp, vp]
     L.fdm_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32, dp]
     L.fdm_set_async.argtypes = [vp, i32]
+    L.fdm_debug_barrier_timeout.argtypes = [dp]
     _lib = L
     return L
 

@@ -239,6 +239,11 @@ int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out);
  * the WLS stencil in the reference's list order. */
 int fdm_debug_requests(fdm_handle *h, int64_t cap, int32_t *kind, uint64_t *node,
                        double *xy, int32_t *m12, uint64_t *mem);
+/* The bounded waits of the batched kernel's grid barrier: two blocks wait
+ * for a third that never arrives, give up at the iteration limit and
+ * return.  Returns FDM_ERR_TIMEOUT (the expected outcome) with the device
+ * time of the waits in *seconds; the context stays usable. */
+int fdm_debug_barrier_timeout(double *seconds);
 /* AMR indicators rot/div of the interior leaves (src/solution.F90:424-466). */
 int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double *div,
                       double *srot_sdiv_ne);
