@@ -18,6 +18,13 @@ BufferLayerLVL of src/MAIN.F90:42-45) to the initial mesh, and
 
 writes the reference's diagnostic files there (Residual.dat every 100 steps
 and at t_end, accuracy_error.dat at t_end; src/solution.F90:217-234).
+
+    --case ensemble --members 64 [--bps 0|1|2]
+
+runs the ensemble configuration (random four-quadrant members, seeds from
+1000, maximum level drawn from 2..5, learned gate on) as one batch to each
+member's t_end (or --steps), regrids included.  The gate itself is trained
+by ``python -m fdm_cell_based_amr_cartesian_b200.learned``.
 """
 from __future__ import annotations
 
@@ -50,9 +57,54 @@ def config(args) -> P.Config:
     return cfg
 
 
+def run_ensemble(args) -> int:
+    """The ensemble configuration as one batch (fdm_batch_solute), each
+    member to its own t_end."""
+    from . import ensemble as E
+    from . import learned
+    from .solver import Batch
+    cfgs = E.ensemble_configs(seeds=tuple(range(1000, 1000 + args.members)))
+    sols = []
+    for cfg, (k, p) in zip(cfgs, E.ensemble_meshes(cfgs)):
+        g = Solver(cfg)
+        g.upload(k, p)
+        g.body_boundary(1)
+        learned.enable(g)
+        sols.append(g)
+    leaves0 = sum(g.counters()["n_interior"] for g in sols)
+    batch = Batch(sols)
+    batch.set_blocks_per_sm(args.bps)
+    t0 = time.perf_counter()
+    n = 0
+    target = args.steps if args.steps > 0 else None
+    while target is None or n < target:
+        k = batch.solute(min(100, target - n) if target is not None else 100)
+        n += k
+        if k == 0 or all(g.scalars()["tt"] >= g.cfg.params.t_end for g in sols):
+            break
+    batch.sync()
+    seconds = time.perf_counter() - t0
+    tts = [g.scalars()["tt"] for g in sols]
+    out = {"case": "ensemble", "members": len(sols), "steps": n, "seconds": seconds,
+           "interior_leaves_at_start": leaves0,
+           "interior_leaves_at_end": sum(g.counters()["n_interior"] for g in sols),
+           "regrids": sum(g.counters()["n_regrids"] for g in sols),
+           "members_at_t_end": sum(1 for g, t in zip(sols, tts) if t >= g.cfg.params.t_end),
+           "tt_min": min(tts), "tt_max": max(tts), "batch": batch.info()}
+    batch.close()
+    for g in sols:
+        g.close()
+    print(json.dumps(out))
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m fdm_cell_based_amr_cartesian_b200")
-    ap.add_argument("--case", default="riemann4", choices=["riemann4", "vortex", "double_mach", "reference"])
+    ap.add_argument("--case", default="riemann4",
+                    choices=["riemann4", "vortex", "double_mach", "reference", "ensemble"])
+    ap.add_argument("--members", type=int, default=64, help="ensemble members (--case ensemble)")
+    ap.add_argument("--bps", type=int, default=0,
+                    help="ensemble: 1 or 2 blocks per SM of the persistent kernel, 0 the members' own graphs")
     ap.add_argument("--base", type=int, default=128, help="background cells (per side; rows for double_mach)")
     ap.add_argument("--lvl-amr", type=int, default=4)
     ap.add_argument("--t-end", type=float, default=0.0, help="end time (0: the case's own)")
@@ -62,6 +114,8 @@ def main(argv=None) -> int:
     ap.add_argument("--block", nargs=6, metavar=("LVL", "X1", "X2", "Y1", "Y2", "BUF"), default=None,
                     help="static block refinement of the initial mesh (lvlBlock, Block_size, BufferLayerLVL)")
     args = ap.parse_args(argv)
+    if args.case == "ensemble":
+        return run_ensemble(args)
 
     cfg = config(args)
     g = Solver(cfg)

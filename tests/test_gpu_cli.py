@@ -30,3 +30,10 @@ def test_cli_writes_the_reference_diagnostics(tmp_path, capsys):
     # the flow has moved by (0.5, 0.5) at t = 0.5
     l1 = float(err[1][16:30])
     assert 0.0 < l1 < 1.0
+
+
+def test_cli_ensemble_run(capsys):
+    assert main(["--case", "ensemble", "--members", "4", "--steps", "20"]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["members"] == 4 and out["steps"] == 20
+    assert out["regrids"] >= 4 * 2 and 0 < out["tt_min"] <= out["tt_max"]
