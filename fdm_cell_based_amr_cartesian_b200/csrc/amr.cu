@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(32) k_ordered_sums(int64_t NI, const double2 *
 
 // rot/div of the current state into rot/div buffers; ordered sums to out3
 static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3) {
+    Nvtx range("fdm regrid: indicators");
     const int64_t NI = h->NI;
     launch_requests(h, h->B[0].as<double4>());
     Carve cv;
@@ -1477,6 +1478,7 @@ static int emit_buffers(fdm_handle *h, int64_t n, Emit &E) {
 // One gridmodify1 pass over the node set A -> A; *did: a node was refined
 // or coarsened (otherwise A is left as it is).
 static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
+    Nvtx range("fdm regrid: gridmodify1");
     const int TB = 256;
     const int64_t n = X.A.n;
     Carve cv;
@@ -1541,6 +1543,7 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
 // One gridmodify4 pass over the node set A -> A; *did: something was
 // refined (otherwise A is left as it is).
 static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
+    Nvtx range("fdm regrid: gridmodify4");
     const int TB = 256;
     const int64_t n = X.A.n;
     Carve cv;
@@ -1635,6 +1638,7 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
 // AMR (src/solution.F90:408-421) after the trigger test: indicators,
 // refine/coarsen, lvlAMR rounds of gridmodify1 + gridmodify4, new tables.
 int run_amr(fdm_handle *h) {
+    Nvtx range("fdm regrid");
     const int TB = 256;
     const int64_t NL = h->NL, NI = h->NI, NInt = h->NInt;
     if (h->p.window_rows != 0) {

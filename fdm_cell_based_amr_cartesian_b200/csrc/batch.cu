@@ -659,6 +659,7 @@ int fdm_batch_last_error(const fdm_batch *b, char *buf, size_t n) {
 // nsteps solute iterations of every unfinished member, no regrid and no
 // host synchronisation (graph replays on the batch stream).
 int fdm_batch_advance(fdm_batch *b, int64_t nsteps) {
+    fdm::Nvtx range("fdm_batch_advance");
     if (!b || nsteps < 0) return FDM_ERR_ARG;
     cudaSetDevice(b->device);
     for (fdm_handle *h : b->mem) {
@@ -692,6 +693,7 @@ int fdm_batch_advance(fdm_batch *b, int64_t nsteps) {
 // regrid is due are regridded before the next step.  steps_done: steps
 // taken.  Members past t_end are left alone.
 int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done) {
+    fdm::Nvtx range("fdm_batch_solute");
     if (!b || nsteps < 0) return FDM_ERR_ARG;
     cudaSetDevice(b->device);
     const int n = (int)b->mem.size();

@@ -648,6 +648,7 @@ static int read_back(fdm_handle *h, int32_t he[8], int64_t *tot, int nt) {
     } while (0)
 
 int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double *prim_in) {
+    Nvtx range("fdm tables");
     const int TB = 256;
     cudaStream_t s = h->s;
     if (n <= 0 || n >= (1ll << 31) - 1) return arg_fail(h, "leaf count out of range");

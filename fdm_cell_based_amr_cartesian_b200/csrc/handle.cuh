@@ -5,9 +5,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fdm_common.cuh"
 
 namespace fdm {
+
+// A named NVTX range over a scope (profilers show the library's phases;
+// without a tool attached a push/pop costs a pointer test).
+struct Nvtx {
+    explicit Nvtx(const char *name) { nvtxRangePushA(name); }
+    ~Nvtx() { nvtxRangePop(); }
+    Nvtx(const Nvtx &) = delete;
+    Nvtx &operator=(const Nvtx &) = delete;
+};
+
 
 // Device buffer that only grows; freed with the handle.
 struct DevBuf {

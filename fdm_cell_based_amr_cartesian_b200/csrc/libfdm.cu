@@ -343,6 +343,7 @@ int fdm_last_error(const fdm_handle *h, char *buf, size_t n) {
 }
 
 int fdm_upload_leaves(fdm_handle *h, int64_t n, const uint64_t *keys, const double *prim) {
+    Nvtx range("fdm_upload_leaves");
     CHECK_H(h);
     if (n <= 0 || !keys || !prim) return arg_fail(h, "empty leaf set");
     DevBuf dk, dp;
@@ -509,6 +510,7 @@ int fdm_step_control(fdm_handle *h, double *tstep, double *lambda_x, double *lam
 }
 
 int fdm_time_advance_rk(fdm_handle *h, double tstep) {
+    Nvtx range("fdm_time_advance_rk");
     CHECK_H(h);
     CHECK_LOADED(h);
     launch_set_tstep(h, tstep);
@@ -567,6 +569,7 @@ int fdm_residual(fdm_handle *h, double res_max[4], double res_rms[4]) {
 }
 
 int fdm_solute_step(fdm_handle *h) {
+    Nvtx range("fdm_solute_step");
     CHECK_H(h);
     CHECK_LOADED(h);
     RC(ensure_lambda(h));
@@ -596,6 +599,7 @@ int fdm_solute_step(fdm_handle *h) {
 // device's own; after a NaN the ghost cells may have been refreshed once more
 // than solute_step leaves them.
 int fdm_solute(fdm_handle *h, int64_t nsteps, int64_t *steps_done) {
+    Nvtx range("fdm_solute");
     CHECK_H(h);
     CHECK_LOADED(h);
     int64_t k = 0;
@@ -642,6 +646,7 @@ int fdm_solute(fdm_handle *h, int64_t nsteps, int64_t *steps_done) {
 // no host synchronisation and no regrid inside (the caller keeps the window
 // between regrids).  Used for the timed windows of the benchmark.
 int fdm_advance(fdm_handle *h, int64_t nsteps) {
+    Nvtx range("fdm_advance");
     CHECK_H(h);
     CHECK_LOADED(h);
     RC(ensure_lambda(h));
