@@ -501,6 +501,40 @@ def full_run(S, gate, ulp=False, case="riemann4"):
     return out, leaves
 
 
+def full_run_batched(S, case="double_mach"):
+    """The same full run through the batched path: the autotuner picks the
+    face launch shape, then a batch of one member advances it with the
+    persistent kernel (2 blocks per SM, one launch per RK3 stage, CUDA-graph
+    steps) and regrids when due."""
+    import torch
+    make, desc, golden = FULL_RUNS[case]
+    cfg = make()
+    gf = S.Solver(cfg)
+    gf.creat_mesh_and_initial()
+    tuned, _ = gf.autotune(reps=3)
+    b = S.Batch([gf])
+    b.set_blocks_per_sm(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    steps = 0
+    while gf.scalars()["tt"] < cfg.params.t_end:
+        k = b.solute(10 * cfg.params.pstep_adapt)
+        steps += k
+        if k == 0:
+            break
+    b.sync()
+    t_full = time.perf_counter() - t0
+    keys, prim = gf.leaves()
+    cf = gf.counters()
+    out = {"workload": desc + "; batched persistent kernel, autotuned face launch shape",
+           "seconds": t_full, "steps": steps, "regrids": cf["n_regrids"], "face_variant": tuned,
+           "batch": b.info(), "leaves_at_end": cf["n_leaves"],
+           "bit_identical_to_oracle_run": matches_golden(golden, keys, prim, steps, cf["n_regrids"])}
+    b.close()
+    gf.close()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -644,6 +678,10 @@ def run_ours(args):
             full["double_mach"] = full_run(S, gate=False, case="double_mach")[0]
         except Exception as ex:
             full["double_mach"] = {"error": f"{type(ex).__name__}: {ex}"}
+        try:
+            full["double_mach"]["batched"] = full_run_batched(S, case="double_mach")
+        except Exception as ex:
+            full["double_mach"]["batched"] = {"error": f"{type(ex).__name__}: {ex}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1

@@ -48,3 +48,33 @@ def test_gpu_reproduces_golden_run(name):
     assert g.counters()["n_gm4_nonleaf"] == want["gm4_nonleaf"]
     for k in ("n_leaves", "sha256_keys", "sha256_prim"):
         assert rec[k] == want[k], (k, rec, want)
+
+
+@pytest.mark.parametrize("name", ["riemann4_32_l2_to_t0.3", "double_mach_64x16_l2_to_t0.2"])
+def test_batched_persistent_kernel_reproduces_golden_run(name):
+    """The same whole runs through the batched path (a batch of one member,
+    the persistent kernel at 2 blocks per SM, regrids when due), after the
+    autotuner has picked the face launch shape."""
+    from fdm_cell_based_amr_cartesian_b200.solver import Batch
+    make, steps = make_golden.cases(long=True)[name]
+    cfg = make()
+    g = Solver(cfg)
+    g.creat_mesh_and_initial()
+    g.autotune(reps=2)
+    b = Batch([g])
+    b.set_blocks_per_sm(2)
+    n = 0
+    while g.scalars()["tt"] < cfg.params.t_end:
+        k = b.solute(50)
+        n += k
+        if k == 0:
+            break
+    b.sync()
+    keys, prim = g.leaves()
+    rec = make_golden.digest(keys, prim)
+    want = GOLDEN[name]
+    assert n == want["steps"] and g.counters()["n_regrids"] == want["regrids"]
+    for k in ("n_leaves", "sha256_keys", "sha256_prim"):
+        assert rec[k] == want[k], (k, rec, want)
+    b.close()
+    g.close()
