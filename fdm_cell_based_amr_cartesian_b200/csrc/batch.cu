@@ -705,6 +705,14 @@ int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done) {
         if (rc) { b->err = "member: " + h->err; return rc; }
     }
     for (; k < nsteps; ++k) {
+        // a member regridded in the last iteration takes lambda over its new
+        // leaves, as the step control of fdm_solute_step does (enqueued on
+        // the member's stream, which the join below orders before the step)
+        for (fdm_handle *h : b->mem) {
+            rc = member_ready(h);
+            if (rc) { b->err = "member: " + h->err; break; }
+        }
+        if (rc) break;
         // scalars before the step: finished members and regrids due after it
         rc = join_members(b);
         if (rc) break;
