@@ -19,6 +19,15 @@ BufferLayerLVL of src/MAIN.F90:42-45) to the initial mesh, and
 writes the reference's diagnostic files there (Residual.dat every 100 steps
 and at t_end, accuracy_error.dat at t_end; src/solution.F90:217-234).
 
+    --strips N
+
+runs the configuration as N strips of background rows with the halo
+exchange after every stage (all on this GPU); under torchrun (WORLD_SIZE > 1)
+one strip per rank over NCCL, rank 0 holding the whole-mesh regrid host:
+
+    python -m torch.distributed.run --nproc-per-node 4 --master-addr 127.0.0.1 \
+        -m fdm_cell_based_amr_cartesian_b200 --case riemann4 --base 128 --lvl-amr 4 --strips 4
+
     --case ensemble --members 64 [--bps 0|1|2]
 
 runs the ensemble configuration (random four-quadrant members, seeds from
@@ -30,6 +39,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import sys
 import time
 
@@ -55,6 +65,59 @@ def config(args) -> P.Config:
         lvl, x1, x2, y1, y2, buf = block
         P.with_block(cfg, int(lvl), (float(x1), float(x2), float(y1), float(y2)), int(buf))
     return cfg
+
+
+def run_strips(args, cfg) -> int:
+    """The configuration on strips of one mesh (strips.StripRun): all in this
+    process, or one per rank of a torchrun world (NCCL)."""
+    import datetime
+
+    import torch
+
+    from . import strips as SP
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    nstrips = args.strips if world == 1 else world
+    if world > 1:
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    # creat_mesh + initial with the ghost fill of the whole mesh, on rank 0
+    box = [None]
+    if rank == 0:
+        g0 = Solver(cfg)
+        g0.creat_mesh_and_initial()
+        box = [g0.leaves()]
+        g0.close()
+    if world > 1:
+        torch.distributed.broadcast_object_list(box, src=0)
+    keys, prim = box[0]
+    run = SP.StripRun(cfg, keys, prim, nstrips,
+                      lambda plan, s, v: SP.GpuStrip(plan, s, v, asynchronous=True),
+                      lambda k, v: SP.GpuRegridHost(cfg, k, v),
+                      rank=None if world == 1 else rank, device=dev)
+    t0 = time.perf_counter()
+    target = args.steps if args.steps > 0 else None
+    n = 0
+    while (target is None or n < target) and run.tt < cfg.params.t_end:
+        k = run.solute(min(100, target - n) if target is not None else 100)
+        n += k
+        if k == 0:
+            break
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    whole = run.gather()
+    if rank == 0:
+        print(json.dumps({"case": args.case, "strips": nstrips, "ranks": world, "steps": n,
+                          "seconds": seconds, "tt": run.tt, "regrids": run.regrids,
+                          "leaves": int(len(whole[0]))}))
+    run.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
 
 
 def run_ensemble(args) -> int:
@@ -103,6 +166,8 @@ def main(argv=None) -> int:
     ap.add_argument("--case", default="riemann4",
                     choices=["riemann4", "vortex", "double_mach", "reference", "ensemble"])
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--case ensemble)")
+    ap.add_argument("--strips", type=int, default=0,
+                    help="run as this many strips with halo exchange (one per rank under torchrun)")
     ap.add_argument("--bps", type=int, default=0,
                     help="ensemble: 1 or 2 blocks per SM of the persistent kernel, 0 the members' own graphs")
     ap.add_argument("--base", type=int, default=128, help="background cells (per side; rows for double_mach)")
@@ -118,6 +183,8 @@ def main(argv=None) -> int:
         return run_ensemble(args)
 
     cfg = config(args)
+    if args.strips > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        return run_strips(args, cfg)
     g = Solver(cfg)
     g.creat_mesh_and_initial()
     if args.gate:

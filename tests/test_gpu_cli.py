@@ -37,3 +37,14 @@ def test_cli_ensemble_run(capsys):
     out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert out["members"] == 4 and out["steps"] == 20
     assert out["regrids"] >= 4 * 2 and 0 < out["tt_min"] <= out["tt_max"]
+
+
+def test_cli_strips_run_matches_the_whole_run(capsys):
+    args = ["--case", "riemann4", "--base", "32", "--lvl-amr", "2", "--steps", "25"]
+    assert main(args) == 0
+    whole = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert main(args + ["--strips", "3"]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["strips"] == 3 and out["steps"] == 25
+    assert out["tt"] == whole["tt"] and out["regrids"] == whole["counters"]["n_regrids"] == 3
+    assert out["leaves"] == whole["counters"]["n_leaves"]
