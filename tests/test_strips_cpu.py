@@ -179,6 +179,7 @@ def oracle_start(oracle_mod, cfg):
 @pytest.mark.parametrize("make,nstrips,nsteps", [
     (lambda: P.riemann4(base=32, lvl_amr=2), 3, 25),
     (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), 2, 12),
+    (lambda: P.double_mach(base_y=16, lvl_amr=2, t_end=0.2), 3, 16),
 ])
 def test_oracle_strip_run_with_regrids(oracle_mod, make, nstrips, nsteps):
     """The time loop with AMR on: ghost refresh after every step, regrids on
