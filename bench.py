@@ -641,9 +641,11 @@ def run_ours(args):
     if not args.no_learned:
         gated = learned_window(args, cfg, keys, prim, NI, flush, world)
 
-    # one mesh as 4 strips with the halo exchange (all on this GPU)
+    # one mesh as 4 strips with the halo exchange (all on this GPU); this leg
+    # and the full runs below are single-GPU figures, taken at N = 1 only
+    # (every rank would repeat the same work)
     strips = None
-    if not args.no_strips:
+    if not args.no_strips and world == 1:
         try:
             strips = strips_window(keys, prim, asynchronous=True)
             strips["synchronous"] = strips_window(keys, prim, asynchronous=False)
@@ -659,7 +661,7 @@ def run_ours(args):
     # device regrid every 10 steps (time to solution, all regrids included),
     # plain and learned-gated, and the gated run's density error at t = 0.3
     full = None
-    if not args.no_full_run:
+    if not args.no_full_run and world == 1:
         from fdm_cell_based_amr_cartesian_b200 import learned as LG
         full, leaves_plain = full_run(S, gate=False)
         cfg_full = P.riemann4(base=128, lvl_amr=4)
