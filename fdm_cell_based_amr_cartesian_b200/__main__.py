@@ -75,6 +75,8 @@ def run_strips(args, cfg) -> int:
     import torch
 
     from . import strips as SP
+    if P.BC_PERIODIC in (cfg.params.kind_ymbc, cfg.params.kind_ypbc):
+        raise SystemExit(f"--strips: {args.case} has periodic y sides, which cannot be cut into strips")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     nstrips = args.strips if world == 1 else world

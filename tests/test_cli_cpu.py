@@ -33,3 +33,12 @@ def test_cli_block_option():
 
 def test_cli_vortex_end_time():
     assert config(_args(case="vortex", base=32, lvl_amr=2, t_end=0.5)).params.t_end == 0.5
+
+
+def test_cli_strips_refuse_periodic_y():
+    import pytest
+    from fdm_cell_based_amr_cartesian_b200.__main__ import run_strips
+    args = _args(case="vortex", base=32, lvl_amr=2)
+    args.strips = 2
+    with pytest.raises(SystemExit):
+        run_strips(args, config(args))
