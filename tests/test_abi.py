@@ -93,3 +93,24 @@ def test_initial_state_matches_oracle(oracle_mod):
         row, col = root // cfg.m, root % cfg.m
         inter = (row >= 3) & (row < cfg.n - 3) & (col >= 3) & (col < cfg.m - 3)
         assert (mine[inter] == prim[inter]).all(), cfg.name
+
+
+def test_create_validates_parameters_before_any_device_call(lib):
+    """fdm_create refuses inconsistent parameters with FDM_ERR_ARG (1) or
+    FDM_ERR_UNSUPPORTED (7) before it touches CUDA, so this runs without a
+    GPU; null arguments are refused the same way."""
+    L = S.load_library()
+
+    def create(**kw):
+        q = P.FdmParams.from_buffer_copy(P.riemann4(base=32, lvl_amr=2).params)
+        for k, v in kw.items():
+            setattr(q, k, v)
+        h = ctypes.c_void_p()
+        return L.fdm_create(ctypes.byref(q), ctypes.byref(h))
+
+    assert create(h=0.0) == 1                       # no cell size
+    assert create(m=40) == 1                        # m disagrees with the padded domain
+    assert create(lvl_amr=99) == 1                  # beyond the level tables
+    assert create(flux_variant=2) == 7              # no such flux variant
+    assert create(kind_xmbc=P.BC_EXCHANGE) == 1     # x sides are never cut
+    assert L.fdm_create(None, None) == 1
