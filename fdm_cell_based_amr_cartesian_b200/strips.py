@@ -441,6 +441,13 @@ class DistExchange:
         if ops:
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
+            # device buffers of a synchronous strip: the waits above only
+            # hold torch's current stream, and the unpack runs on the
+            # handle's own stream, so the host waits for the transfers
+            if getattr(e, "stream", None) is None and any(
+                    getattr(b, "is_cuda", False) for _, b in recvs):
+                import torch
+                torch.cuda.current_stream().synchronize()
         for name, buf in recvs:
             e.unpack(name, buf)
 
