@@ -28,6 +28,11 @@ one strip per rank over NCCL, rank 0 holding the whole-mesh regrid host:
     python -m torch.distributed.run --nproc-per-node 4 --master-addr 127.0.0.1 \
         -m fdm_cell_based_amr_cartesian_b200 --case riemann4 --base 128 --lvl-amr 4 --strips 4
 
+    --save-config FILE / --config FILE
+
+write the configuration's parameters as JSON / run from such a file
+(every fdm_params field, the initial condition, the block refinement).
+
     --case ensemble --members 64 [--bps 0|1|2]
 
 runs the ensemble configuration (random four-quadrant members, seeds from
@@ -48,6 +53,10 @@ from .solver import Solver
 
 
 def config(args) -> P.Config:
+    path = getattr(args, "config", None)
+    if path:
+        with open(path) as f:
+            return P.config_from_dict(json.load(f))
     if args.case == "riemann4":
         cfg = P.riemann4(base=args.base, lvl_amr=args.lvl_amr, t_end=args.t_end or 0.3)
     elif args.case == "vortex":
@@ -168,6 +177,8 @@ def main(argv=None) -> int:
     ap.add_argument("--case", default="riemann4",
                     choices=["riemann4", "vortex", "double_mach", "reference", "ensemble"])
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--case ensemble)")
+    ap.add_argument("--config", default=None, help="run the configuration in this JSON file")
+    ap.add_argument("--save-config", default=None, help="write the configuration as JSON and exit")
     ap.add_argument("--strips", type=int, default=0,
                     help="run as this many strips with halo exchange (one per rank under torchrun)")
     ap.add_argument("--bps", type=int, default=0,
@@ -185,6 +196,10 @@ def main(argv=None) -> int:
         return run_ensemble(args)
 
     cfg = config(args)
+    if args.save_config:
+        with open(args.save_config, "w") as f:
+            json.dump(P.config_to_dict(cfg), f, indent=1)
+        return 0
     if args.strips > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1:
         return run_strips(args, cfg)
     g = Solver(cfg)

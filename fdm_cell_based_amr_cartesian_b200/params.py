@@ -142,6 +142,48 @@ def with_block(cfg: Config, lvlblock: int, block_size, buffer_layer_lvl: int = 0
     return cfg
 
 
+def config_to_dict(cfg: Config) -> dict:
+    """A configuration as plain data (JSON): every fdm_params field, the
+    initial condition and the block refinement.  Floats keep every bit
+    (JSON writes the shortest repr that reads back to the same double)."""
+    p = cfg.params
+    params = {}
+    for name, ctype in FdmParams._fields_:
+        v = getattr(p, name)
+        if hasattr(ctype, "_length_"):
+            params[name] = [list(r) if hasattr(r, "_length_") else r for r in v]
+        else:
+            params[name] = v
+    return {"name": cfg.name, "ic_kind": int(cfg.ic_kind), "ic_params": [float(x) for x in cfg.ic_params],
+            "max_steps": int(cfg.max_steps),
+            "block": None if not cfg.block else [cfg.block[0], list(cfg.block[1]), cfg.block[2]],
+            "params": params}
+
+
+def config_from_dict(d: dict) -> Config:
+    """The inverse of config_to_dict; fields left out keep their zero."""
+    p = FdmParams()
+    for name, ctype in FdmParams._fields_:
+        if name not in d["params"]:
+            continue
+        v = d["params"][name]
+        if hasattr(ctype, "_length_"):
+            arr = getattr(p, name)
+            for i, x in enumerate(v):
+                if hasattr(arr[i], "_length_"):
+                    for j, y in enumerate(x):
+                        arr[i][j] = y
+                else:
+                    arr[i] = x
+        else:
+            setattr(p, name, v)
+    cfg = Config(d["name"], p, int(d["ic_kind"]), list(d.get("ic_params", [])), int(d.get("max_steps", 10 ** 9)))
+    if d.get("block"):
+        lvl, box, buf = d["block"]
+        cfg.block = (int(lvl), tuple(float(x) for x in box), int(buf))
+    return cfg
+
+
 def reference_default() -> Config:
     """The parameter set the reference ships (src/MAIN.F90:36-50): uniform
     h = 0.5 vortex, AMR and CFL stepping off, tstep = 1e-4, t_end = 10."""

@@ -6,7 +6,7 @@ from fdm_cell_based_amr_cartesian_b200.__main__ import config
 
 
 def _args(**kw):
-    base = dict(case="riemann4", base=128, lvl_amr=4, t_end=0.0, steps=0, gate=False, block=None)
+    base = dict(case="riemann4", base=128, lvl_amr=4, t_end=0.0, steps=0, gate=False, block=None, config=None)
     base.update(kw)
     return argparse.Namespace(**base)
 
@@ -42,3 +42,21 @@ def test_cli_strips_refuse_periodic_y():
     args.strips = 2
     with pytest.raises(SystemExit):
         run_strips(args, config(args))
+
+
+def test_configuration_files_round_trip(tmp_path):
+    """Every named configuration written as JSON and read back gives the
+    same fdm_params bytes, initial condition and block refinement."""
+    from fdm_cell_based_amr_cartesian_b200 import params as P
+    from fdm_cell_based_amr_cartesian_b200.__main__ import main
+    cfgs = [P.vortex(), P.riemann4(base=64, lvl_amr=3), P.double_mach(base_y=32, lvl_amr=3),
+            P.reference_default(), P.random_riemann4(1007, base=64),
+            P.with_block(P.vortex(), 2, (2.5, 7.5, 2.5, 7.5), 2)]
+    for c in cfgs:
+        d = P.config_from_dict(P.config_to_dict(c))
+        assert bytes(d.params) == bytes(c.params) and d.name == c.name
+        assert d.ic_kind == c.ic_kind and d.ic_params == list(c.ic_params) and d.block == c.block
+    path = str(tmp_path / "c.json")
+    assert main(["--case", "double_mach", "--base", "32", "--lvl-amr", "3", "--save-config", path]) == 0
+    c = config(_args(config=path))
+    assert bytes(c.params) == bytes(P.double_mach(base_y=32, lvl_amr=3).params)
