@@ -250,3 +250,16 @@ def test_two_gloo_ranks_strip_run_with_regrids(oracle_mod):
     ks, Us = out[0][3]
     assert out[1][3] is None
     assert np.array_equal(ks, kw) and np.array_equal(Us[:, [0, 1, 2, 4]], pw)
+
+
+def test_plan_refuses_bad_leaf_sets():
+    cfg, keys, _ = riemann_mesh()
+    with pytest.raises(ValueError):
+        SP.StripPlan(cfg, keys[::-1], 2)                       # not in key order
+    with pytest.raises(ValueError):
+        SP.StripPlan(cfg, np.concatenate([keys[:1], keys]), 2)  # a duplicate leaf
+    plan = SP.StripPlan(cfg, keys, 2)
+    with pytest.raises(ValueError):
+        SP.StripPlan(plan.config(0), keys, 2)                  # already a strip
+    one = SP.StripPlan(cfg, keys, 1)                           # one strip: the whole mesh
+    assert one.strips[0].params.window_rows == 0 and len(one.strips[0].keys) == len(keys)
