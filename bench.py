@@ -284,9 +284,17 @@ def ensemble_window(args, world):
     from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
     if not os.path.exists(LG.PARAMS_PATH):
         return {"unavailable": "no trained gate parameters"}
+    from fdm_cell_based_amr_cartesian_b200.ensemble import sum_over_ranks
     t_setup = time.perf_counter()
-    cfgs = E.ensemble_configs()
-    meshes = E.ensemble_meshes(cfgs)
+    cfgs_all = E.ensemble_configs()
+    meshes_all = E.ensemble_meshes(cfgs_all)
+    # the natural shard: whole members per rank, balanced by leaf count, no
+    # collective on the data path (every rank computes the same owner map)
+    rank = int(os.environ.get("RANK", "0"))
+    owner = E.partition([len(k) for k, _ in meshes_all], world)
+    mine = [i for i in range(len(cfgs_all)) if owner[i] == rank]
+    cfgs = [cfgs_all[i] for i in mine]
+    meshes = [meshes_all[i] for i in mine]
     sols = []
     for cfg, (k, p) in zip(cfgs, meshes):
         g = S.Solver(cfg)
@@ -294,7 +302,8 @@ def ensemble_window(args, world):
         g.body_boundary(1)
         LG.enable(g)
         sols.append(g)
-    NI = sum(g.counters()["n_interior"] for g in sols)
+    NI_rank = sum(g.counters()["n_interior"] for g in sols)
+    NI = int(sum_over_ranks(NI_rank, device="cuda"))
     batch = S.Batch(sols)
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t_setup
@@ -353,29 +362,33 @@ def ensemble_window(args, world):
     batch.close()
     for g in sols:
         g.close()
-    # accuracy of the gate: one member per level, gated against plain
+    # accuracy of the gate: one member per level, gated against plain (on
+    # rank 0; no collective inside)
     acc = {}
-    for L in (2, 3, 4, 5):
-        i = next(j for j, c in enumerate(cfgs) if int(c.params.lvl_amr) == L)
+    for L in ((2, 3, 4, 5) if rank == 0 else ()):
+        i = next(j for j, c in enumerate(cfgs_all) if int(c.params.lvl_amr) == L)
         pair = []
         for gate in (False, True):
-            g = S.Solver(cfgs[i])
-            g.upload(*meshes[i])
+            g = S.Solver(cfgs_all[i])
+            g.upload(*meshes_all[i])
             g.body_boundary(1)
             if gate:
                 LG.enable(g)
             g.advance(args.warmup + args.steps)
             pair.append(g.leaves())
             g.close()
-        l1, linf = LG.density_errors(cfgs[i], pair[0], pair[1])
+        l1, linf = LG.density_errors(cfgs_all[i], pair[0], pair[1])
         acc[f"level{L}_seed{E.ENSEMBLE_SEEDS[i]}"] = {"l1": l1, "linf": linf}
-    per = lambda ms: NI * world * args.steps / (ms / 1e3)
+    # NI counts the members of every rank: whole-job updates per second
+    per = lambda ms: NI * args.steps / (ms / 1e3)
     return {"workload": f"64 random four-quadrant problems (seeds 1000-1063, rho,p~U[0.1,2], u,v~U[-1,1]), "
                         f"base {E.ENSEMBLE_BASE}^2, max level U{{2..5}}, band-refined meshes, learned gate on",
             "blocks_per_sm_ms_per_step": tune,
             "strategy": ("member step graphs on their own streams" if best_bps == 0
                          else f"persistent kernel, {best_bps} block(s) per SM"),
-            "members": len(cfgs), "interior_leaves": int(NI), "value": per(ms_gated), "unit": UNIT,
+            "members": len(cfgs_all), "members_on_rank0": len(cfgs) if rank == 0 else None,
+            "sharding": f"whole members per rank, balanced by leaf count over {world} rank(s)",
+            "interior_leaves": int(NI), "value": per(ms_gated), "unit": UNIT,
             "ms_per_step": ms_gated / args.steps, "gated_face_fraction": gated / max(total, 1),
             "plain_batched": {"value": per(ms_plain), "ms_per_step": ms_plain / args.steps},
             "single_mesh_graphs": {"value": per(ms_single), "ms_per_step": ms_single / args.steps,
@@ -426,6 +439,52 @@ def strips_window(keys, prim, nstrips=4, steps=3, asynchronous=False):
             "note": "all strips on one GPU (synchronous: every split-API call waits; asynchronous: each strip "
                     "on its own stream, ordered by events, one host wait per strip at step control and step "
                     "end): the cost of the protocol, not a multi-GPU scaling figure; host-timed"}
+
+
+def strips_window_dist(keys, prim, rank, world, steps=5):
+    """One mesh split over the ranks: strip r of the benchmark mesh on rank r,
+    the halo exchange after every stage over NCCL (paired send/recv between
+    neighbouring ranks) and one all-reduce(max) of the wave speeds per step.
+    Device-timed (CUDA events on each strip's stream, max over ranks); rank 0
+    gathers the strips and checks them bit for bit against the whole mesh."""
+    import torch
+    import torch.distributed as dist
+    from fdm_cell_based_amr_cartesian_b200 import solver as S
+    from fdm_cell_based_amr_cartesian_b200 import strips as SP
+    from fdm_cell_based_amr_cartesian_b200.ensemble import max_over_ranks
+    cfg = P.riemann4(base=128, lvl_amr=4)
+    cfg.params.iflag_amr = 0
+    t_end = cfg.params.t_end
+    dev = torch.device("cuda", torch.cuda.current_device())
+    plan = SP.StripPlan(cfg, keys, world)
+    eng = SP.GpuStrip(plan, rank, prim, asynchronous=True)
+    xchg = SP.DistExchange(eng, rank, world, dev)
+    tt, it, _ = SP.run([eng], xchg, 1, t_end)          # warm-up step
+    torch.cuda.synchronize()
+    dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(eng.stream)
+    tt, it, k = SP.run([eng], xchg, steps, t_end, tt, it)
+    b.record(eng.stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b), device=dev)
+    got = [None] * world if rank == 0 else None
+    dist.gather_object(eng.leaves(), got, dst=0)
+    eng.close()
+    out = {"strips": world, "ranks": world, "rows": [list(st.own) for st in plan.strips], "steps": k,
+           "ms_per_step": ms / k, "transport": "NCCL send/recv of the halo rows, all-reduce(max) per step"}
+    if rank == 0:
+        ks, ps = plan.gather(got)
+        whole = S.Solver(cfg)
+        whole.upload(keys, prim)
+        for _ in range(1 + steps):
+            whole.solute_step()
+        kw, pw = whole.leaves()
+        ni = whole.counters()["n_interior"]
+        whole.close()
+        out.update({"value": ni * k / (ms / 1e3), "unit": UNIT,
+                    "bit_identical_to_whole_mesh": bool(np.array_equal(ks, kw) and np.array_equal(ps, pw))})
+    return out
 
 
 GOLDEN_RUNS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "oracle_runs.json")
@@ -532,6 +591,47 @@ def full_run_batched(S, case="double_mach"):
            "bit_identical_to_oracle_run": matches_golden(golden, keys, prim, steps, cf["n_regrids"])}
     b.close()
     gf.close()
+    return out
+
+
+def summary(line):
+    """The key figures of the legs in a few short fields (the end of the line)."""
+    def get(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    def r3(x):
+        return None if x is None else float(f"{x:.4g}")
+    plain_ms = line["ms_per_step"]
+    out = {"plain_ms_per_step": r3(plain_ms), "face_pair_ms": r3(get(line, "roofline", "ms_per_launch")),
+           "fp64_frac": r3(get(line, "roofline_fp64", "frac")), "hbm_frac_faces": r3(get(line, "roofline", "frac"))}
+    g = line.get("learned") or {}
+    if "ms_per_step" in g:
+        out["gated_ms_per_step"] = r3(g["ms_per_step"])
+        out["gated_speedup"] = r3(plain_ms / g["ms_per_step"])
+        out["gated_l1_window"] = r3(g.get("l1_density_vs_plain"))
+    e = line.get("ensemble") or {}
+    if "ms_per_step" in e:
+        out["ensemble_gated_ms"] = r3(e["ms_per_step"])
+        out["ensemble_plain_ms"] = r3(get(e, "plain_batched", "ms_per_step"))
+        out["ensemble_gated_per_s"] = r3(e.get("value"))
+        out["ensemble_strategy"] = e.get("strategy")
+    f = line.get("full_run") or {}
+    if "seconds" in f:
+        out["cfg2_full_s"] = r3(f["seconds"])
+        out["cfg2_gated_full_s"] = r3(get(f, "gated", "seconds"))
+        out["cfg2_gated_l1_shared_regrids"] = r3(get(f, "gated_shared_regrids", "l1_density_vs_plain"))
+        out["cfg2_golden"] = f.get("bit_identical_to_oracle_run")
+        out["cfg3_full_s"] = r3(get(f, "double_mach", "seconds"))
+        out["cfg3_golden"] = get(f, "double_mach", "bit_identical_to_oracle_run")
+        out["cfg3_batched_full_s"] = r3(get(f, "double_mach", "batched", "seconds"))
+    st = line.get("strips") or {}
+    if "ms_per_step" in st:
+        out["strips_ms_per_step"] = r3(st["ms_per_step"])
+        out["strips_bit_identical"] = st.get("bit_identical_to_whole_mesh")
     return out
 
 
@@ -651,6 +751,10 @@ def run_ours(args):
             strips["synchronous"] = strips_window(keys, prim, asynchronous=False)
         except Exception as ex:          # an auxiliary leg never costs the line
             strips = {"error": f"{type(ex).__name__}: {ex}"}
+    elif not args.no_strips:
+        # N > 1: one strip of the same mesh per rank (every rank runs it: its
+        # collectives are taken by all ranks in the same order)
+        strips = strips_window_dist(keys, prim, rank, world)
 
     # the batched ensemble (configuration 5)
     ens = None
@@ -669,6 +773,14 @@ def run_ours(args):
             full_g, leaves_gated = full_run(S, gate=True)
             l1, linf = LG.density_errors(cfg_full, leaves_plain, leaves_gated)
             full["gated"] = dict(full_g, l1_density_vs_plain=l1, linf_density_vs_plain=linf)
+            # the gate's own error over the whole run: the gated run takes the
+            # plain run's time steps and regrid decisions (one leaf set)
+            t0 = time.perf_counter()
+            pr = LG.compare_paired(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
+            full["gated_shared_regrids"] = {
+                "l1_density_vs_plain": pr["l1"], "linf_density_vs_plain": pr["linf"], "steps": pr["steps"],
+                "regrids": pr["regrids"], "leaves_at_end": pr["leaves"], "seconds_both_runs": time.perf_counter() - t0,
+                "note": "plain and gated in lockstep (fdm_solute_paired): same time steps, same regrid decisions"}
         # the same plain run from an initial density one ulp higher: the spread
         # that the regrid decisions alone give a whole run
         full_u, leaves_ulp = full_run(S, gate=False, ulp=True)
@@ -713,6 +825,7 @@ def run_ours(args):
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
                 "counters": cnt, "state_finite_after_timed_steps": finite, "cpu_baseline": cpu,
                 "fast_flux": fastf, "learned": gated, "ensemble": ens, "full_run": full, "strips": strips}
+        line["summary"] = summary(line)      # last key: the end of the line carries the key figures
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

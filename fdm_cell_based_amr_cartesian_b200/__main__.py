@@ -14,10 +14,12 @@ the device time of each regrid phase, summed over the run.
 adds creat_mesh's static block refinement (lvlBlock, Block_size,
 BufferLayerLVL of src/MAIN.F90:42-45) to the initial mesh, and
 
-    --output DIR
+    --output DIR [--dump-every N]
 
 writes the reference's diagnostic files there (Residual.dat every 100 steps
-and at t_end, accuracy_error.dat at t_end; src/solution.F90:217-234).
+and at t_end, accuracy_error.dat at t_end with the norms formed on the
+device; src/solution.F90:217-234) and, with --dump-every, a field dump of
+the leaves (field_<it>.npz) every N steps, read back while the run goes on.
 
     --strips N
 
@@ -50,6 +52,10 @@ import time
 
 from . import params as P
 from .solver import Solver
+
+
+# options that set the configuration itself (refused beside --config FILE)
+CONFIG_OPTIONS = ("case", "base", "lvl_amr", "t_end", "block", "members")
 
 
 def config(args) -> P.Config:
@@ -189,9 +195,18 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=0, help="steps to run (0: run to t_end)")
     ap.add_argument("--gate", action="store_true", help="learned face gate on")
     ap.add_argument("--output", default=None, help="directory for Residual.dat / accuracy_error.dat")
+    ap.add_argument("--dump-every", type=int, default=0,
+                    help="field dump (keys, rho, u, v, p as field_<it>.npz in --output) every this many steps")
     ap.add_argument("--block", nargs=6, metavar=("LVL", "X1", "X2", "Y1", "Y2", "BUF"), default=None,
                     help="static block refinement of the initial mesh (lvlBlock, Block_size, BufferLayerLVL)")
+    argv = list(sys.argv[1:] if argv is None else argv)
     args = ap.parse_args(argv)
+    if args.config:
+        # the file fixes the configuration: options that would change it are refused
+        given = [o for a in ap._actions if a.dest in CONFIG_OPTIONS for o in a.option_strings
+                 if any(t == o or t.startswith(o + "=") for t in argv)]
+        if given:
+            ap.error(f"--config FILE fixes the configuration; drop {', '.join(given)}")
     if args.case == "ensemble":
         return run_ensemble(args)
 
@@ -207,26 +222,36 @@ def main(argv=None) -> int:
     if args.gate:
         from . import learned
         learned.enable(g)
-    diag = None
+    diag = dump = None
     if args.output:
         from .output import PSTEP_RES, Output
         diag = Output(args.output)
+    if args.dump_every > 0:
+        from .output import FieldDump
+        dump = FieldDump(args.output or "Output")
+    # chunks end on multiples of Pstep_Res = 100, where output_Res writes,
+    # and of the dump interval
+    every = 100 if dump is None else min(100, args.dump_every)
     t0 = time.perf_counter()
     n = 0
     target = args.steps if args.steps > 0 else None
     while (target is None or n < target) and g.scalars()["tt"] < cfg.params.t_end:
-        # chunks end on multiples of Pstep_Res = 100, where output_Res writes
-        k = g.solute(min(100, target - n) if target is not None else 100)
+        it0 = g.scalars()["it"]
+        k = g.solute(min(every - it0 % every, target - n) if target is not None else every - it0 % every)
         n += k
         sc = g.scalars()
         if diag is not None and (sc["it"] % PSTEP_RES == 0 or sc["tt"] == cfg.params.t_end):
             print(diag.res(g), file=sys.stderr)
+        if dump is not None and sc["it"] % args.dump_every == 0:
+            dump.dump(g)
         if k == 0:
             break
     tt = g.scalars()["tt"]   # waits for the device
     seconds = time.perf_counter() - t0
     if diag is not None and tt == cfg.params.t_end:
         diag.error(g)
+    if dump is not None:
+        dump.close()
     out = {"case": args.case, "steps": n, "seconds": seconds, "tt": tt,
            "counters": g.counters(), "regrid_device_ms_total": g.amr_phase_ms(total=True)}
     g.close()

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfdm.so")
 SOURCES = ["build.cu", "stage.cu", "amr.cu", "libfdm.cu", "timing.cu", "static_uniform.cu", "gate.cu", "batch.cu",
-           "fast_flux.cu"]
+           "fast_flux.cu", "diag.cu"]
 # fast_flux.cu is the one file built with FMA contraction (flux_variant 1)
 FMAD_TRUE = {"fast_flux.cu"}
 

@@ -106,9 +106,10 @@ static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3
     double2 *sq = cv.at<double2>(h->tmp[0], 4);
     k_rot_div<<<nblk(NI, 256), 256, 0, h->s>>>(h->tables(), h->lt, h->B[0].as<double4>(), rot, div, k0, i0);
     size_t bytes = 0;
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0, k1, i0, i1, (int)NI, 0, 64, h->s));
+    const int kb = 30 + root_bits(h);   // dfs keys: root << 30 | path
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0, k1, i0, i1, (int)NI, 0, kb, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, k0, k1, i0, i1, (int)NI, 0, 64, h->s));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, k0, k1, i0, i1, (int)NI, 0, kb, h->s));
     k_ordered_squares<<<nblk(NI, 256), 256, 0, h->s>>>(NI, i1, rot, div, sq);
     k_ordered_sums<<<1, 32, 0, h->s>>>(NI, sq, out3);
     return FDM_OK;
@@ -346,9 +347,10 @@ static int sort_into(fdm_handle *h, int64_t n, const uint64_t *keys, const uint8
     int32_t *iota = h->amr[6].as<int32_t>(), *perm = h->amr[7].as<int32_t>();
     k_iota<<<nblk(n, TB), TB, 0, h->s>>>(n, iota);
     size_t bytes = 0;
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, out.key, iota, perm, (int)n, 0, 64, h->s));
+    const int kb = 34 + root_bits(h);   // node keys
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, out.key, iota, perm, (int)n, 0, kb, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys, out.key, iota, perm, (int)n, 0, 64, h->s));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys, out.key, iota, perm, (int)n, 0, kb, h->s));
     k_gather_nodes<<<nblk(n, TB), TB, 0, h->s>>>(n, perm, leaf, val, out.leaf, out.val);
     out.n = n;
     return FDM_OK;
@@ -395,9 +397,10 @@ int init_internal(fdm_handle *h) {
     uint64_t *anc = h->amr[9].as<uint64_t>(), *srt = anc + na;
     k_anc_emit<<<nblk(NL, TB), TB, 0, h->s>>>(NL, h->lkey.as<uint64_t>(), off, anc);
     size_t bytes = 0;
-    FDM_CK(h, cub::DeviceRadixSort::SortKeys(nullptr, bytes, anc, srt, (int)na, 0, 64, h->s));
+    const int kb = 34 + root_bits(h);   // ancestor node keys
+    FDM_CK(h, cub::DeviceRadixSort::SortKeys(nullptr, bytes, anc, srt, (int)na, 0, kb, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortKeys(h->cub_tmp.p, bytes, anc, srt, (int)na, 0, 64, h->s));
+    FDM_CK(h, cub::DeviceRadixSort::SortKeys(h->cub_tmp.p, bytes, anc, srt, (int)na, 0, kb, h->s));
     FDM_CK(h, h->ikey.ensure(na * 8));
     FDM_CK(h, h->amr[10].ensure(16));
     int64_t *nsel = h->amr[10].as<int64_t>();
@@ -1497,9 +1500,10 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     int32_t *cnt = cv.at<int32_t>(b, 13), *off = cv.at<int32_t>(b, 14);
     k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L, pk, pi);
     size_t bytes = 0;
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, pk, pk2, pi, pi2, (int)n, 0, 64, h->s));
+    const int kb = 45 + root_bits(h);   // post-order ranks: root << 45 | 3 bits per level
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, pk, pk2, pi, pi2, (int)n, 0, kb, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, pk, pk2, pi, pi2, (int)n, 0, 64, h->s));
+    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, pk, pk2, pi, pi2, (int)n, 0, kb, h->s));
     k_scatter_rank<<<nblk(n, TB), TB, 0, h->s>>>(n, pi2, L.rank);
     FDM_CK(h, cudaMemsetAsync(d0, 0, n, h->s));
     int8_t *cur = d0, *nxt = d1;
@@ -1637,7 +1641,42 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
 
 // AMR (src/solution.F90:408-421) after the trigger test: indicators,
 // refine/coarsen, lvlAMR rounds of gridmodify1 + gridmodify4, new tables.
-int run_amr(fdm_handle *h) {
+static int run_amr_impl(fdm_handle *h, fdm_handle *lead);
+
+// A regrid that fails part way (an allocation, a CUDA call) leaves the node
+// set and the tables out of step: the handle then counts as not loaded, so
+// every stage call returns FDM_ERR_STATE until the next upload.  With a
+// leader (lead != nullptr), the refine/coarsen decisions come from the
+// leader's indicators on the leader's state; both must hold the same leaf
+// set, which is checked on the device.
+int run_amr(fdm_handle *h, fdm_handle *lead) {
+    const int rc = run_amr_impl(h, lead);
+    if (rc && rc != FDM_ERR_UNSUPPORTED && rc != FDM_ERR_ARG) h->loaded = false;
+    return rc;
+}
+
+__global__ void k_keys_differ(int64_t n, const uint64_t *__restrict__ a, const uint64_t *__restrict__ b,
+                              int32_t *flag) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n && a[i] != b[i]) *flag = 1;
+}
+
+// the same leaf set (keys in the same order) in both handles
+static int same_leaves(fdm_handle *h, fdm_handle *lead, bool *same) {
+    *same = false;
+    if (h->NL != lead->NL || h->NI != lead->NI || h->NInt != lead->NInt) return FDM_OK;
+    FDM_CK(h, cudaStreamSynchronize(lead->s));
+    int32_t *flag = h->flag.as<int32_t>() + 7;
+    FDM_CK(h, cudaMemsetAsync(flag, 0, 4, h->s));
+    k_keys_differ<<<nblk(h->NL, 256), 256, 0, h->s>>>(h->NL, h->lkey.as<uint64_t>(), lead->lkey.as<uint64_t>(), flag);
+    int32_t f = 1;
+    FDM_CK(h, cudaMemcpyAsync(&f, flag, 4, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    *same = f == 0;
+    return FDM_OK;
+}
+
+static int run_amr_impl(fdm_handle *h, fdm_handle *lead) {
     Nvtx range("fdm regrid");
     const int TB = 256;
     const int64_t NL = h->NL, NI = h->NI, NInt = h->NInt;
@@ -1658,7 +1697,19 @@ int run_amr(fdm_handle *h) {
     FDM_CK(h, h->amr[18].ensure(ci.total));
     double *rot = ci.at<double>(h->amr[18], 0), *div = ci.at<double>(h->amr[18], 1), *sums = ci.at<double>(h->amr[18], 2);
     int8_t *rflag = ci.at<int8_t>(h->amr[18], 3), *cflag = ci.at<int8_t>(h->amr[18], 4);
-    AMR_RC(compute_rot_div(h, rot, div, sums));
+    if (lead) {
+        bool same = false;
+        AMR_RC(same_leaves(h, lead, &same));
+        if (!same) {
+            h->err = "the leader's leaf set differs from this handle's";
+            return FDM_ERR_ARG;
+        }
+        const int rc = compute_rot_div(lead, rot, div, sums);
+        if (rc) { h->err = "leader's indicators: " + lead->err; return rc; }
+        FDM_CK(h, cudaStreamSynchronize(lead->s));
+    } else {
+        AMR_RC(compute_rot_div(h, rot, div, sums));
+    }
     FDM_CK(h, cudaEventRecord(h->amr_ev[1], h->s));
     // 2. solute_ref: refine and coarsen flags, applied at once
     const Tables T = h->tables();
@@ -1715,7 +1766,7 @@ int run_amr(fdm_handle *h) {
     FDM_CK(h, cudaEventRecord(h->amr_ev[4], h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     h->NInt = nint;
-    const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>());
+    const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>(), 34 + root_bits(h));
     if (rc) return rc;
     FDM_CK(h, cudaEventRecord(h->amr_ev[5], h->s));
     FDM_CK(h, cudaEventSynchronize(h->amr_ev[5]));

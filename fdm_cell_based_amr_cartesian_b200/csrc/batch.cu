@@ -13,9 +13,11 @@
 // so a member advanced in a batch matches the same handle advanced alone.
 //
 // The launch is cooperative (all blocks resident), and every wait in the
-// grid barrier has an iteration limit: a barrier that does not complete
-// sets an error word and the kernel returns, which the host reports.
+// grid barrier has a time limit, measured on the global timer: a barrier
+// that does not complete sets an error word and the kernel returns, which
+// the host reports as FDM_ERR_TIMEOUT.
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -58,6 +60,7 @@ struct GridBar {
     unsigned gen;
     int err;
     int pad;
+    unsigned long long limit_ns;   // wait limit of one barrier; 0: BAR_WAIT_NS
 };
 
 struct BatchArgs {
@@ -79,7 +82,11 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
-constexpr unsigned long long BAR_SPIN_LIMIT = 1ull << 24;   // x >= 64 ns of sleep: about a second
+// A wait gives up after BAR_WAIT_NS of global-timer time (or the batch's
+// own limit), whatever the load on the GPU; the poll count is a second
+// bound that holds even if the timer stood still (2^31 polls of >= 64 ns).
+constexpr unsigned long long BAR_WAIT_NS = 2000000000ull;   // 2 s
+constexpr unsigned long long BAR_POLL_CAP = 1ull << 31;
 
 // Grid-wide barrier among the co-resident blocks of a cooperative launch.
 // Returns false when any block gave up waiting; the caller then returns.
@@ -95,9 +102,11 @@ __device__ bool grid_bar(GridBar *b, unsigned nblocks) {
             __threadfence();
             atomicAdd(&b->gen, 1u);
         } else {
-            unsigned long long spins = 0;
+            const unsigned long long lim = b->limit_ns ? b->limit_ns : BAR_WAIT_NS;
+            const unsigned long long t0 = gtimer();
+            unsigned long long polls = 0;
             while (*vgen == g0) {
-                if (++spins > BAR_SPIN_LIMIT || *(volatile int *)&b->err) {
+                if (*(volatile int *)&b->err || gtimer() - t0 > lim || ++polls > BAR_POLL_CAP) {
                     atomicExch(&b->err, 1);
                     break;
                 }
@@ -375,6 +384,7 @@ struct fdm_batch {
     std::vector<bool> gates;
     std::vector<float> thr;
     cudaEvent_t ev = nullptr;
+    unsigned long long wait_ns = 0;  // the grid barrier's wait limit (0: BAR_WAIT_NS)
     std::string err;
 };
 
@@ -589,7 +599,14 @@ static int check_barrier(fdm_batch *b) {
     GridBar gb;
     BCK(b, cudaMemcpyAsync(&gb, b->d_bar.p, sizeof gb, cudaMemcpyDeviceToHost, b->s));
     BCK(b, cudaStreamSynchronize(b->s));
-    if (gb.err) { b->err = "a grid barrier of the batch kernel timed out"; return FDM_ERR_CUDA; }
+    if (gb.err) {
+        // every block has left the kernel (the stream is idle): the barrier
+        // starts again from zero for the next launch, its limit kept
+        BCK(b, cudaMemsetAsync(b->d_bar.p, 0, offsetof(GridBar, limit_ns), b->s));
+        BCK(b, cudaStreamSynchronize(b->s));
+        b->err = "a grid barrier of the batch kernel gave up waiting (members' states of this step are undefined)";
+        return FDM_ERR_TIMEOUT;
+    }
     return FDM_OK;
 }
 
@@ -779,6 +796,19 @@ int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t bps) {
     int rc = batch_grid(b);
     if (rc) return rc;
     drop_batch_graph(b);
+    return FDM_OK;
+}
+
+// Wait limit of one grid barrier of the persistent kernel, in seconds
+// (default 2 s); the next launch uses it.
+int fdm_batch_set_wait_limit(fdm_batch *b, double seconds) {
+    if (!b || !(seconds > 0.0) || seconds > 3600.0) return FDM_ERR_ARG;
+    cudaSetDevice(b->device);
+    b->wait_ns = (unsigned long long)(seconds * 1e9);
+    if (b->wait_ns == 0) b->wait_ns = 1;
+    BCK(b, cudaMemcpyAsync((char *)b->d_bar.p + offsetof(GridBar, limit_ns), &b->wait_ns, sizeof b->wait_ns,
+                           cudaMemcpyHostToDevice, b->s));
+    BCK(b, cudaStreamSynchronize(b->s));
     return FDM_OK;
 }
 

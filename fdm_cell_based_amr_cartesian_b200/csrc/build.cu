@@ -647,7 +647,7 @@ static int read_back(fdm_handle *h, int32_t he[8], int64_t *tot, int nt) {
         if (rc_) return rc_;      \
     } while (0)
 
-int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double *prim_in) {
+int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double *prim_in, int key_bits) {
     Nvtx range("fdm tables");
     const int TB = 256;
     cudaStream_t s = h->s;
@@ -666,10 +666,10 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
         k_iota_b<<<nblk(n, TB), TB, 0, s>>>(n, iota);
         size_t bytes = 0;
         FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
-                                                  h->tmp[1].as<int32_t>(), (int)n, 0, 64, s));
+                                                  h->tmp[1].as<int32_t>(), (int)n, 0, key_bits, s));
         FDM_CK(h, h->cub_tmp.ensure(bytes));
         FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
-                                                  h->tmp[1].as<int32_t>(), (int)n, 0, 64, s));
+                                                  h->tmp[1].as<int32_t>(), (int)n, 0, key_bits, s));
     }
     const uint64_t *lkey = h->lkey.as<uint64_t>();
     const int32_t *perm = h->tmp[1].as<int32_t>();

@@ -1,5 +1,6 @@
 // handle.cuh — host-side state of one libfdm handle.
 #pragma once
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -21,6 +22,16 @@ struct Nvtx {
 };
 
 
+// Allocation-failure injection (fdm_debug_fail_alloc): the number of device
+// buffer allocations that still succeed before DevBuf::ensure reports
+// cudaErrorMemoryAllocation without calling cudaMalloc; negative: off.
+inline std::atomic<long long> g_alloc_budget{-1};
+inline bool alloc_refused() {
+    long long b = g_alloc_budget.load();
+    while (b > 0 && !g_alloc_budget.compare_exchange_weak(b, b - 1)) {}
+    return b == 0;
+}
+
 // Device buffer that only grows; freed with the handle.
 struct DevBuf {
     void *p = nullptr;
@@ -39,6 +50,7 @@ struct DevBuf {
         bytes = 0;
         size_t nb = nbytes ? nbytes : 16;
         if (nbytes > 0) nb += nbytes / 4 + (1u << 20);
+        if (alloc_refused()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, nb);
         if (e != cudaSuccess && nb > nbytes) {   // no room for headroom
             cudaGetLastError();
@@ -122,6 +134,8 @@ struct fdm_handle {
 
     // learned gate of the face flux
     fdm::DevBuf io;   // staging of fdm_set_values / fdm_download_leaves (grows, kept)
+    fdm::DevBuf diag; // per-leaf terms and sums of fdm_output_error
+    fdm::DevBuf key_stage[2];   // staging of fdm_download_keys_async
     // asynchronous value transfers: a copy stream each way (uploads, read-
     // backs), two staging buffers each way, and the events that order them
     // with the compute stream
@@ -191,7 +205,18 @@ inline int arg_fail(fdm_handle *h, const char *msg) {
 }
 
 // table construction (build.cu)
-int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_dev, const double *prim_dev);
+// key_bits: the low bits of the keys that the key sort orders (64 for keys
+// from a caller, root_bits(h) + 34 for keys the device made itself)
+int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_dev, const double *prim_dev, int key_bits = 64);
+// bits of the largest background-cell (root) index m*n - 1: a leaf key
+// (root << 34 | path << 4 | lvl) made on the device has no bit set at or
+// above 34 + root_bits, so radix sorts of such keys stop there
+inline int root_bits(const fdm_handle *h) {
+    const uint64_t top = (uint64_t)h->p.m * (uint64_t)h->p.n;
+    int b = 1;
+    while (b < 30 && (1ull << b) < top) ++b;
+    return b;
+}
 // per-stage pipeline (stage.cu)
 void launch_requests(fdm_handle *h, const double4 *cur);
 void launch_faces(fdm_handle *h, const double4 *cur, int krk);
@@ -218,7 +243,7 @@ void launch_faces_list_fast(fdm_handle *h, const double4 *cur, const int32_t *hx
                             const uint32_t *cnt, int lx, int ly);
 size_t gate_list_bytes(const fdm_handle *h);
 // AMR (amr.cu)
-int run_amr(fdm_handle *h);
+int run_amr(fdm_handle *h, fdm_handle *lead = nullptr);
 int init_internal(fdm_handle *h);
 
 }  // namespace fdm

@@ -135,6 +135,15 @@ static int push_scalars(fdm_handle *h) {
     return FDM_OK;
 }
 
+// the lambda maxima of a leading handle, taken before a step (paired runs)
+__global__ void k_take_lambda(const DevScalars *__restrict__ from, DevScalars *to) {
+    if (threadIdx.x || blockIdx.x) return;
+    to->lambda_x = from->lambda_x;
+    to->lambda_y = from->lambda_y;
+    to->lam_next_x = from->lam_next_x;
+    to->lam_next_y = from->lam_next_y;
+}
+
 static int ensure_lambda(fdm_handle *h) {
     if (h->lam_fresh) return FDM_OK;
     k_reset_lam<<<1, 32, 0, h->s>>>(h->scal.as<DevScalars>());
@@ -357,8 +366,9 @@ int fdm_upload_leaves(fdm_handle *h, int64_t n, const uint64_t *keys, const doub
     dp.release();
     if (rc) { h->loaded = false; return rc; }
     rc = prepare_buffers(h);
-    if (rc) return rc;
-    return init_internal(h);
+    if (!rc) rc = init_internal(h);
+    if (rc) h->loaded = false;   // tables without their buffers: upload again
+    return rc;
 }
 
 int64_t fdm_num_leaves(const fdm_handle *h) { return h && h->loaded ? h->NL : 0; }
@@ -441,6 +451,37 @@ int fdm_download_values_async(fdm_handle *h, int64_t cap, double *prim) {
     FDM_CK(h, cudaStreamWaitEvent(h->cs_out, h->out_ready[b], 0));
     FDM_CK(h, cudaMemcpyAsync(prim, h->out_stage[b].p, h->NL * 32, cudaMemcpyDeviceToHost, h->cs_out));
     FDM_CK(h, cudaEventRecord(h->out_free[b], h->cs_out));
+    return FDM_OK;
+}
+
+// the leaf keys (key order) into pinned host memory on the read-back
+// stream, after the work queued so far; complete at fdm_io_sync
+int fdm_download_keys_async(fdm_handle *h, int64_t cap, uint64_t *keys) {
+    CHECK_H(h);
+    CHECK_LOADED(h);
+    if (cap < h->NL || !keys) return arg_fail(h, "capacity below the leaf count");
+    RC(io_setup(h));
+    DevBuf &st = h->key_stage[h->out_b];
+    if (st.bytes < (size_t)h->NL * 8) {
+        FDM_CK(h, cudaStreamSynchronize(h->cs_out));   // the buffer may still be copied out
+        FDM_CK(h, st.ensure(h->NL * 8));
+    }
+    // the copy on the handle's stream keeps the keys of this point of the
+    // run even if a regrid follows before the read-back lands
+    FDM_CK(h, cudaStreamWaitEvent(h->s, h->out_free[h->out_b], 0));
+    FDM_CK(h, cudaMemcpyAsync(st.p, h->lkey.p, h->NL * 8, cudaMemcpyDeviceToDevice, h->s));
+    FDM_CK(h, cudaEventRecord(h->out_ready[h->out_b], h->s));
+    FDM_CK(h, cudaStreamWaitEvent(h->cs_out, h->out_ready[h->out_b], 0));
+    FDM_CK(h, cudaMemcpyAsync(keys, st.p, h->NL * 8, cudaMemcpyDeviceToHost, h->cs_out));
+    FDM_CK(h, cudaEventRecord(h->out_free[h->out_b], h->cs_out));
+    return FDM_OK;
+}
+
+// waits for the read-backs queued so far (the read-back stream only); the
+// one call that another host thread may make while the handle is in use
+int fdm_readback_wait(fdm_handle *h) {
+    CHECK_H(h);
+    if (h->cs_out && cudaStreamSynchronize(h->cs_out) != cudaSuccess) return FDM_ERR_CUDA;
     return FDM_OK;
 }
 
@@ -657,12 +698,84 @@ int fdm_advance(fdm_handle *h, int64_t nsteps) {
     return FDM_OK;
 }
 
+// nsteps solute iterations of two handles on the same leaf set in
+// lockstep: `follow` takes the time step and the regrid decisions of
+// `lead` (its lambda maxima before every step; at a regrid, the refine and
+// coarsen flags of lead's indicators), so the two runs keep one leaf set and
+// one time axis and differ only by their face fluxes (e.g. follow with the
+// learned gate on, lead on the exact flux).  lead advances exactly as
+// fdm_solute would advance it.
+int fdm_solute_paired(fdm_handle *lead, fdm_handle *follow, int64_t nsteps, int64_t *steps_done) {
+    Nvtx range("fdm_solute_paired");
+    CHECK_H(lead);
+    CHECK_H(follow);
+    if (lead == follow || nsteps < 0) return FDM_ERR_ARG;
+    CHECK_LOADED(lead);
+    CHECK_LOADED(follow);
+    if (lead->device != follow->device) { follow->err = "the two handles are on different devices"; return FDM_ERR_ARG; }
+    int64_t k = 0;
+    RC(sync_scalars_from_device(lead));
+    RC(sync_scalars_from_device(follow));
+    if (lead->hs->it != follow->hs->it || lead->hs->tt != follow->hs->tt || lead->NL != follow->NL) {
+        follow->err = "paired handles must start at the same iteration, time and leaf count";
+        return FDM_ERR_STATE;
+    }
+    int rc = FDM_OK;
+    while (k < nsteps && lead->hs->tt < lead->p.t_end) {
+        const bool regrid = amr_due(lead, lead->hs->it + 1);
+        RC(ensure_lambda(lead));
+        RC(ensure_lambda(follow));
+        FDM_CK(follow, cudaStreamSynchronize(lead->s));
+        k_take_lambda<<<1, 32, 0, follow->s>>>(lead->scal.as<DevScalars>(), follow->scal.as<DevScalars>());
+        cudaGraphExec_t gl = nullptr, gf = nullptr;
+        RC(step_graph(lead, &gl, lead->p.iflag_amr != 0 && !regrid));
+        RC(step_graph(follow, &gf, follow->p.iflag_amr != 0 && !regrid));
+        FDM_CK(lead, cudaGraphLaunch(gl, lead->s));
+        FDM_CK(follow, cudaGraphLaunch(gf, follow->s));
+        lead->lam_fresh = follow->lam_fresh = true;
+        RC(sync_scalars_from_device(lead));
+        RC(sync_scalars_from_device(follow));
+        ++k;
+        if (lead->hs->status == FDM_ERR_NAN || follow->hs->status == FDM_ERR_NAN) {
+            (lead->hs->status == FDM_ERR_NAN ? lead : follow)->err = "NaN in the residual RMS (the reference stops here)";
+            rc = FDM_ERR_NAN;
+            break;
+        }
+        if (follow->hs->tt != lead->hs->tt || follow->hs->it != lead->hs->it) {
+            follow->err = "the paired runs took different time steps";
+            rc = FDM_ERR_STATE;
+            break;
+        }
+        if (regrid) {
+            rc = run_amr(follow, lead);
+            if (!rc) rc = prepare_buffers(follow);
+            if (rc) break;
+            rc = fdm_amr(lead);
+            if (rc) break;
+            launch_ghosts(lead, lead->B[0].as<double4>(), 1);
+            launch_ghosts(follow, follow->B[0].as<double4>(), 1);
+            FDM_CK(lead, cudaStreamSynchronize(lead->s));
+            FDM_CK(follow, cudaStreamSynchronize(follow->s));
+        }
+    }
+    if (steps_done) *steps_done = k;
+    return rc;
+}
+
 int fdm_amr(fdm_handle *h) {
     CHECK_H(h);
     CHECK_LOADED(h);
     int rc = run_amr(h);
-    if (rc) return rc;
-    return prepare_buffers(h);
+    if (!rc) rc = prepare_buffers(h);
+    return rc;
+}
+
+// Allocation-failure injection for tests: the next `after` device buffer
+// allocations succeed, the one after fails with FDM_ERR_NOMEM (no cudaMalloc
+// is made for it) and so do all later ones; after < 0 turns it off.
+int fdm_debug_fail_alloc(int64_t after) {
+    fdm::g_alloc_budget.store(after < 0 ? -1 : (long long)after);
+    return FDM_OK;
 }
 
 int fdm_get_counters(fdm_handle *h, fdm_counters *c) {

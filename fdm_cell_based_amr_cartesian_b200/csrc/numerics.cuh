@@ -19,6 +19,23 @@ namespace fdm {
 
 struct Prim { double r, u, v, p; };
 
+// ---------------------------------------------------- division policies
+// Every division of the face flux goes through a policy object.  DivIEEE
+// divides as written (the compiler's correctly rounded division); DivNR
+// (numerics_nr.cuh) forms the same correctly rounded quotients without
+// branches.  A Den is a denominator with its reciprocal where the policy
+// uses one; gm1 = gama - 1 and d2 of WCNS_Z3 are the constant denominators.
+struct Den {
+    double b, y;
+};
+struct DivIEEE {
+    Den gm1, d2;
+    __device__ __forceinline__ explicit DivIEEE(double g) : gm1{g - 1.0, 0.0}, d2{FDM_D2_WCNS, 0.0} {}
+    __device__ __forceinline__ Den den(double b) const { return Den{b, 0.0}; }
+    __device__ __forceinline__ double q(double a, const Den &d) const { return a / d.b; }
+    __device__ __forceinline__ double q(double a, double b) const { return a / b; }
+};
+
 __device__ __forceinline__ Prim load_prim(const double4 *__restrict__ s, int64_t i) {
     const double4 q = s[i];
     return Prim{q.x, q.y, q.z, q.w};
@@ -69,50 +86,57 @@ struct Eig {
     double Ri[4][4];
 };
 
-template <int DIR>
-__device__ __forceinline__ void eigen(const double Um[4], double g, Eig &E) {
+template <int DIR, class D>
+__device__ __forceinline__ void eigen_d(const double Um[4], double g, D &dv, Eig &E) {
     const double r0 = Um[0];
-    const double u = Um[1] / Um[0];
-    const double v = Um[2] / Um[0];
-    const double p = (g - 1.0) * r0 * (Um[3] / r0 - 0.5 * (u * u + v * v));
-    const double a = sqrt(g * p / r0);
+    const Den dr = dv.den(Um[0]);
+    const double u = dv.q(Um[1], dr);
+    const double v = dv.q(Um[2], dr);
+    const double p = (g - 1.0) * r0 * (dv.q(Um[3], dr) - 0.5 * (u * u + v * v));
+    const double a = sqrt(dv.q(g * p, dr));
     const double q2 = 0.5 * (u * u + v * v);
     const double aa = a * a, a2 = 2.0 * a * a;
+    const Den daa = dv.den(aa), da2 = dv.den(a2);
     E.u = u; E.v = v; E.a = a; E.q2 = q2;
     const double c = DIR == 0 ? u : v;
-    E.H1 = a * a / (g - 1) + q2 - c * a;
-    E.H2 = a * a / (g - 1) + q2 + c * a;
+    E.H1 = dv.q(a * a, dv.gm1) + q2 - c * a;
+    E.H2 = dv.q(a * a, dv.gm1) + q2 + c * a;
     if (DIR == 0) {
-        E.Ri[0][0] = ((g - 1.0) * q2 + a * u) / a2;
-        E.Ri[1][0] = (aa - (g - 1.0) * q2) / aa;
-        E.Ri[2][0] = ((g - 1.0) * q2 - a * u) / a2;
+        E.Ri[0][0] = dv.q((g - 1.0) * q2 + a * u, da2);
+        E.Ri[1][0] = dv.q(aa - (g - 1.0) * q2, daa);
+        E.Ri[2][0] = dv.q((g - 1.0) * q2 - a * u, da2);
         E.Ri[3][0] = v;
-        E.Ri[0][1] = ((1.0 - g) * u - a) / a2;
-        E.Ri[1][1] = ((g - 1.0) * u) / aa;
-        E.Ri[2][1] = ((1.0 - g) * u + a) / a2;
+        E.Ri[0][1] = dv.q((1.0 - g) * u - a, da2);
+        E.Ri[1][1] = dv.q((g - 1.0) * u, daa);
+        E.Ri[2][1] = dv.q((1.0 - g) * u + a, da2);
         E.Ri[3][1] = 0.0;
-        E.Ri[0][2] = ((1.0 - g) * v) / a2;
-        E.Ri[1][2] = ((g - 1.0) * v) / aa;
-        E.Ri[2][2] = ((1.0 - g) * v) / a2;
+        E.Ri[0][2] = dv.q((1.0 - g) * v, da2);
+        E.Ri[1][2] = dv.q((g - 1.0) * v, daa);
+        E.Ri[2][2] = dv.q((1.0 - g) * v, da2);
         E.Ri[3][2] = -1.0;
     } else {
-        E.Ri[0][0] = ((g - 1.0) * q2 + a * v) / a2;
-        E.Ri[1][0] = (aa - (g - 1.0) * q2) / aa;
-        E.Ri[2][0] = ((g - 1.0) * q2 - a * v) / a2;
+        E.Ri[0][0] = dv.q((g - 1.0) * q2 + a * v, da2);
+        E.Ri[1][0] = dv.q(aa - (g - 1.0) * q2, daa);
+        E.Ri[2][0] = dv.q((g - 1.0) * q2 - a * v, da2);
         E.Ri[3][0] = -u;
-        E.Ri[0][1] = ((1.0 - g) * u) / a2;
-        E.Ri[1][1] = ((g - 1.0) * u) / aa;
-        E.Ri[2][1] = ((1.0 - g) * u) / a2;
+        E.Ri[0][1] = dv.q((1.0 - g) * u, da2);
+        E.Ri[1][1] = dv.q((g - 1.0) * u, daa);
+        E.Ri[2][1] = dv.q((1.0 - g) * u, da2);
         E.Ri[3][1] = 1.0;
-        E.Ri[0][2] = ((1.0 - g) * v - a) / a2;
-        E.Ri[1][2] = ((g - 1.0) * v) / aa;
-        E.Ri[2][2] = ((1.0 - g) * v + a) / a2;
+        E.Ri[0][2] = dv.q((1.0 - g) * v - a, da2);
+        E.Ri[1][2] = dv.q((g - 1.0) * v, daa);
+        E.Ri[2][2] = dv.q((1.0 - g) * v + a, da2);
         E.Ri[3][2] = 0.0;
     }
-    E.Ri[0][3] = (g - 1.0) / a2;
-    E.Ri[1][3] = (1.0 - g) / aa;
-    E.Ri[2][3] = (g - 1.0) / a2;
+    E.Ri[0][3] = dv.q(g - 1.0, da2);
+    E.Ri[1][3] = dv.q(1.0 - g, daa);
+    E.Ri[2][3] = dv.q(g - 1.0, da2);
     E.Ri[3][3] = 0.0;
+}
+template <int DIR>
+__device__ __forceinline__ void eigen(const double Um[4], double g, Eig &E) {
+    DivIEEE dv(g);
+    eigen_d<DIR>(Um, g, dv, E);
 }
 
 // w = Ri * X (one column), MATMUL order; the 4th row of Ri is sparse
@@ -142,7 +166,8 @@ __device__ __forceinline__ void back_project(const Eig &E, const double uL[4], d
 
 // Scalar body of the WCNS_Z3 loop (src/nnd_center_RK.F90:330-347) for one
 // characteristic component: third-order Z-type interpolation.
-__device__ __forceinline__ double wcns_z3(double u1, double u2, double u3) {
+template <class D>
+__device__ __forceinline__ double wcns_z3_d(double u1, double u2, double u3, D &dv) {
     const double d1 = FDM_D1_WCNS, d2 = FDM_D2_WCNS;
     double t = -u1 + u2;
     double IS1 = t * t;
@@ -151,16 +176,21 @@ __device__ __forceinline__ double wcns_z3(double u1, double u2, double u3) {
     t = u1 - 2. * u2 + u3;
     const double IS3 = t * t;
     const double p1 = u2;
-    const double p2 = ((-u1 + 6.0 * u2 + 3.0 * u3) / 8.0 - d1 * p1) / d2;
+    const double p2 = dv.q((-u1 + 6.0 * u2 + 3.0 * u3) / 8.0 - d1 * p1, dv.d2);
     IS1 = fmin(IS1, IS2a);
     const double IS2 = IS3 + u1 * u1 + u2 * u2 + u3 * u3 - u1 * u2 - u2 * u3 - u1 * u3;
     t = 10. * fabs(IS2 - 3. * IS1);
     const double tau3 = t * t;
-    const double a1 = d1 * (1.0 + tau3 / (FDM_EPS_WCNS + IS1));
-    const double a2 = d2 * (1.0 + tau3 / (FDM_EPS_WCNS + IS2));
-    const double w1 = a1 / (a1 + a2);
-    const double w2 = a2 / (a1 + a2);
+    const double a1 = d1 * (1.0 + dv.q(tau3, FDM_EPS_WCNS + IS1));
+    const double a2 = d2 * (1.0 + dv.q(tau3, FDM_EPS_WCNS + IS2));
+    const Den ds = dv.den(a1 + a2);
+    const double w1 = dv.q(a1, ds);
+    const double w2 = dv.q(a2, ds);
     return w1 * p1 + w2 * p2;
+}
+__device__ __forceinline__ double wcns_z3(double u1, double u2, double u3) {
+    DivIEEE dv(1.4);   // gm1 is not used here
+    return wcns_z3_d(u1, u2, u3, dv);
 }
 
 // the record of slot i read again through the non-coherent path, as an
@@ -175,13 +205,34 @@ __device__ __forceinline__ Prim load_prim_again(const double4 *s, int64_t i) {
     return Prim{a, b, c, d};
 }
 // the conserved state of cons_flux alone (the same operations)
-template <int DIR>
-__device__ __forceinline__ void cons_state(const Prim &q, double g, double U[4]) {
+template <int DIR, class D>
+__device__ __forceinline__ void cons_state_d(const Prim &q, D &dv, double U[4]) {
     const double ke = q.u * q.u + q.v * q.v;
     U[0] = q.r;
     U[1] = q.r * q.u;
     U[2] = q.r * q.v;
-    U[3] = q.p / (g - 1.0) + 0.5 * q.r * ke;
+    U[3] = dv.q(q.p, dv.gm1) + 0.5 * q.r * ke;
+}
+template <int DIR>
+__device__ __forceinline__ void cons_state(const Prim &q, double g, double U[4]) {
+    DivIEEE dv(g);
+    cons_state_d<DIR>(q, dv, U);
+}
+// the physical flux of cons_flux alone (the same operations)
+template <int DIR, class D>
+__device__ __forceinline__ void phys_flux_d(const Prim &q, D &dv, double F[4]) {
+    const double ke = q.u * q.u + q.v * q.v;
+    if (DIR == 0) {
+        F[0] = q.r * q.u;
+        F[1] = q.r * q.u * q.u + q.p;
+        F[2] = q.r * q.u * q.v;
+        F[3] = q.u * (dv.q(q.p, dv.gm1) + 0.5 * q.r * ke + q.p);
+    } else {
+        F[0] = q.r * q.v;
+        F[1] = q.r * q.u * q.v;
+        F[2] = q.r * q.v * q.v + q.p;
+        F[3] = q.v * (dv.q(q.p, dv.gm1) + 0.5 * q.r * ke + q.p);
+    }
 }
 // Numerical flux at the face between s1 and s2 from the 4-point stencil
 // s0..s3 (one half of LXL_X_wcns3 / LXL_Y_wcns3, src/nnd_center_RK.F90:84-106,
@@ -274,52 +325,60 @@ __device__ __forceinline__ void face_flux(const Prim &s0, const Prim &s1, const 
 }
 
 // face_flux in the split order, reading the stencil records (slots a..d of
-// cur) once for the state half and again for the flux half
-template <int DIR>
-__device__ __forceinline__ void face_flux_slots(const double4 *__restrict__ cur, int32_t ia, int32_t ib,
-                                                int32_t ic, int32_t id, double g, double lam, double out[4]) {
+// cur) once for the state half and again for the flux half; every division
+// through the policy dv
+template <int DIR, class D>
+__device__ __forceinline__ void face_flux_slots_d(const double4 *__restrict__ cur, int32_t ia, int32_t ib,
+                                                  int32_t ic, int32_t id, double g, D &dv, double lam,
+                                                  double out[4]) {
     double wL[4], wR[4];
     Eig E;
     {
         const Prim s0 = load_prim(cur, ia), s1 = load_prim(cur, ib), s2 = load_prim(cur, ic), s3 = load_prim(cur, id);
         double U0[4], U1[4], U2[4], U3[4];
-        cons_state<DIR>(s1, g, U1);
-        cons_state<DIR>(s2, g, U2);
+        cons_state_d<DIR>(s1, dv, U1);
+        cons_state_d<DIR>(s2, dv, U2);
         double Um[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
-        eigen<DIR>(Um, g, E);
-        cons_state<DIR>(s0, g, U0);
-        cons_state<DIR>(s3, g, U3);
+        eigen_d<DIR>(Um, g, dv, E);
+        cons_state_d<DIR>(s0, dv, U0);
+        cons_state_d<DIR>(s3, dv, U3);
         double w0[4], w1[4], w2[4], w3[4], uwL[4], uwR[4];
         project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
         project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            uwL[r] = wcns_z3(w0[r], w1[r], w2[r]);
-            uwR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+            uwL[r] = wcns_z3_d(w0[r], w1[r], w2[r], dv);
+            uwR[r] = wcns_z3_d(w3[r], w2[r], w1[r], dv);
         }
         back_project<DIR>(E, uwL, wL);
         back_project<DIR>(E, uwR, wR);
     }
     double F0[4], F1[4], F2[4], F3[4];
-    phys_flux<DIR>(load_prim_again(cur, ia), g, F0);
-    phys_flux<DIR>(load_prim_again(cur, ib), g, F1);
-    phys_flux<DIR>(load_prim_again(cur, ic), g, F2);
-    phys_flux<DIR>(load_prim_again(cur, id), g, F3);
+    phys_flux_d<DIR>(load_prim_again(cur, ia), dv, F0);
+    phys_flux_d<DIR>(load_prim_again(cur, ib), dv, F1);
+    phys_flux_d<DIR>(load_prim_again(cur, ic), dv, F2);
+    phys_flux_d<DIR>(load_prim_again(cur, id), dv, F3);
     double w0[4], w1[4], w2[4], w3[4], ugL[4], ugR[4];
     project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
     project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        ugL[r] = wcns_z3(w0[r], w1[r], w2[r]);
-        ugR[r] = wcns_z3(w3[r], w2[r], w1[r]);
+        ugL[r] = wcns_z3_d(w0[r], w1[r], w2[r], dv);
+        ugR[r] = wcns_z3_d(w3[r], w2[r], w1[r], dv);
     }
     double gL[4], gR[4];
     back_project<DIR>(E, ugL, gL);
     back_project<DIR>(E, ugR, gR);
 #pragma unroll
     for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
+}
+template <int DIR>
+__device__ __forceinline__ void face_flux_slots(const double4 *__restrict__ cur, int32_t ia, int32_t ib,
+                                                int32_t ic, int32_t id, double g, double lam, double out[4]) {
+    DivIEEE dv(g);
+    face_flux_slots_d<DIR>(cur, ia, ib, ic, id, g, dv, lam, out);
 }
 
 // ------------------------------------------------ face flux, 4 lanes/face

@@ -1,0 +1,97 @@
+// numerics_nr.cuh — correctly rounded FP64 division without branches, for
+// the face flux of the exact build.
+//
+// The compiler's division is correctly rounded, but each one ends in a
+// range test with a branch to a slow path, and the branches split the face
+// flux into short straight-line pieces: the scheduler cannot interleave the
+// independent reconstructions of a face across them, and the kernel waits on
+// dependent FP64 chains.  DivNR forms the same quotients, bit for bit, from
+// published methods in straight-line code:
+//
+//  - Reciprocal: the hardware approximation (PTX rcp.approx.ftz.f64) refined
+//    by two Newton-Raphson steps, e = 1 - b*y, y = y + y*e (each step squares
+//    the relative error), which leaves y within about one ulp of 1/b.
+//  - Quotient from such a y: q = a*y, then one correction q = q + (a - b*q)*y
+//    with the remainder formed by an FMA; q is then a faithful rounding of
+//    a/b (within one ulp).
+//  - Rounding decision (exact remainder test): for a faithful q the
+//    remainder r = a - b*q is exactly representable and a/b = q + r/b, so
+//    RN(a/b) is q or its neighbour towards r/b, and the neighbour is taken
+//    exactly when |r| > |b| * (half the gap to it), a comparison of exact
+//    values (the half gap is a power of two).  A quotient of two 53-bit
+//    numbers is never a midpoint of two doubles, so there are no ties.
+//  - Shared denominators: y = RN(1/b) by the same test (a = 1), then for
+//    every numerator Markstein's two corrections, q = RN(a*y),
+//    q = q + (a - b*q)*y twice: with y within half an ulp of 1/b and the
+//    first correction faithful, the second gives RN(a/b) (P. Markstein,
+//    "Computation of elementary functions on the IBM RISC System/6000
+//    processor", IBM J. Res. Dev. 34(1), 1990).
+//
+// The steps are exact only away from underflow and overflow, so every
+// operand is checked to lie in [2^-450, 2^450] (or to be zero, whose sign
+// is taken from a*y): then quotients, remainders and half gaps stay normal.
+// An operand outside clears `ok`, and the caller computes the face again
+// with the compiler's division.
+#pragma once
+#include "numerics.cuh"
+
+namespace fdm {
+
+struct DivNR {
+    Den gm1, d2;     // constant denominators, y = RN(1/b) from the host
+    bool ok = true;
+
+    __device__ __forceinline__ DivNR(Den g1, Den dd) : gm1(g1), d2(dd) {}
+
+    // |x| in [2^-450, 2^450): biased exponent in [573, 1473)
+    __device__ __forceinline__ static bool in_range(double x) {
+        const unsigned e = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
+        return e - 573u < 900u;
+    }
+    __device__ __forceinline__ static double rcp_newton(double b) {
+        double y;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+        double e = __fma_rn(-b, y, 1.0);
+        y = __fma_rn(y, e, y);
+        e = __fma_rn(-b, y, 1.0);
+        return __fma_rn(y, e, y);
+    }
+    // RN(a/b) from a faithful q (exact remainder test); a, b, q in range
+    __device__ __forceinline__ static double round_quotient(double a, double b, double q) {
+        const double r = __fma_rn(-b, q, a);                 // exact
+        const int qhi = __double2hiint(q), qlo = __double2loint(q);
+        const unsigned eq = ((unsigned)qhi >> 20) & 0x7ffu;
+        // the step moves |q| up when r/b has the sign of q
+        const bool up = ((__double2hiint(r) ^ __double2hiint(b)) >> 31) == ((unsigned)qhi >> 31);
+        const bool pow2 = ((qhi & 0x000fffff) | qlo) == 0;   // gap below |q| is half the gap above
+        const unsigned sh = (!up && pow2) ? 54u : 53u;
+        const double half_gap = __hiloint2double((int)((eq - sh) << 20), 0);
+        const bool move = fabs(r) > fabs(b) * half_gap;
+        const long long qb = __double_as_longlong(q);
+        return __longlong_as_double(qb + (move ? (up ? 1ll : -1ll) : 0ll));
+    }
+    // a denominator with its correctly rounded reciprocal
+    __device__ __forceinline__ Den den(double b) {
+        ok = ok && in_range(b);
+        const double y = rcp_newton(b);
+        return Den{b, round_quotient(1.0, b, y)};
+    }
+    // a / d.b with y = RN(1/d.b): Markstein's two corrections
+    __device__ __forceinline__ double q(double a, const Den &d) {
+        ok = ok && (a == 0.0 || in_range(a));
+        const double q0 = a * d.y;
+        const double q1 = __fma_rn(__fma_rn(-d.b, q0, a), d.y, q0);
+        const double q2 = __fma_rn(__fma_rn(-d.b, q1, a), d.y, q1);
+        return a == 0.0 ? q0 : q2;
+    }
+    // a / b, b used once
+    __device__ __forceinline__ double q(double a, double b) {
+        ok = ok && in_range(b) && (a == 0.0 || in_range(a));
+        const double y = rcp_newton(b);
+        const double q0 = a * y;
+        const double q1 = __fma_rn(__fma_rn(-b, q0, a), y, q0);   // faithful
+        return a == 0.0 ? q0 : round_quotient(a, b, q1);
+    }
+};
+
+}  // namespace fdm

@@ -14,6 +14,7 @@
 #include "handle.cuh"
 #include "items.cuh"
 #include "numerics.cuh"
+#include "numerics_nr.cuh"
 
 namespace fdm {
 
@@ -44,6 +45,27 @@ __global__ void __launch_bounds__(TB, MINB) k_faces(Tables T, const double4 *__r
     const int64_t nu = DIR == 0 ? T.nux : T.nuy;
     if (f >= T.NI + nu) return;
     face_item<DIR>(T, cur, F, DIR == 0 ? sc->lambda_x : sc->lambda_y, g, f);
+}
+
+// The same faces with every division formed by DivNR (numerics_nr.cuh):
+// identical quotients without the branches of the compiler's division, so
+// the reconstructions of a face can be interleaved.  A face with an operand
+// outside DivNR's range is computed again with the compiler's division.
+template <int DIR, int TB, int MINB>
+__global__ void __launch_bounds__(TB, MINB) k_faces_nr(Tables T, const double4 *__restrict__ cur, double4 *F,
+                                                       const DevScalars *__restrict__ sc, double g, Den gm1,
+                                                       Den d2) {
+    const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nu = DIR == 0 ? T.nux : T.nuy;
+    if (f >= T.NI + nu) return;
+    int32_t a, b, c, d;
+    face_slots<DIR>(T, f, a, b, c, d);
+    const double lam = DIR == 0 ? sc->lambda_x : sc->lambda_y;
+    double out[4];
+    DivNR dv(gm1, d2);
+    face_flux_slots_d<DIR>(cur, a, b, c, d, g, dv, lam, out);
+    if (!dv.ok) face_flux_slots<DIR>(cur, a, b, c, d, g, lam, out);
+    F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 
 // Four lanes per face (see face_flux in numerics.cuh for the per-face
@@ -212,6 +234,17 @@ static void faces_1lane(fdm_handle *h, const double4 *cur) {
     k_faces<0, TB, MINB><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, h->G.gama);
     k_faces<1, TB, MINB><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, h->G.gama);
 }
+template <int TB, int MINB>
+static void faces_nr(fdm_handle *h, const double4 *cur) {
+    const Tables T = h->tables();
+    const DevScalars *sc = h->scal.as<DevScalars>();
+    const double g = h->G.gama;
+    // constant denominators with their correctly rounded reciprocals (IEEE
+    // division on the host)
+    const Den gm1{g - 1.0, 1.0 / (g - 1.0)}, d2{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};
+    k_faces_nr<0, TB, MINB><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
+    k_faces_nr<1, TB, MINB><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
+}
 static void faces_4lane(fdm_handle *h, const double4 *cur) {
     const Tables T = h->tables();
     const DevScalars *sc = h->scal.as<DevScalars>();
@@ -228,6 +261,10 @@ const char *face_variant_name(int v) {
         case 4: return "4 threads/face, 256 threads";
         case 5: return "1 thread/face, 128 threads, >=5 blocks/SM";
         case 6: return "1 thread/face, 64 threads, >=10 blocks/SM";
+        case 7: return "1 thread/face, branch-free division, 128 threads, >=3 blocks/SM";
+        case 8: return "1 thread/face, branch-free division, 128 threads, >=4 blocks/SM";
+        case 9: return "1 thread/face, branch-free division, 256 threads, >=2 blocks/SM";
+        case 10: return "1 thread/face, branch-free division, 64 threads, >=10 blocks/SM";
         default: return "?";
     }
 }
@@ -248,6 +285,10 @@ void launch_faces(fdm_handle *h, const double4 *cur, int krk) {
         case 4: faces_4lane(h, cur); break;
         case 5: faces_1lane<128, 5>(h, cur); break;
         case 6: faces_1lane<64, 10>(h, cur); break;
+        case 7: faces_nr<128, 3>(h, cur); break;
+        case 8: faces_nr<128, 4>(h, cur); break;
+        case 9: faces_nr<256, 2>(h, cur); break;
+        case 10: faces_nr<64, 10>(h, cur); break;
         default: faces_1lane<128, 3>(h, cur); break;
     }
 }

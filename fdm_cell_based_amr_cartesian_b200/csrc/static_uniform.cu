@@ -14,7 +14,7 @@
 // handle path, same operation order), so the result equals fdm_time_advance_rk
 // on the same uniform periodic leaf set.
 #include <algorithm>
-#include <mutex>
+#include <cstdint>
 
 #include "handle.cuh"
 #include "numerics.cuh"
@@ -31,25 +31,16 @@ constexpr int64_t SCRATCH_RECORDS = 2 * GRID_CAP + 2 * FACE_CAP;
 // symbol; its device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) double4 scratch[SCRATCH_RECORDS];
 
-constexpr int MAX_DEVICES = 64;
-static double4 *scratch_ptr[MAX_DEVICES] = {nullptr};
-static std::mutex scratch_mu;
-
-// Device address of the scratch on the current device, looked up once per
-// device with that device current.
+// Device address of the scratch on the current device.  It is looked up on
+// every call, with the caller's device current: a cached address would go
+// stale when the context that loaded the module is torn down and created
+// again (cudaDeviceReset), and the lookup is a cheap runtime call.  The
+// first call on a device also loads the module there (lazy loading).
 static cudaError_t scratch_address(double4 **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(scratch_mu);
-    if (!scratch_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, scratch);
-        if (e != cudaSuccess) return e;
-        scratch_ptr[dev] = (double4 *)p;
-    }
-    *out = scratch_ptr[dev];
+    *out = (double4 *)p;
     return cudaSuccess;
 }
 
@@ -162,7 +153,7 @@ extern "C" int fdm_time_advance_rk_uniform_static(const double *prim_in, double 
                                                   double lambda_x, double lambda_y, double tstep,
                                                   void *stream) {
     using namespace fdm::uniform_static;
-    if (!prim_in || !prim_out || prim_in == (const double *)prim_out) return FDM_ERR_ARG;
+    if (!prim_in || !prim_out) return FDM_ERR_ARG;
     if (nx < 3 || ny < 3 || nx > FDM_STATIC_MAX_SIDE || ny > FDM_STATIC_MAX_SIDE ||
         (int64_t)nx * ny > FDM_STATIC_MAX_CELLS)
         return FDM_ERR_ARG;   // outside the fixed scratch: nothing was enqueued
@@ -170,6 +161,13 @@ extern "C" int fdm_time_advance_rk_uniform_static(const double *prim_in, double 
     const int64_t nface = std::max((int64_t)(nx + 1) * ny, (int64_t)nx * (ny + 1));
     if (ngrid > GRID_CAP || nface > FACE_CAP) return FDM_ERR_ARG;
     if (((uintptr_t)prim_in | (uintptr_t)prim_out) & 31) return FDM_ERR_ARG;   // 32-byte records
+    // stage 3 reads prim_in while it writes prim_out, and the corners are
+    // copied from prim_in last: the two ranges must not share a byte
+    const uintptr_t ia = (uintptr_t)prim_in, oa = (uintptr_t)prim_out, nbytes = (uintptr_t)ngrid * 32;
+    if (ia < oa + nbytes && oa < ia + nbytes) return FDM_ERR_ARG;
+    // an error left pending by earlier, unrelated work is the caller's, not
+    // this call's: refuse before enqueueing anything rather than report it
+    if (cudaPeekAtLastError() != cudaSuccess) return FDM_ERR_CUDA;
     double4 *base = nullptr;
     if (scratch_address(&base) != cudaSuccess) return FDM_ERR_CUDA;
     double4 *U1 = base, *U2 = base + GRID_CAP, *Fx = base + 2 * GRID_CAP, *Fy = Fx + FACE_CAP;

@@ -229,6 +229,33 @@ def compare(cfg: P.Config, steps: int, params=None, threshold: float = THRESHOLD
             "leaves_gated": len(gl[0])}
 
 
+def compare_paired(cfg: P.Config, steps: int | None = None, params=None, threshold: float = THRESHOLD,
+                   chunk: int = 100):
+    """The plain and the gated solver in lockstep (fdm_solute_paired): the
+    gated run takes the plain run's time steps and regrid decisions, so both
+    keep one leaf set and the density difference at the end is the gate's
+    error alone.  Runs to t_end (or `steps` iterations); returns the density
+    errors, the steps and regrids taken and the leaf count at the end."""
+    plain, gated = Solver(cfg), Solver(cfg)
+    plain.creat_mesh_and_initial()
+    gated.creat_mesh_and_initial()
+    enable(gated, params, threshold)
+    n = 0
+    while (steps is None or n < steps) and plain.scalars()["tt"] < cfg.params.t_end:
+        k = plain.solute_paired(gated, chunk if steps is None else min(chunk, steps - n))
+        n += k
+        if k == 0:
+            break
+    pl, gl = plain.leaves(), gated.leaves()
+    assert np.array_equal(pl[0], gl[0]), "paired runs ended on different leaf sets"
+    l1, linf = density_errors(cfg, pl, gl)
+    out = {"l1": l1, "linf": linf, "steps": n, "tt": plain.scalars()["tt"],
+           "regrids": plain.counters()["n_regrids"], "leaves": len(pl[0])}
+    plain.close()
+    gated.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", action="store_true")

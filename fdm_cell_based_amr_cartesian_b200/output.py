@@ -150,11 +150,74 @@ class Output:
         return con
 
     def error(self, solver) -> dict:
-        """output_error for a Solver (the vortex configurations)."""
-        keys, prim = solver.leaves()
-        e = error_norms(solver.cfg, keys, prim)
+        """output_error for a Solver (the vortex configurations): the norms
+        are formed on the device (fdm_output_error), so no leaf crosses to
+        the host."""
+        e = solver.output_error_device()
         with open(os.path.join(self.dir, "accuracy_error.dat"), "a") as f:
             for line in error_lines(solver.scalars()["it"], e, self._first_error):
                 f.write(line + "\n")
         self._first_error = False
         return e
+
+
+class FieldDump:
+    """Field dumps (no reference counterpart): the leaf keys and (rho, u, v,
+    p) of a solver written as ``field_<it>.npz`` in ``directory``.  The
+    read-back is queued on the solver's read-back stream into one of two
+    pinned host buffers and a writer thread waits for it and writes the file,
+    so the steps after a dump overlap its transfer and its file output.  A
+    buffer is reused only after its file is written."""
+
+    def __init__(self, directory: str):
+        import threading
+        self.dir = directory
+        os.makedirs(directory, exist_ok=True)
+        self._buf = [None, None]
+        self._busy = [threading.Event(), threading.Event()]
+        for e in self._busy:
+            e.set()            # set: the buffer is free
+        self._k = 0
+        self._threads = []
+        self.written = []
+
+    def _pinned(self, b, n):
+        import torch
+        cur = self._buf[b]
+        if cur is None or cur[0].shape[0] < n:
+            keys = torch.empty(n, dtype=torch.int64, pin_memory=True)
+            vals = torch.empty((n, 4), dtype=torch.float64, pin_memory=True)
+            cur = (keys, vals)
+            self._buf[b] = cur
+        return cur
+
+    def dump(self, solver):
+        """Queue a dump of the solver's current leaves; returns at once."""
+        import threading
+        b = self._k % 2
+        self._k += 1
+        self._busy[b].wait()
+        self._busy[b].clear()
+        n = solver.num_leaves()
+        kt, vt = self._pinned(b, n)
+        keys = kt.numpy()[:n].view(np.uint64)
+        vals = vt.numpy()[:n]
+        solver.download_keys_async(keys)
+        solver.download_values_async(vals)
+        it = solver.scalars()["it"]
+        path = os.path.join(self.dir, f"field_{it:08d}.npz")
+
+        def write():
+            solver.readback_wait()           # the read-back stream only
+            np.savez(path, keys=keys.copy(), prim=vals.copy())
+            self.written.append(path)
+            self._busy[b].set()
+
+        t = threading.Thread(target=write, daemon=True)
+        t.start()
+        self._threads.append(t)
+
+    def close(self):
+        for t in self._threads:
+            t.join()
+        self._threads = []

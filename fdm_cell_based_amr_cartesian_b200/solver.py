@@ -27,7 +27,7 @@ FDM_ERR_NAN = 3
 ERRORS = {1: "FDM_ERR_ARG", 2: "FDM_ERR_CUDA", 3: "FDM_ERR_NAN", 4: "FDM_ERR_TIMEOUT",
           5: "FDM_ERR_NOMEM", 6: "FDM_ERR_STATE", 7: "FDM_ERR_UNSUPPORTED"}
 
-FACE_VARIANTS = 7   # FDM_FACE_VARIANTS of include/fdm.h
+FACE_VARIANTS = 11   # FDM_FACE_VARIANTS of include/fdm.h
 
 # every extern "C" symbol declared in include/fdm.h
 EXPORTS = [
@@ -41,10 +41,12 @@ EXPORTS = [
     "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
     "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
     "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
-    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
+    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_set_wait_limit", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
     "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
     "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
     "fdm_download_internal", "fdm_set_internal", "fdm_set_async", "fdm_debug_barrier_timeout",
+    "fdm_debug_fail_alloc", "fdm_solute_paired", "fdm_output_error", "fdm_download_keys_async",
+    "fdm_readback_wait",
 ]
 
 
@@ -128,6 +130,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_batch_solute.argtypes = [vp, i64, ctypes.POINTER(i64)]
     L.fdm_batch_sync.argtypes = [vp]
     L.fdm_batch_set_blocks_per_sm.argtypes = [vp, i32]
+    L.fdm_batch_set_wait_limit.argtypes = [vp, ctypes.c_double]
     L.fdm_batch_info.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64)]
     L.fdm_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.fdm_batch_phase_us.argtypes = [vp, dp]
@@ -139,6 +142,11 @@ def load_library(path: str = LIB_PATH):
     L.fdm_step_control_global.argtypes = [vp, ctypes.c_double, ctypes.c_double, i32, dp]
     L.fdm_set_async.argtypes = [vp, i32]
     L.fdm_debug_barrier_timeout.argtypes = [dp]
+    L.fdm_debug_fail_alloc.argtypes = [i64]
+    L.fdm_solute_paired.argtypes = [vp, vp, i64, ctypes.POINTER(i64)]
+    L.fdm_output_error.argtypes = [vp, dp, ctypes.POINTER(i64)]
+    L.fdm_download_keys_async.argtypes = [vp, i64, u64p]
+    L.fdm_readback_wait.argtypes = [vp]
     _lib = L
     return L
 
@@ -299,6 +307,27 @@ class Solver:
         assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"]
         self._check(self.L.fdm_download_values_async(self.h, len(out), _dp(out)))
 
+    def download_keys_async(self, out):
+        """Asynchronous read-back of the leaf keys into pinned out (uint64)."""
+        assert out.dtype == np.uint64 and out.flags["C_CONTIGUOUS"]
+        self._check(self.L.fdm_download_keys_async(self.h, len(out), _u64p(out)))
+
+    def output_error_device(self) -> dict:
+        """output_error's density norms computed on the device (only the
+        norms cross to the host)."""
+        nm = np.zeros(9)
+        ct = (ctypes.c_int64 * 3)()
+        self._check(self.L.fdm_output_error(self.h, _dp(nm), ct))
+        return dict(n_res=int(ct[0]), L1_rho=nm[0], L2_rho=nm[1], Loo_rho=nm[2], P1_rho=nm[3], P2_rho=nm[4],
+                    Poo_rho=nm[5], n_0=int(ct[1]), n_patch=int(ct[2]), L1_rho0=nm[6], L2_rho0=nm[7],
+                    Loo_rho0=nm[8])
+
+    def readback_wait(self):
+        """Wait for the queued read-backs only (safe from another thread)."""
+        rc = self.L.fdm_readback_wait(self.h)
+        if rc:
+            raise FdmError(rc, "fdm_readback_wait failed")
+
     def io_sync(self):
         self._check(self.L.fdm_io_sync(self.h))
 
@@ -426,6 +455,20 @@ class Solver:
         self._check(self.L.fdm_solute(self.h, int(nsteps), ctypes.byref(done)))
         return done.value
 
+    def solute_paired(self, follower: "Solver", nsteps: int) -> int:
+        """nsteps iterations of this solver and ``follower`` in lockstep: the
+        follower takes this solver's time step and regrid decisions
+        (fdm_solute_paired); returns the steps taken."""
+        k = ctypes.c_int64()
+        rc = self.L.fdm_solute_paired(self.h, follower.h, int(nsteps), ctypes.byref(k))
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            self.L.fdm_last_error(follower.h, buf, 512)
+            msg = buf.value.decode(errors="replace")
+            self.L.fdm_last_error(self.h, buf, 512)
+            raise FdmError(rc, f"follower: {msg}; leader: {buf.value.decode(errors='replace')}")
+        return k.value
+
     def advance(self, nsteps: int):
         self._check(self.L.fdm_advance(self.h, int(nsteps)))
 
@@ -543,6 +586,11 @@ class Batch:
         """1 or 2 resident blocks per SM for the persistent kernel, or 0: each
         member's own step graph on its own stream."""
         self._check(self.L.fdm_batch_set_blocks_per_sm(self.b, int(k)))
+
+    def set_wait_limit(self, seconds: float):
+        """Wait limit of one grid barrier of the persistent kernel (default
+        2 s); a wait that runs past it ends the step with FDM_ERR_TIMEOUT."""
+        self._check(self.L.fdm_batch_set_wait_limit(self.b, float(seconds)))
 
     def info(self) -> dict:
         g, bps, sm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()

@@ -21,11 +21,12 @@ the strips' leaf values are gathered into it (without a table rebuild, so its
 internal nodes keep the values the whole run gives them: they change only at
 regrids), it regrids, and its new leaf set is split again (``StripRun``).
 
-Engines: ``GpuStrip`` (a libfdm strip handle) and ``OracleStrip`` (the CPU
-restatement, for tests), with the regrid hosts ``GpuRegridHost`` and
-``OracleRegridHost``.  Transports: ``LocalExchange`` (all strips in this
-process, e.g. on one GPU) and ``DistExchange`` (one strip per rank over
-torch.distributed: NCCL between GPUs, gloo on CPU).
+Engine: ``GpuStrip`` (a libfdm strip handle) with the regrid host
+``GpuRegridHost``; any object with the same methods can stand in for them
+(the tests drive the CPU restatement through this protocol).  Transports:
+``LocalExchange`` (all strips in this process, e.g. on one GPU) and
+``DistExchange`` (one strip per rank over torch.distributed: NCCL between
+GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
@@ -223,70 +224,6 @@ class GpuStrip:
         self.g.close()
 
 
-class OracleStrip:
-    """The CPU restatement holding one strip (test infrastructure)."""
-
-    width = 7   # U(1:7) per leaf
-
-    def __init__(self, plan: StripPlan, s: int, values: np.ndarray, oracle_mod, threads=1):
-        st = plan.strips[s]
-        self.strip = st
-        self.o = oracle_mod.Oracle(plan.config(s), threads=threads, initial=False)
-        set_oracle_leaves(self.o, st.keys, values[st.sel])
-        self._idx = {name: np.arange(*r, dtype=np.int64)
-                     for name, r in (("send_down", st.send_down), ("send_up", st.send_up),
-                                     ("recv_down", st.recv_down), ("recv_up", st.recv_up))}
-
-    def step_control(self):
-        self.o.step_control()
-        sc = self.o.scalars()
-        return sc["lambda_x"], sc["lambda_y"], sc["l_max"]
-
-    def step_control_global(self, lx, ly, lm):
-        return self.o.step_control_global(lx, ly, lm)
-
-    def stage(self, krk: int):
-        self.o.stage(krk)
-
-    def buffer(self, name: str):
-        return np.zeros((len(self._idx[name]), 7))
-
-    def pack(self, name: str, buf):
-        if len(self._idx[name]):
-            buf[:] = self.o.get_U(self._idx[name])
-
-    def unpack(self, name: str, buf):
-        if len(self._idx[name]):
-            self.o.set_U(self._idx[name], buf)
-
-    def end_step(self, lx, ly, tstep, tt, it):
-        self.o.set_scalars(lx, ly, tstep, tt, it)
-
-    def body_boundary(self, j: int):
-        self.o.body_boundary(j)
-
-    def leaves(self):
-        k, v, _ = self.o.leaves()
-        return k, v
-
-    def values(self):
-        return self.o.get_U(np.arange(self.o.num_leaves()))
-
-    def close(self):
-        self.o.close()
-
-
-def set_oracle_leaves(o, keys, values):
-    """Leaves into an oracle instance from (rho, u, v, p) rows, or from full
-    U(1:7) rows (which also carry T and the two unused slots)."""
-    values = np.asarray(values, np.float64)
-    if values.shape[1] == 7:
-        o.set_leaves(keys, values[:, [0, 1, 2, 4]], values[:, 3])
-        o.set_U(np.arange(len(keys)), values)
-    else:
-        o.set_leaves(keys, values)
-
-
 class GpuRegridHost:
     """The whole mesh in one libfdm handle, used only at regrids.  It holds
     the mesh from the start of the run, so its internal nodes carry the
@@ -311,27 +248,6 @@ class GpuRegridHost:
 
     def close(self):
         self.g.close()
-
-
-class OracleRegridHost:
-    """The CPU restatement's whole mesh, used only at regrids (tests)."""
-
-    def __init__(self, cfg: P.Config, keys, values, oracle_mod, threads=1):
-        self.o = oracle_mod.Oracle(cfg, threads=threads, initial=False)
-        set_oracle_leaves(self.o, keys, values)
-        self.keys = np.asarray(keys, np.uint64)
-
-    def regrid(self, keys, values, lx, ly, tstep, tt, it):
-        if not np.array_equal(keys, self.keys):
-            raise RuntimeError("the strips' leaf set differs from the regrid host's")
-        self.o.set_U(np.arange(len(keys)), values)  # leaves only
-        self.o.set_scalars(lx, ly, tstep, tt, it)
-        self.o.amr()                                # amr_core + body_boundary(1)
-        self.keys = self.o.leaves()[0]
-        return self.keys, self.o.get_U(np.arange(len(self.keys)))
-
-    def close(self):
-        self.o.close()
 
 
 # --------------------------------------------------------------- transports

@@ -222,6 +222,39 @@ int fdm_amr(fdm_handle *h);
 
 int fdm_get_counters(fdm_handle *h, fdm_counters *c);
 
+/* Diagnostics of output_error (src/output_ADT.F90:18-75) on the device:
+ * the density of every interior leaf against the isentropic vortex of
+ * strength 5 at (5, 5), summed left to right in cell_NS (key) order as the
+ * reference does.  norms[0..8] = L1_rho, L2_rho, Loo_rho over the interior
+ * leaves, P1_rho, P2_rho, Poo_rho over the refined ones (0 when there are
+ * none) and L1, L2, Loo over the level-0 ones; counts[0..2] = interior,
+ * level-0 and refined leaf counts.  Only these numbers cross to the host.
+ * The vortex density uses the device's exp and pow. */
+int fdm_output_error(fdm_handle *h, double norms[9], int64_t counts[3]);
+/* The leaf keys (key order) into pinned host memory, queued like
+ * fdm_download_values_async on the read-back stream (a field dump of keys
+ * and values overlaps the steps after it); complete at fdm_io_sync. */
+int fdm_download_keys_async(fdm_handle *h, int64_t cap, uint64_t *keys);
+/* Waits until every read-back queued so far (fdm_download_values_async,
+ * fdm_download_keys_async) has landed in host memory.  It touches only the
+ * read-back stream, so unlike every other call it may be made from another
+ * host thread while the handle is in use (a writer thread of field dumps). */
+int fdm_readback_wait(fdm_handle *h);
+
+/* Paired runs, no reference counterpart: nsteps solute iterations of two
+ * handles holding the same leaf set at the same iteration and time, in
+ * lockstep.  `follow` takes `lead`'s lambda maxima before every step (so
+ * the same time step) and, at every regrid, the refine/coarsen decisions of
+ * `lead`'s indicators on `lead`'s state (so the same new leaf set); `lead`
+ * advances exactly as fdm_solute advances it.  The two runs then differ only
+ * by how their face fluxes are computed: with the learned gate on in
+ * `follow` and off in `lead`, the difference of their states is the gate's
+ * error alone, free of the regrid decisions that any perturbation flips.
+ * Returns FDM_ERR_STATE if the handles do not start together, FDM_ERR_ARG
+ * if a regrid finds different leaf sets. */
+int fdm_solute_paired(fdm_handle *lead, fdm_handle *follow, int64_t nsteps,
+                      int64_t *steps_done);
+
 /* ----------------------------------------------- test / integration hooks */
 /* The 8 stencil values per interior leaf (Tip, Tim, Tjp, Tjm, Tipp, Timm,
  * Tjpp, Tjmm of src/XuanGua.F90:401-590) for the current values, in interior
@@ -240,10 +273,18 @@ int fdm_debug_neighbors(fdm_handle *h, int64_t cap, uint64_t *out);
 int fdm_debug_requests(fdm_handle *h, int64_t cap, int32_t *kind, uint64_t *node,
                        double *xy, int32_t *m12, uint64_t *mem);
 /* The bounded waits of the batched kernel's grid barrier: two blocks wait
- * for a third that never arrives, give up at the iteration limit and
- * return.  Returns FDM_ERR_TIMEOUT (the expected outcome) with the device
- * time of the waits in *seconds; the context stays usable. */
+ * for a third that never arrives, give up at the default wait limit (2 s of
+ * global-timer time) and return.  Returns FDM_ERR_TIMEOUT (the expected
+ * outcome) with the device time of the waits in *seconds; the context stays
+ * usable. */
 int fdm_debug_barrier_timeout(double *seconds);
+/* Host-side allocation-failure injection (no GPU fault): the next `after`
+ * device buffer allocations of the library succeed and every later one
+ * fails as if cudaMalloc had run out of memory, so the calls that need it
+ * return FDM_ERR_NOMEM; after < 0 turns the injection off.  A handle whose
+ * upload or regrid failed this way is left not loaded (FDM_ERR_STATE until
+ * the next successful upload). */
+int fdm_debug_fail_alloc(int64_t after);
 /* AMR indicators rot/div of the interior leaves (src/solution.F90:424-466). */
 int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double *div,
                       double *srot_sdiv_ne);
@@ -268,7 +309,7 @@ int fdm_fp64_peak(double *tflops);
  * FDM_FACE_VARIANTS variants on the current leaf set (ms[v] = ms per x+y
  * launch pair; ms holds FDM_FACE_VARIANTS doubles), keeps the fastest for
  * this handle and reports it in *best.  fdm_set_variant forces one. */
-#define FDM_FACE_VARIANTS 7
+#define FDM_FACE_VARIANTS 11
 int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms);
 int fdm_set_variant(fdm_handle *h, int32_t face_variant);
 
@@ -324,6 +365,11 @@ int fdm_amr_phase_ms(const fdm_handle *h, double ms[10]);
  * and before the members' own streams).  fdm_batch_solute: nsteps steps with
  * each member's regrids when due, stopping with FDM_ERR_NAN at a NaN.
  * fdm_batch_sync waits for the batch and reports a barrier that timed out.
+ * A grid-barrier wait that runs past its limit (fdm_batch_set_wait_limit,
+ * default 2 s) makes fdm_batch_solute / fdm_batch_sync return
+ * FDM_ERR_TIMEOUT (the FDM_ERR_TIMEOUT of the error contract: a device wait
+ * limit hit); the members' states of that step are then undefined and must
+ * be restored (upload) by the caller, while the batch itself stays usable.
  * Members must stay alive and must not be used from another thread while
  * the batch exists. */
 typedef struct fdm_batch fdm_batch;
@@ -340,6 +386,9 @@ int fdm_batch_sync(fdm_batch *b);
  * are the same bits either way; which is faster depends on the members'
  * sizes (measure both). */
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t blocks_per_sm);
+/* Wait limit of one grid barrier of the persistent kernel in seconds
+ * (0 < seconds <= 3600; default 2), measured on the GPU's global timer. */
+int fdm_batch_set_wait_limit(fdm_batch *b, double seconds);
 int fdm_batch_info(const fdm_batch *b, int32_t *grid, int32_t *blocks_per_sm,
                    int64_t *smem_bytes);
 int fdm_batch_stream(const fdm_batch *b, void **stream);
@@ -371,9 +420,13 @@ int fdm_batch_phase_us(fdm_batch *b, double us[48]);
  * written earlier by the same call, so nothing carries over from a previous
  * call; calls that overlap on the GPU (different streams, or different host
  * threads on one device) race on it and must be serialised by the caller.
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. */
+ * Every call looks up the array's device address (cudaGetSymbolAddress)
+ * with the caller's device current, so the address stays right after a
+ * context is torn down and created again; the first call on each device
+ * also loads the module there, so make that first call before any stream
+ * capture.  prim_in and prim_out must not overlap (FDM_ERR_ARG).  A CUDA
+ * error already pending when the call starts is returned as FDM_ERR_CUDA
+ * before anything is enqueued (it belongs to earlier work). */
 #define FDM_STATIC_MAX_SIDE  1024
 #define FDM_STATIC_MAX_CELLS 65536
 int fdm_time_advance_rk_uniform_static(const double *prim_in, double *prim_out,

@@ -60,3 +60,21 @@ def test_configuration_files_round_trip(tmp_path):
     assert main(["--case", "double_mach", "--base", "32", "--lvl-amr", "3", "--save-config", path]) == 0
     c = config(_args(config=path))
     assert bytes(c.params) == bytes(P.double_mach(base_y=32, lvl_amr=3).params)
+
+
+def test_config_file_refuses_configuration_options(tmp_path):
+    """--config FILE fixes the configuration: --case/--base/--lvl-amr/--t-end/
+    --block beside it are refused with a message, not silently ignored."""
+    import pytest
+    from fdm_cell_based_amr_cartesian_b200.__main__ import main
+    path = str(tmp_path / "c.json")
+    assert main(["--case", "vortex", "--base", "32", "--lvl-amr", "2", "--save-config", path]) == 0
+    for extra in (["--base", "64"], ["--lvl-amr=3"], ["--t-end", "0.1"], ["--case", "riemann4"],
+                  ["--block", "2", "2.5", "7.5", "2.5", "7.5", "2"]):
+        with pytest.raises(SystemExit) as ei:
+            main(["--config", path, *extra])
+        assert ei.value.code == 2
+    # the file alone, with --save-config, is accepted and round-trips
+    path2 = str(tmp_path / "d.json")
+    assert main(["--config", path, "--save-config", path2]) == 0
+    assert open(path).read() == open(path2).read()

@@ -48,3 +48,17 @@ def test_cli_strips_run_matches_the_whole_run(capsys):
     assert out["strips"] == 3 and out["steps"] == 25
     assert out["tt"] == whole["tt"] and out["regrids"] == whole["counters"]["n_regrids"] == 3
     assert out["leaves"] == whole["counters"]["n_leaves"]
+
+
+def test_cli_field_dumps(tmp_path, capsys):
+    d = str(tmp_path / "Output")
+    assert main(["--case", "vortex", "--base", "32", "--lvl-amr", "2", "--steps", "30", "--output", d,
+                 "--dump-every", "10"]) == 0
+    import os
+
+    import numpy as np
+    names = sorted(f for f in os.listdir(d) if f.startswith("field_"))
+    assert names == ["field_00000010.npz", "field_00000020.npz", "field_00000030.npz"]
+    z = np.load(os.path.join(d, names[-1]))
+    assert z["keys"].dtype == np.uint64 and z["prim"].shape == (len(z["keys"]), 4)
+    assert np.isfinite(z["prim"]).all()

@@ -69,6 +69,45 @@ def test_gated_solver_accuracy(name):
 
 
 @pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+@pytest.mark.parametrize("name", ["vortex", "riemann4", "double_mach"])
+def test_gated_whole_run_with_shared_regrids(name):
+    """Whole runs with every regrid: the gated run takes the plain run's time
+    steps and regrid decisions (fdm_solute_paired), so both end on one leaf
+    set and the area-weighted L1 density error (relative) is the gate's
+    alone: <= 1e-3 at the end of configuration 1 (200 steps), of the
+    four-quadrant problem at 64^2 / 3 levels to t = 0.3 and of the double Mach
+    reflection at 64 x 16 / 2 levels to t = 0.2."""
+    cfg = {"vortex": lambda: P.vortex(), "riemann4": lambda: P.riemann4(base=64, lvl_amr=3, t_end=0.3),
+           "double_mach": lambda: P.double_mach(base_y=16, lvl_amr=2)}[name]()
+    r = learned.compare_paired(cfg, 200 if name == "vortex" else None)
+    print(name, r)
+    assert r["regrids"] >= 10, r
+    if name != "vortex":
+        assert r["tt"] == cfg.params.t_end, r
+    assert r["l1"] <= 1e-3, r
+
+
+def test_paired_plain_runs_are_identical():
+    """Two plain solvers in lockstep: the follower takes the leader's time
+    steps and regrid decisions and, with the same flux, ends on the same bits
+    as the leader (which itself advances exactly as fdm_solute)."""
+    cfg = P.riemann4(base=32, lvl_amr=2, t_end=0.3)
+    lead, fol, solo = Solver(cfg), Solver(cfg), Solver(cfg)
+    for s in (lead, fol, solo):
+        s.creat_mesh_and_initial()
+    n = lead.solute_paired(fol, 120)
+    assert n == 120 and solo.solute(120) == 120
+    kl, pl = lead.leaves()
+    kf, pf = fol.leaves()
+    ks, ps = solo.leaves()
+    assert np.array_equal(kl, ks) and np.array_equal(pl, ps)
+    assert np.array_equal(kl, kf) and np.array_equal(pl, pf)
+    assert lead.counters()["n_regrids"] >= 10
+    for s in (lead, fol, solo):
+        s.close()
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
 def test_gated_path_is_faster_at_bounded_error():
     """What the trained network buys: on a statically refined four-quadrant
     mesh (base 64, 4 levels) the gated step is at least 1.25x faster than the

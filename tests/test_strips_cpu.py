@@ -10,6 +10,7 @@ import pytest
 
 from fdm_cell_based_amr_cartesian_b200 import params as P
 from fdm_cell_based_amr_cartesian_b200 import strips as SP
+import oracle_strips as OS
 from fdm_cell_based_amr_cartesian_b200.solver import distance_refined_keys, initial_state
 
 BAND = [0.2, 0.15]
@@ -79,7 +80,7 @@ def test_oracle_strips_equal_whole_mesh(oracle_mod, mesh, nstrips):
     nsteps = 4
     k0, v0, sc0 = whole_run(oracle_mod, cfg, keys, prim, nsteps)
     plan = SP.StripPlan(cfg, keys, nstrips)
-    engines = [SP.OracleStrip(plan, s, prim, oracle_mod) for s in range(nstrips)]
+    engines = [OS.OracleStrip(plan, s, prim, oracle_mod) for s in range(nstrips)]
     tt, it, k = SP.run(engines, SP.LocalExchange(engines), nsteps, cfg.params.t_end)
     assert k == nsteps and tt == sc0["tt"]
     kg, vg = plan.gather([e.leaves() for e in engines])
@@ -110,7 +111,7 @@ def _rank(rank, world, port, q):
     try:
         cfg, keys, prim = riemann_mesh()
         plan = SP.StripPlan(cfg, keys, world)
-        e = SP.OracleStrip(plan, rank, prim, oracle_mod)
+        e = OS.OracleStrip(plan, rank, prim, oracle_mod)
         tt, it, k = SP.run([e], SP.DistExchange(e, rank, world), 4, cfg.params.t_end)
         lk, lv = e.leaves()
         q.put((rank, tt, lk, lv))
@@ -188,8 +189,8 @@ def test_oracle_strip_run_with_regrids(oracle_mod, make, nstrips, nsteps):
     cfg = make()
     whole, keys, U = oracle_start(oracle_mod, cfg)
     run = SP.StripRun(cfg, keys, U, nstrips,
-                      lambda plan, s, v: SP.OracleStrip(plan, s, v, oracle_mod),
-                      lambda k, v: SP.OracleRegridHost(cfg, k, v, oracle_mod, threads=2))
+                      lambda plan, s, v: OS.OracleStrip(plan, s, v, oracle_mod),
+                      lambda k, v: OS.OracleRegridHost(cfg, k, v, oracle_mod, threads=2))
     for _ in range(nsteps):
         assert whole.solute_step() == 0
         run.solute_step()
@@ -217,8 +218,8 @@ def _rank_amr(rank, world, port, q):
         o, keys, U = oracle_start(oracle_mod, cfg)
         o.close()
         run = SP.StripRun(cfg, keys, U, world,
-                          lambda plan, s, v: SP.OracleStrip(plan, s, v, oracle_mod),
-                          lambda k, v: SP.OracleRegridHost(cfg, k, v, oracle_mod), rank=rank)
+                          lambda plan, s, v: OS.OracleStrip(plan, s, v, oracle_mod),
+                          lambda k, v: OS.OracleRegridHost(cfg, k, v, oracle_mod), rank=rank)
         run.solute(22)
         out = run.gather()
         q.put((rank, run.tt, run.regrids, out))

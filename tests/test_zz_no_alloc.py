@@ -63,3 +63,16 @@ def test_uniform_static_rejects_sizes_beyond_the_limit():
     # 300 x 300 exceeds FDM_STATIC_MAX_CELLS; 2 x 8 is below the minimum side
     for nx, ny in ((300, 300), (2, 8), (2000, 16)):
         assert fn(buf.data_ptr(), buf.data_ptr() + 64, nx, ny, 0.1, 1.0, 1.4, 1.0, 1.0, 0.01, None) == 1
+
+
+def test_uniform_static_rejects_overlapping_buffers():
+    L = load_library()
+    fn = L.fdm_time_advance_rk_uniform_static
+    import torch
+    nx = ny = 3
+    ngrid = (nx + 6) * (ny + 6)
+    buf = torch.zeros(2 * ngrid * 4, dtype=torch.float64, device="cuda")
+    base = buf.data_ptr()
+    # out starts inside in, and in starts inside out: nothing is enqueued
+    for a, b in ((base, base + 32 * 40), (base + 32 * 40, base), (base, base)):
+        assert fn(a, b, nx, ny, 0.1, 1.0, 1.4, 1.0, 1.0, 0.01, None) == 1
