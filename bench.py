@@ -264,10 +264,16 @@ def learned_window(args, cfg, keys, prim, NI, flush, world):
     kt = gl.time_kernels(reps=5)
     gl.close()
     ref.close()
+    # what the network buys: the plain jump rule on the same features at the
+    # same gated share of faces (host-timed windows, same mesh)
+    try:
+        rvn = LG.rule_vs_network(cfg, keys, prim, args.steps)
+    except Exception as ex:              # an auxiliary leg never costs the line
+        rvn = {"error": f"{type(ex).__name__}: {ex}"}
     return {"value": NI * world * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
             "gated_face_fraction": gated / max(total, 1), "threshold": LG.THRESHOLD,
             "l1_density_vs_plain": l1, "linf_density_vs_plain": linf,
-            "error_window_steps": args.warmup + args.steps, "kernel_ms": kt}
+            "error_window_steps": args.warmup + args.steps, "kernel_ms": kt, "rule_vs_network": rvn}
 
 
 def ensemble_window(args, world):
@@ -613,6 +619,12 @@ def summary(line):
         out["gated_ms_per_step"] = r3(g["ms_per_step"])
         out["gated_speedup"] = r3(plain_ms / g["ms_per_step"])
         out["gated_l1_window"] = r3(g.get("l1_density_vs_plain"))
+        rv = g.get("rule_vs_network") or {}
+        if "jump_rule" in rv:
+            out["net_vs_rule_l1"] = [r3(rv["network"]["l1_density_vs_plain"]),
+                                     r3(rv["jump_rule"]["l1_density_vs_plain"])]
+            out["net_vs_rule_gated"] = [r3(rv["network"]["stage1_gated_fraction"]),
+                                        r3(rv["jump_rule"]["stage1_gated_fraction"])]
     e = line.get("ensemble") or {}
     if "ms_per_step" in e:
         out["ensemble_gated_ms"] = r3(e["ms_per_step"])

@@ -35,11 +35,12 @@ one strip per rank over NCCL, rank 0 holding the whole-mesh regrid host:
 write the configuration's parameters as JSON / run from such a file
 (every fdm_params field, the initial condition, the block refinement).
 
-    --case ensemble --members 64 [--bps 0|1|2]
+    --case ensemble --members 64 [--bps 0|1|2] [--plain] [--save-leaves F.npz]
 
 runs the ensemble configuration (random four-quadrant members, seeds from
-1000, maximum level drawn from 2..5, learned gate on) as one batch to each
-member's t_end (or --steps), regrids included.  The gate itself is trained
+1000, maximum level drawn from 2..5, learned gate on unless --plain) as one
+batch to each member's t_end (or --steps), regrids included, and prints the
+per-member steps and leaf counts.  The gate itself is trained
 by ``python -m fdm_cell_based_amr_cartesian_b200.learned``.
 """
 from __future__ import annotations
@@ -139,7 +140,9 @@ def run_strips(args, cfg) -> int:
 
 def run_ensemble(args) -> int:
     """The ensemble configuration as one batch (fdm_batch_solute), each
-    member to its own t_end."""
+    member to its own t_end; learned gate on unless --plain.  Prints the
+    whole run's time and the per-member steps, leaf counts (interior leaves
+    at the start and at the end; smallest and largest member) and times."""
     from . import ensemble as E
     from . import learned
     from .solver import Batch
@@ -149,9 +152,11 @@ def run_ensemble(args) -> int:
         g = Solver(cfg)
         g.upload(k, p)
         g.body_boundary(1)
-        learned.enable(g)
+        if not args.plain:
+            learned.enable(g)
         sols.append(g)
-    leaves0 = sum(g.counters()["n_interior"] for g in sols)
+    lv0 = [g.counters()["n_interior"] for g in sols]
+    peak = list(lv0)
     batch = Batch(sols)
     batch.set_blocks_per_sm(args.bps)
     t0 = time.perf_counter()
@@ -160,17 +165,32 @@ def run_ensemble(args) -> int:
     while target is None or n < target:
         k = batch.solute(min(100, target - n) if target is not None else 100)
         n += k
+        for i, g in enumerate(sols):
+            peak[i] = max(peak[i], g.counters()["n_interior"])
         if k == 0 or all(g.scalars()["tt"] >= g.cfg.params.t_end for g in sols):
             break
     batch.sync()
     seconds = time.perf_counter() - t0
-    tts = [g.scalars()["tt"] for g in sols]
-    out = {"case": "ensemble", "members": len(sols), "steps": n, "seconds": seconds,
-           "interior_leaves_at_start": leaves0,
-           "interior_leaves_at_end": sum(g.counters()["n_interior"] for g in sols),
+    sc = [g.scalars() for g in sols]
+    lv1 = [g.counters()["n_interior"] for g in sols]
+    tts = [s["tt"] for s in sc]
+    out = {"case": "ensemble", "gate": not args.plain, "members": len(sols), "steps": n, "seconds": seconds,
+           "interior_leaves_at_start": sum(lv0), "interior_leaves_at_end": sum(lv1),
+           "member_interior_leaves_at_start": [min(lv0), max(lv0)],
+           "member_interior_leaves_peak": [min(peak), max(peak)],
+           "member_interior_leaves_at_end": [min(lv1), max(lv1)],
+           "member_steps": [min(s["it"] for s in sc), max(s["it"] for s in sc)],
+           "member_updates": int(sum(s["it"] for s in sc)),
            "regrids": sum(g.counters()["n_regrids"] for g in sols),
            "members_at_t_end": sum(1 for g, t in zip(sols, tts) if t >= g.cfg.params.t_end),
-           "tt_min": min(tts), "tt_max": max(tts), "batch": batch.info()}
+           "tt_min": min(tts), "tt_max": max(tts), "batch": batch.info(),
+           "per_member": [{"seed": 1000 + i, "lvl_amr": int(c.params.lvl_amr), "steps": s["it"], "tt": s["tt"],
+                           "interior_leaves": [a, p, b]}
+                          for i, (c, s, a, p, b) in enumerate(zip(cfgs, sc, lv0, peak, lv1))]}
+    if args.save_leaves:
+        import numpy as np
+        np.savez(args.save_leaves, **{f"m{i}_keys": g.leaves()[0] for i, g in enumerate(sols)},
+                 **{f"m{i}_prim": g.leaves()[1] for i, g in enumerate(sols)})
     batch.close()
     for g in sols:
         g.close()
@@ -194,6 +214,8 @@ def main(argv=None) -> int:
     ap.add_argument("--t-end", type=float, default=0.0, help="end time (0: the case's own)")
     ap.add_argument("--steps", type=int, default=0, help="steps to run (0: run to t_end)")
     ap.add_argument("--gate", action="store_true", help="learned face gate on")
+    ap.add_argument("--plain", action="store_true", help="ensemble: learned gate off")
+    ap.add_argument("--save-leaves", default=None, help="ensemble: write every member's final leaves (.npz)")
     ap.add_argument("--output", default=None, help="directory for Residual.dat / accuracy_error.dat")
     ap.add_argument("--dump-every", type=int, default=0,
                     help="field dump (keys, rho, u, v, p as field_<it>.npz in --output) every this many steps")

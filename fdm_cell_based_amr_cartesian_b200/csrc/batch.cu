@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "gate_items.cuh"
+#include "numerics_nr.cuh"
 
 struct fdm_batch;
 
@@ -31,6 +32,7 @@ __host__ __device__ __forceinline__ int64_t cdiv(int64_t a, int64_t b) { return 
 
 constexpr int BT = 256;        // threads per block
 constexpr int BW = BT / 32;    // warps per block
+static_assert(BT == 4 * RQ_TILE, "a request tile is one block of four threads per request");
 
 enum { PH_REQ = 0, PH_FACE, PH_HARD, PH_CELL, PH_GHOST, PH_GHOST1, N_PHASE };
 
@@ -50,9 +52,11 @@ struct Member {
     // learned gate
     int32_t gate_on;
     float logit_thr;
+    float jump_thr;
     const float *gate_P;
     GateLists GL;
     int64_t nfx, nfy;
+    Den gm1;                 // gama - 1 with its correctly rounded reciprocal (branch-free division)
 };
 
 struct GridBar {
@@ -74,7 +78,28 @@ struct BatchArgs {
     int32_t *act;                  // member not finished at the start of the step
     const int32_t *skip_j1;        // host: a regrid follows this step (no body_boundary(1) here)
     unsigned long long *stamp;     // [3][16] global-timer stamps at the phase ends of each stage
+    Den d2;                        // d2 of WCNS_Z3 with its correctly rounded reciprocal
 };
+
+// The full WCNS flux of face f of member M: in the reference's operation
+// order (NRF false), or in the split order with the branch-free division
+// (NRF true, the same bits; a face with an operand outside its range is
+// computed again with the compiler's division).
+template <int DIR, bool NRF>
+__device__ __forceinline__ void batch_face(const Member &M, const double4 *__restrict__ cur, double4 *F, double lam,
+                                           const Den &d2, int64_t f) {
+    if constexpr (NRF) {
+        int32_t a, b, c, d;
+        face_slots<DIR>(M.T, f, a, b, c, d);
+        double out[4];
+        DivNR dv(M.gm1, d2);
+        face_flux_slots_d<DIR>(cur, a, b, c, d, M.gama, dv, lam, out);
+        if (!dv.ok) face_flux_slots<DIR>(cur, a, b, c, d, M.gama, lam, out);
+        F[f] = make_double4(out[0], out[1], out[2], out[3]);
+    } else {
+        face_item<DIR, false>(M.T, cur, F, lam, M.gama, f);
+    }
+}
 
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
@@ -154,6 +179,7 @@ struct GateSmem {
     XTile xt[BW];
 };
 union BatchSmem {
+    double geo[RQ_TILE * RQ_GEO];   // geometry blocks of a request tile
     GateSmem gate;
     RestrictSmem rs[BW];
     CellsSmem cells;
@@ -195,7 +221,7 @@ __device__ __forceinline__ double4 *stage_next(const Member &M, int krk) {
 
 // One RK stage (krk) of every member; MINB resident blocks per SM (the
 // register budget follows: 128 per thread at 2, up to 255 at 1).
-template <int MINB>
+template <int MINB, bool NRF>
 __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BatchSmem &S = *reinterpret_cast<BatchSmem *>(smem_raw);
@@ -234,8 +260,13 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
         double4 *cur = const_cast<double4 *>(stage_cur(M, krk));
         const int64_t nthr = cdiv(4 * M.T.NR, BT);   // four threads per request, one per component
         if (t < nthr) {
+            // the tile's geometry blocks are contiguous: one staged copy
+            // instead of four threads re-reading 768 bytes each
+            stage_request_geometry(M.T, t * RQ_TILE, S.geo, BT);
             const int64_t q = t * BT + threadIdx.x;
-            if ((q >> 2) < M.T.NR) request_item_var(M.T, cur, q >> 2, (int)(q & 3));
+            if ((q >> 2) < M.T.NR)
+                request_item_var(M.T, cur, q >> 2, (int)(q & 3), S.geo + (threadIdx.x >> 2) * RQ_GEO);
+            __syncthreads();   // the next tile's copy overwrites S.geo
         } else {
             const int64_t r = (t - nthr) * BW + wid;
             if (r < M.T.NR) request_restrict_warp(M.T, cur, r, S.rs[wid]);
@@ -258,8 +289,8 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
         if (!M.gate_on) {
             const int64_t f = lt * BT + threadIdx.x;
             if (f < nf) {
-                if (dir == 0) face_item<0, false>(M.T, cur, M.Fx, lam, M.gama, f);
-                else face_item<1, false>(M.T, cur, M.Fy, lam, M.gama, f);
+                if (dir == 0) batch_face<0, NRF>(M, cur, M.Fx, lam, A.d2, f);
+                else batch_face<1, NRF>(M, cur, M.Fy, lam, A.d2, f);
             }
             return;
         }
@@ -275,10 +306,10 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
             }
             if (w * 32 < nf) {
                 if (dir == 0)
-                    gate_linear_chunk<0>(M.T, cur, M.Fx, S.gate.W, S.gate.xt[wid], M.logit_thr, lam, ig1, M.gama,
+                    gate_linear_chunk<0>(M.T, cur, M.Fx, S.gate.W, S.gate.xt[wid], M.logit_thr, M.jump_thr, lam, ig1, M.gama,
                                          M.GL.hx, M.GL.cnt, M.GL.jx, w);
                 else
-                    gate_linear_chunk<1>(M.T, cur, M.Fy, S.gate.W, S.gate.xt[wid], M.logit_thr, lam, ig1, M.gama,
+                    gate_linear_chunk<1>(M.T, cur, M.Fy, S.gate.W, S.gate.xt[wid], M.logit_thr, M.jump_thr, lam, ig1, M.gama,
                                          M.GL.hy, M.GL.cnt + 1, M.GL.jy, w);
             }
         } else if (w * 32 < nf) {
@@ -310,10 +341,10 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
             const int64_t tx = cdiv(M.GL.cnt[0], BT);
             if (t < tx) {
                 const int64_t i = t * BT + threadIdx.x;
-                if (i < M.GL.cnt[0]) face_item<0, false>(M.T, cur, M.Fx, M.sc->lambda_x, M.gama, M.GL.hx[i]);
+                if (i < M.GL.cnt[0]) batch_face<0, NRF>(M, cur, M.Fx, M.sc->lambda_x, A.d2, M.GL.hx[i]);
             } else {
                 const int64_t i = (t - tx) * BT + threadIdx.x;
-                if (i < M.GL.cnt[1]) face_item<1, false>(M.T, cur, M.Fy, M.sc->lambda_y, M.gama, M.GL.hy[i]);
+                if (i < M.GL.cnt[1]) batch_face<1, NRF>(M, cur, M.Fy, M.sc->lambda_y, A.d2, M.GL.hy[i]);
             }
         });
         BAR_STAMP(5);
@@ -376,13 +407,14 @@ struct fdm_batch {
     DevBuf d_mem, d_off, d_ctr, d_bar, d_act, d_skip, d_stamp;
     std::vector<int32_t> h_skip;
     int grid = 0, blocks_per_sm = 0, want_bps = 2;   // want_bps 0: the members' own step graphs
+    bool face_nr = false;                            // branch-free division in the face phases
     size_t smem = 0;
     bool any_gate = false;
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;           // off when cooperative launches cannot be captured here
     std::vector<int64_t> versions;   // member table versions the descriptors were built for
     std::vector<bool> gates;
-    std::vector<float> thr;
+    std::vector<float> thr, jthr;
     cudaEvent_t ev = nullptr;
     unsigned long long wait_ns = 0;  // the grid barrier's wait limit (0: BAR_WAIT_NS)
     std::string err;
@@ -430,9 +462,11 @@ static int batch_refresh(fdm_batch *b) {
         d.nfx = h->NI + h->nux;
         d.nfy = h->NI + h->nuy;
         d.gate_on = h->gate_on;
+        d.gm1 = Den{h->G.gama - 1.0, 1.0 / (h->G.gama - 1.0)};   // IEEE division on the host
         if (h->gate_on) {
             b->any_gate = true;
             d.logit_thr = h->gate_logit_thr;
+            d.jump_thr = h->gate_jump_thr;
             d.gate_P = h->gate_params.as<float>();
             d.GL = gate_lists(h->gate_flag.p, d.nfx, d.nfy);
         }
@@ -453,10 +487,12 @@ static int batch_refresh(fdm_batch *b) {
     b->versions.resize(n);
     b->gates.resize(n);
     b->thr.resize(n);
+    b->jthr.resize(n);
     for (int m = 0; m < n; ++m) {
         b->versions[m] = b->mem[m]->table_version;
         b->gates[m] = b->mem[m]->gate_on;
         b->thr[m] = b->mem[m]->gate_logit_thr;
+        b->jthr[m] = b->mem[m]->gate_jump_thr;
     }
     drop_batch_graph(b);
     return FDM_OK;
@@ -465,9 +501,15 @@ static int batch_refresh(fdm_batch *b) {
 static bool batch_stale(const fdm_batch *b) {
     for (size_t m = 0; m < b->mem.size(); ++m)
         if (b->versions[m] != b->mem[m]->table_version || b->gates[m] != b->mem[m]->gate_on ||
-            b->thr[m] != b->mem[m]->gate_logit_thr)
+            b->thr[m] != b->mem[m]->gate_logit_thr || b->jthr[m] != b->mem[m]->gate_jump_thr)
             return true;
     return false;
+}
+
+// the persistent kernel of the batch's launch shape and face flux
+static const void *batch_kernel(const fdm_batch *b) {
+    if (b->want_bps == 1) return b->face_nr ? (const void *)k_batch_stage<1, true> : (const void *)k_batch_stage<1, false>;
+    return b->face_nr ? (const void *)k_batch_stage<2, true> : (const void *)k_batch_stage<2, false>;
 }
 
 static int batch_grid(fdm_batch *b) {
@@ -477,13 +519,9 @@ static int batch_grid(fdm_batch *b) {
     }
     int sms = 0, bps = 0;
     BCK(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    if (b->want_bps == 1) {
-        BCK(b, cudaFuncSetAttribute(k_batch_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
-        BCK(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_stage<1>, BT, b->smem));
-    } else {
-        BCK(b, cudaFuncSetAttribute(k_batch_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
-        BCK(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_stage<2>, BT, b->smem));
-    }
+    const void *fn = batch_kernel(b);
+    BCK(b, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    BCK(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, BT, b->smem));
     if (bps <= 0) { b->err = "the batch kernel does not fit on an SM"; return FDM_ERR_UNSUPPORTED; }
     b->blocks_per_sm = std::min(bps, b->want_bps);
     b->grid = sms * b->blocks_per_sm;
@@ -502,6 +540,7 @@ static int enqueue_batch_stage(fdm_batch *b, int krk) {
     A.act = b->d_act.as<int32_t>();
     A.skip_j1 = b->d_skip.as<int32_t>();
     A.stamp = b->d_stamp.as<unsigned long long>();
+    A.d2 = Den{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};   // IEEE division on the host
     BCK(b, cudaMemsetAsync(A.ctr, 0, sizeof(unsigned long long) * N_PHASE, b->s));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)b->grid);
@@ -513,8 +552,13 @@ static int enqueue_batch_stage(fdm_batch *b, int krk) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (b->want_bps == 1) BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<1>, A, krk));
-    else BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<2>, A, krk));
+    if (b->want_bps == 1) {
+        if (b->face_nr) BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<1, true>, A, krk));
+        else BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<1, false>, A, krk));
+    } else {
+        if (b->face_nr) BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<2, true>, A, krk));
+        else BCK(b, cudaLaunchKernelEx(&cfg, k_batch_stage<2, false>, A, krk));
+    }
     return FDM_OK;
 }
 
@@ -793,6 +837,18 @@ int fdm_batch_sync(fdm_batch *b) {
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t bps) {
     if (!b || bps < 0 || bps > 2) return FDM_ERR_ARG;
     b->want_bps = bps;
+    int rc = batch_grid(b);
+    if (rc) return rc;
+    drop_batch_graph(b);
+    return FDM_OK;
+}
+
+// Face phases of the persistent kernel: the reference's operation order
+// (0) or the split order with the branch-free division (1); the same bits.
+int fdm_batch_set_face_flux(fdm_batch *b, int32_t branch_free) {
+    if (!b || branch_free < 0 || branch_free > 1) return FDM_ERR_ARG;
+    cudaSetDevice(b->device);
+    b->face_nr = branch_free != 0;
     int rc = batch_grid(b);
     if (rc) return rc;
     drop_batch_graph(b);

@@ -24,7 +24,8 @@ static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 template <int DIR>
 __global__ void __launch_bounds__(128, 4) k_gate_linear(Tables T, const double4 *__restrict__ cur, double4 *F,
                                                         const float *__restrict__ P, float logit_thr,
-                                                        const DevScalars *__restrict__ sc, double g, int32_t *hard,
+                                                        float jump_thr, const DevScalars *__restrict__ sc, double g,
+                                                        int32_t *hard,
                                                         uint32_t *count, float *jump1) {
     __shared__ GateWeights W;
     __shared__ XTile tiles[4];
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__(128, 4) k_gate_linear(Tables T, const double4 
     for (int k = GF; k < XLD; ++k) Tt.X[lane][k] = __float2bfloat16_rn(0.f);
     const int64_t nwarps = (int64_t)gridDim.x * 4;
     for (int64_t w = blockIdx.x * 4 + wid; w * 32 < nf; w += nwarps)
-        gate_linear_chunk<DIR>(T, cur, F, W, Tt, logit_thr, lam, ig1, g, hard, count, jump1, w);
+        gate_linear_chunk<DIR>(T, cur, F, W, Tt, logit_thr, jump_thr, lam, ig1, g, hard, count, jump1, w);
 }
 
 // Stages 2 and 3: the guard on the faces that were linear at stage 1.
@@ -301,8 +302,8 @@ void launch_gated_faces(fdm_handle *h, const double4 *cur, int krk) {
     if (krk == 1 || !h->gate_stage1_valid) {
         const int gx = (int)std::min<int64_t>(nblk(nfx, 128), 4 * sms), gy = (int)std::min<int64_t>(nblk(nfy, 128), 4 * sms);
         cudaMemsetAsync(cnt, 0, 2 * sizeof(uint32_t), h->s);
-        if (gx > 0) k_gate_linear<0><<<gx, 128, 0, h->s>>>(T, cur, h->Fx.as<double4>(), P, h->gate_logit_thr, sc, h->G.gama, hx, cnt, jx);
-        if (gy > 0) k_gate_linear<1><<<gy, 128, 0, h->s>>>(T, cur, h->Fy.as<double4>(), P, h->gate_logit_thr, sc, h->G.gama, hy, cnt + 1, jy);
+        if (gx > 0) k_gate_linear<0><<<gx, 128, 0, h->s>>>(T, cur, h->Fx.as<double4>(), P, h->gate_logit_thr, h->gate_jump_thr, sc, h->G.gama, hx, cnt, jx);
+        if (gy > 0) k_gate_linear<1><<<gy, 128, 0, h->s>>>(T, cur, h->Fy.as<double4>(), P, h->gate_logit_thr, h->gate_jump_thr, sc, h->G.gama, hy, cnt + 1, jy);
         cudaMemcpyAsync(cnt + 2, cnt, 2 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->s);
         h->gate_stage1_valid = true;
     } else {
@@ -352,8 +353,22 @@ extern "C" int fdm_gate_set(fdm_handle *h, const float *params, float threshold,
         FDM_CK(h, h->gate_params.ensure(P_N * sizeof(float)));
         FDM_CK(h, cudaMemcpy(h->gate_params.p, params, P_N * sizeof(float), cudaMemcpyHostToDevice));
         h->gate_logit_thr = logf(threshold / (1.f - threshold));
+        h->gate_jump_thr = -1.f;
     }
     h->gate_on = enable != 0;
+    h->gate_stage1_valid = false;
+    h->graph_version = -1;
+    return FDM_OK;
+}
+
+// The plain jump rule in place of the network: a face is linear at stage 1
+// when its largest normalised jump (the unsquashed gate features) is at most
+// jump_threshold; a negative value restores the network.  The gate must have
+// been enabled by fdm_gate_set.
+extern "C" int fdm_gate_set_jump_rule(fdm_handle *h, float jump_threshold) {
+    if (!h) return FDM_ERR_ARG;
+    if (!h->gate_on || !h->gate_params.p) { h->err = "the gate is off: fdm_gate_set first"; return FDM_ERR_STATE; }
+    h->gate_jump_thr = jump_threshold >= 0.f ? jump_threshold : -1.f;
     h->gate_stage1_valid = false;
     h->graph_version = -1;
     return FDM_OK;

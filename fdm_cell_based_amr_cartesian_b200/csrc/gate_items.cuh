@@ -419,11 +419,13 @@ __device__ __forceinline__ void append_hard(bool want, int64_t f, int lane, int3
 // Stage 1: the 32 faces of warp chunk w.  Features, the MLP on the tensor
 // cores, and g >= thr: the face gets the linear-weight flux here and its
 // jump is kept; otherwise it is appended to the hard list for the full WCNS
-// flux.  X columns GF.. of the warp's tile must be zero.
+// flux.  X columns GF.. of the warp's tile must be zero.  jump_thr >= 0
+// replaces the MLP by the plain rule "largest jump <= jump_thr" on the same
+// features (the baseline the network is measured against).
 template <int DIR>
 __device__ __forceinline__ void gate_linear_chunk(const Tables &T, const double4 *__restrict__ cur, double4 *F,
-                                                  const GateWeights &W, XTile &Tt, float logit_thr, double lam,
-                                                  double ig1, double g, int32_t *hard, uint32_t *count,
+                                                  const GateWeights &W, XTile &Tt, float logit_thr, float jump_thr,
+                                                  double lam, double ig1, double g, int32_t *hard, uint32_t *count,
                                                   float *jump1, int64_t w) {
     const int lane = threadIdx.x & 31;
     const int64_t nf = T.NI + (DIR == 0 ? T.nux : T.nuy);
@@ -447,7 +449,7 @@ __device__ __forceinline__ void gate_linear_chunk(const Tables &T, const double4
     float z[2][2];
     mlp_logits_regs(W, Tt.X, z);
     const float zl = row_logit(z, lane);
-    const bool lin = in && zl >= logit_thr;
+    const bool lin = in && (jump_thr >= 0.f ? jm <= jump_thr : zl >= logit_thr);
     if (lin) {
         double out[4];
         face_flux_linear<DIR>(p0, p1, p2, p3, ig1, lam, out);

@@ -145,6 +145,7 @@ struct fdm_handle {
     int in_b = 0, out_b = 0;
     fdm::DevBuf gate_params, gate_flag;   // gate_flag: per-stage hard-face lists
     float gate_logit_thr = 0.f;
+    float gate_jump_thr = -1.f;   // >= 0: the plain jump rule instead of the network
     bool gate_on = false;
     bool gate_stage1_valid = false;   // stage-1 decisions exist for the current tables
 

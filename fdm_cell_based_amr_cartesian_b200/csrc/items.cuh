@@ -175,7 +175,46 @@ __device__ __forceinline__ void request_item(const Tables &T, double4 *cur, int6
 
 // component v (0..3) of hanging-node request r of kind WLS or COPY: the
 // four components of a value are independent, so four threads can share a
-// request
+// request.  geo: the request's geometry block (global memory, or a copy of
+// it in shared memory).
+__device__ __forceinline__ void request_item_var(const Tables &T, double4 *cur, int64_t r, int v,
+                                                 const double *geo) {
+    const int64_t out = T.NI + T.NG + T.NC + r;
+    const int kind = T.rq_kind[r];
+    const int32_t *mem = T.rq_mem + r * WLS_MAXM;
+    double *o = reinterpret_cast<double *>(cur + out) + v;
+    if (kind == RQ_COPY) {
+        *o = reinterpret_cast<const double *>(cur + mem[0])[v];
+        return;
+    }
+    if (kind == RQ_RESTRICT) return;
+    const int m1 = T.rq_m[2 * r], m2 = T.rq_m[2 * r + 1];
+    const int m = m1 + m2;
+    double ph[WLS_MAXM];
+#pragma unroll
+    for (int i = 0; i < WLS_MAXM; ++i) ph[i] = i < m ? reinterpret_cast<const double *>(cur + mem[i])[v] : 0.0;
+    *o = wls_eval_var(geo, m1, m2, ph);
+}
+
+// The geometry blocks of the RQ_TILE requests from r0 on (contiguous in
+// rq_geo) into shared memory, 16 bytes per cp.async; all BT threads of the
+// block call it, and it returns after the copy has landed and the block has
+// synchronised.
+constexpr int RQ_TILE = 64;
+__device__ __forceinline__ void stage_request_geometry(const Tables &T, int64_t r0, double *smem_geo, int nthreads) {
+    int64_t nreq = T.NR - r0;
+    if (nreq > RQ_TILE) nreq = RQ_TILE;
+    const int nch = nreq > 0 ? (int)(nreq * RQ_GEO / 2) : 0;   // 16-byte chunks
+    const double *src = T.rq_geo + r0 * RQ_GEO;
+    for (int k = threadIdx.x; k < nch; k += nthreads) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(smem_geo + 2 * k);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 2 * k));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+}
+
 __device__ __forceinline__ void request_item_var(const Tables &T, double4 *cur, int64_t r, int v) {
     const int64_t out = T.NI + T.NG + T.NC + r;
     const int kind = T.rq_kind[r];

@@ -78,6 +78,87 @@ def disable(solver: Solver):
         raise FdmError(rc, "fdm_gate_set failed")
 
 
+def jump_rule(solver: Solver, jump_threshold: float):
+    """The plain rule in place of the network (the gate must be enabled):
+    linear when the largest normalised jump <= jump_threshold; a negative
+    threshold restores the network."""
+    rc = solver.L.fdm_gate_set_jump_rule(solver.h, float(jump_threshold))
+    if rc:
+        raise FdmError(rc, "fdm_gate_set_jump_rule failed")
+
+
+def stage1_fraction(cfg: P.Config, keys, prim, setup) -> float:
+    """Gated share of the faces at stage 1 of one step from (keys, prim)
+    with the gate as `setup(solver)` leaves it."""
+    g = Solver(cfg)
+    g.upload(keys, prim)
+    g.body_boundary(1)
+    g.step_control()
+    setup(g)
+    g.solution_cells(1)
+    a, b = stats(g)
+    g.close()
+    return a / max(b, 1)
+
+
+def rule_vs_network(cfg: P.Config, keys, prim, steps: int, params=None, threshold: float = THRESHOLD):
+    """What the network buys: the network gate against the plain jump rule
+    on the same eight features, the rule's threshold tuned (bisection) so
+    that it gates the same share of faces at stage 1 as the network.  Both
+    run `steps` steps from (keys, prim) beside a plain run; returns their
+    gated shares, ms per step and density errors against the plain run."""
+    import torch
+
+    def on_net(g):
+        enable(g, params, threshold)
+
+    frac_net = stage1_fraction(cfg, keys, prim, on_net)
+    lo, hi = 0.0, 1.0
+    while stage1_fraction(cfg, keys, prim, lambda g: (on_net(g), jump_rule(g, hi))) < frac_net and hi < 1e6:
+        lo, hi = hi, hi * 4.0
+    for _ in range(24):
+        mid = 0.5 * (lo + hi)
+        if stage1_fraction(cfg, keys, prim, lambda g: (on_net(g), jump_rule(g, mid))) < frac_net:
+            lo = mid
+        else:
+            hi = mid
+    thr_rule = hi
+
+    def run(setup):
+        g = Solver(cfg)
+        g.upload(keys, prim)
+        g.body_boundary(1)
+        g.step_control()
+        setup(g)
+        g.advance(2)                     # warm-up (graph capture)
+        g.upload(keys, prim)
+        g.body_boundary(1)
+        g.step_control()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.advance(steps)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / steps
+        a, b = stats(g)
+        out = g.leaves()
+        g.close()
+        return out, ms, a / max(b, 1)
+
+    plain, ms_plain, _ = run(lambda g: None)
+    net, ms_net, last_net = run(on_net)
+    rule, ms_rule, last_rule = run(lambda g: (on_net(g), jump_rule(g, thr_rule)))
+    l1n, lin_n = density_errors(cfg, plain, net)
+    l1r, lin_r = density_errors(cfg, plain, rule)
+    return {"steps": steps, "plain_ms_per_step": ms_plain,
+            "network": {"stage1_gated_fraction": frac_net, "last_stage_gated_fraction": last_net,
+                        "ms_per_step": ms_net, "l1_density_vs_plain": l1n, "linf_density_vs_plain": lin_n},
+            "jump_rule": {"jump_threshold": thr_rule,
+                          "stage1_gated_fraction": stage1_fraction(
+                              cfg, keys, prim, lambda g: (on_net(g), jump_rule(g, thr_rule))),
+                          "last_stage_gated_fraction": last_rule, "ms_per_step": ms_rule,
+                          "l1_density_vs_plain": l1r, "linf_density_vs_plain": lin_r}}
+
+
 def load_params() -> np.ndarray:
     return np.load(PARAMS_PATH).astype(np.float32)
 

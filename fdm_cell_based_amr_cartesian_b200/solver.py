@@ -41,12 +41,12 @@ EXPORTS = [
     "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
     "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
     "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
-    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_set_wait_limit", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
+    "fdm_batch_sync", "fdm_batch_set_blocks_per_sm", "fdm_batch_set_wait_limit", "fdm_batch_set_face_flux", "fdm_batch_info", "fdm_batch_stream", "fdm_batch_phase_us",
     "fdm_set_values_async", "fdm_download_values_async", "fdm_io_sync",
     "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
     "fdm_download_internal", "fdm_set_internal", "fdm_set_async", "fdm_debug_barrier_timeout",
     "fdm_debug_fail_alloc", "fdm_solute_paired", "fdm_output_error", "fdm_download_keys_async",
-    "fdm_readback_wait",
+    "fdm_readback_wait", "fdm_gate_set_jump_rule",
 ]
 
 
@@ -131,6 +131,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_batch_sync.argtypes = [vp]
     L.fdm_batch_set_blocks_per_sm.argtypes = [vp, i32]
     L.fdm_batch_set_wait_limit.argtypes = [vp, ctypes.c_double]
+    L.fdm_batch_set_face_flux.argtypes = [vp, i32]
     L.fdm_batch_info.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64)]
     L.fdm_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.fdm_batch_phase_us.argtypes = [vp, dp]
@@ -147,6 +148,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_output_error.argtypes = [vp, dp, ctypes.POINTER(i64)]
     L.fdm_download_keys_async.argtypes = [vp, i64, u64p]
     L.fdm_readback_wait.argtypes = [vp]
+    L.fdm_gate_set_jump_rule.argtypes = [vp, ctypes.c_float]
     _lib = L
     return L
 
@@ -586,6 +588,11 @@ class Batch:
         """1 or 2 resident blocks per SM for the persistent kernel, or 0: each
         member's own step graph on its own stream."""
         self._check(self.L.fdm_batch_set_blocks_per_sm(self.b, int(k)))
+
+    def set_face_flux(self, branch_free: bool):
+        """Face phases of the persistent kernel in the reference's order (False)
+        or the split order with the branch-free division (True): same bits."""
+        self._check(self.L.fdm_batch_set_face_flux(self.b, 1 if branch_free else 0))
 
     def set_wait_limit(self, seconds: float):
         """Wait limit of one grid barrier of the persistent kernel (default

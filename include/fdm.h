@@ -341,6 +341,12 @@ int fdm_gate_train_step(const float *X, const float *Y, int64_t n, int64_t idx0,
                         float lr, float *loss, void *stream);
 int fdm_gate_eval(const float *X, int64_t n, const float *params, float *prob,
                   void *stream);
+/* The plain rule in place of the network, the baseline the network is
+ * measured against: a face takes the linear path at stage 1 when the largest
+ * of its normalised jumps (the gate's features before squashing) is at most
+ * jump_threshold; jump_threshold < 0 restores the network.  Requires the
+ * gate to be on (fdm_gate_set). */
+int fdm_gate_set_jump_rule(fdm_handle *h, float jump_threshold);
 /* faces that took the linear path in the last gated stage / all faces */
 int fdm_gate_stats(fdm_handle *h, int64_t *gated, int64_t *total);
 
@@ -386,6 +392,10 @@ int fdm_batch_sync(fdm_batch *b);
  * are the same bits either way; which is faster depends on the members'
  * sizes (measure both). */
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t blocks_per_sm);
+/* Face phases of the persistent kernel: 0 the reference's operation order
+ * (default), 1 the split order with the branch-free correctly rounded
+ * division of face variants 7-10 (the same bits; one may be faster). */
+int fdm_batch_set_face_flux(fdm_batch *b, int32_t branch_free);
 /* Wait limit of one grid barrier of the persistent kernel in seconds
  * (0 < seconds <= 3600; default 2), measured on the GPU's global timer. */
 int fdm_batch_set_wait_limit(fdm_batch *b, double seconds);

@@ -133,3 +133,21 @@ def test_streams_strategy_advance_matches_single_steps():
     for (bm, solo) in pairs:
         solo.solute(6)
         _assert_same(bm, solo)
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+@pytest.mark.parametrize("bps", [1, 2])
+def test_branch_free_face_phases_match_single(bps):
+    """The persistent kernel with the split-order, branch-free face flux
+    (fdm_batch_set_face_flux(1)): plain and gated members, regrids; every
+    member ends bit-identical to its twin advanced alone."""
+    cfgs = _cfgs()
+    pairs = [_pair(c, gate=(k % 2 == 1)) for k, c in enumerate(cfgs)]
+    batch = Batch([p[0] for p in pairs])
+    batch.set_blocks_per_sm(bps)
+    batch.set_face_flux(True)
+    assert batch.solute(25) == 25
+    for (bm, solo) in pairs:
+        solo.solute(25)
+        _assert_same(bm, solo)
+    assert pairs[0][0].counters()["n_regrids"] >= 2

@@ -198,3 +198,21 @@ def test_gate_off_is_exact(oracle_mod):
     o.solute_step()
     g.solute_step()
     assert np.array_equal(g.leaves()[1], o.leaves()[1])
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+def test_network_against_plain_jump_rule():
+    """The network against the plain rule on its own features (largest
+    normalised jump <= t), t tuned to gate the same share of faces at stage
+    1: both runs advance 20 steps on a statically refined four-quadrant mesh
+    and their density errors against the plain run are recorded.  The
+    network must be at least as accurate as the rule at that equal share."""
+    from fdm_cell_based_amr_cartesian_b200.solver import distance_refined_keys, initial_state
+    cfg = P.riemann4(base=64, lvl_amr=4, pstep_adapt=1000)
+    keys = distance_refined_keys(cfg, [("x", 0.5), ("y", 0.5)], [0.2, 0.15, 0.1, 0.05])
+    prim = initial_state(cfg, keys)
+    r = learned.rule_vs_network(cfg, keys, prim, 20)
+    print(r)
+    fn, fr = r["network"]["stage1_gated_fraction"], r["jump_rule"]["stage1_gated_fraction"]
+    assert abs(fn - fr) <= 0.01, (fn, fr)
+    assert r["network"]["l1_density_vs_plain"] <= r["jump_rule"]["l1_density_vs_plain"], r
