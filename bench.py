@@ -329,7 +329,7 @@ def ensemble_window(args, world):
     # the persistent kernel at 1 or 2 resident blocks per SM, or (0) the
     # members' own step graphs on their own streams: the fastest
     tune = {}
-    for bps in (0, 1, 2):
+    for bps in (0, 1, 2, 3):
         batch.set_blocks_per_sm(bps)
         batch.advance(2)
         batch.sync()
@@ -390,8 +390,9 @@ def ensemble_window(args, world):
     return {"workload": f"64 random four-quadrant problems (seeds 1000-1063, rho,p~U[0.1,2], u,v~U[-1,1]), "
                         f"base {E.ENSEMBLE_BASE}^2, max level U{{2..5}}, band-refined meshes, learned gate on",
             "blocks_per_sm_ms_per_step": tune,
-            "strategy": ("member step graphs on their own streams" if best_bps == 0
-                         else f"persistent kernel, {best_bps} block(s) per SM"),
+            "strategy": {0: "member step graphs on their own streams",
+                         3: "phase kernels: one launch per phase over every member"}.get(
+                             best_bps, f"persistent kernel, {best_bps} block(s) per SM"),
             "members": len(cfgs_all), "members_on_rank0": len(cfgs) if rank == 0 else None,
             "sharding": f"whole members per rank, balanced by leaf count over {world} rank(s)",
             "interior_leaves": int(NI), "value": per(ms_gated), "unit": UNIT,

@@ -212,6 +212,155 @@ __device__ __forceinline__ double4 *stage_next(const Member &M, int krk) {
     return krk == 1 ? M.B1 : krk == 2 ? M.B2 : M.B0;
 }
 
+// ---- the phases of one stage, each item as the single-mesh code forms it.
+// Shared by the persistent kernel (phases separated by grid barriers, tiles
+// taken by work stealing) and the phase kernels (one launch per phase).
+
+// step control and per-stage resets of member m (one thread)
+__device__ __forceinline__ void ph_begin_member(const BatchArgs &A, int krk, int m) {
+    const Member &M = A.mem[m];
+    if (krk == 1) {
+        A.act[m] = (!M.sc->done && M.sc->tt < M.p.t_end) ? 1 : 0;
+        if (A.act[m]) step_control_item(M.sc, M.p, 1);
+    }
+    if (!A.act[m]) return;
+    if (krk == 3) { M.sc->lam_next_x = 0.0; M.sc->lam_next_y = 0.0; }
+    if (M.gate_on) {
+        if (krk == 1) { M.GL.cnt[0] = 0; M.GL.cnt[1] = 0; }
+        else { M.GL.cnt[0] = M.GL.cnt[2]; M.GL.cnt[1] = M.GL.cnt[3]; }
+    }
+}
+
+// hanging-node requests: tile t of member m (whole block).  WLS tiles hold
+// RQ_TILE requests, four threads each; interpA tiles hold BW listed
+// fallbacks, one warp each.
+__device__ __forceinline__ void ph_request_tile(const BatchArgs &A, int krk, int m, int64_t t, BatchSmem &S) {
+    const Member &M = A.mem[m];
+    if (!A.act[m]) return;
+    double4 *cur = const_cast<double4 *>(stage_cur(M, krk));
+    const int64_t nthr = cdiv(4 * M.T.NR, BT);
+    const int wid = threadIdx.x >> 5;
+    if (t < nthr) {
+        // the tile's geometry blocks are contiguous: one staged copy
+        // instead of four threads re-reading 768 bytes each
+        stage_request_geometry(M.T, t * RQ_TILE, S.geo, BT);
+        const int64_t q = t * BT + threadIdx.x;
+        if ((q >> 2) < M.T.NR)
+            request_item_var(M.T, cur, q >> 2, (int)(q & 3), S.geo + (threadIdx.x >> 2) * RQ_GEO);
+        __syncthreads();   // the next tile's copy overwrites S.geo
+    } else {
+        const int64_t w = (t - nthr) * BW + wid;
+        if (w < M.T.NRR) request_restrict_warp(M.T, cur, M.T.rq_rlist[w], S.rs[wid]);
+    }
+}
+
+// faces: plain flux, or gate / guard with the linear flux (whole block);
+// s_loaded names the gate weights held in S.gate
+template <bool NRF>
+__device__ __forceinline__ void ph_face_tile(const BatchArgs &A, int krk, int m, int64_t t, BatchSmem &S,
+                                             const float *&s_loaded) {
+    const Member &M = A.mem[m];
+    if (!A.act[m]) return;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const double4 *cur = stage_cur(M, krk);
+    const int64_t tx = cdiv(M.nfx, BT);
+    const int dir = t < tx ? 0 : 1;
+    const int64_t lt = dir == 0 ? t : t - tx;
+    const int64_t nf = dir == 0 ? M.nfx : M.nfy;
+    const double lam = dir == 0 ? M.sc->lambda_x : M.sc->lambda_y;
+    if (!M.gate_on) {
+        const int64_t f = lt * BT + threadIdx.x;
+        if (f < nf) {
+            if (dir == 0) batch_face<0, NRF>(M, cur, M.Fx, lam, A.d2, f);
+            else batch_face<1, NRF>(M, cur, M.Fy, lam, A.d2, f);
+        }
+        return;
+    }
+    const double ig1 = 1.0 / (M.gama - 1.0);
+    const int64_t w = lt * BW + wid;   // warp chunk of 32 faces
+    if (krk == 1) {
+        if (s_loaded != M.gate_P) {
+            __syncthreads();
+            load_weights_smem(S.gate.W, M.gate_P);
+            for (int k = GF; k < XLD; ++k) S.gate.xt[wid].X[lane][k] = __float2bfloat16_rn(0.f);
+            if (threadIdx.x == 0) s_loaded = M.gate_P;
+            __syncthreads();
+        }
+        if (w * 32 < nf) {
+            if (dir == 0)
+                gate_linear_chunk<0>(M.T, cur, M.Fx, S.gate.W, S.gate.xt[wid], M.logit_thr, M.jump_thr, lam, ig1,
+                                     M.gama, M.GL.hx, M.GL.cnt, M.GL.jx, w);
+            else
+                gate_linear_chunk<1>(M.T, cur, M.Fy, S.gate.W, S.gate.xt[wid], M.logit_thr, M.jump_thr, lam, ig1,
+                                     M.gama, M.GL.hy, M.GL.cnt + 1, M.GL.jy, w);
+        }
+    } else if (w * 32 < nf) {
+        if (dir == 0)
+            guard_linear_chunk<0>(M.T, cur, M.Fx, M.GL.jx, lam, ig1, M.gama, M.GL.hx, M.GL.cnt, w);
+        else
+            guard_linear_chunk<1>(M.T, cur, M.Fy, M.GL.jy, lam, ig1, M.gama, M.GL.hy, M.GL.cnt + 1, w);
+    }
+}
+
+// tile offsets of the hard faces of gated members (one thread)
+__device__ __forceinline__ void ph_hard_offsets(const BatchArgs &A, int krk) {
+    int64_t acc = 0;
+    for (int m = 0; m < A.nmem; ++m) {
+        A.off_hard[m] = acc;
+        const Member &M = A.mem[m];
+        if (!A.act[m] || !M.gate_on) continue;
+        if (krk == 1) { M.GL.cnt[2] = M.GL.cnt[0]; M.GL.cnt[3] = M.GL.cnt[1]; }
+        acc += cdiv(M.GL.cnt[0], BT) + cdiv(M.GL.cnt[1], BT);
+    }
+    A.off_hard[A.nmem] = acc;
+}
+
+// hard faces (full WCNS flux) of tile t of member m
+template <bool NRF>
+__device__ __forceinline__ void ph_hard_tile(const BatchArgs &A, int krk, int m, int64_t t) {
+    const Member &M = A.mem[m];
+    const double4 *cur = stage_cur(M, krk);
+    const int64_t tx = cdiv(M.GL.cnt[0], BT);
+    if (t < tx) {
+        const int64_t i = t * BT + threadIdx.x;
+        if (i < M.GL.cnt[0]) batch_face<0, NRF>(M, cur, M.Fx, M.sc->lambda_x, A.d2, M.GL.hx[i]);
+    } else {
+        const int64_t i = (t - tx) * BT + threadIdx.x;
+        if (i < M.GL.cnt[1]) batch_face<1, NRF>(M, cur, M.Fy, M.sc->lambda_y, A.d2, M.GL.hy[i]);
+    }
+}
+
+// cells: residual, candidate, RK blend, residual partials, lambda (whole block)
+__device__ __forceinline__ void ph_cell_tile(const BatchArgs &A, int krk, int m, int64_t t, CellsSmem &S) {
+    const Member &M = A.mem[m];
+    if (!A.act[m]) return;
+    const int64_t i = t * BT + threadIdx.x;
+    double rm[4] = {0.0, 0.0, 0.0, 0.0}, rs[4] = {0.0, 0.0, 0.0, 0.0};
+    double lx = 0.0, ly = 0.0;
+    if (i < M.T.NI)
+        cell_item(M.T, M.LT, stage_cur(M, krk), M.B0, stage_next(M, krk), M.Fx, M.Fy, M.sc->tstep, krk, 0, M.gama, i,
+                  rm, rs, lx, ly);
+    cells_block_reduce(rm, rs, lx, ly, M.res_part + t * 8, M.sc, krk == 3, S);
+}
+
+// ghosts of member m, tile t: j = 3 after a stage, j = 1 after a step
+__device__ __forceinline__ void ph_ghost_tile(const BatchArgs &A, int krk, int j, int m, int64_t t, int32_t *rlist,
+                                              int *rn, RestrictSmem *rs) {
+    const Member &M = A.mem[m];
+    if (!A.act[m]) return;
+    if (j == 1 && (!M.amr_on || A.skip_j1[m])) return;
+    ghost_tile(M.T, j == 1 ? M.B0 : stage_next(M, krk), M.GS, M.sc, j, t, rlist, rn, rs);
+}
+
+// end of the step of member m: residual norms, tt, it, NaN, t_end (whole block)
+__device__ __forceinline__ void ph_end_member(const BatchArgs &A, int m, double (*fin)[8]) {
+    const Member &M = A.mem[m];
+    if (!A.act[m]) return;
+    res_finalize_block(M.res_part, (int)cdiv(M.T.NI, BT), M.sc, fin);
+    if (threadIdx.x == 0) step_end_item(M.sc, M.T.NI);
+    __syncthreads();
+}
+
 // barrier, then block 0 stamps the time (phase k of stage krk ended)
 #define BAR_STAMP(k)                                                                   \
     do {                                                                               \
@@ -231,164 +380,125 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(BatchArgs A, int krk) 
     __shared__ int32_t s_rlist[BT];
     __shared__ int s_rn;
     const unsigned nb = gridDim.x;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int np1 = A.nmem + 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) A.stamp[(krk - 1) * 16] = gtimer();
 
     // ---- step control / per-stage resets (one thread per member)
-    if (blockIdx.x == 0) {
-        for (int m = threadIdx.x; m < A.nmem; m += BT) {
-            const Member &M = A.mem[m];
-            if (krk == 1) {
-                A.act[m] = (!M.sc->done && M.sc->tt < M.p.t_end) ? 1 : 0;
-                if (A.act[m]) step_control_item(M.sc, M.p, 1);
-            }
-            if (!A.act[m]) continue;
-            if (krk == 3) { M.sc->lam_next_x = 0.0; M.sc->lam_next_y = 0.0; }
-            if (M.gate_on) {
-                if (krk == 1) { M.GL.cnt[0] = 0; M.GL.cnt[1] = 0; }
-                else { M.GL.cnt[0] = M.GL.cnt[2]; M.GL.cnt[1] = M.GL.cnt[3]; }
-            }
-        }
-    }
+    if (blockIdx.x == 0)
+        for (int m = threadIdx.x; m < A.nmem; m += BT) ph_begin_member(A, krk, m);
     BAR_STAMP(1);
 
     // ---- hanging-node requests
-    run_tiles(A, PH_REQ, A.off + PH_REQ * np1, &s_t, s_off, [&](int m, int64_t t) {
-        const Member &M = A.mem[m];
-        if (!A.act[m]) return;
-        double4 *cur = const_cast<double4 *>(stage_cur(M, krk));
-        const int64_t nthr = cdiv(4 * M.T.NR, BT);   // four threads per request, one per component
-        if (t < nthr) {
-            // the tile's geometry blocks are contiguous: one staged copy
-            // instead of four threads re-reading 768 bytes each
-            stage_request_geometry(M.T, t * RQ_TILE, S.geo, BT);
-            const int64_t q = t * BT + threadIdx.x;
-            if ((q >> 2) < M.T.NR)
-                request_item_var(M.T, cur, q >> 2, (int)(q & 3), S.geo + (threadIdx.x >> 2) * RQ_GEO);
-            __syncthreads();   // the next tile's copy overwrites S.geo
-        } else {
-            const int64_t r = (t - nthr) * BW + wid;
-            if (r < M.T.NR) request_restrict_warp(M.T, cur, r, S.rs[wid]);
-        }
-    });
+    run_tiles(A, PH_REQ, A.off + PH_REQ * np1, &s_t, s_off,
+              [&](int m, int64_t t) { ph_request_tile(A, krk, m, t, S); });
     BAR_STAMP(2);
 
     // ---- faces: plain flux, or gate / guard with the linear flux
     if (threadIdx.x == 0) s_loaded = nullptr;
     __syncthreads();
-    run_tiles(A, PH_FACE, A.off + PH_FACE * np1, &s_t, s_off, [&](int m, int64_t t) {
-        const Member &M = A.mem[m];
-        if (!A.act[m]) return;
-        const double4 *cur = stage_cur(M, krk);
-        const int64_t tx = cdiv(M.nfx, BT);
-        const int dir = t < tx ? 0 : 1;
-        const int64_t lt = dir == 0 ? t : t - tx;
-        const int64_t nf = dir == 0 ? M.nfx : M.nfy;
-        const double lam = dir == 0 ? M.sc->lambda_x : M.sc->lambda_y;
-        if (!M.gate_on) {
-            const int64_t f = lt * BT + threadIdx.x;
-            if (f < nf) {
-                if (dir == 0) batch_face<0, NRF>(M, cur, M.Fx, lam, A.d2, f);
-                else batch_face<1, NRF>(M, cur, M.Fy, lam, A.d2, f);
-            }
-            return;
-        }
-        const double ig1 = 1.0 / (M.gama - 1.0);
-        const int64_t w = lt * BW + wid;   // warp chunk of 32 faces
-        if (krk == 1) {
-            if (s_loaded != M.gate_P) {
-                __syncthreads();
-                load_weights_smem(S.gate.W, M.gate_P);
-                for (int k = GF; k < XLD; ++k) S.gate.xt[wid].X[lane][k] = __float2bfloat16_rn(0.f);
-                if (threadIdx.x == 0) s_loaded = M.gate_P;
-                __syncthreads();
-            }
-            if (w * 32 < nf) {
-                if (dir == 0)
-                    gate_linear_chunk<0>(M.T, cur, M.Fx, S.gate.W, S.gate.xt[wid], M.logit_thr, M.jump_thr, lam, ig1, M.gama,
-                                         M.GL.hx, M.GL.cnt, M.GL.jx, w);
-                else
-                    gate_linear_chunk<1>(M.T, cur, M.Fy, S.gate.W, S.gate.xt[wid], M.logit_thr, M.jump_thr, lam, ig1, M.gama,
-                                         M.GL.hy, M.GL.cnt + 1, M.GL.jy, w);
-            }
-        } else if (w * 32 < nf) {
-            if (dir == 0)
-                guard_linear_chunk<0>(M.T, cur, M.Fx, M.GL.jx, lam, ig1, M.gama, M.GL.hx, M.GL.cnt, w);
-            else
-                guard_linear_chunk<1>(M.T, cur, M.Fy, M.GL.jy, lam, ig1, M.gama, M.GL.hy, M.GL.cnt + 1, w);
-        }
-    });
+    run_tiles(A, PH_FACE, A.off + PH_FACE * np1, &s_t, s_off,
+              [&](int m, int64_t t) { ph_face_tile<NRF>(A, krk, m, t, S, s_loaded); });
     BAR_STAMP(3);
 
     // ---- hard faces of gated members (full WCNS flux)
     if (A.any_gate) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            int64_t acc = 0;
-            for (int m = 0; m < A.nmem; ++m) {
-                A.off_hard[m] = acc;
-                const Member &M = A.mem[m];
-                if (!A.act[m] || !M.gate_on) continue;
-                if (krk == 1) { M.GL.cnt[2] = M.GL.cnt[0]; M.GL.cnt[3] = M.GL.cnt[1]; }
-                acc += cdiv(M.GL.cnt[0], BT) + cdiv(M.GL.cnt[1], BT);
-            }
-            A.off_hard[A.nmem] = acc;
-        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) ph_hard_offsets(A, krk);
         BAR_STAMP(4);
-        run_tiles(A, PH_HARD, A.off_hard, &s_t, s_off, [&](int m, int64_t t) {
-            const Member &M = A.mem[m];
-            const double4 *cur = stage_cur(M, krk);
-            const int64_t tx = cdiv(M.GL.cnt[0], BT);
-            if (t < tx) {
-                const int64_t i = t * BT + threadIdx.x;
-                if (i < M.GL.cnt[0]) batch_face<0, NRF>(M, cur, M.Fx, M.sc->lambda_x, A.d2, M.GL.hx[i]);
-            } else {
-                const int64_t i = (t - tx) * BT + threadIdx.x;
-                if (i < M.GL.cnt[1]) batch_face<1, NRF>(M, cur, M.Fy, M.sc->lambda_y, A.d2, M.GL.hy[i]);
-            }
-        });
+        run_tiles(A, PH_HARD, A.off_hard, &s_t, s_off, [&](int m, int64_t t) { ph_hard_tile<NRF>(A, krk, m, t); });
         BAR_STAMP(5);
     }
 
     // ---- cells: residual, candidate, RK blend, residual partials, lambda
-    run_tiles(A, PH_CELL, A.off + PH_CELL * np1, &s_t, s_off, [&](int m, int64_t t) {
-        const Member &M = A.mem[m];
-        if (!A.act[m]) return;
-        const int64_t i = t * BT + threadIdx.x;
-        double rm[4] = {0.0, 0.0, 0.0, 0.0}, rs[4] = {0.0, 0.0, 0.0, 0.0};
-        double lx = 0.0, ly = 0.0;
-        if (i < M.T.NI)
-            cell_item(M.T, M.LT, stage_cur(M, krk), M.B0, stage_next(M, krk), M.Fx, M.Fy, M.sc->tstep, krk, 0,
-                      M.gama, i, rm, rs, lx, ly);
-        cells_block_reduce(rm, rs, lx, ly, M.res_part + t * 8, M.sc, krk == 3, S.cells);
-    });
+    run_tiles(A, PH_CELL, A.off + PH_CELL * np1, &s_t, s_off,
+              [&](int m, int64_t t) { ph_cell_tile(A, krk, m, t, S.cells); });
     BAR_STAMP(6);
 
     // ---- ghosts of the new stage value (body_boundary_RK)
-    run_tiles(A, PH_GHOST, A.off + PH_GHOST * np1, &s_t, s_off, [&](int m, int64_t t) {
-        const Member &M = A.mem[m];
-        if (!A.act[m]) return;
-        ghost_tile(M.T, stage_next(M, krk), M.GS, M.sc, 3, t, s_rlist, &s_rn, S.rs);
-    });
+    run_tiles(A, PH_GHOST, A.off + PH_GHOST * np1, &s_t, s_off,
+              [&](int m, int64_t t) { ph_ghost_tile(A, krk, 3, m, t, s_rlist, &s_rn, S.rs); });
     if (krk != 3) return;
     BAR_STAMP(7);
 
     // ---- end of the step: residual norms, tt, it, NaN, t_end
-    for (int m = blockIdx.x; m < A.nmem; m += nb) {
-        const Member &M = A.mem[m];
-        if (!A.act[m]) continue;
-        res_finalize_block(M.res_part, (int)cdiv(M.T.NI, BT), M.sc, S.fin);
-        if (threadIdx.x == 0) step_end_item(M.sc, M.T.NI);
-        __syncthreads();
-    }
+    for (int m = blockIdx.x; m < A.nmem; m += nb) ph_end_member(A, m, S.fin);
     BAR_STAMP(8);
 
     // ---- body_boundary(1) after the step on AMR members
-    run_tiles(A, PH_GHOST1, A.off + PH_GHOST1 * np1, &s_t, s_off, [&](int m, int64_t t) {
-        const Member &M = A.mem[m];
-        if (!A.act[m] || !M.amr_on || A.skip_j1[m]) return;
-        ghost_tile(M.T, M.B0, M.GS, M.sc, 1, t, s_rlist, &s_rn, S.rs);
-    });
+    run_tiles(A, PH_GHOST1, A.off + PH_GHOST1 * np1, &s_t, s_off,
+              [&](int m, int64_t t) { ph_ghost_tile(A, krk, 1, m, t, s_rlist, &s_rn, S.rs); });
+}
+
+// ---- phase kernels: one launch per phase covering every member, no grid
+// barrier (the launches are ordered on the batch stream), each with the
+// launch shape of its own work.  Blocks take the phase's tiles in a
+// grid-stride loop; the member of a tile is found by binary search over the
+// phase's tile offsets.
+template <class Fn>
+__device__ __forceinline__ void flat_tiles(const BatchArgs &A, const int64_t *goff, int64_t *s_off, Fn &&fn) {
+    const int64_t *off = goff;
+    if (A.nmem + 1 <= OFF_CAP) {
+        for (int k = threadIdx.x; k <= A.nmem; k += blockDim.x) s_off[k] = goff[k];
+        __syncthreads();
+        off = s_off;
+    }
+    const int64_t total = off[A.nmem];
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        int lo = 0, hi = A.nmem;   // off[lo] <= t < off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (off[mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        fn(lo, t - off[lo]);
+    }
+}
+
+__global__ void __launch_bounds__(BT) k_bp_begin(BatchArgs A, int krk) {
+    for (int m = threadIdx.x; m < A.nmem; m += BT) ph_begin_member(A, krk, m);
+}
+__global__ void __launch_bounds__(BT) k_bp_requests(BatchArgs A, int krk) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSmem &S = *reinterpret_cast<BatchSmem *>(smem_raw);
+    __shared__ int64_t s_off[OFF_CAP];
+    flat_tiles(A, A.off + PH_REQ * (A.nmem + 1), s_off, [&](int m, int64_t t) { ph_request_tile(A, krk, m, t, S); });
+}
+template <bool NRF>
+__global__ void __launch_bounds__(BT, 2) k_bp_faces(BatchArgs A, int krk) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSmem &S = *reinterpret_cast<BatchSmem *>(smem_raw);
+    __shared__ int64_t s_off[OFF_CAP];
+    __shared__ const float *s_loaded;
+    if (threadIdx.x == 0) s_loaded = nullptr;
+    __syncthreads();
+    flat_tiles(A, A.off + PH_FACE * (A.nmem + 1), s_off,
+               [&](int m, int64_t t) { ph_face_tile<NRF>(A, krk, m, t, S, s_loaded); });
+}
+__global__ void k_bp_hard_offsets(BatchArgs A, int krk) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) ph_hard_offsets(A, krk);
+}
+template <bool NRF>
+__global__ void __launch_bounds__(BT, 2) k_bp_hard(BatchArgs A, int krk) {
+    __shared__ int64_t s_off[OFF_CAP];
+    flat_tiles(A, A.off_hard, s_off, [&](int m, int64_t t) { ph_hard_tile<NRF>(A, krk, m, t); });
+}
+__global__ void __launch_bounds__(BT, 3) k_bp_cells(BatchArgs A, int krk) {
+    __shared__ CellsSmem s_cells;
+    __shared__ int64_t s_off[OFF_CAP];
+    flat_tiles(A, A.off + PH_CELL * (A.nmem + 1), s_off,
+               [&](int m, int64_t t) { ph_cell_tile(A, krk, m, t, s_cells); });
+}
+__global__ void __launch_bounds__(BT) k_bp_ghosts(BatchArgs A, int krk, int j) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RestrictSmem *s_rs = reinterpret_cast<BatchSmem *>(smem_raw)->rs;
+    __shared__ int32_t s_rlist[BT];
+    __shared__ int s_rn;
+    __shared__ int64_t s_off[OFF_CAP];
+    flat_tiles(A, A.off + (j == 1 ? PH_GHOST1 : PH_GHOST) * (A.nmem + 1), s_off,
+               [&](int m, int64_t t) { ph_ghost_tile(A, krk, j, m, t, s_rlist, &s_rn, s_rs); });
+}
+__global__ void __launch_bounds__(BT) k_bp_end(BatchArgs A) {
+    __shared__ double s_fin[BT][8];
+    for (int m = blockIdx.x; m < A.nmem; m += gridDim.x) ph_end_member(A, m, s_fin);
 }
 
 // Test of the bounded waits: a grid barrier that waits for one block more
@@ -406,7 +516,10 @@ struct fdm_batch {
     cudaStream_t s = nullptr;
     DevBuf d_mem, d_off, d_ctr, d_bar, d_act, d_skip, d_stamp;
     std::vector<int32_t> h_skip;
-    int grid = 0, blocks_per_sm = 0, want_bps = 2;   // want_bps 0: the members' own step graphs
+    int grid = 0, blocks_per_sm = 0, want_bps = 2;   // want_bps 0: the members' own step graphs,
+                                                     // 3: phase kernels (no persistent kernel)
+    std::vector<int64_t> h_off;                      // tile offsets per phase (host copy)
+    int sms = 0;
     bool face_nr = false;                            // branch-free division in the face phases
     size_t smem = 0;
     bool any_gate = false;
@@ -471,7 +584,7 @@ static int batch_refresh(fdm_batch *b) {
             d.GL = gate_lists(h->gate_flag.p, d.nfx, d.nfy);
         }
         const int64_t tiles[N_PHASE] = {
-            cdiv(4 * h->NR, BT) + (d.has_restrict ? cdiv(h->NR, BW) : 0),   // PH_REQ
+            cdiv(4 * h->NR, BT) + cdiv(h->n_restrict, BW),               // PH_REQ
             cdiv(d.nfx, BT) + cdiv(d.nfy, BT),                          // PH_FACE
             0,                                                          // PH_HARD (device)
             cdiv(h->NI, BT),                                            // PH_CELL
@@ -483,6 +596,7 @@ static int batch_refresh(fdm_batch *b) {
     BCK(b, b->d_off.ensure(sizeof(int64_t) * off.size()));
     BCK(b, cudaMemcpyAsync(b->d_mem.p, M.data(), sizeof(Member) * n, cudaMemcpyHostToDevice, b->s));
     BCK(b, cudaMemcpyAsync(b->d_off.p, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice, b->s));
+    b->h_off = off;
     BCK(b, cudaStreamSynchronize(b->s));
     b->versions.resize(n);
     b->gates.resize(n);
@@ -517,6 +631,16 @@ static int batch_grid(fdm_batch *b) {
         b->blocks_per_sm = 0;
         return FDM_OK;
     }
+    if (b->want_bps == 3) {   // phase kernels: each launch sized by its own tiles
+        BCK(b, cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
+        BCK(b, cudaFuncSetAttribute(k_bp_requests, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        BCK(b, cudaFuncSetAttribute(k_bp_ghosts, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        BCK(b, cudaFuncSetAttribute(k_bp_faces<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        BCK(b, cudaFuncSetAttribute(k_bp_faces<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        b->blocks_per_sm = 0;
+        b->grid = 0;
+        return FDM_OK;
+    }
     int sms = 0, bps = 0;
     BCK(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
     const void *fn = batch_kernel(b);
@@ -525,6 +649,36 @@ static int batch_grid(fdm_batch *b) {
     if (bps <= 0) { b->err = "the batch kernel does not fit on an SM"; return FDM_ERR_UNSUPPORTED; }
     b->blocks_per_sm = std::min(bps, b->want_bps);
     b->grid = sms * b->blocks_per_sm;
+    return FDM_OK;
+}
+
+// One stage as phase kernels on the batch stream: each launch covers every
+// member's tiles of one phase, in the order the persistent kernel runs the
+// phases (the stream orders them; no grid barrier).
+static int enqueue_phase_kernels(fdm_batch *b, const BatchArgs &A, int krk) {
+    const int n1 = A.nmem + 1;
+    auto total = [&](int ph) { return b->h_off[(size_t)ph * n1 + A.nmem]; };
+    auto grid = [](int64_t t) { return (unsigned)std::min<int64_t>(t, 1ll << 30); };
+    k_bp_begin<<<1, BT, 0, b->s>>>(A, krk);
+    if (total(PH_REQ) > 0) k_bp_requests<<<grid(total(PH_REQ)), BT, b->smem, b->s>>>(A, krk);
+    if (total(PH_FACE) > 0) {
+        if (b->face_nr) k_bp_faces<true><<<grid(total(PH_FACE)), BT, b->smem, b->s>>>(A, krk);
+        else k_bp_faces<false><<<grid(total(PH_FACE)), BT, b->smem, b->s>>>(A, krk);
+    }
+    if (A.any_gate) {
+        // hard-face tiles are known on the device only: a grid-stride launch
+        k_bp_hard_offsets<<<1, 32, 0, b->s>>>(A, krk);
+        const unsigned g = (unsigned)(4 * b->sms);
+        if (b->face_nr) k_bp_hard<true><<<g, BT, 0, b->s>>>(A, krk);
+        else k_bp_hard<false><<<g, BT, 0, b->s>>>(A, krk);
+    }
+    if (total(PH_CELL) > 0) k_bp_cells<<<grid(total(PH_CELL)), BT, 0, b->s>>>(A, krk);
+    if (total(PH_GHOST) > 0) k_bp_ghosts<<<grid(total(PH_GHOST)), BT, b->smem, b->s>>>(A, krk, 3);
+    if (krk == 3) {
+        k_bp_end<<<(unsigned)A.nmem, BT, 0, b->s>>>(A);
+        if (total(PH_GHOST1) > 0) k_bp_ghosts<<<grid(total(PH_GHOST1)), BT, b->smem, b->s>>>(A, krk, 1);
+    }
+    BCK(b, cudaGetLastError());
     return FDM_OK;
 }
 
@@ -542,6 +696,7 @@ static int enqueue_batch_stage(fdm_batch *b, int krk) {
     A.stamp = b->d_stamp.as<unsigned long long>();
     A.d2 = Den{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};   // IEEE division on the host
     BCK(b, cudaMemsetAsync(A.ctr, 0, sizeof(unsigned long long) * N_PHASE, b->s));
+    if (b->want_bps == 3) return enqueue_phase_kernels(b, A, krk);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)b->grid);
     cfg.blockDim = dim3(BT);
@@ -831,11 +986,11 @@ int fdm_batch_sync(fdm_batch *b) {
 }
 
 // 1 or 2 resident blocks per SM for the persistent kernel (the next graph
-// uses the new grid), or 0: no persistent kernel, each member's own step
-// graph on its own stream (faster when the members are large enough to fill
-// the GPU between them).
+// uses the new grid); 0: no persistent kernel, each member's own step graph
+// on its own stream; 3: no persistent kernel, one launch per phase covering
+// every member (each phase at the launch shape of its own work).
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t bps) {
-    if (!b || bps < 0 || bps > 2) return FDM_ERR_ARG;
+    if (!b || bps < 0 || bps > 3) return FDM_ERR_ARG;
     b->want_bps = bps;
     int rc = batch_grid(b);
     if (rc) return rc;

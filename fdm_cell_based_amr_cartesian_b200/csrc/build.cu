@@ -647,6 +647,12 @@ static int read_back(fdm_handle *h, int32_t he[8], int64_t *tot, int nt) {
         if (rc_) return rc_;      \
     } while (0)
 
+__global__ void k_restrict_list(int64_t NR, const int32_t *__restrict__ kind, int32_t *list,
+                                unsigned long long *count) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < NR && kind[r] == RQ_RESTRICT) list[atomicAdd(count, 1ull)] = (int32_t)r;
+}
+
 int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double *prim_in, int key_bits) {
     Nvtx range("fdm tables");
     const int TB = 256;
@@ -762,6 +768,13 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
                  h->rq_geo.as<double>(), h->rq_node.as<uint64_t>(), counts};
         k_gather<<<nblk(NR, 64), 64, 0, s>>>(T, h->G, RD, O, err);
     }
+    // the interpA fallbacks among the requests, listed (in no particular
+    // order: each writes only its own value), so that their warps are
+    // launched for them alone
+    FDM_CK(h, h->rq_rlist.ensure((NR > 0 ? NR : 1) * 4));
+    if (NR > 0)
+        k_restrict_list<<<nblk(NR, TB), TB, 0, s>>>(NR, h->rq_kind.as<int32_t>(), h->rq_rlist.as<int32_t>(),
+                                                    counts + 6);
     // 6. ghosts
     const int64_t ngh = NG > 0 ? NG : 1;
     FDM_CK(h, h->gh_kind.ensure(ngh * 4));
@@ -834,11 +847,12 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     k_lmax<<<nblk(NI, TB), TB, 0, s>>>(NI, h->ilvl.as<uint8_t>(), dl);
     k_set_lmax<<<1, 32, 0, s>>>(dl, h->scal.as<DevScalars>());
     int32_t he[8];
-    unsigned long long hc[5];
+    unsigned long long hc[7];
     FDM_CK(h, cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, s));
     FDM_CK(h, cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s));
     FDM_CK(h, cudaStreamSynchronize(s));
     FDM_CK(h, cudaGetLastError());
+    if (hc[2] != hc[6]) return arg_fail(h, "internal table check failed: restrict list");
     if (he[BE_OVERFLOW]) return arg_fail(h, "hanging-node stencil larger than supported");
     if (he[BE_INDEX]) return arg_fail(h, "internal table check failed: an index is out of range");
     h->l_max = he[7];

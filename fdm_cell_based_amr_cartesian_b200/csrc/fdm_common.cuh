@@ -69,6 +69,8 @@ struct Tables {
     const int32_t *rq_mem;            // [NR][WLS_MAXM] member slots
     const double *rq_geo;             // [NR][RQ_GEO] geometry block
     const uint64_t *rq_node;          // [NR] key of the node the value belongs to
+    const int32_t *rq_rlist;          // [NRR] the requests of kind RQ_RESTRICT (interpA fallbacks)
+    int64_t NRR;
     // ghosts (slots NI .. NI+NG)
     const int32_t *gh_kind;           // [NG]
     const int32_t *gh_a;              // [NG] source slot / range lo

@@ -105,7 +105,7 @@ struct fdm_handle {
     // tables
     fdm::DevBuf lkey, lslot, slot_leaf, lcx, lcy, lcross;
     fdm::DevBuf ist, ilvl, ifxl, ifyl, uxl, uyl;
-    fdm::DevBuf rq_kind, rq_m, rq_mem, rq_geo, rq_node;
+    fdm::DevBuf rq_kind, rq_m, rq_mem, rq_geo, rq_node, rq_rlist;
     fdm::DevBuf gh_kind, gh_a, gh_b, gh_flip, gh_x, gh_y;
     // state: three slot arrays (step start / stage 1 / stage 2)
     fdm::DevBuf B[3];
@@ -171,6 +171,8 @@ struct fdm_handle {
         T.uyl = uyl.as<int32_t>();
         T.nux = nux; T.nuy = nuy;
         T.rq_kind = rq_kind.as<int32_t>();
+        T.rq_rlist = rq_rlist.as<int32_t>();
+        T.NRR = n_restrict;
         T.rq_m = rq_m.as<int32_t>();
         T.rq_mem = rq_mem.as<int32_t>();
         T.rq_geo = rq_geo.as<double>();

@@ -28,12 +28,12 @@ __global__ void __launch_bounds__(256) k_requests4(Tables T, double4 *cur) {
     request_item_var(T, cur, r, (int)(g & 3));
 }
 
-// interpA fallbacks of parent_value_weno: one warp per request
+// interpA fallbacks of parent_value_weno: one warp per listed request
 __global__ void __launch_bounds__(128) k_requests_restrict(Tables T, double4 *cur) {
     __shared__ RestrictSmem sm[4];
-    const int64_t r = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (r >= T.NR) return;
-    request_restrict_warp(T, cur, r, sm[threadIdx.x >> 5]);
+    const int64_t w = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (w >= T.NRR) return;
+    request_restrict_warp(T, cur, T.rq_rlist[w], sm[threadIdx.x >> 5]);
 }
 
 // One thread per face; TB threads per block, at least MINB blocks per SM
@@ -224,7 +224,8 @@ __global__ void k_set_tstep(DevScalars *sc, double tstep) {
 void launch_requests(fdm_handle *h, const double4 *cur) {
     if (h->NR == 0) return;
     k_requests4<<<nblk(4 * h->NR, 256), 256, 0, h->s>>>(h->tables(), (double4 *)cur);
-    if (h->n_restrict > 0) k_requests_restrict<<<nblk(h->NR, 4), 128, 0, h->s>>>(h->tables(), (double4 *)cur);
+    if (h->n_restrict > 0)
+        k_requests_restrict<<<nblk(h->n_restrict, 4), 128, 0, h->s>>>(h->tables(), (double4 *)cur);
 }
 // Launch shapes of the face kernel that the autotuner chooses from.
 template <int TB, int MINB>

@@ -585,8 +585,9 @@ class Batch:
         self._check(self.L.fdm_batch_sync(self.b))
 
     def set_blocks_per_sm(self, k: int):
-        """1 or 2 resident blocks per SM for the persistent kernel, or 0: each
-        member's own step graph on its own stream."""
+        """1 or 2 resident blocks per SM for the persistent kernel; 0: each
+        member's own step graph on its own stream; 3: one launch per phase
+        covering every member."""
         self._check(self.L.fdm_batch_set_blocks_per_sm(self.b, int(k)))
 
     def set_face_flux(self, branch_free: bool):

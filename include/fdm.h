@@ -388,9 +388,12 @@ int fdm_batch_sync(fdm_batch *b);
 /* blocks_per_sm 1 or 2: resident blocks of the persistent kernel per SM;
  * 0: no persistent kernel, each member's own step graph on its own stream
  * (the batch stream is joined to the members' streams around every call,
- * so ordering and event timing on the batch stream are unchanged).  Results
- * are the same bits either way; which is faster depends on the members'
- * sizes (measure both). */
+ * so ordering and event timing on the batch stream are unchanged);
+ * 3: no persistent kernel, one launch per phase of a stage covering the
+ * tiles of every member (requests, faces, hard faces, cells, ghosts, each
+ * with its own launch shape), ordered on the batch stream.  Results are the
+ * same bits every way; which is faster depends on the members' sizes
+ * (measure). */
 int fdm_batch_set_blocks_per_sm(fdm_batch *b, int32_t blocks_per_sm);
 /* Face phases of the persistent kernel: 0 the reference's operation order
  * (default), 1 the split order with the branch-free correctly rounded

@@ -151,3 +151,24 @@ def test_branch_free_face_phases_match_single(bps):
         solo.solute(25)
         _assert_same(bm, solo)
     assert pairs[0][0].counters()["n_regrids"] >= 2
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+@pytest.mark.parametrize("branch_free", [False, True])
+def test_phase_kernels_match_single(branch_free):
+    """blocks_per_sm 3: no persistent kernel, one launch per phase over every
+    member; plain and gated members, regrids, a member reaching t_end early:
+    every member ends bit-identical to its twin advanced alone."""
+    cfgs = _cfgs() + [P.riemann4(base=32, lvl_amr=2, t_end=0.004)]
+    pairs = [_pair(c, gate=(k % 2 == 1)) for k, c in enumerate(cfgs)]
+    batch = Batch([p[0] for p in pairs])
+    batch.set_blocks_per_sm(3)
+    batch.set_face_flux(branch_free)
+    assert batch.solute(25) == 25
+    batch.advance(3)
+    batch.sync()
+    for (bm, solo) in pairs:
+        solo.solute(25)
+        solo.solute(3)
+        _assert_same(bm, solo)
+    assert pairs[0][0].counters()["n_regrids"] >= 2
