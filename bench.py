@@ -122,6 +122,18 @@ def profile_traffic():
     return profile_figure("traffic_bytes_per_launch")
 
 
+def profile_text(name):
+    """A text field of the face kernel's ncu summary (a line 'name: value')."""
+    path = os.path.join(ROOT, "profiles", "face_flux_riemann4.md")
+    try:
+        for line in open(path):
+            if line.startswith(name + ":"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 # ------------------------------------------------------------ CPU legs
 def cpu_sample(cfg, keys, prim, lam, tstep, steps):
     """Time the oracle (the CPU restatement of the reference OpenMP path) on
@@ -824,7 +836,13 @@ def run_ours(args):
                 "config": workload_desc(len(keys), NI),
                 "roofline": {"bound": "hbm", "achieved": face_gbs, "peak": hbm_peak, "unit": "GB/s",
                              "frac": face_gbs / hbm_peak, "traffic": traffic,
-                             "kernel": "k_faces (x+y)", "ms_per_launch": kt["faces"],
+                             "kernel": f"face flux (x+y), autotuned variant {tuned}",
+                             "ms_per_launch": kt["faces"],
+                             "algorithmic_bytes": face_bytes,
+                             "achieved_from_traffic_gbs": (traffic / (kt["faces"] * 1e-3) / 1e9) if traffic else None,
+                             "traffic_profile_kernel": profile_text("traffic_kernel"),
+                             "note": "achieved/frac use the algorithmic bytes; traffic is the ncu DRAM bytes of "
+                                     "one x+y pair of the profiled kernel",
                              "peak_source": "measured" if peaks else "fallback"},
                 "roofline_fp64": {"achieved": face_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                                   "frac": face_tflops / fp64_peak, "flops_per_face": FLOPS_PER_FACE,

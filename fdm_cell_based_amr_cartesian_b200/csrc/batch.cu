@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(BT, 2) k_bp_hard(BatchArgs A, int krk) {
     __shared__ int64_t s_off[OFF_CAP];
     flat_tiles(A, A.off_hard, s_off, [&](int m, int64_t t) { ph_hard_tile<NRF>(A, krk, m, t); });
 }
-__global__ void __launch_bounds__(BT, 3) k_bp_cells(BatchArgs A, int krk) {
+__global__ void __launch_bounds__(BT) k_bp_cells(BatchArgs A, int krk) {
     __shared__ CellsSmem s_cells;
     __shared__ int64_t s_off[OFF_CAP];
     flat_tiles(A, A.off + PH_CELL * (A.nmem + 1), s_off,

@@ -43,24 +43,29 @@ __device__ __forceinline__ Prim load_prim(const double4 *__restrict__ s, int64_t
 
 // conserved variables and the physical flux of one point
 // (compute_E / compute_F, src/nnd_center_RK.F90:171-185, 293-307)
-template <int DIR>
-__device__ __forceinline__ void cons_flux(const Prim &q, double g, double U[4], double F[4]) {
+template <int DIR, class D>
+__device__ __forceinline__ void cons_flux_d(const Prim &q, D &dv, double U[4], double F[4]) {
     const double ke = q.u * q.u + q.v * q.v;
     U[0] = q.r;
     U[1] = q.r * q.u;
     U[2] = q.r * q.v;
-    U[3] = q.p / (g - 1.0) + 0.5 * q.r * ke;
+    U[3] = dv.q(q.p, dv.gm1) + 0.5 * q.r * ke;
     if (DIR == 0) {
         F[0] = q.r * q.u;
         F[1] = q.r * q.u * q.u + q.p;
         F[2] = q.r * q.u * q.v;
-        F[3] = q.u * (q.p / (g - 1.0) + 0.5 * q.r * ke + q.p);
+        F[3] = q.u * (dv.q(q.p, dv.gm1) + 0.5 * q.r * ke + q.p);
     } else {
         F[0] = q.r * q.v;
         F[1] = q.r * q.u * q.v;
         F[2] = q.r * q.v * q.v + q.p;
-        F[3] = q.v * (q.p / (g - 1.0) + 0.5 * q.r * ke + q.p);
+        F[3] = q.v * (dv.q(q.p, dv.gm1) + 0.5 * q.r * ke + q.p);
     }
+}
+template <int DIR>
+__device__ __forceinline__ void cons_flux(const Prim &q, double g, double U[4], double F[4]) {
+    DivIEEE dv(g);
+    cons_flux_d<DIR>(q, dv, U, F);
 }
 template <int DIR>
 __device__ __forceinline__ void phys_flux(const Prim &q, double g, double F[4]) {
@@ -234,6 +239,47 @@ __device__ __forceinline__ void phys_flux_d(const Prim &q, D &dv, double F[4]) {
         F[3] = q.v * (dv.q(q.p, dv.gm1) + 0.5 * q.r * ke + q.p);
     }
 }
+// The face flux in the reference's order: the four conserved states and the
+// four fluxes formed first, then the projections and reconstructions;
+// every division through the policy dv.
+template <int DIR, class D>
+__device__ __forceinline__ void face_flux_ref_d(const Prim &s0, const Prim &s1, const Prim &s2, const Prim &s3,
+                                                double g, D &dv, double lam, double out[4]) {
+    double U0[4], U1[4], U2[4], U3[4], F0[4], F1[4], F2[4], F3[4];
+    cons_flux_d<DIR>(s0, dv, U0, F0);
+    cons_flux_d<DIR>(s1, dv, U1, F1);
+    cons_flux_d<DIR>(s2, dv, U2, F2);
+    cons_flux_d<DIR>(s3, dv, U3, F3);
+    double Um[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
+    Eig E;
+    eigen_d<DIR>(Um, g, dv, E);
+    double w0[4], w1[4], w2[4], w3[4];
+    double uwL[4], uwR[4], ugL[4], ugR[4];
+    project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
+    project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        uwL[r] = wcns_z3_d(w0[r], w1[r], w2[r], dv);
+        uwR[r] = wcns_z3_d(w3[r], w2[r], w1[r], dv);
+    }
+    project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
+    project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        ugL[r] = wcns_z3_d(w0[r], w1[r], w2[r], dv);
+        ugR[r] = wcns_z3_d(w3[r], w2[r], w1[r], dv);
+    }
+    double wL[4], wR[4], gL[4], gR[4];
+    back_project<DIR>(E, uwL, wL);
+    back_project<DIR>(E, uwR, wR);
+    back_project<DIR>(E, ugL, gL);
+    back_project<DIR>(E, ugR, gR);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
+}
+
 // Numerical flux at the face between s1 and s2 from the 4-point stencil
 // s0..s3 (one half of LXL_X_wcns3 / LXL_Y_wcns3, src/nnd_center_RK.F90:84-106,
 // 205-227): characteristic projection at the face mean, four WCNS_Z3
@@ -288,39 +334,8 @@ __device__ __forceinline__ void face_flux(const Prim &s0, const Prim &s1, const 
     } else {
         // the same values with the four states and fluxes formed first (for
         // the batched kernel, whose register budget this order suits better)
-        double U0[4], U1[4], U2[4], U3[4], F0[4], F1[4], F2[4], F3[4];
-        cons_flux<DIR>(s0, g, U0, F0);
-        cons_flux<DIR>(s1, g, U1, F1);
-        cons_flux<DIR>(s2, g, U2, F2);
-        cons_flux<DIR>(s3, g, U3, F3);
-        double Um[4];
-    #pragma unroll
-        for (int r = 0; r < 4; ++r) Um[r] = (U1[r] + U2[r]) / 2.0;
-        Eig E;
-        eigen<DIR>(Um, g, E);
-        double w0[4], w1[4], w2[4], w3[4];
-        double uwL[4], uwR[4], ugL[4], ugR[4];
-        project<DIR>(E, U0, w0); project<DIR>(E, U1, w1);
-        project<DIR>(E, U2, w2); project<DIR>(E, U3, w3);
-    #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            uwL[r] = wcns_z3(w0[r], w1[r], w2[r]);
-            uwR[r] = wcns_z3(w3[r], w2[r], w1[r]);
-        }
-        project<DIR>(E, F0, w0); project<DIR>(E, F1, w1);
-        project<DIR>(E, F2, w2); project<DIR>(E, F3, w3);
-    #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            ugL[r] = wcns_z3(w0[r], w1[r], w2[r]);
-            ugR[r] = wcns_z3(w3[r], w2[r], w1[r]);
-        }
-        double wL[4], wR[4], gL[4], gR[4];
-        back_project<DIR>(E, uwL, wL);
-        back_project<DIR>(E, uwR, wR);
-        back_project<DIR>(E, ugL, gL);
-        back_project<DIR>(E, ugR, gR);
-    #pragma unroll
-        for (int r = 0; r < 4; ++r) out[r] = 0.5 * (gL[r] + gR[r] - lam * (wR[r] - wL[r]));
+        DivIEEE dv(g);
+        face_flux_ref_d<DIR>(s0, s1, s2, s3, g, dv, lam, out);
     }
 }
 

@@ -62,7 +62,7 @@ struct DivNR {
         const int qhi = __double2hiint(q), qlo = __double2loint(q);
         const unsigned eq = ((unsigned)qhi >> 20) & 0x7ffu;
         // the step moves |q| up when r/b has the sign of q
-        const bool up = ((__double2hiint(r) ^ __double2hiint(b)) >> 31) == ((unsigned)qhi >> 31);
+        const bool up = (((unsigned)__double2hiint(r) ^ (unsigned)__double2hiint(b)) >> 31) == ((unsigned)qhi >> 31);
         const bool pow2 = ((qhi & 0x000fffff) | qlo) == 0;   // gap below |q| is half the gap above
         const unsigned sh = (!up && pow2) ? 54u : 53u;
         const double half_gap = __hiloint2double((int)((eq - sh) << 20), 0);

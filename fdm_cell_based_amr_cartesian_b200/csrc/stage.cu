@@ -68,6 +68,32 @@ __global__ void __launch_bounds__(TB, MINB) k_faces_nr(Tables T, const double4 *
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 
+// One thread per face in the reference's operation order (the four states
+// and fluxes formed first), with the compiler's division (NR false) or the
+// branch-free one (NR true; a face with an operand outside its range is
+// computed again with the compiler's division).
+template <int DIR, int TB, int MINB, bool NR>
+__global__ void __launch_bounds__(TB, MINB) k_faces_ref(Tables T, const double4 *__restrict__ cur, double4 *F,
+                                                        const DevScalars *__restrict__ sc, double g, Den gm1,
+                                                        Den d2) {
+    const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nu = DIR == 0 ? T.nux : T.nuy;
+    if (f >= T.NI + nu) return;
+    int32_t a, b, c, d;
+    face_slots<DIR>(T, f, a, b, c, d);
+    const double lam = DIR == 0 ? sc->lambda_x : sc->lambda_y;
+    const Prim p0 = load_prim(cur, a), p1 = load_prim(cur, b), p2 = load_prim(cur, c), p3 = load_prim(cur, d);
+    double out[4];
+    if constexpr (NR) {
+        DivNR dv(gm1, d2);
+        face_flux_ref_d<DIR>(p0, p1, p2, p3, g, dv, lam, out);
+        if (!dv.ok) face_flux<DIR, false>(p0, p1, p2, p3, g, lam, out);
+    } else {
+        face_flux<DIR, false>(p0, p1, p2, p3, g, lam, out);
+    }
+    F[f] = make_double4(out[0], out[1], out[2], out[3]);
+}
+
 // Four lanes per face (see face_flux in numerics.cuh for the per-face
 // algebra).  All 32 lanes of a warp run the shuffles; lanes past the last
 // face work on a clamped face and do not store.
@@ -246,6 +272,15 @@ static void faces_nr(fdm_handle *h, const double4 *cur) {
     k_faces_nr<0, TB, MINB><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
     k_faces_nr<1, TB, MINB><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
 }
+template <int TB, int MINB, bool NR>
+static void faces_ref(fdm_handle *h, const double4 *cur) {
+    const Tables T = h->tables();
+    const DevScalars *sc = h->scal.as<DevScalars>();
+    const double g = h->G.gama;
+    const Den gm1{g - 1.0, 1.0 / (g - 1.0)}, d2{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};
+    k_faces_ref<0, TB, MINB, NR><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
+    k_faces_ref<1, TB, MINB, NR><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
+}
 static void faces_4lane(fdm_handle *h, const double4 *cur) {
     const Tables T = h->tables();
     const DevScalars *sc = h->scal.as<DevScalars>();
@@ -266,6 +301,10 @@ const char *face_variant_name(int v) {
         case 8: return "1 thread/face, branch-free division, 128 threads, >=4 blocks/SM";
         case 9: return "1 thread/face, branch-free division, 256 threads, >=2 blocks/SM";
         case 10: return "1 thread/face, branch-free division, 64 threads, >=10 blocks/SM";
+        case 11: return "1 thread/face, reference order, 256 threads, >=2 blocks/SM";
+        case 12: return "1 thread/face, reference order, 128 threads, >=4 blocks/SM";
+        case 13: return "1 thread/face, reference order, branch-free division, 256 threads, >=2 blocks/SM";
+        case 14: return "1 thread/face, reference order, branch-free division, 128 threads, >=4 blocks/SM";
         default: return "?";
     }
 }
@@ -290,6 +329,10 @@ void launch_faces(fdm_handle *h, const double4 *cur, int krk) {
         case 8: faces_nr<128, 4>(h, cur); break;
         case 9: faces_nr<256, 2>(h, cur); break;
         case 10: faces_nr<64, 10>(h, cur); break;
+        case 11: faces_ref<256, 2, false>(h, cur); break;
+        case 12: faces_ref<128, 4, false>(h, cur); break;
+        case 13: faces_ref<256, 2, true>(h, cur); break;
+        case 14: faces_ref<128, 4, true>(h, cur); break;
         default: faces_1lane<128, 3>(h, cur); break;
     }
 }
