@@ -152,6 +152,19 @@ def cpu_sample(cfg, keys, prim, lam, tstep, steps):
     return n_int, dt
 
 
+FORTRAN_COMPILERS = ("gfortran", "gfortran-14", "gfortran-13", "gfortran-12", "flang", "flang-new", "ifx", "ifort",
+                     "nvfortran", "pgfortran", "lfortran", "f95", "f77")
+
+
+def fortran_probe() -> str:
+    """Which Fortran compilers this box has (the reference is Fortran only)."""
+    import shutil
+    found = [c for c in FORTRAN_COMPILERS if shutil.which(c)]
+    if found:
+        return "Fortran compilers on the box: " + ", ".join(found) + "; the reference is not built by the bench"
+    return "probed on the box: no Fortran compiler (" + ", ".join(FORTRAN_COMPILERS) + " absent)"
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -186,7 +199,7 @@ def run_reference(args):
             "data": "synthetic", "config": workload_desc(len(keys), n_int),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{len(per)} RK3 steps of the full mesh, OpenMP restatement of "
-                                       "Time_advance_RK (no Fortran compiler on the box)"},
+                                       f"Time_advance_RK ({fortran_probe()})"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0

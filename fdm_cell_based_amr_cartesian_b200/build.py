@@ -68,7 +68,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             if verbose and err:
                 print(err, file=sys.stderr)
     if force or jobs or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-ldl"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-ldl", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {r.stdout}\n{r.stderr}")

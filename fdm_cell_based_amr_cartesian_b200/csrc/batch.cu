@@ -17,8 +17,10 @@
 // that does not complete sets an error word and the kernel returns, which
 // the host reports as FDM_ERR_TIMEOUT.
 #include <algorithm>
+#include <atomic>
 #include <cstddef>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "gate_items.cuh"
@@ -788,6 +790,44 @@ static int launch_member_steps(fdm_batch *b, int64_t nsteps, const std::vector<i
     return join_members(b);
 }
 
+// The regrids of the members due after this step.  They are independent
+// (each member's own tables, buffers and stream), so several run at once,
+// each from its own host thread with the batch's device current; the
+// result of each is the one a serial loop gives.  The first failing member
+// (lowest index) is reported.
+constexpr int REGRID_THREADS = 16;
+static int regrid_due_members(fdm_batch *b) {
+    std::vector<int> due;
+    for (int m = 0; m < (int)b->mem.size(); ++m)
+        if (b->h_skip[m]) due.push_back(m);
+    if (due.empty()) return FDM_OK;
+    std::vector<int> rcs(due.size(), FDM_OK);
+    if (due.size() == 1) {
+        rcs[0] = member_regrid(b->mem[due[0]]);
+    } else {
+        std::atomic<size_t> next{0};
+        auto work = [&]() {
+            if (cudaSetDevice(b->device) != cudaSuccess) return;
+            for (size_t i = next++; i < due.size(); i = next++) rcs[i] = member_regrid(b->mem[due[i]]);
+        };
+        const int nt = (int)std::min<size_t>(due.size(), REGRID_THREADS);
+        std::vector<std::thread> pool;
+        pool.reserve(nt);
+        for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+        for (auto &t : pool) t.join();
+        if (next.load() < due.size()) {   // a thread could not select the device
+            b->err = "regrid threads could not select the device";
+            return FDM_ERR_CUDA;
+        }
+    }
+    for (size_t i = 0; i < due.size(); ++i)
+        if (rcs[i]) {
+            b->err = "member " + std::to_string(due[i]) + " regrid: " + b->mem[due[i]]->err;
+            return rcs[i];
+        }
+    return FDM_OK;
+}
+
 static int check_barrier(fdm_batch *b) {
     if (b->want_bps == 0) {   // no grid barrier: the members' streams
         int rc = join_members(b);
@@ -967,12 +1007,7 @@ int fdm_batch_solute(fdm_batch *b, int64_t nsteps, int64_t *steps_done) {
             }
         }
         if (rc) { ++k; break; }
-        for (int m = 0; m < n && !rc; ++m) {
-            if (!b->h_skip[m]) continue;
-            fdm_handle *h = b->mem[m];
-            rc = member_regrid(h);
-            if (rc) b->err = "member " + std::to_string(m) + " regrid: " + h->err;
-        }
+        rc = regrid_due_members(b);
         if (rc) { ++k; break; }
     }
     if (steps_done) *steps_done = k;
