@@ -30,8 +30,10 @@
 // The steps are exact only away from underflow and overflow, so every
 // operand is checked to lie in [2^-450, 2^450] (or to be zero, whose sign
 // is taken from a*y): then quotients, remainders and half gaps stay normal.
-// An operand outside clears `ok`, and the caller computes the face again
-// with the compiler's division.
+// Smaller numerators are scaled into that range by a power of two and the
+// quotient scaled back (both exact while the quotient is normal).  An
+// operand outside clears `ok`, and the caller computes the face again with
+// the compiler's division.
 #pragma once
 #include "numerics.cuh"
 
@@ -76,21 +78,37 @@ struct DivNR {
         const double y = rcp_newton(b);
         return Den{b, round_quotient(1.0, b, y)};
     }
+    // A numerator below 2^-450 (the characteristic differences of a nearly
+    // constant region square down to such values) is scaled by 2^600, which
+    // is exact, and the quotient scaled back by 2^-600, which is exact while
+    // the quotient stays normal (|q| >= 2^-1022, checked with a margin).
+    __device__ __forceinline__ static bool tiny(double a) {
+        return (((unsigned)__double2hiint(a) >> 20) & 0x7ffu) < 573u;
+    }
+    __device__ __forceinline__ bool unscale_ok(double qs) {
+        return (((unsigned)__double2hiint(qs) >> 20) & 0x7ffu) >= 603u;
+    }
     // a / d.b with y = RN(1/d.b): Markstein's two corrections
     __device__ __forceinline__ double q(double a, const Den &d) {
-        ok = ok && (a == 0.0 || in_range(a));
-        const double q0 = a * d.y;
-        const double q1 = __fma_rn(__fma_rn(-d.b, q0, a), d.y, q0);
-        const double q2 = __fma_rn(__fma_rn(-d.b, q1, a), d.y, q1);
-        return a == 0.0 ? q0 : q2;
+        const bool t = tiny(a);
+        const double as = t ? a * 0x1p600 : a;
+        const double q0 = as * d.y;
+        const double q1 = __fma_rn(__fma_rn(-d.b, q0, as), d.y, q0);
+        const double q2 = __fma_rn(__fma_rn(-d.b, q1, as), d.y, q1);
+        const double qs = as == 0.0 ? q0 : q2;
+        ok = ok && (as == 0.0 || (in_range(as) && (!t || unscale_ok(qs))));
+        return t ? qs * 0x1p-600 : qs;
     }
     // a / b, b used once
     __device__ __forceinline__ double q(double a, double b) {
-        ok = ok && in_range(b) && (a == 0.0 || in_range(a));
+        const bool t = tiny(a);
+        const double as = t ? a * 0x1p600 : a;
         const double y = rcp_newton(b);
-        const double q0 = a * y;
-        const double q1 = __fma_rn(__fma_rn(-b, q0, a), y, q0);   // faithful
-        return a == 0.0 ? q0 : round_quotient(a, b, q1);
+        const double q0 = as * y;
+        const double q1 = __fma_rn(__fma_rn(-b, q0, as), y, q0);   // faithful
+        const double qs = as == 0.0 ? q0 : round_quotient(as, b, q1);
+        ok = ok && in_range(b) && (as == 0.0 || (in_range(as) && (!t || unscale_ok(qs))));
+        return t ? qs * 0x1p-600 : qs;
     }
 };
 
