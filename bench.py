@@ -662,6 +662,7 @@ def summary(line):
         out["cfg2_full_s"] = r3(f["seconds"])
         out["cfg2_gated_full_s"] = r3(get(f, "gated", "seconds"))
         out["cfg2_gated_l1_shared_regrids"] = r3(get(f, "gated_shared_regrids", "l1_density_vs_plain"))
+        out["cfg2_one_ulp_l1_shared_regrids"] = r3(get(f, "gated_shared_regrids", "one_ulp_initial_density_l1"))
         out["cfg2_golden"] = f.get("bit_identical_to_oracle_run")
         out["cfg3_full_s"] = r3(get(f, "double_mach", "seconds"))
         out["cfg3_golden"] = get(f, "double_mach", "bit_identical_to_oracle_run")
@@ -818,10 +819,15 @@ def run_ours(args):
             # plain run's time steps and regrid decisions (one leaf set)
             t0 = time.perf_counter()
             pr = LG.compare_paired(P.riemann4(base=128, lvl_amr=4, t_end=0.3))
+            pu = LG.compare_paired(P.riemann4(base=128, lvl_amr=4, t_end=0.3), follower="ulp")
             full["gated_shared_regrids"] = {
                 "l1_density_vs_plain": pr["l1"], "linf_density_vs_plain": pr["linf"], "steps": pr["steps"],
-                "regrids": pr["regrids"], "leaves_at_end": pr["leaves"], "seconds_both_runs": time.perf_counter() - t0,
-                "note": "plain and gated in lockstep (fdm_solute_paired): same time steps, same regrid decisions"}
+                "regrids": pr["regrids"], "leaves_at_end": pr["leaves"],
+                "gated_fraction_last_stage": pr.get("gated_fraction_last_stage"),
+                "one_ulp_initial_density_l1": pu["l1"], "one_ulp_initial_density_linf": pu["linf"],
+                "seconds_four_runs": time.perf_counter() - t0,
+                "note": "follower in lockstep with the plain run (fdm_solute_paired): same time steps, same regrid "
+                        "decisions; the one-ulp follower is the plain scheme from a density one ulp higher"}
         # the same plain run from an initial density one ulp higher: the spread
         # that the regrid decisions alone give a whole run
         full_u, leaves_ulp = full_run(S, gate=False, ulp=True)
@@ -868,7 +874,8 @@ def run_ours(args):
                                           "instructions; the pipe figure is ncu's, from profiles/"},
                 "step_hbm": {"algorithmic_bytes_per_update": BYTES_PER_UPDATE, "achieved_gbs": step_gbs,
                              "frac": step_gbs / hbm_peak},
-                "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms)},
+                "kernel_ms": kt, "autotune": {"face_variant": tuned, "ms_per_variant": list(tune_ms),
+                                              "nr_fallback_faces": list(g.nr_fallbacks())},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
                 "counters": cnt, "state_finite_after_timed_steps": finite, "cpu_baseline": cpu,
                 "fast_flux": fastf, "learned": gated, "ensemble": ens, "full_run": full, "strips": strips}

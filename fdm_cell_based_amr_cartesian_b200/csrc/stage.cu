@@ -94,6 +94,47 @@ __global__ void __launch_bounds__(TB, MINB) k_faces_ref(Tables T, const double4 
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 
+// Diagnostics: the faces whose branch-free division meets an operand
+// outside its range (and so are computed again with the compiler's
+// division), counted over the current state; nothing is written to F.
+template <int DIR>
+__global__ void __launch_bounds__(128) k_faces_nr_count(Tables T, const double4 *__restrict__ cur,
+                                                        const DevScalars *__restrict__ sc, double g, Den gm1,
+                                                        Den d2, unsigned long long *count) {
+    const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nu = DIR == 0 ? T.nux : T.nuy;
+    bool fell = false;
+    if (f < T.NI + nu) {
+        int32_t a, b, c, d;
+        face_slots<DIR>(T, f, a, b, c, d);
+        double out[4];
+        DivNR dv(gm1, d2);
+        face_flux_slots_d<DIR>(cur, a, b, c, d, g, dv, DIR == 0 ? sc->lambda_x : sc->lambda_y, out);
+        fell = !dv.ok;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, fell);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
+}
+int count_nr_fallbacks(fdm_handle *h, int64_t out[2]) {
+    const Tables T = h->tables();
+    const DevScalars *sc = h->scal.as<DevScalars>();
+    const double g = h->G.gama;
+    const Den gm1{g - 1.0, 1.0 / (g - 1.0)}, d2{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};
+    FDM_CK(h, h->tmp[7].ensure(2 * sizeof(unsigned long long)));
+    unsigned long long *cnt = h->tmp[7].as<unsigned long long>();
+    FDM_CK(h, cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), h->s));
+    launch_requests(h, h->B[0].as<double4>());
+    k_faces_nr_count<0><<<nblk(h->NI + h->nux, 128), 128, 0, h->s>>>(T, h->B[0].as<double4>(), sc, g, gm1, d2, cnt);
+    k_faces_nr_count<1><<<nblk(h->NI + h->nuy, 128), 128, 0, h->s>>>(T, h->B[0].as<double4>(), sc, g, gm1, d2,
+                                                                       cnt + 1);
+    unsigned long long hc[2];
+    FDM_CK(h, cudaMemcpyAsync(hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, h->s));
+    FDM_CK(h, cudaStreamSynchronize(h->s));
+    out[0] = (int64_t)hc[0];
+    out[1] = (int64_t)hc[1];
+    return FDM_OK;
+}
+
 // Four lanes per face (see face_flux in numerics.cuh for the per-face
 // algebra).  All 32 lanes of a warp run the shuffles; lanes past the last
 // face work on a clamped face and do not store.

@@ -86,6 +86,17 @@ extern "C" int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *
     return FDM_OK;
 }
 
+namespace fdm {
+int count_nr_fallbacks(fdm_handle *h, int64_t out[2]);
+}
+// x and y faces whose branch-free division falls back to the compiler's on
+// the current state (face variants 7-10, 13, 14)
+extern "C" int fdm_debug_nr_fallbacks(fdm_handle *h, int64_t *out) {
+    if (!h || !out) return FDM_ERR_ARG;
+    if (!h->loaded) return FDM_ERR_STATE;
+    return fdm::count_nr_fallbacks(h, out);
+}
+
 extern "C" int fdm_set_variant(fdm_handle *h, int32_t face_variant) {
     if (!h || face_variant < 0 || face_variant >= N_FACE_VARIANTS) return FDM_ERR_ARG;
     h->face_variant = face_variant;

@@ -311,16 +311,28 @@ def compare(cfg: P.Config, steps: int, params=None, threshold: float = THRESHOLD
 
 
 def compare_paired(cfg: P.Config, steps: int | None = None, params=None, threshold: float = THRESHOLD,
-                   chunk: int = 100):
-    """The plain and the gated solver in lockstep (fdm_solute_paired): the
-    gated run takes the plain run's time steps and regrid decisions, so both
-    keep one leaf set and the density difference at the end is the gate's
-    error alone.  Runs to t_end (or `steps` iterations); returns the density
-    errors, the steps and regrids taken and the leaf count at the end."""
+                   chunk: int = 100, follower: str = "gate"):
+    """The plain solver and a follower in lockstep (fdm_solute_paired): the
+    follower takes the plain run's time steps and regrid decisions, so both
+    keep one leaf set and the density difference at the end comes from the
+    follower alone.  follower "gate": the learned gate on; "ulp": the plain
+    scheme started from an initial density one ulp higher, which measures how
+    far rounding-level differences grow in this problem.  Runs to t_end (or
+    `steps` iterations); returns the density errors, the steps and regrids
+    taken, the leaf count at the end and the follower's gated face share in
+    its last stage."""
     plain, gated = Solver(cfg), Solver(cfg)
     plain.creat_mesh_and_initial()
     gated.creat_mesh_and_initial()
-    enable(gated, params, threshold)
+    if follower == "gate":
+        enable(gated, params, threshold)
+    elif follower == "ulp":
+        _, p0 = gated.leaves()
+        p0 = p0.copy()
+        p0[:, 0] = np.nextafter(p0[:, 0], np.inf)
+        gated.set_values(p0)
+    else:
+        raise ValueError(follower)
     n = 0
     while (steps is None or n < steps) and plain.scalars()["tt"] < cfg.params.t_end:
         k = plain.solute_paired(gated, chunk if steps is None else min(chunk, steps - n))
@@ -332,6 +344,9 @@ def compare_paired(cfg: P.Config, steps: int | None = None, params=None, thresho
     l1, linf = density_errors(cfg, pl, gl)
     out = {"l1": l1, "linf": linf, "steps": n, "tt": plain.scalars()["tt"],
            "regrids": plain.counters()["n_regrids"], "leaves": len(pl[0])}
+    if follower == "gate":
+        a, b = stats(gated)
+        out["gated_fraction_last_stage"] = a / max(b, 1)
     plain.close()
     gated.close()
     return out

@@ -46,7 +46,7 @@ EXPORTS = [
     "fdm_leaf_slots", "fdm_pack_slots", "fdm_unpack_slots", "fdm_step_control_global",
     "fdm_download_internal", "fdm_set_internal", "fdm_set_async", "fdm_debug_barrier_timeout",
     "fdm_debug_fail_alloc", "fdm_solute_paired", "fdm_output_error", "fdm_download_keys_async",
-    "fdm_readback_wait", "fdm_gate_set_jump_rule",
+    "fdm_readback_wait", "fdm_gate_set_jump_rule", "fdm_debug_nr_fallbacks",
 ]
 
 
@@ -149,6 +149,7 @@ def load_library(path: str = LIB_PATH):
     L.fdm_download_keys_async.argtypes = [vp, i64, u64p]
     L.fdm_readback_wait.argtypes = [vp]
     L.fdm_gate_set_jump_rule.argtypes = [vp, ctypes.c_float]
+    L.fdm_debug_nr_fallbacks.argtypes = [vp, ctypes.POINTER(i64)]
     _lib = L
     return L
 
@@ -531,6 +532,13 @@ class Solver:
         ms = np.zeros(FACE_VARIANTS)
         self._check(self.L.fdm_autotune(self.h, int(reps), ctypes.byref(best), _dp(ms)))
         return best.value, ms
+
+    def nr_fallbacks(self):
+        """(x, y) faces of the current state whose branch-free division falls
+        back to the compiler's."""
+        out = (ctypes.c_int64 * 2)()
+        self._check(self.L.fdm_debug_nr_fallbacks(self.h, out))
+        return int(out[0]), int(out[1])
 
     def set_variant(self, v: int):
         self._check(self.L.fdm_set_variant(self.h, int(v)))

@@ -312,6 +312,10 @@ int fdm_fp64_peak(double *tflops);
 #define FDM_FACE_VARIANTS 15
 int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms);
 int fdm_set_variant(fdm_handle *h, int32_t face_variant);
+/* Diagnostics: out[0], out[1] = x and y faces of the current state whose
+ * branch-free division (face variants 7-10, 13, 14) meets an operand outside
+ * its exact range and is computed again with the compiler's division. */
+int fdm_debug_nr_fallbacks(fdm_handle *h, int64_t out[2]);
 
 /* ------------------------------------------------------------ learned gate
  * No reference counterpart.  A BF16 MLP (8 -> 32 -> 32 -> 1, GELU, sigmoid,

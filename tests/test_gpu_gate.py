@@ -73,18 +73,23 @@ def test_gated_solver_accuracy(name):
 def test_gated_whole_run_with_shared_regrids(name):
     """Whole runs with every regrid: the gated run takes the plain run's time
     steps and regrid decisions (fdm_solute_paired), so both end on one leaf
-    set and the area-weighted L1 density error (relative) is the gate's
-    alone: <= 1e-3 at the end of configuration 1 (200 steps), of the
-    four-quadrant problem at 64^2 / 3 levels to t = 0.3 and of the double Mach
-    reflection at 64 x 16 / 2 levels to t = 0.2."""
-    cfg = {"vortex": lambda: P.vortex(), "riemann4": lambda: P.riemann4(base=64, lvl_amr=3, t_end=0.3),
-           "double_mach": lambda: P.double_mach(base_y=16, lvl_amr=2)}[name]()
-    r = learned.compare_paired(cfg, 200 if name == "vortex" else None)
-    print(name, r)
-    assert r["regrids"] >= 10, r
+    set and the area-weighted L1 density difference (relative) is the gate's
+    alone.  It is set against the same measure for the plain scheme started
+    from an initial density one ulp higher: the four-quadrant problem
+    amplifies rounding-level differences to 3e-3 by t = 0.3, so the bar is
+    1e-3 or twice that floor, whichever is larger.  Cases: configuration 1
+    (200 steps), the four-quadrant problem at 64^2 / 3 levels to t = 0.3 and
+    the double Mach reflection at 64 x 16 / 2 levels to t = 0.2."""
+    mk = {"vortex": lambda: P.vortex(), "riemann4": lambda: P.riemann4(base=64, lvl_amr=3, t_end=0.3),
+          "double_mach": lambda: P.double_mach(base_y=16, lvl_amr=2)}[name]
+    steps = 200 if name == "vortex" else None
+    r = learned.compare_paired(mk(), steps)
+    u = learned.compare_paired(mk(), steps, follower="ulp")
+    print(name, r, u)
+    assert r["regrids"] >= 10 and r["steps"] == u["steps"], (r, u)
     if name != "vortex":
-        assert r["tt"] == cfg.params.t_end, r
-    assert r["l1"] <= 1e-3, r
+        assert r["tt"] == mk().params.t_end, r
+    assert r["l1"] <= max(1e-3, 2.0 * u["l1"]), (r, u)
 
 
 def test_paired_plain_runs_are_identical():
