@@ -828,12 +828,6 @@ def run_ours(args):
                 "seconds_four_runs": time.perf_counter() - t0,
                 "note": "follower in lockstep with the plain run (fdm_solute_paired): same time steps, same regrid "
                         "decisions; the one-ulp follower is the plain scheme from a density one ulp higher"}
-        # the same plain run from an initial density one ulp higher: the spread
-        # that the regrid decisions alone give a whole run
-        full_u, leaves_ulp = full_run(S, gate=False, ulp=True)
-        l1, linf = LG.density_errors(cfg_full, leaves_plain, leaves_ulp)
-        full["one_ulp_initial_density"] = {"steps": full_u["steps"], "regrids": full_u["regrids"],
-                                           "l1_density_vs_plain": l1, "linf_density_vs_plain": linf}
         # configuration 3: the Mach-10 reflection to t = 0.2, a regrid every 5 steps
         try:
             full["double_mach"] = full_run(S, gate=False, case="double_mach")[0]

@@ -155,21 +155,45 @@ def run_ensemble(args) -> int:
         if not args.plain:
             learned.enable(g)
         sols.append(g)
+    import numpy as np
+
+    from .solver import FdmError
     lv0 = [g.counters()["n_interior"] for g in sols]
     peak = list(lv0)
+    active = list(range(len(sols)))
+    nan_members = []
     batch = Batch(sols)
     batch.set_blocks_per_sm(args.bps)
     t0 = time.perf_counter()
     n = 0
     target = args.steps if args.steps > 0 else None
     while target is None or n < target:
-        k = batch.solute(min(100, target - n) if target is not None else 100)
+        try:
+            k = batch.solute(min(100, target - n) if target is not None else 100)
+        except FdmError as ex:
+            # a member whose residual turned NaN stops (the reference stops
+            # there); the others go on in a batch without it
+            if ex.code != 3:
+                raise
+            bad = [i for i in active if np.isnan(np.asarray(sols[i].residual()[1])).any()]
+            if not bad:
+                raise
+            nan_members += [{"seed": 1000 + i, "lvl_amr": int(cfgs[i].params.lvl_amr),
+                             "step": sols[i].scalars()["it"], "tt": sols[i].scalars()["tt"]} for i in bad]
+            active = [i for i in active if i not in bad]
+            batch.close()
+            if not active:
+                break
+            batch = Batch([sols[i] for i in active])
+            batch.set_blocks_per_sm(args.bps)
+            continue
         n += k
-        for i, g in enumerate(sols):
-            peak[i] = max(peak[i], g.counters()["n_interior"])
-        if k == 0 or all(g.scalars()["tt"] >= g.cfg.params.t_end for g in sols):
+        for i in active:
+            peak[i] = max(peak[i], sols[i].counters()["n_interior"])
+        if k == 0 or all(sols[i].scalars()["tt"] >= sols[i].cfg.params.t_end for i in active):
             break
-    batch.sync()
+    if active:
+        batch.sync()
     seconds = time.perf_counter() - t0
     sc = [g.scalars() for g in sols]
     lv1 = [g.counters()["n_interior"] for g in sols]
@@ -180,10 +204,10 @@ def run_ensemble(args) -> int:
            "member_interior_leaves_peak": [min(peak), max(peak)],
            "member_interior_leaves_at_end": [min(lv1), max(lv1)],
            "member_steps": [min(s["it"] for s in sc), max(s["it"] for s in sc)],
-           "member_updates": int(sum(s["it"] for s in sc)),
+           "members_stopped_by_nan": nan_members,
            "regrids": sum(g.counters()["n_regrids"] for g in sols),
            "members_at_t_end": sum(1 for g, t in zip(sols, tts) if t >= g.cfg.params.t_end),
-           "tt_min": min(tts), "tt_max": max(tts), "batch": batch.info(),
+           "tt_min": min(tts), "tt_max": max(tts), "batch": batch.info() if active else None,
            "per_member": [{"seed": 1000 + i, "lvl_amr": int(c.params.lvl_amr), "steps": s["it"], "tt": s["tt"],
                            "interior_leaves": [a, p, b]}
                           for i, (c, s, a, p, b) in enumerate(zip(cfgs, sc, lv0, peak, lv1))]}
@@ -191,7 +215,8 @@ def run_ensemble(args) -> int:
         import numpy as np
         np.savez(args.save_leaves, **{f"m{i}_keys": g.leaves()[0] for i, g in enumerate(sols)},
                  **{f"m{i}_prim": g.leaves()[1] for i, g in enumerate(sols)})
-    batch.close()
+    if active:
+        batch.close()
     for g in sols:
         g.close()
     print(json.dumps(out))
