@@ -112,4 +112,33 @@ struct DivNR {
     }
 };
 
+// Division by the two constant denominators (gama - 1 and d2 of WCNS_Z3)
+// with one correction, every other division as the compiler forms it.
+// With y = RN(1/c) from the host, q0 = RN(a*y) is already within one ulp of
+// a/c for every a when |y*c - 1| < 2^-54 (the error of a*y is then below
+// 0.86 ulp of a/c); y*c - 1 is -2^-72 for gama - 1 and -2^-54.46 for d2, so
+// one correction q0 + (a - c*q0)*y gives RN(a/c) by Markstein's theorem.
+// Numerators below 2^-450 are scaled as in DivNR; any other operand outside
+// the range clears ok (the caller computes the face again).
+struct DenC {
+    double b, y;
+};
+struct DivConst {
+    DenC gm1, d2;
+    bool ok = true;
+    __device__ __forceinline__ DivConst(DenC g1, DenC dd) : gm1(g1), d2(dd) {}
+    __device__ __forceinline__ Den den(double b) const { return Den{b, 0.0}; }
+    __device__ __forceinline__ double q(double a, const Den &d) const { return a / d.b; }
+    __device__ __forceinline__ double q(double a, double b) const { return a / b; }
+    __device__ __forceinline__ double q(double a, const DenC &d) {
+        const bool t = DivNR::tiny(a);
+        const double as = t ? a * 0x1p600 : a;
+        const double q0 = as * d.y;
+        const double q1 = __fma_rn(__fma_rn(-d.b, q0, as), d.y, q0);
+        const double qs = as == 0.0 ? q0 : q1;
+        ok = ok && (as == 0.0 || (DivNR::in_range(as) && (!t || (((unsigned)__double2hiint(qs) >> 20) & 0x7ffu) >= 603u)));
+        return t ? qs * 0x1p-600 : qs;
+    }
+};
+
 }  // namespace fdm

@@ -94,6 +94,34 @@ __global__ void __launch_bounds__(TB, MINB) k_faces_ref(Tables T, const double4 
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
 
+// The faces with the constant denominators divided by one correction
+// (DivConst, numerics_nr.cuh), every other division as the compiler forms
+// it; SPLIT: the split order (state half, then flux half), else the
+// reference's order.  A face with an operand outside the range is computed
+// again with the compiler's division.
+template <int DIR, int TB, int MINB, bool SPLIT>
+__global__ void __launch_bounds__(TB, MINB) k_faces_c(Tables T, const double4 *__restrict__ cur, double4 *F,
+                                                      const DevScalars *__restrict__ sc, double g, DenC gm1,
+                                                      DenC d2) {
+    const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nu = DIR == 0 ? T.nux : T.nuy;
+    if (f >= T.NI + nu) return;
+    int32_t a, b, c, d;
+    face_slots<DIR>(T, f, a, b, c, d);
+    const double lam = DIR == 0 ? sc->lambda_x : sc->lambda_y;
+    double out[4];
+    DivConst dv(gm1, d2);
+    if constexpr (SPLIT) {
+        face_flux_slots_d<DIR>(cur, a, b, c, d, g, dv, lam, out);
+        if (!dv.ok) face_flux_slots<DIR>(cur, a, b, c, d, g, lam, out);
+    } else {
+        const Prim p0 = load_prim(cur, a), p1 = load_prim(cur, b), p2 = load_prim(cur, c), p3 = load_prim(cur, d);
+        face_flux_ref_d<DIR>(p0, p1, p2, p3, g, dv, lam, out);
+        if (!dv.ok) face_flux<DIR, false>(p0, p1, p2, p3, g, lam, out);
+    }
+    F[f] = make_double4(out[0], out[1], out[2], out[3]);
+}
+
 // Diagnostics: the faces whose branch-free division meets an operand
 // outside its range (and so are computed again with the compiler's
 // division), counted over the current state; nothing is written to F.
@@ -322,6 +350,15 @@ static void faces_ref(fdm_handle *h, const double4 *cur) {
     k_faces_ref<0, TB, MINB, NR><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
     k_faces_ref<1, TB, MINB, NR><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
 }
+template <int TB, int MINB, bool SPLIT>
+static void faces_c(fdm_handle *h, const double4 *cur) {
+    const Tables T = h->tables();
+    const DevScalars *sc = h->scal.as<DevScalars>();
+    const double g = h->G.gama;
+    const DenC gm1{g - 1.0, 1.0 / (g - 1.0)}, d2{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};
+    k_faces_c<0, TB, MINB, SPLIT><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
+    k_faces_c<1, TB, MINB, SPLIT><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
+}
 static void faces_4lane(fdm_handle *h, const double4 *cur) {
     const Tables T = h->tables();
     const DevScalars *sc = h->scal.as<DevScalars>();
@@ -346,6 +383,9 @@ const char *face_variant_name(int v) {
         case 12: return "1 thread/face, reference order, 128 threads, >=4 blocks/SM";
         case 13: return "1 thread/face, reference order, branch-free division, 256 threads, >=2 blocks/SM";
         case 14: return "1 thread/face, reference order, branch-free division, 128 threads, >=4 blocks/SM";
+        case 15: return "1 thread/face, constant divisors by one correction, 256 threads, >=2 blocks/SM";
+        case 16: return "1 thread/face, constant divisors by one correction, 64 threads, >=10 blocks/SM";
+        case 17: return "1 thread/face, reference order, constant divisors by one correction, 256 threads, >=2 blocks/SM";
         default: return "?";
     }
 }
@@ -374,6 +414,9 @@ void launch_faces(fdm_handle *h, const double4 *cur, int krk) {
         case 12: faces_ref<128, 4, false>(h, cur); break;
         case 13: faces_ref<256, 2, true>(h, cur); break;
         case 14: faces_ref<128, 4, true>(h, cur); break;
+        case 15: faces_c<256, 2, true>(h, cur); break;
+        case 16: faces_c<64, 10, true>(h, cur); break;
+        case 17: faces_c<256, 2, false>(h, cur); break;
         default: faces_1lane<128, 3>(h, cur); break;
     }
 }
