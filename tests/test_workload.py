@@ -68,3 +68,21 @@ def test_bench_golden_check(tmp_path, monkeypatch):
     # every full run names its configuration and golden record
     for name, (make, desc, golden) in bench.FULL_RUNS.items():
         assert make().params.t_end > 0 and desc and golden
+
+
+def test_bench_summary_tolerates_missing_legs():
+    """The compact summary at the end of the bench line is built from
+    whatever legs ran (a leg that failed or was skipped leaves no key)."""
+    import bench
+    line = {"ms_per_step": 1.5, "roofline": {"ms_per_launch": 0.39, "frac": 0.04},
+            "roofline_fp64": {"frac": 0.2}, "learned": {"error": "x"}, "ensemble": None, "full_run": None,
+            "strips": {"error": "y"}}
+    s = bench.summary(line)
+    assert s["plain_ms_per_step"] == 1.5 and s["face_pair_ms"] == 0.39
+    assert "gated_ms_per_step" not in s and "cfg2_full_s" not in s
+    line["learned"] = {"ms_per_step": 0.75, "l1_density_vs_plain": 5e-7,
+                       "rule_vs_network": {"network": {"l1_density_vs_plain": 1e-7, "stage1_gated_fraction": 0.9},
+                                           "jump_rule": {"l1_density_vs_plain": 2e-7,
+                                                         "stage1_gated_fraction": 0.9}}}
+    s = bench.summary(line)
+    assert s["gated_speedup"] == 2.0 and s["net_vs_rule_l1"] == [1e-7, 2e-7]
