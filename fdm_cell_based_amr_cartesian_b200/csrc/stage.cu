@@ -15,6 +15,7 @@
 #include "items.cuh"
 #include "numerics.cuh"
 #include "numerics_nr.cuh"
+#include "numerics_sm.cuh"
 
 namespace fdm {
 
@@ -118,6 +119,29 @@ __global__ void __launch_bounds__(TB, MINB) k_faces_c(Tables T, const double4 *_
         const Prim p0 = load_prim(cur, a), p1 = load_prim(cur, b), p2 = load_prim(cur, c), p3 = load_prim(cur, d);
         face_flux_ref_d<DIR>(p0, p1, p2, p3, g, dv, lam, out);
         if (!dv.ok) face_flux<DIR, false>(p0, p1, p2, p3, g, lam, out);
+    }
+    F[f] = make_double4(out[0], out[1], out[2], out[3]);
+}
+
+// Variant 15's arithmetic with the face's characteristic basis in shared
+// memory (numerics_sm.cuh): fewer live registers, so more warps per SM.
+template <int DIR, int TB, int MINB>
+__global__ void __launch_bounds__(TB, MINB) k_faces_sm(Tables T, const double4 *__restrict__ cur, double4 *F,
+                                                       const DevScalars *__restrict__ sc, double g, DenC gm1,
+                                                       DenC d2) {
+    __shared__ EigShared<TB> S;
+    const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nu = DIR == 0 ? T.nux : T.nuy;
+    if (f >= T.NI + nu) return;
+    int32_t a, b, c, d;
+    face_slots<DIR>(T, f, a, b, c, d);
+    const double lam = DIR == 0 ? sc->lambda_x : sc->lambda_y;
+    double out[4];
+    DivConst dv(gm1, d2);
+    face_flux_slots_sm<DIR, TB>(cur, a, b, c, d, g, dv, lam, S, threadIdx.x, out);
+    if (!dv.ok) {   // the compiler's division, the basis again in shared memory
+        DivIEEE di(g);
+        face_flux_slots_sm<DIR, TB>(cur, a, b, c, d, g, di, lam, S, threadIdx.x, out);
     }
     F[f] = make_double4(out[0], out[1], out[2], out[3]);
 }
@@ -359,6 +383,15 @@ static void faces_c(fdm_handle *h, const double4 *cur) {
     k_faces_c<0, TB, MINB, SPLIT><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
     k_faces_c<1, TB, MINB, SPLIT><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
 }
+template <int TB, int MINB>
+static void faces_sm(fdm_handle *h, const double4 *cur) {
+    const Tables T = h->tables();
+    const DevScalars *sc = h->scal.as<DevScalars>();
+    const double g = h->G.gama;
+    const DenC gm1{g - 1.0, 1.0 / (g - 1.0)}, d2{FDM_D2_WCNS, 1.0 / FDM_D2_WCNS};
+    k_faces_sm<0, TB, MINB><<<nblk(h->NI + h->nux, TB), TB, 0, h->s>>>(T, cur, h->Fx.as<double4>(), sc, g, gm1, d2);
+    k_faces_sm<1, TB, MINB><<<nblk(h->NI + h->nuy, TB), TB, 0, h->s>>>(T, cur, h->Fy.as<double4>(), sc, g, gm1, d2);
+}
 static void faces_4lane(fdm_handle *h, const double4 *cur) {
     const Tables T = h->tables();
     const DevScalars *sc = h->scal.as<DevScalars>();
@@ -386,6 +419,9 @@ const char *face_variant_name(int v) {
         case 15: return "1 thread/face, constant divisors by one correction, 256 threads, >=2 blocks/SM";
         case 16: return "1 thread/face, constant divisors by one correction, 64 threads, >=10 blocks/SM";
         case 17: return "1 thread/face, reference order, constant divisors by one correction, 256 threads, >=2 blocks/SM";
+        case 18: return "1 thread/face, variant 15 with the basis in shared memory, 128 threads, >=4 blocks/SM";
+        case 19: return "1 thread/face, variant 15 with the basis in shared memory, 128 threads, >=5 blocks/SM";
+        case 20: return "1 thread/face, variant 15 with the basis in shared memory, 128 threads, >=6 blocks/SM";
         default: return "?";
     }
 }
@@ -417,6 +453,9 @@ void launch_faces(fdm_handle *h, const double4 *cur, int krk) {
         case 15: faces_c<256, 2, true>(h, cur); break;
         case 16: faces_c<64, 10, true>(h, cur); break;
         case 17: faces_c<256, 2, false>(h, cur); break;
+        case 18: faces_sm<128, 4>(h, cur); break;
+        case 19: faces_sm<128, 5>(h, cur); break;
+        case 20: faces_sm<128, 6>(h, cur); break;
         default: faces_1lane<128, 3>(h, cur); break;
     }
 }

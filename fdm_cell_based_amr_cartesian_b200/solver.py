@@ -27,7 +27,7 @@ FDM_ERR_NAN = 3
 ERRORS = {1: "FDM_ERR_ARG", 2: "FDM_ERR_CUDA", 3: "FDM_ERR_NAN", 4: "FDM_ERR_TIMEOUT",
           5: "FDM_ERR_NOMEM", 6: "FDM_ERR_STATE", 7: "FDM_ERR_UNSUPPORTED"}
 
-FACE_VARIANTS = 18   # FDM_FACE_VARIANTS of include/fdm.h
+FACE_VARIANTS = 21   # FDM_FACE_VARIANTS of include/fdm.h
 
 # every extern "C" symbol declared in include/fdm.h
 EXPORTS = [

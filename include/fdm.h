@@ -309,7 +309,7 @@ int fdm_fp64_peak(double *tflops);
  * FDM_FACE_VARIANTS variants on the current leaf set (ms[v] = ms per x+y
  * launch pair; ms holds FDM_FACE_VARIANTS doubles), keeps the fastest for
  * this handle and reports it in *best.  fdm_set_variant forces one. */
-#define FDM_FACE_VARIANTS 18
+#define FDM_FACE_VARIANTS 21
 int fdm_autotune(fdm_handle *h, int32_t reps, int32_t *best, double *ms);
 int fdm_set_variant(fdm_handle *h, int32_t face_variant);
 /* Diagnostics: out[0], out[1] = x and y faces of the current state whose
