@@ -2,6 +2,7 @@
 #include <cub/cub.cuh>
 
 #include "handle.cuh"
+#include "ordered_sum.cuh"
 #include "topo.cuh"
 
 namespace fdm {
@@ -46,47 +47,14 @@ __global__ void k_ordered_squares(int64_t NI, const int32_t *__restrict__ order,
 }
 
 // Srot, Sdiv: left-to-right sums in traversal order, as the reference's
-// recursive loop forms them (one lane adds; the warp streams the squares
-// through shared memory with cp.async, one chunk ahead)
-constexpr int SUM_CHUNK = 1024;   // double2 per chunk: 16 KB
-__device__ __forceinline__ void cp16(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__global__ void __launch_bounds__(32) k_ordered_sums(int64_t NI, const double2 *__restrict__ sq, double *out) {
-    __shared__ double2 buf[2][SUM_CHUNK];
-    const int lane = threadIdx.x;
-    const int64_t nch = (NI + SUM_CHUNK - 1) / SUM_CHUNK;
-    auto fetch = [&](int64_t c) {
-        const int64_t base = c * SUM_CHUNK;
-        for (int j = lane; j < SUM_CHUNK; j += 32)
-            if (base + j < NI) cp16(&buf[c & 1][j], sq + base + j);
-        asm volatile("cp.async.commit_group;\n" ::);
-    };
-    double sr = 0.0, sd = 0.0;
-    if (nch > 0) fetch(0);
-    for (int64_t c = 0; c < nch; ++c) {
-        if (c + 1 < nch) {
-            fetch(c + 1);
-            asm volatile("cp.async.wait_group 1;\n" ::);
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            const int64_t rest = NI - c * SUM_CHUNK;
-            const int m = rest < SUM_CHUNK ? (int)rest : SUM_CHUNK;
-            const double2 *b = buf[c & 1];
-#pragma unroll 8
-            for (int j = 0; j < m; ++j) {
-                const double2 v = b[j];
-                sr = sr + v.x;
-                sd = sd + v.y;
-            }
-        }
-        __syncwarp();
-    }
-    if (lane == 0) {
+// recursive loop forms them (src/solution.F90:430-457), bit for bit, by one
+// block (ordered_sum.cuh)
+__global__ void __launch_bounds__(OSUM_NT) k_ordered_sums(int64_t NI, const double2 *__restrict__ sq, double *out) {
+    __shared__ OSumShared sh;
+    const double *x = reinterpret_cast<const double *>(sq);
+    const double sr = ordered_sum_block<OSUM_NT, OSUM_EPT>(x, 2, NI, sh);
+    const double sd = ordered_sum_block<OSUM_NT, OSUM_EPT>(x + 1, 2, NI, sh);
+    if (threadIdx.x == 0) {
         out[0] = sr;
         out[1] = sd;
         out[2] = (double)NI;
@@ -111,7 +79,7 @@ static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3
     FDM_CK(h, h->cub_tmp.ensure(bytes));
     FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, k0, k1, i0, i1, (int)NI, 0, kb, h->s));
     k_ordered_squares<<<nblk(NI, 256), 256, 0, h->s>>>(NI, i1, rot, div, sq);
-    k_ordered_sums<<<1, 32, 0, h->s>>>(NI, sq, out3);
+    k_ordered_sums<<<1, OSUM_NT, 0, h->s>>>(NI, sq, out3);
     return FDM_OK;
 }
 
@@ -128,6 +96,8 @@ struct NodeSet {
     uint64_t *key = nullptr;
     uint8_t *leaf = nullptr;
     double4 *val = nullptr;
+    const int32_t *rf = nullptr;   // per-cell index of key (index_set), or null
+    int64_t nroots = 0;
 };
 
 enum { D_NONE = 0, D_REFINE = 1, D_COARSEN = 2 };
@@ -142,6 +112,34 @@ __device__ __forceinline__ int64_t find_key(const uint64_t *__restrict__ keys, i
         else hi = mid;
     }
     return (lo < n && keys[lo] == k) ? lo : -1;
+}
+
+// find_key within the nodes of k's background cell when the set is indexed
+// (every cell holds at least its root node, and its nodes are contiguous)
+__device__ __forceinline__ int64_t find_key_set(const NodeSet &A, uint64_t k) {
+    const int64_t r = (int64_t)(k >> 34);
+    if (!A.rf || r >= A.nroots) return find_key(A.key, A.n, k);
+    int64_t lo = __ldg(A.rf + r), hi = __ldg(A.rf + r + 1);
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const uint64_t v = A.key[mid];
+        if (v < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < A.n && A.key[lo] == k) ? lo : -1;
+}
+
+// find_key on the leaf table, within k's background cell (T.rfirst)
+__device__ __forceinline__ int64_t find_key_t(const Tables &T, uint64_t k) {
+    const int64_t r = (int64_t)(k >> 34);
+    if (!T.rfirst || r >= T.nroots) return find_key_t(T, k);
+    int64_t lo = __ldg(T.rfirst + r), hi = __ldg(T.rfirst + r + 1);
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldg(T.lkey + mid) < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < T.NL && __ldg(T.lkey + lo) == k) ? lo : -1;
 }
 
 // The helpers below work on the interleaved path bits directly.  Level j's
@@ -311,6 +309,7 @@ static void bind_sets(fdm_handle *h, AmrCtx &X) {
         S[s]->key = h->amr[3 * b + 0].as<uint64_t>();
         S[s]->leaf = h->amr[3 * b + 1].as<uint8_t>();
         S[s]->val = h->amr[3 * b + 2].as<double4>();
+        S[s]->rf = nullptr;
     }
     X.A.n = na;
     X.B.n = nb;
@@ -334,6 +333,16 @@ static int grow_nodes(fdm_handle *h, AmrCtx &X, int64_t n) {
     }
     X.cap = c;
     bind_sets(h, X);
+    return FDM_OK;
+}
+
+// per-cell index of A's keys (amr[22]) for the root-confined searches
+static int index_set(fdm_handle *h, NodeSet &A) {
+    const int64_t nroots = (int64_t)h->G.m * h->G.n;
+    FDM_CK(h, h->amr[22].ensure((nroots + 1) * 4));
+    k_root_first<<<nblk(A.n + 1, 256), 256, 0, h->s>>>(A.n, A.key, nroots, h->amr[22].as<int32_t>());
+    A.rf = h->amr[22].as<int32_t>();
+    A.nroots = nroots;
     return FDM_OK;
 }
 
@@ -449,7 +458,7 @@ __global__ void k_coarsen_flags(int64_t NInt, const uint64_t *ikey, Tables T, fd
     if ((int)(k & 15u) >= P.lvl_amr) return;
     double r[4], d[4];
     for (int q = 0; q < 4; ++q) {
-        const int64_t li = find_key(T.lkey, T.NL, child_key(k, q));
+        const int64_t li = find_key_t(T, child_key(k, q));
         if (li < 0 || rflag[li]) return;
         const int32_t s = T.lslot[li];
         r[q] = s < T.NI ? rot_slot[s] : 0.0;
@@ -502,7 +511,7 @@ __global__ void k_ref_emit(Tables T, const double4 *B0, const int8_t *rflag, con
         okey[o] = key;
         if (cflag[i]) {   // Coarse_cell: interpA of the four leaf sons (src/mesh.F90:397-408)
             double4 c[4];
-            for (int q = 0; q < 4; ++q) c[q] = B0[T.lslot[find_key(T.lkey, T.NL, child_key(key, q))]];
+            for (int q = 0; q < 4; ++q) c[q] = B0[T.lslot[find_key_t(T, child_key(key, q))]];
             oleaf[o] = 1;
             oval[o] = mean4(c[0], c[1], c[2], c[3]);
         } else {
@@ -523,14 +532,14 @@ __global__ void k_gm1_links(NodeSet A, Geometry G, Links L, uint64_t *pkey, int3
     if (i >= A.n) return;
     const uint64_t k = A.key[i];
     const int lvl = (int)(k & 15u);
-    L.parent[i] = lvl > 0 ? (int32_t)find_key(A.key, A.n, parent_key(k)) : -1;
+    L.parent[i] = lvl > 0 ? (int32_t)find_key_set(A, parent_key(k)) : -1;
     L.leaf0[i] = A.leaf[i];
     L.cross[i] = (int8_t)root_cross(G, (int64_t)(k >> 34));
     for (int q = 0; q < 4; ++q)
-        L.child[4 * i + q] = A.leaf[i] ? -1 : (int32_t)find_key(A.key, A.n, child_key(k, q));
+        L.child[4 * i + q] = A.leaf[i] ? -1 : (int32_t)find_key_set(A, child_key(k, q));
     for (int d = 0; d < 4; ++d) {
         uint64_t nk;
-        L.nb[4 * i + d] = shift_key(G, k, d, nk) ? (int32_t)find_key(A.key, A.n, nk) : -1;
+        L.nb[4 * i + d] = shift_key(G, k, d, nk) ? (int32_t)find_key_set(A, nk) : -1;
     }
     pkey[i] = post_rank(k);
     pidx[i] = (int32_t)i;
@@ -621,7 +630,7 @@ __device__ int64_t live_nb_set(const NodeSet &A, const Geometry &G, uint64_t k, 
     uint64_t t;
     if (!shift_key(G, k, dir, t)) return -1;
     for (;;) {
-        const int64_t i = find_key(A.key, A.n, t);
+        const int64_t i = find_key_set(A, t);
         if (i >= 0) return i;
         if ((t & 15u) == 0) return -1;
         t = parent_key(t);
@@ -1498,6 +1507,7 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     int8_t *d0 = cv.at<int8_t>(b, 10), *d1 = cv.at<int8_t>(b, 11);
     int32_t *changed = cv.at<int32_t>(b, 12);
     int32_t *cnt = cv.at<int32_t>(b, 13), *off = cv.at<int32_t>(b, 14);
+    AMR_RC(index_set(h, X.A));
     k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L, pk, pi);
     size_t bytes = 0;
     const int kb = 45 + root_bits(h);   // post-order ranks: root << 45 | 3 bits per level
@@ -1558,6 +1568,7 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     uint64_t *rk = cv.at<uint64_t>(b, 1), *srk = cv.at<uint64_t>(b, 3);
     int32_t *foff = cv.at<int32_t>(b, 5);
     int64_t *nsel = cv.at<int64_t>(b, 6);
+    AMR_RC(index_set(h, X.A));
     k_gm4_triggers<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, flag, rk, idx);
     // keep the triggering leaves, sorted by traversal rank
     size_t bytes = 0;
@@ -1766,7 +1777,7 @@ static int run_amr_impl(fdm_handle *h, fdm_handle *lead) {
     FDM_CK(h, cudaEventRecord(h->amr_ev[4], h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     h->NInt = nint;
-    const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>(), 34 + root_bits(h));
+    const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>(), 0);   // split keeps key order
     if (rc) return rc;
     FDM_CK(h, cudaEventRecord(h->amr_ev[5], h->s));
     FDM_CK(h, cudaEventSynchronize(h->amr_ev[5]));
@@ -1812,5 +1823,38 @@ extern "C" int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double
     if (sums) FDM_CK(h, cudaMemcpyAsync(sums, ds, 24, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     d.release();
+    return FDM_OK;
+}
+
+namespace fdm {
+__global__ void k_interleave2(int64_t n, const double *__restrict__ a, const double *__restrict__ b, double2 *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_double2(a[i], b[i]);
+}
+}  // namespace fdm
+
+extern "C" int fdm_debug_ordered_sum(const double *a, const double *b, int64_t n, double *sums) {
+    using namespace fdm;
+    if (!a || !b || !sums || n < 0 || n >= (1ll << 31)) return FDM_ERR_ARG;
+    double *da = nullptr, *db = nullptr, *dout = nullptr;
+    double2 *dq = nullptr;
+    const size_t bytes = (size_t)(n > 0 ? n : 1) * 8;
+    cudaError_t e = cudaMalloc(&da, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&db, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dq, 2 * bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, 32);
+    if (e == cudaSuccess && n > 0) e = cudaMemcpy(da, a, n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n > 0) e = cudaMemcpy(db, b, n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        if (n > 0) k_interleave2<<<nblk(n, 256), 256>>>(n, da, db, dq);
+        k_ordered_sums<<<1, OSUM_NT>>>(n, dq, dout);
+        e = cudaGetLastError();
+    }
+    double out[3] = {0.0, 0.0, 0.0};
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, 24, cudaMemcpyDeviceToHost);
+    cudaFree(da); cudaFree(db); cudaFree(dq); cudaFree(dout);
+    if (e != cudaSuccess) return FDM_ERR_CUDA;
+    sums[0] = out[0];
+    sums[1] = out[1];
     return FDM_OK;
 }

@@ -216,8 +216,8 @@ __device__ void g_search(const Tables &T, const NodeRef &X, double x, double y, 
         return;
     }
     const uint64_t p0 = node_pos(X.n);
-    const int64_t lo = lower_bound_pos(T.lkey, T.NL, p0);
-    const int64_t hi = lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(X.n.lvl));
+    const int64_t lo = lower_bound_pos_t(T, p0);
+    const int64_t hi = lower_bound_pos_t(T, p0 + span_of_level(X.n.lvl));
     uint64_t best_rank[8];
     int32_t best_leaf[8];
     for (int s = 0; s < 8; ++s) { best_rank[s] = ~0ull; best_leaf[s] = -1; }
@@ -241,29 +241,79 @@ __device__ void g_search(const Tables &T, const NodeRef &X, double x, double y, 
 
 // brinv (src/XuanGua.F90:593-660): full-pivot Gauss-Jordan in place;
 // returns false on the singular test (the partially reduced matrix stays).
+// The matrix lives in registers: every loop is unrolled, and the row and
+// column exchanges with the pivot (whose indices are data) are selects over
+// the rows and columns at or after the step, so the arithmetic is the
+// reference's, operation for operation.
 template <int N>
-__device__ bool brinv_dev(double *r) {
+__device__ __forceinline__ void brinv_swap_rows(double (&r)[N][N], int k, int p) {
+#pragma unroll
+    for (int q = 0; q < N; ++q)
+        if (q > k) {   // q == p > k: exchange rows k and q
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                const double a = r[k][j], b = r[q][j];
+                const bool sw = q == p;
+                r[k][j] = sw ? b : a;
+                r[q][j] = sw ? a : b;
+            }
+        }
+}
+template <int N>
+__device__ __forceinline__ void brinv_swap_cols(double (&r)[N][N], int k, int p) {
+#pragma unroll
+    for (int q = 0; q < N; ++q)
+        if (q > k) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const double a = r[i][k], b = r[i][q];
+                const bool sw = q == p;
+                r[i][k] = sw ? b : a;
+                r[i][q] = sw ? a : b;
+            }
+        }
+}
+template <int N>
+__device__ __forceinline__ bool brinv_reg(double (&r)[N][N]) {
     int is[N], js[N];
-    for (int k = 0; k < N; ++k) { is[k] = 0; js[k] = 0; }
+    bool ok = true;
+#pragma unroll
     for (int k = 0; k < N; ++k) {
-        double d = 0.0;
-        for (int i = k; i < N; ++i)
-            for (int j = k; j < N; ++j)
-                if (fabs(r[i * N + j]) > d) { d = fabs(r[i * N + j]); is[k] = i; js[k] = j; }
-        if (d + 1.0 == 1.0) return false;
-        for (int j = 0; j < N; ++j) { double t = r[k * N + j]; r[k * N + j] = r[is[k] * N + j]; r[is[k] * N + j] = t; }
-        for (int i = 0; i < N; ++i) { double t = r[i * N + k]; r[i * N + k] = r[i * N + js[k]]; r[i * N + js[k]] = t; }
-        r[k * N + k] = 1.0 / r[k * N + k];
-        for (int j = 0; j < N; ++j) if (j != k) r[k * N + j] = r[k * N + j] * r[k * N + k];
-        for (int i = 0; i < N; ++i)
-            if (i != k)
+        is[k] = 0; js[k] = 0;
+        if (ok) {
+            double d = 0.0;
+            int pi = 0, pj = 0;
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+#pragma unroll
                 for (int j = 0; j < N; ++j)
-                    if (j != k) r[i * N + j] = r[i * N + j] - r[i * N + k] * r[k * N + j];
-        for (int i = 0; i < N; ++i) if (i != k) r[i * N + k] = -r[i * N + k] * r[k * N + k];
+                    if (i >= k && j >= k && fabs(r[i][j]) > d) { d = fabs(r[i][j]); pi = i; pj = j; }
+            is[k] = pi; js[k] = pj;
+            if (d + 1.0 == 1.0) {
+                ok = false;
+            } else {
+                brinv_swap_rows<N>(r, k, pi);
+                brinv_swap_cols<N>(r, k, pj);
+                r[k][k] = 1.0 / r[k][k];
+#pragma unroll
+                for (int j = 0; j < N; ++j) if (j != k) r[k][j] = r[k][j] * r[k][k];
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                    if (i != k)
+#pragma unroll
+                        for (int j = 0; j < N; ++j)
+                            if (j != k) r[i][j] = r[i][j] - r[i][k] * r[k][j];
+#pragma unroll
+                for (int i = 0; i < N; ++i) if (i != k) r[i][k] = -r[i][k] * r[k][k];
+            }
+        }
     }
+    if (!ok) return false;
+    // undo the exchanges: row k with row js[k], column k with column is[k]
+#pragma unroll
     for (int k = N - 1; k >= 0; --k) {
-        for (int j = 0; j < N; ++j) { double t = r[k * N + j]; r[k * N + j] = r[js[k] * N + j]; r[js[k] * N + j] = t; }
-        for (int i = 0; i < N; ++i) { double t = r[i * N + k]; r[i * N + k] = r[i * N + is[k]]; r[i * N + is[k]] = t; }
+        brinv_swap_rows<N>(r, k, js[k]);
+        brinv_swap_cols<N>(r, k, is[k]);
     }
     return true;
 }
@@ -313,8 +363,8 @@ __global__ void k_gather(Tables T, Geometry G, ReqDesc D, ReqOut O, int32_t *err
         if (g.m1 + g.m2 < 7) {
             const uint64_t p0 = node_pos(c.n);
             O.kind[r] = RQ_RESTRICT;
-            O.m[2 * r] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0);
-            O.m[2 * r + 1] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(c.n.lvl));
+            O.m[2 * r] = (int32_t)lower_bound_pos_t(T, p0);
+            O.m[2 * r + 1] = (int32_t)lower_bound_pos_t(T, p0 + span_of_level(c.n.lvl));
             geo[G_LVL] = (double)c.n.lvl;
             atomicAdd(O.counts + 2, 1ull);
             return;
@@ -375,24 +425,54 @@ __global__ void k_gather(Tables T, Geometry G, ReqDesc D, ReqOut O, int32_t *err
         P[i][3] = gx[i] * gy[i]; P[i][4] = gx[i] * gx[i]; P[i][5] = gy[i] * gy[i];
     }
     double *L = geo + G_L, *A = geo + G_A, *B = geo + G_B;
-    for (int a = 0; a < 6; ++a)
-        for (int b = 0; b < 6; ++b) {
-            double s = 0.0;
-            for (int i = 0; i < m; ++i) s = s + P[i][a] * (gw[i] * P[i][b]);
-            L[a * 6 + b] = s;
-        }
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) {
-            double s = 0.0, t = 0.0;
-            for (int i = 0; i < m1; ++i) s = s + P[i][a] * (gw[i] * P[i][b]);
-            for (int i = m1; i < m; ++i) t = t + P[i][a] * (gw[i] * P[i][b]);
-            A[a * 3 + b] = s;
-            B[a * 3 + b] = t;
-        }
     unsigned long long ns = 0;
-    if (!brinv_dev<6>(L)) ++ns;
-    if (!brinv_dev<3>(A)) ++ns;
-    if (!brinv_dev<3>(B)) ++ns;
+    {
+        double R[6][6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+            for (int b = 0; b < 6; ++b) R[a][b] = 0.0;
+        for (int i = 0; i < m; ++i) {
+            const double pw[6] = {gw[i] * P[i][0], gw[i] * P[i][1], gw[i] * P[i][2],
+                                  gw[i] * P[i][3], gw[i] * P[i][4], gw[i] * P[i][5]};
+#pragma unroll
+            for (int a = 0; a < 6; ++a)
+#pragma unroll
+                for (int b = 0; b < 6; ++b) R[a][b] = R[a][b] + P[i][a] * pw[b];
+        }
+        if (!brinv_reg<6>(R)) ++ns;
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+            for (int b = 0; b < 6; ++b) L[a * 6 + b] = R[a][b];
+    }
+    {
+        double RA[3][3], RB[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) { RA[a][b] = 0.0; RB[a][b] = 0.0; }
+        for (int i = 0; i < m1; ++i) {
+            const double pw[3] = {gw[i] * P[i][0], gw[i] * P[i][1], gw[i] * P[i][2]};
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) RA[a][b] = RA[a][b] + P[i][a] * pw[b];
+        }
+        for (int i = m1; i < m; ++i) {
+            const double pw[3] = {gw[i] * P[i][0], gw[i] * P[i][1], gw[i] * P[i][2]};
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) RB[a][b] = RB[a][b] + P[i][a] * pw[b];
+        }
+        if (!brinv_reg<3>(RA)) ++ns;
+        if (!brinv_reg<3>(RB)) ++ns;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) { A[a * 3 + b] = RA[a][b]; B[a * 3 + b] = RB[a][b]; }
+    }
     if (ns) atomicAdd(O.counts + 0, ns);
     atomicAdd(O.counts + 1, 1ull);
     // smoothness box of the node (compute_smoothness, src/XuanGua.F90:318-323)
@@ -423,8 +503,8 @@ __device__ __forceinline__ void ghost_from_ref(const Tables &T, const NodeRef &i
         const uint64_t p0 = node_pos(img.n);
         O.kind[g] = GH_RESTRICT;
         atomicAdd(O.n_restrict, 1ull);
-        O.a[g] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0);
-        O.b[g] = (int32_t)lower_bound_pos(T.lkey, T.NL, p0 + span_of_level(img.n.lvl));
+        O.a[g] = (int32_t)lower_bound_pos_t(T, p0);
+        O.b[g] = (int32_t)lower_bound_pos_t(T, p0 + span_of_level(img.n.lvl));
     }
 }
 
@@ -630,6 +710,20 @@ static __global__ void k_iota_b(int64_t n, int32_t *a) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < n) a[i] = (int32_t)i;
 }
+// rf[r] = first sorted leaf of background cell r, rf[nroots] = n; cells
+// without leaves (rejected later by the partition check) get the next
+// cell's start; roots beyond the grid (rejected as well) are clamped
+__global__ void k_root_first(int64_t n, const uint64_t *__restrict__ lkey, int64_t nroots, int32_t *rf) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i > n) return;
+    auto root = [&](int64_t k) -> int64_t {
+        const int64_t r = (int64_t)(lkey[k] >> 34);
+        return r < nroots ? r : nroots;
+    };
+    const int64_t prev = i == 0 ? -1 : root(i - 1);
+    const int64_t cur = i == n ? nroots : root(i);
+    for (int64_t x = prev + 1; x <= cur; ++x) rf[x] = (int32_t)i;
+}
 static __global__ void k_set_lmax(const int32_t *lmax, DevScalars *sc) {
     if (threadIdx.x == 0) sc->l_max = *lmax;
 }
@@ -669,16 +763,26 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     int64_t *dtot = h->tmp[7].as<int64_t>();
     {
         int32_t *iota = h->tmp[0].as<int32_t>();
-        k_iota_b<<<nblk(n, TB), TB, 0, s>>>(n, iota);
-        size_t bytes = 0;
-        FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
-                                                  h->tmp[1].as<int32_t>(), (int)n, 0, key_bits, s));
-        FDM_CK(h, h->cub_tmp.ensure(bytes));
-        FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
-                                                  h->tmp[1].as<int32_t>(), (int)n, 0, key_bits, s));
+        if (key_bits <= 0) {
+            k_iota_b<<<nblk(n, TB), TB, 0, s>>>(n, h->tmp[1].as<int32_t>());
+            FDM_CK(h, cudaMemcpyAsync(h->lkey.as<uint64_t>(), keys_in, n * 8, cudaMemcpyDeviceToDevice, s));
+        } else {
+            k_iota_b<<<nblk(n, TB), TB, 0, s>>>(n, iota);
+            size_t bytes = 0;
+            FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
+                                                      h->tmp[1].as<int32_t>(), (int)n, 0, key_bits, s));
+            FDM_CK(h, h->cub_tmp.ensure(bytes));
+            FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys_in, h->lkey.as<uint64_t>(), iota,
+                                                      h->tmp[1].as<int32_t>(), (int)n, 0, key_bits, s));
+        }
     }
     const uint64_t *lkey = h->lkey.as<uint64_t>();
     const int32_t *perm = h->tmp[1].as<int32_t>();
+    {
+        const int64_t nroots = (int64_t)h->G.m * h->G.n;
+        FDM_CK(h, h->rfirst.ensure((nroots + 1) * 4));
+        k_root_first<<<nblk(n + 1, TB), TB, 0, s>>>(n, lkey, nroots, h->rfirst.as<int32_t>());
+    }
     // 2. classify + partition check
     Carve c2;
     for (int q = 0; q < 6; ++q) c2.add(n * 4);

@@ -57,6 +57,8 @@ struct Tables {
     const int32_t *lslot;             // sorted leaf -> slot
     const int32_t *slot_leaf;         // slot (< NI+NG+NC) -> sorted leaf
     const double *lcx, *lcy;          // leaf centres (sorted order)
+    const int32_t *rfirst;            // [nroots + 1] first sorted leaf of each background cell
+    int64_t nroots;                   // background cells (m * n)
     // interior leaves (slot order == key order of interior leaves)
     const int32_t *ist;               // [NI][8] stencil slots
     const uint8_t *ilvl;              // [NI]

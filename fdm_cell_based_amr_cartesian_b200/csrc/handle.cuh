@@ -103,7 +103,7 @@ struct fdm_handle {
     int64_t n_singular = 0, n_regrids = 0, n_restrict = 0, n_ghost_restrict = 0;
 
     // tables
-    fdm::DevBuf lkey, lslot, slot_leaf, lcx, lcy, lcross;
+    fdm::DevBuf lkey, lslot, slot_leaf, lcx, lcy, lcross, rfirst;
     fdm::DevBuf ist, ilvl, ifxl, ifyl, uxl, uyl;
     fdm::DevBuf rq_kind, rq_m, rq_mem, rq_geo, rq_node, rq_rlist;
     fdm::DevBuf gh_kind, gh_a, gh_b, gh_flip, gh_x, gh_y;
@@ -122,7 +122,8 @@ struct fdm_handle {
     // stale U in every refined node; gridmodify4 can copy it back)
     fdm::DevBuf ikey, ival;
     int64_t NInt = 0;
-    fdm::DevBuf amr[22];     // regrid scratch: [0..5] node sets, [6..19] work arrays, [20, 21] new leaves
+    fdm::DevBuf amr[23];     // regrid scratch: [0..5] node sets, [6..19] work arrays, [20, 21] new leaves,
+                             // [22] per-cell index of the node set
     int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0, gm4_triggers = 0, gm4_refines = 0, gm4_steps = 0;
     // device-timeline phases of the last regrid (events recorded on the stream)
     static constexpr int AMR_PHASES = 5;
@@ -163,6 +164,8 @@ struct fdm_handle {
         T.slot_leaf = slot_leaf.as<int32_t>();
         T.lcx = lcx.as<double>();
         T.lcy = lcy.as<double>();
+        T.rfirst = rfirst.as<int32_t>();
+        T.nroots = (int64_t)G.m * G.n;
         T.ist = ist.as<int32_t>();
         T.ilvl = ilvl.as<uint8_t>();
         T.ifxl = ifxl.as<int32_t>();
@@ -210,6 +213,8 @@ inline int arg_fail(fdm_handle *h, const char *msg) {
 // table construction (build.cu)
 // key_bits: the low bits of the keys that the key sort orders (64 for keys
 // from a caller, root_bits(h) + 34 for keys the device made itself)
+// key_bits: the low bits the sort looks at; 0: the keys are already sorted
+// (the regrid emits them in key order), so they are only copied
 int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_dev, const double *prim_dev, int key_bits = 64);
 // bits of the largest background-cell (root) index m*n - 1: a leaf key
 // (root << 34 | path << 4 | lvl) made on the device has no bit set at or

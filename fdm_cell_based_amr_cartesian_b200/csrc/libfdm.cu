@@ -315,7 +315,7 @@ void fdm_destroy(fdm_handle *h) {
     if (!h) return;
     if (h->s) cudaStreamSynchronize(h->s);
     drop_graph(h);
-    DevBuf *bufs[] = {&h->lkey, &h->lslot, &h->slot_leaf, &h->lcx, &h->lcy, &h->lcross, &h->ist, &h->ilvl,
+    DevBuf *bufs[] = {&h->lkey, &h->lslot, &h->slot_leaf, &h->lcx, &h->lcy, &h->lcross, &h->rfirst, &h->ist, &h->ilvl,
                       &h->ifxl, &h->ifyl, &h->uxl, &h->uyl, &h->rq_kind, &h->rq_m, &h->rq_mem, &h->rq_geo, &h->rq_node,
                       &h->gh_kind, &h->gh_a, &h->gh_b, &h->gh_flip, &h->gh_x, &h->gh_y, &h->B[0], &h->B[1],
                       &h->B[2], &h->Fx, &h->Fy, &h->Ut, &h->scal, &h->res_part, &h->cub_tmp, &h->flag,

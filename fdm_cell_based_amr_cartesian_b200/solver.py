@@ -37,7 +37,7 @@ EXPORTS = [
     "fdm_update_rk", "fdm_body_boundary", "fdm_residual", "fdm_solute_step", "fdm_solute",
     "fdm_advance", "fdm_amr", "fdm_get_counters", "fdm_debug_stencil", "fdm_debug_neighbors",
     "fdm_debug_requests",
-    "fdm_debug_rot_div", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
+    "fdm_debug_rot_div", "fdm_debug_ordered_sum", "fdm_device_state", "fdm_time_kernels", "fdm_fp64_peak", "fdm_autotune",
     "fdm_set_variant", "fdm_time_advance_rk_uniform_static", "fdm_gate_param_count", "fdm_gate_set",
     "fdm_gate_samples", "fdm_gate_train_step", "fdm_gate_eval", "fdm_gate_stats", "fdm_amr_phase_ms",
     "fdm_batch_create", "fdm_batch_destroy", "fdm_batch_last_error", "fdm_batch_advance", "fdm_batch_solute",
@@ -113,6 +113,7 @@ def load_library(path: str = LIB_PATH):
     i32p = ctypes.POINTER(ctypes.c_int32)
     L.fdm_debug_requests.argtypes = [vp, i64, i32p, u64p, dp, i32p, u64p]
     L.fdm_debug_rot_div.argtypes = [vp, i64, dp, dp, dp]
+    L.fdm_debug_ordered_sum.argtypes = [dp, dp, i64, dp]
     L.fdm_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(dp), ctypes.POINTER(i64)]
     L.fdm_time_kernels.argtypes = [vp, i32, dp]
     L.fdm_fp64_peak.argtypes = [dp]

@@ -288,6 +288,11 @@ int fdm_debug_fail_alloc(int64_t after);
 /* AMR indicators rot/div of the interior leaves (src/solution.F90:424-466). */
 int fdm_debug_rot_div(fdm_handle *h, int64_t cap, double *rot, double *div,
                       double *srot_sdiv_ne);
+/* The device's left-to-right sums of two host arrays of n non-negative
+ * addends (the kernel that forms Srot and Sdiv, src/solution.F90:430-457):
+ * sums[0] = (...((0 + a[0]) + a[1]) + ...) + a[n-1], sums[1] the same over b.
+ * For testing the summation on chosen inputs; runs on the current device. */
+int fdm_debug_ordered_sum(const double *a, const double *b, int64_t n, double *sums);
 
 /* Device-resident state for in-process callers (bench, Python mirror):
  * the CUDA stream of the handle and the device pointer of the (rho,u,v,p)

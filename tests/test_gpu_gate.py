@@ -28,7 +28,27 @@ def test_forward_matches_oracle():
     prob = learned.probabilities(torch.tensor(X, device="cuda"), p).cpu().numpy()
     z = mlp_ref.forward(p, X)[-1]
     ref = 1 / (1 + np.exp(-z))
-    assert np.max(np.abs(prob - ref)) < 2e-3
+    # The oracle rounds to BF16 where the kernel does; what is left is the
+    # hardware tanh of the GELU (relative error near 2^-11), which moves an
+    # activation by one BF16 ulp where it lies next to a rounding boundary.
+    # Measured on a B200: 1.9e-4 (seeds 1, 5, 11: 1.9e-4, 0.9e-4, 1.8e-4).
+    assert np.max(np.abs(prob - ref)) < 5e-4
+
+
+@pytest.mark.skipif(not os.path.exists(learned.PARAMS_PATH), reason="no trained gate parameters")
+def test_forward_trained_matches_oracle():
+    """The trained weights are larger, so a flipped BF16 rounding moves the
+    logit further: measured 5.0e-4, 1.9e-3 and 5.9e-4 on three inputs."""
+    import torch
+    X, _ = _data(4096, 5)
+    p = learned.load_params()
+    prob = learned.probabilities(torch.tensor(X, device="cuda"), p).cpu().numpy()
+    z = mlp_ref.forward(p, X)[-1]
+    ref = 1 / (1 + np.exp(-z))
+    err = np.abs(prob - ref)
+    assert np.max(err) < 4e-3
+    # a flip is rare: nearly every probability agrees far more closely
+    assert np.quantile(err, 0.99) < 1e-3
 
 
 @pytest.mark.parametrize("neg_weight", [1.0, 4.0])
@@ -39,12 +59,15 @@ def test_gradients_match_oracle(neg_weight):
     g_gpu, loss_gpu = learned.gradients(torch.tensor(X, device="cuda"), torch.tensor(Y, device="cuda"), p, 2048,
                                         neg_weight=neg_weight)
     loss, g = mlp_ref.loss_and_grads(p, X, Y, neg_weight=neg_weight)
-    assert abs(loss_gpu / 2048 - loss) < 1e-3 * abs(loss) + 1e-5
+    # Measured on a B200 (data seeds 2 and 9, both weights): loss within
+    # 1.6e-7 relative, gradient within 5.2e-6 relative, every block within
+    # 2.4e-5; the bounds leave a margin of about ten.
+    assert abs(loss_gpu / 2048 - loss) < 1e-5 * abs(loss) + 1e-7
     rel = np.linalg.norm(g_gpu - g) / np.linalg.norm(g)
-    assert rel < 2e-2, rel
+    assert rel < 1e-4, rel
     # every block of the gradient, not only the norm
     for a, b in ((0, 256), (256, 288), (288, 1312), (1312, 1344), (1344, 1376)):
-        assert np.linalg.norm(g_gpu[a:b] - g[a:b]) <= 3e-2 * np.linalg.norm(g[a:b]) + 1e-7, (a, b)
+        assert np.linalg.norm(g_gpu[a:b] - g[a:b]) <= 3e-4 * np.linalg.norm(g[a:b]) + 1e-9, (a, b)
 
 
 def test_training_reduces_loss():
