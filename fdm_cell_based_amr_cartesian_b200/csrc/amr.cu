@@ -336,6 +336,48 @@ static int grow_nodes(fdm_handle *h, AmrCtx &X, int64_t n) {
     return FDM_OK;
 }
 
+// Merge of two key-sorted runs (keys distinct) into the node set out: an
+// entry's place is its index in its run plus the number of keys of the
+// other run below it.
+__global__ void k_merge_runs(const uint64_t *__restrict__ ka, const uint8_t *__restrict__ la,
+                             const double4 *__restrict__ va, int64_t na, const uint64_t *__restrict__ kb,
+                             const uint8_t *__restrict__ lb, const double4 *__restrict__ vb, int64_t nb, NodeSet out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= na + nb) return;
+    const bool in_a = i < na;
+    const int64_t j = in_a ? i : i - na;
+    const uint64_t k = in_a ? ka[j] : kb[j];
+    const uint64_t *other = in_a ? kb : ka;
+    int64_t lo = 0, hi = in_a ? nb : na;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (other[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    const int64_t o = j + lo;
+    out.key[o] = k;
+    out.leaf[o] = in_a ? la[j] : lb[j];
+    out.val[o] = in_a ? va[j] : vb[j];
+}
+// the runs [0, m) and [m, n) of (keys, leaf, val), each sorted, into out
+static void merge_into(fdm_handle *h, const uint64_t *keys, const uint8_t *leaf, const double4 *val, int64_t m,
+                       int64_t n, NodeSet &out) {
+    if (n > 0)
+        k_merge_runs<<<nblk(n, 256), 256, 0, h->s>>>(keys, leaf, val, m, keys + m, leaf + m, val + m, n - m, out);
+    out.n = n;
+}
+// (keys, leaf, val) of length n, already in key order, into out
+static int copy_into(fdm_handle *h, int64_t n, const uint64_t *keys, const uint8_t *leaf, const double4 *val,
+                     NodeSet &out) {
+    if (n > 0) {
+        FDM_CK(h, cudaMemcpyAsync(out.key, keys, n * 8, cudaMemcpyDeviceToDevice, h->s));
+        FDM_CK(h, cudaMemcpyAsync(out.leaf, leaf, n, cudaMemcpyDeviceToDevice, h->s));
+        FDM_CK(h, cudaMemcpyAsync(out.val, val, n * 32, cudaMemcpyDeviceToDevice, h->s));
+    }
+    out.n = n;
+    return FDM_OK;
+}
+
 // per-cell index of A's keys (amr[22]) for the root-confined searches
 static int index_set(fdm_handle *h, NodeSet &A) {
     const int64_t nroots = (int64_t)h->G.m * h->G.n;
@@ -346,35 +388,22 @@ static int index_set(fdm_handle *h, NodeSet &A) {
     return FDM_OK;
 }
 
-// sort (keys, leaf, val) of length n (unsorted, in the given device arrays)
-// into the node set `out`
-static int sort_into(fdm_handle *h, int64_t n, const uint64_t *keys, const uint8_t *leaf, const double4 *val,
-                     NodeSet &out) {
-    const int TB = 256;
-    FDM_CK(h, h->amr[6].ensure(n * 4 + 16));
-    FDM_CK(h, h->amr[7].ensure(n * 4 + 16));
-    int32_t *iota = h->amr[6].as<int32_t>(), *perm = h->amr[7].as<int32_t>();
-    k_iota<<<nblk(n, TB), TB, 0, h->s>>>(n, iota);
-    size_t bytes = 0;
-    const int kb = 34 + root_bits(h);   // node keys
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, out.key, iota, perm, (int)n, 0, kb, h->s));
-    FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, keys, out.key, iota, perm, (int)n, 0, kb, h->s));
-    k_gather_nodes<<<nblk(n, TB), TB, 0, h->s>>>(n, perm, leaf, val, out.leaf, out.val);
-    out.n = n;
-    return FDM_OK;
-}
 
-static int scan_total32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n, int64_t &total) {
+// exclusive scan of n counts and their total; *at_val: the prefix at index
+// at (0 <= at < n), read back in the same round trip
+static int scan_total32(fdm_handle *h, const int32_t *in, int32_t *out, int64_t n, int64_t &total,
+                        int64_t at = -1, int64_t *at_val = nullptr) {
     size_t bytes = 0;
     FDM_CK(h, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, h->s));
     FDM_CK(h, h->cub_tmp.ensure(bytes));
     FDM_CK(h, cub::DeviceScan::ExclusiveSum(h->cub_tmp.p, bytes, in, out, (int)n, h->s));
-    int32_t a = 0, b = 0;
+    int32_t a = 0, b = 0, c = 0;
     FDM_CK(h, cudaMemcpyAsync(&a, in + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaMemcpyAsync(&b, out + n - 1, 4, cudaMemcpyDeviceToHost, h->s));
+    if (at_val && at >= 0 && at < n) FDM_CK(h, cudaMemcpyAsync(&c, out + at, 4, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));
     total = (int64_t)a + b;
+    if (at_val) *at_val = at >= n ? total : (int64_t)c;
     return FDM_OK;
 }
 
@@ -523,11 +552,12 @@ __global__ void k_ref_emit(Tables T, const double4 *B0, const int8_t *rflag, con
 
 // ----------------------------------------------------------- gridmodify1
 struct Links {
-    int32_t *parent, *child, *nb, *rank;   // child[4 n], nb[4 n] (up, down, right, left)
+    int32_t *parent, *child, *nb;   // child[4 n], nb[4 n] (up, down, right, left)
+    uint64_t *rank;                 // post-order rank key of the visit (post_rank): compared, never indexed
     uint8_t *leaf0;
     int8_t *cross;
 };
-__global__ void k_gm1_links(NodeSet A, Geometry G, Links L, uint64_t *pkey, int32_t *pidx) {
+__global__ void k_gm1_links(NodeSet A, Geometry G, Links L) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     const uint64_t k = A.key[i];
@@ -541,16 +571,11 @@ __global__ void k_gm1_links(NodeSet A, Geometry G, Links L, uint64_t *pkey, int3
         uint64_t nk;
         L.nb[4 * i + d] = shift_key(G, k, d, nk) ? (int32_t)find_key_set(A, nk) : -1;
     }
-    pkey[i] = post_rank(k);
-    pidx[i] = (int32_t)i;
-}
-__global__ void k_scatter_rank(int64_t n, const int32_t *sorted_idx, int32_t *rank) {
-    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r < n) rank[sorted_idx[r]] = (int32_t)r;
+    L.rank[i] = post_rank(k);
 }
 // "the same-level node N exists and has sons" when x is visited: decisions
 // of earlier-visited nodes applied
-__device__ __forceinline__ bool gm1_has_son(const Links &L, const int8_t *d, int32_t N, int32_t rx) {
+__device__ __forceinline__ bool gm1_has_son(const Links &L, const int8_t *d, int32_t N, uint64_t rx) {
     if (N < 0) return false;
     for (int32_t a = L.parent[N]; a >= 0; a = L.parent[a])
         if (d[a] == D_COARSEN && L.rank[a] < rx) return false;
@@ -565,7 +590,7 @@ __global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, in
     if (x >= n) return;
     int8_t r = D_NONE;
     if (L.cross[x] == 0) {
-        const int32_t rx = L.rank[x];
+        const uint64_t rx = L.rank[x];
         const bool up = gm1_has_son(L, d, L.nb[4 * x + DIR_UP], rx);
         const bool down = gm1_has_son(L, d, L.nb[4 * x + DIR_DOWN], rx);
         const bool left = gm1_has_son(L, d, L.nb[4 * x + DIR_LEFT], rx);
@@ -1494,27 +1519,18 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     const int TB = 256;
     const int64_t n = X.A.n;
     Carve cv;
-    cv.add(n * 4); cv.add(n * 16); cv.add(n * 16); cv.add(n * 4); cv.add(n); cv.add(n);
-    cv.add(n * 8); cv.add(n * 4); cv.add(n * 8); cv.add(n * 4); cv.add(n); cv.add(n); cv.add(16);
-    cv.add(n * 4); cv.add(n * 4);
+    cv.add(n * 4); cv.add(n * 16); cv.add(n * 16); cv.add(n * 8); cv.add(n); cv.add(n);
+    cv.add(n); cv.add(n); cv.add(16); cv.add(n * 4); cv.add(n * 4);
     FDM_CK(h, h->amr[14].ensure(cv.total));
     DevBuf &b = h->amr[14];
     Links L;
     L.parent = cv.at<int32_t>(b, 0); L.child = cv.at<int32_t>(b, 1); L.nb = cv.at<int32_t>(b, 2);
-    L.rank = cv.at<int32_t>(b, 3); L.leaf0 = cv.at<uint8_t>(b, 4); L.cross = cv.at<int8_t>(b, 5);
-    uint64_t *pk = cv.at<uint64_t>(b, 6), *pk2 = cv.at<uint64_t>(b, 8);
-    int32_t *pi = cv.at<int32_t>(b, 7), *pi2 = cv.at<int32_t>(b, 9);
-    int8_t *d0 = cv.at<int8_t>(b, 10), *d1 = cv.at<int8_t>(b, 11);
-    int32_t *changed = cv.at<int32_t>(b, 12);
-    int32_t *cnt = cv.at<int32_t>(b, 13), *off = cv.at<int32_t>(b, 14);
+    L.rank = cv.at<uint64_t>(b, 3); L.leaf0 = cv.at<uint8_t>(b, 4); L.cross = cv.at<int8_t>(b, 5);
+    int8_t *d0 = cv.at<int8_t>(b, 6), *d1 = cv.at<int8_t>(b, 7);
+    int32_t *changed = cv.at<int32_t>(b, 8);
+    int32_t *cnt = cv.at<int32_t>(b, 9), *off = cv.at<int32_t>(b, 10);
     AMR_RC(index_set(h, X.A));
-    k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L, pk, pi);
-    size_t bytes = 0;
-    const int kb = 45 + root_bits(h);   // post-order ranks: root << 45 | 3 bits per level
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, pk, pk2, pi, pi2, (int)n, 0, kb, h->s));
-    FDM_CK(h, h->cub_tmp.ensure(bytes));
-    FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, pk, pk2, pi, pi2, (int)n, 0, kb, h->s));
-    k_scatter_rank<<<nblk(n, TB), TB, 0, h->s>>>(n, pi2, L.rank);
+    k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L);
     FDM_CK(h, cudaMemsetAsync(d0, 0, n, h->s));
     int8_t *cur = d0, *nxt = d1;
     // Sweeps are enqueued GM1_SWEEPS at a time and the change flag of the
@@ -1549,7 +1565,9 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     AMR_RC(emit_buffers(h, total, E));
     k_gm1_emit<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, off, E.key, E.leaf, E.val);
     AMR_RC(grow_nodes(h, X, total));
-    AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
+    // the emit keeps key order: a refined leaf's sons follow it directly and
+    // lie before every later node (they fill the leaf's own span)
+    AMR_RC(copy_into(h, total, E.key, E.leaf, E.val, X.B));
     swap_sets(h, X);
     return FDM_OK;
 }
@@ -1639,13 +1657,36 @@ static int gridmodify4_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     FDM_CK(h, h->amr[17].ensure(ce.total));
     int32_t *live = ce.at<int32_t>(h->amr[17], 0), *loff = ce.at<int32_t>(h->amr[17], 1);
     k_pool_live<<<nblk(pn, TB), TB, 0, h->s>>>(pn, P.flags, live);
-    int64_t total = 0;
-    AMR_RC(scan_total32(h, live, loff, pn, total));
+    int64_t total = 0, m = 0;   // m: live nodes of A (pool entries below n, in key order)
+    AMR_RC(scan_total32(h, live, loff, pn, total, n, &m));
     Emit E;
     AMR_RC(emit_buffers(h, total, E));
     k_pool_emit<<<nblk(pn, TB), TB, 0, h->s>>>(pn, P.flags, P.key, P.val, loff, E.key, E.leaf, E.val);
+    // the new nodes (in the order they were made) sorted by key, then merged
+    // with the survivors of A
+    const int64_t nb = total - m;
+    FDM_CK(h, h->amr[23].ensure(nb * 8 + 16));
+    FDM_CK(h, h->amr[24].ensure(nb + 16));
+    FDM_CK(h, h->amr[25].ensure(nb * 32 + 32));
+    uint64_t *bk = h->amr[23].as<uint64_t>();
+    uint8_t *bl = h->amr[24].as<uint8_t>();
+    double4 *bv = h->amr[25].as<double4>();
+    if (nb > 0) {
+        FDM_CK(h, h->amr[6].ensure(nb * 4 + 16));
+        FDM_CK(h, h->amr[7].ensure(nb * 4 + 16));
+        int32_t *iota = h->amr[6].as<int32_t>(), *perm = h->amr[7].as<int32_t>();
+        k_iota<<<nblk(nb, TB), TB, 0, h->s>>>(nb, iota);
+        size_t bytes = 0;
+        const int kb = 34 + root_bits(h);
+        FDM_CK(h, cub::DeviceRadixSort::SortPairs(nullptr, bytes, E.key + m, bk, iota, perm, (int)nb, 0, kb, h->s));
+        FDM_CK(h, h->cub_tmp.ensure(bytes));
+        FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, E.key + m, bk, iota, perm, (int)nb, 0, kb, h->s));
+        k_gather_nodes<<<nblk(nb, TB), TB, 0, h->s>>>(nb, perm, E.leaf + m, E.val + m, bl, bv);
+    }
     AMR_RC(grow_nodes(h, X, total));
-    AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
+    if (total > 0)
+        k_merge_runs<<<nblk(total, TB), TB, 0, h->s>>>(E.key, E.leaf, E.val, m, bk, bl, bv, nb, X.B);
+    X.B.n = total;
     swap_sets(h, X);
     return FDM_OK;
 }
@@ -1732,8 +1773,8 @@ static int run_amr_impl(fdm_handle *h, fdm_handle *lead) {
     FDM_CK(h, h->amr[19].ensure(nn * 8 + 16));
     int32_t *cnt = h->amr[19].as<int32_t>(), *off = cnt + nn;
     k_ref_count<<<nblk(nn, TB), TB, 0, h->s>>>(T, rflag, h->ikey.as<uint64_t>(), NInt, cflag, cnt);
-    int64_t total = 0;
-    AMR_RC(scan_total32(h, cnt, off, nn, total));
+    int64_t total = 0, split = 0;   // the leaves' entries (sorted) come first, then the internal nodes' (sorted)
+    AMR_RC(scan_total32(h, cnt, off, nn, total, NL, &split));
     Emit E;
     AMR_RC(emit_buffers(h, total, E));
     k_ref_emit<<<nblk(nn, TB), TB, 0, h->s>>>(T, h->B[0].as<double4>(), rflag, h->ikey.as<uint64_t>(),
@@ -1742,7 +1783,7 @@ static int run_amr_impl(fdm_handle *h, fdm_handle *lead) {
     X.h = h;
     AMR_RC(grow_nodes(h, X, total));
     bind_sets(h, X);
-    AMR_RC(sort_into(h, total, E.key, E.leaf, E.val, X.B));
+    merge_into(h, E.key, E.leaf, E.val, split, total, X.B);
     swap_sets(h, X);
     FDM_CK(h, cudaEventRecord(h->amr_ev[2], h->s));
     // 3. solute_gridmodify: lvlAMR rounds (src/solution.F90:537-556)

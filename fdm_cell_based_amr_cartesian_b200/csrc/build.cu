@@ -23,12 +23,27 @@ static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 // get_direction (src/XuanGua.F90:33-43): 45-degree sector 1..8 (1 = east,
 // counter-clockwise) of (xx,yy) seen from (x,y).
-__device__ __forceinline__ int get_direction(double xx, double yy, double x, double y) {
-    const double dx = xx - x;
-    const double dy = yy - y;
+__device__ __noinline__ int get_direction_atan(double dx, double dy) {
     const double angle = (atan2(dy, dx) + FDM_ATAN_BIAS) * 180.0 / FDM_PI_REF;
     const int f = (int)floor((angle + 22.5) / 45.0 + 8);
     return ((f % 8) + 8) % 8 + 1;
+}
+// The sector follows from |dy| against tan(22.5) |dx| and tan(67.5) |dx|
+// except next to a sector boundary: a relative margin of 1e-9 on the
+// tangent keeps the point more than 3.5e-10 rad from the boundary, which
+// is more than the 1e-10 rad shift of the bias plus the rounding of atan2
+// and of the angle arithmetic, so the sector is the one the formula above
+// gives; the points within the margin (and dx = dy = 0) take the formula.
+__device__ __forceinline__ int get_direction(double xx, double yy, double x, double y) {
+    const double dx = xx - x;
+    const double dy = yy - y;
+    const double a = fabs(dx), b = fabs(dy);
+    constexpr double T1 = 0.41421356237309503, T2 = 2.414213562373095;   // tan(22.5), tan(67.5)
+    constexpr double LO = 1.0 - 1e-9, HI = 1.0 + 1e-9;
+    if (b < a * (T1 * LO)) return dx > 0.0 ? 1 : 5;
+    if (b > a * (T2 * HI)) return dy > 0.0 ? 3 : 7;
+    if (b > a * (T1 * HI) && b < a * (T2 * LO)) return dx > 0.0 ? (dy > 0.0 ? 2 : 8) : (dy > 0.0 ? 4 : 6);
+    return get_direction_atan(dx, dy);
 }
 
 // ------------------------------------------------------------ classify

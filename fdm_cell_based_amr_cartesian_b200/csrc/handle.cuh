@@ -122,8 +122,8 @@ struct fdm_handle {
     // stale U in every refined node; gridmodify4 can copy it back)
     fdm::DevBuf ikey, ival;
     int64_t NInt = 0;
-    fdm::DevBuf amr[23];     // regrid scratch: [0..5] node sets, [6..19] work arrays, [20, 21] new leaves,
-                             // [22] per-cell index of the node set
+    fdm::DevBuf amr[26];     // regrid scratch: [0..5] node sets, [6..19] work arrays, [20, 21] new leaves,
+                             // [22] per-cell index of the node set, [23..25] the new nodes of a gridmodify4 pass
     int64_t gm1_iters = 0, gm4_visits = 0, gm4_nonleaf = 0, gm4_triggers = 0, gm4_refines = 0, gm4_steps = 0;
     // device-timeline phases of the last regrid (events recorded on the stream)
     static constexpr int AMR_PHASES = 5;
