@@ -833,7 +833,7 @@ __device__ __forceinline__ int32_t hfind(const Pool &P, uint64_t k) {
 }
 // insert or revive a leaf with value v (one lane); pn is the pool size.
 // Returns its pool index or -1
-__device__ int32_t hinsert(Pool &P, uint64_t k, const double4 &v, int64_t &pn) {
+__device__ int32_t hinsert(const Pool &P, uint64_t k, const double4 &v, int64_t &pn) {
     int32_t s;
     uint64_t pos;
     const int r = hlocate(P, k, pos, s);
@@ -873,7 +873,7 @@ struct Queue {
     int head, tail;
     Heap g;
 };
-__device__ bool hpush(Heap &H, const HEnt &x) {
+__device__ __forceinline__ bool hpush(Heap &H, const HEnt &x) {
     if (H.n >= H.cap) return false;
     int64_t i = H.n++;
     while (i > 0) {
@@ -886,7 +886,7 @@ __device__ bool hpush(Heap &H, const HEnt &x) {
     H.e[i] = x;
     return true;
 }
-__device__ HEnt hpop(Heap &H) {
+__device__ __forceinline__ HEnt hpop(Heap &H) {
     const HEnt top = H.e[0];
     const int64_t hn = --H.n;
     const HEnt last = H.e[hn];
@@ -914,8 +914,8 @@ __device__ __forceinline__ HEnt queued_leaf(uint64_t key, int32_t idx, int32_t g
     return x;
 }
 // one lane: into the global heap
-__device__ bool gpush_leaf(Queue &Q, uint64_t key, int32_t idx, int32_t gen) {
-    return hpush(Q.g, queued_leaf(key, idx, gen));
+__device__ __forceinline__ bool gpush_leaf(Heap &H, uint64_t key, int32_t idx, int32_t gen) {
+    return hpush(H, queued_leaf(key, idx, gen));
 }
 
 // The warp inserts the entries x of the lanes with has (at most 4, lanes
@@ -924,7 +924,7 @@ __device__ bool gpush_leaf(Queue &Q, uint64_t key, int32_t idx, int32_t gen) {
 // after the old entries with mk not above its own.  When the array is full
 // its upper half moves to the global heap first.  Returns false when the
 // global heap overflowed.
-__device__ bool sq_insert(Queue &Q, const HEnt &x, bool has) {
+__device__ __forceinline__ bool sq_insert(Queue &Q, const HEnt &x, bool has) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned hm = __ballot_sync(FULL, has);
@@ -995,7 +995,7 @@ __device__ bool sq_insert(Queue &Q, const HEnt &x, bool has) {
 }
 // Entries of the global heap that belong among the first GM4_BATCH come
 // into the sorted array before a merge
-__device__ bool sq_pull(Queue &Q) {
+__device__ __forceinline__ bool sq_pull(Queue &Q) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     bool ok = true;
@@ -1016,7 +1016,7 @@ __device__ bool sq_pull(Queue &Q) {
 // >= l0 + 3 in the four edge-adjacent level-l0 cells can now find one of the
 // new sons as a neighbour (or neighbour's neighbour) two levels coarser.  The
 // reference visits every leaf, so those ahead of the traversal are queued.
-__device__ bool push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uint64_t cur_rank) {
+__device__ __noinline__ bool push_ring(const Pool &P, const Geometry &G, Heap &H, uint64_t pk, uint64_t cur_rank) {
     const int l0 = (int)(pk & 15u);
     const int dirs[4] = {DIR_RIGHT, DIR_LEFT, DIR_UP, DIR_DOWN};
     bool ok = true;
@@ -1035,7 +1035,7 @@ __device__ bool push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uin
                 const int32_t c = hfind(P, ck);
                 if (c < 0) continue;
                 if (P.flags[c] & PF_LEAF) {
-                    if ((int)(ck & 15u) >= l0 + 3 && visit_rank(ck) > cur_rank) ok = gpush_leaf(Q, ck, c, P.gen[c]) && ok;
+                    if ((int)(ck & 15u) >= l0 + 3 && visit_rank(ck) > cur_rank) ok = gpush_leaf(H, ck, c, P.gen[c]) && ok;
                 } else if (sp < 64) {
                     st[sp++] = ck;
                 } else {
@@ -1049,8 +1049,8 @@ __device__ bool push_ring(Pool &P, const Geometry &G, Queue &Q, uint64_t pk, uin
 // Refine_cell (src/mesh.F90:199-260) of a non-leaf whose old subtree is
 // dropped and whose new sons copy its stale value (counted in nl); one lane.
 // cur_rank is the visit rank of the leaf being visited.
-__device__ bool refine_nonleaf(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t cur_rank, int32_t &nl,
-                               int64_t &pn) {
+__device__ __noinline__ bool refine_nonleaf(const Pool &P, const Geometry &G, Heap &H, int32_t p, uint64_t cur_rank,
+                                            int32_t &nl, int64_t &pn) {
     const uint64_t pk = P.key[p];
     bool deep = false, ok = true;
     nl += 1;
@@ -1078,9 +1078,9 @@ __device__ bool refine_nonleaf(Pool &P, const Geometry &G, Queue &Q, int32_t p, 
         const uint64_t ck = child_key(pk, q);
         const int32_t c = hinsert(P, ck, v, pn);
         if (c < 0) return false;
-        if (visit_rank(ck) > cur_rank) ok = gpush_leaf(Q, ck, c, P.gen[c]) && ok;
+        if (visit_rank(ck) > cur_rank) ok = gpush_leaf(H, ck, c, P.gen[c]) && ok;
     }
-    if (deep) ok = push_ring(P, G, Q, pk, cur_rank) && ok;
+    if (deep) ok = push_ring(P, G, H, pk, cur_rank) && ok;
     return ok;
 }
 // Is the node with key s (or the position s stands for) inside node r?
@@ -1158,7 +1158,7 @@ __device__ __forceinline__ void group_dir_lookups(const Pool &P, const Geometry 
 // that slot take it one at a time, lowest lane first, the others probing on
 // past it.  A non-leaf (rare) is refined by lane 0 alone.  pn (the pool
 // size) is uniform.  Returns false when the pool or the queue overflowed.
-__device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t pk, uint64_t cur_rank,
+__device__ __forceinline__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uint64_t pk, uint64_t cur_rank,
                             int32_t &nonleaf, int64_t &pn, unsigned char *lk) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -1178,7 +1178,16 @@ __device__ bool refine_warp(Pool &P, const Geometry &G, Queue &Q, int32_t p, uin
     bool ok = true;
     if (!(fp & PF_LEAF)) {
         int e = 0;
-        if (lane == 0) e = refine_nonleaf(P, G, Q, p, cur_rank, nonleaf, pn) ? 0 : 1;
+        if (lane == 0) {
+            // out of line on copies, so that the queue and counters stay in registers
+            Heap g = Q.g;
+            int32_t nl = nonleaf;
+            int64_t pn1 = pn;
+            e = refine_nonleaf(P, G, g, p, cur_rank, nl, pn1) ? 0 : 1;
+            Q.g.n = g.n;
+            nonleaf = nl;
+            pn = pn1;
+        }
         ok = __shfl_sync(FULL, e, 0) == 0;
         pn = __shfl_sync(FULL, pn, 0);
     } else {
