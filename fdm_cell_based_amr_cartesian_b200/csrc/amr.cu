@@ -557,11 +557,12 @@ struct Links {
     uint8_t *leaf0;
     int8_t *cross;
 };
-__global__ void k_gm1_links(NodeSet A, Geometry G, Links L) {
+__global__ void k_gm1_links(NodeSet A, Geometry G, Links L, int32_t *max_lvl) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     const uint64_t k = A.key[i];
     const int lvl = (int)(k & 15u);
+    if (!A.leaf[i]) atomicMax(max_lvl, lvl);   // the deepest internal node
     L.parent[i] = lvl > 0 ? (int32_t)find_key_set(A, parent_key(k)) : -1;
     L.leaf0[i] = A.leaf[i];
     L.cross[i] = (int8_t)root_cross(G, (int64_t)(k >> 34));
@@ -1539,7 +1540,8 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     int32_t *changed = cv.at<int32_t>(b, 8);
     int32_t *cnt = cv.at<int32_t>(b, 9), *off = cv.at<int32_t>(b, 10);
     AMR_RC(index_set(h, X.A));
-    k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L);
+    FDM_CK(h, cudaMemsetAsync(changed, 0, 16, h->s));
+    k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L, changed + 2);
     FDM_CK(h, cudaMemsetAsync(d0, 0, n, h->s));
     int8_t *cur = d0, *nxt = d1;
     // Sweeps are enqueued GM1_SWEEPS at a time and the change flag of the
@@ -1547,26 +1549,29 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     // nothing, so the extra sweeps leave the fixpoint as it is.
     constexpr int GM1_SWEEPS = 4;
     int64_t it = 0;
+    int deepest = MAXLVL_TAB - 2;   // a coarsened node is internal: no deeper than the deepest internal node
     for (;;) {
         if (it > n + 2 + GM1_SWEEPS) { h->err = "gridmodify1 decisions did not settle"; return FDM_ERR_UNSUPPORTED; }
-        int32_t hc[2] = {0, 0};   // last sweep: changed, any decision
+        int32_t hc[3] = {0, 0, 0};   // last sweep: changed, any decision; deepest internal node
         for (int k = 0; k < GM1_SWEEPS; ++k) {
             const bool last = k == GM1_SWEEPS - 1;
-            if (last) FDM_CK(h, cudaMemsetAsync(changed, 0, 8, h->s));
+            if (last) FDM_CK(h, cudaMemsetAsync(changed, 0, 8, h->s));   // the level stays
             k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed, last ? changed + 1 : nullptr);
             std::swap(cur, nxt);
         }
         it += GM1_SWEEPS;
-        FDM_CK(h, cudaMemcpyAsync(hc, changed, 8, cudaMemcpyDeviceToHost, h->s));
+        FDM_CK(h, cudaMemcpyAsync(hc, changed, 12, cudaMemcpyDeviceToHost, h->s));
         FDM_CK(h, cudaStreamSynchronize(h->s));
         if (!hc[0]) {
             *did = hc[1] != 0;
+            deepest = hc[2];
             break;
         }
     }
     h->gm1_iters += it;
     if (!*did) return FDM_OK;   // every decision is "nothing": A stays
-    for (int l = MAXLVL_TAB - 2; l >= 0; --l) k_gm1_vals<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, l);
+    for (int l = deepest < MAXLVL_TAB - 2 ? deepest : MAXLVL_TAB - 2; l >= 0; --l)
+        k_gm1_vals<<<nblk(n, TB), TB, 0, h->s>>>(X.A, L, cur, l);
     k_gm1_count<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, cnt);
     int64_t total = 0;
     AMR_RC(scan_total32(h, cnt, off, n, total));
