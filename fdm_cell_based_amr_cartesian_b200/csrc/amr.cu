@@ -47,17 +47,15 @@ __global__ void k_ordered_squares(int64_t NI, const int32_t *__restrict__ order,
 }
 
 // Srot, Sdiv: left-to-right sums in traversal order, as the reference's
-// recursive loop forms them (src/solution.F90:430-457), bit for bit, by one
-// block (ordered_sum.cuh)
+// recursive loop forms them (src/solution.F90:430-457), bit for bit, one
+// block each (ordered_sum.cuh); launched with 2 blocks
 __global__ void __launch_bounds__(OSUM_NT) k_ordered_sums(int64_t NI, const double2 *__restrict__ sq, double *out) {
     __shared__ OSumShared sh;
-    const double *x = reinterpret_cast<const double *>(sq);
-    const double sr = ordered_sum_block<OSUM_NT, OSUM_EPT>(x, 2, NI, sh);
-    const double sd = ordered_sum_block<OSUM_NT, OSUM_EPT>(x + 1, 2, NI, sh);
+    const double *x = reinterpret_cast<const double *>(sq) + blockIdx.x;
+    const double v = ordered_sum_block<OSUM_NT, OSUM_EPT>([&](int64_t e) { return x[2 * e]; }, NI, sh);
     if (threadIdx.x == 0) {
-        out[0] = sr;
-        out[1] = sd;
-        out[2] = (double)NI;
+        out[blockIdx.x] = v;
+        if (blockIdx.x == 0) out[2] = (double)NI;
     }
 }
 
@@ -79,7 +77,7 @@ static int compute_rot_div(fdm_handle *h, double *rot, double *div, double *out3
     FDM_CK(h, h->cub_tmp.ensure(bytes));
     FDM_CK(h, cub::DeviceRadixSort::SortPairs(h->cub_tmp.p, bytes, k0, k1, i0, i1, (int)NI, 0, kb, h->s));
     k_ordered_squares<<<nblk(NI, 256), 256, 0, h->s>>>(NI, i1, rot, div, sq);
-    k_ordered_sums<<<1, OSUM_NT, 0, h->s>>>(NI, sq, out3);
+    k_ordered_sums<<<2, OSUM_NT, 0, h->s>>>(NI, sq, out3);
     return FDM_OK;
 }
 
@@ -1902,7 +1900,7 @@ extern "C" int fdm_debug_ordered_sum(const double *a, const double *b, int64_t n
     if (e == cudaSuccess && n > 0) e = cudaMemcpy(db, b, n * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
         if (n > 0) k_interleave2<<<nblk(n, 256), 256>>>(n, da, db, dq);
-        k_ordered_sums<<<1, OSUM_NT>>>(n, dq, dout);
+        k_ordered_sums<<<2, OSUM_NT>>>(n, dq, dout);
         e = cudaGetLastError();
     }
     double out[3] = {0.0, 0.0, 0.0};

@@ -5,10 +5,11 @@
 // strength 5 at (5, 5) and forms L1, L2, Loo over all of them and P1, P2,
 // Poo over the refined ones (lvl /= 0), by sequential sums.  Here one kernel
 // forms the per-leaf terms in parallel, with the reference's operation
-// order, and one warp streams them through shared memory to a single adding
-// lane, so the sums are the reference's left-to-right sums.  Only the norms
-// (a few doubles) come back to the host.
+// order, and the sums are formed in key order by the exact block-parallel
+// summation of ordered_sum.cuh, so they are the reference's left-to-right
+// sums.  Only the norms (a few doubles) come back to the host.
 #include "handle.cuh"
+#include "ordered_sum.cuh"
 
 namespace fdm {
 
@@ -31,70 +32,64 @@ __global__ void k_error_terms(Tables T, LevelTab LT, const double4 *__restrict__
     terms[i] = make_double4(lvl != 0 ? -area : area, fabs(r) * dx * dy, r * r * dx * dy, fabs(r));
 }
 
-constexpr int DIAG_CHUNK = 512;   // double4 per chunk: 16 KB
-__device__ __forceinline__ void cp16_diag(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-
-// sequential sums in key order; out: uni, l1, l2, loo, patch, p1, p2, poo,
-// z, z1, z2, zoo, n_patch, n_0
-__global__ void __launch_bounds__(32) k_error_sums(int64_t n, const double4 *__restrict__ terms, double *out) {
-    __shared__ double4 buf[2][DIAG_CHUNK];
-    const int lane = threadIdx.x;
-    const int64_t nch = (n + DIAG_CHUNK - 1) / DIAG_CHUNK;
-    auto fetch = [&](int64_t c) {
-        const int64_t base = c * DIAG_CHUNK;
-        for (int j = lane; j < 2 * DIAG_CHUNK; j += 32) {
-            const int64_t e = base + (j >> 1);
-            if (e < n) cp16_diag(reinterpret_cast<char *>(&buf[c & 1][j >> 1]) + 16 * (j & 1),
-                                 reinterpret_cast<const char *>(terms + e) + 16 * (j & 1));
-        }
-        asm volatile("cp.async.commit_group;\n" ::);
-    };
-    double uni = 0.0, l1 = 0.0, l2 = 0.0, loo = 0.0, patch = 0.0, p1 = 0.0, p2 = 0.0, poo = 0.0;
-    double z = 0.0, z1 = 0.0, z2 = 0.0, zoo = 0.0;
-    long long np = 0, n0 = 0;
-    if (nch > 0) fetch(0);
-    for (int64_t c = 0; c < nch; ++c) {
-        if (c + 1 < nch) {
-            fetch(c + 1);
-            asm volatile("cp.async.wait_group 1;\n" ::);
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            const int64_t rest = n - c * DIAG_CHUNK;
-            const int m = rest < DIAG_CHUNK ? (int)rest : DIAG_CHUNK;
-            const double4 *b = buf[c & 1];
-            for (int j = 0; j < m; ++j) {
-                const double4 t = b[j];
-                const double a = fabs(t.x);
-                uni = uni + a;
-                l1 = l1 + t.y;
-                l2 = l2 + t.z;
-                loo = fmax(loo, t.w);
-                if (t.x < 0.0) {
-                    ++np;
-                    patch = patch + a;
-                    p1 = p1 + t.y;
-                    p2 = p2 + t.z;
-                    poo = fmax(poo, t.w);
-                } else {
-                    ++n0;
-                    z = z + a;
-                    z1 = z1 + t.y;
-                    z2 = z2 + t.z;
-                    zoo = fmax(zoo, t.w);
-                }
-            }
-        }
-        __syncwarp();
+// The sums in key order, each by one block (ordered_sum.cuh), so each is
+// the reference's left-to-right sum bit for bit; a sum over the refined
+// (or level-0) leaves alone takes +0 for the others.  Block q < 9 forms sum
+// q of uni, l1, l2, patch, p1, p2, z, z1, z2; block 9 the maxima (fmax
+// ignores order) and the counts.  out: uni, l1, l2, loo, patch, p1, p2,
+// poo, z, z1, z2, zoo, n_patch, n_0.
+__global__ void __launch_bounds__(OSUM_NT) k_error_sums(int64_t n, const double4 *__restrict__ terms, double *out) {
+    __shared__ OSumShared sh;
+    __shared__ double red[3][OSUM_NT / 32];
+    __shared__ unsigned long long cnt[2];
+    const int q = blockIdx.x;
+    if (q < 9) {
+        const int comp = q % 3;      // area, |r| dx dy, r^2 dx dy
+        const int subset = q / 3;    // all, refined, level 0
+        const double v = ordered_sum_block<OSUM_NT, OSUM_EPT>(
+            [&](int64_t e) {
+                const double4 t = terms[e];
+                const bool in = subset == 0 || (subset == 1 ? t.x < 0.0 : !(t.x < 0.0));
+                const double x = comp == 0 ? fabs(t.x) : (comp == 1 ? t.y : t.z);
+                return in ? x : 0.0;
+            },
+            n, sh);
+        const int pos[9] = {0, 1, 2, 4, 5, 6, 8, 9, 10};
+        if (threadIdx.x == 0) out[pos[q]] = v;
+        return;
     }
+    double loo = 0.0, poo = 0.0, zoo = 0.0;
+    unsigned long long np = 0, n0 = 0;
+    for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+        const double4 t = terms[e];
+        loo = fmax(loo, t.w);
+        if (t.x < 0.0) { ++np; poo = fmax(poo, t.w); }
+        else { ++n0; zoo = fmax(zoo, t.w); }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        loo = fmax(loo, __shfl_xor_sync(0xffffffffu, loo, d));
+        poo = fmax(poo, __shfl_xor_sync(0xffffffffu, poo, d));
+        zoo = fmax(zoo, __shfl_xor_sync(0xffffffffu, zoo, d));
+        np += __shfl_xor_sync(0xffffffffu, np, d);
+        n0 += __shfl_xor_sync(0xffffffffu, n0, d);
+    }
+    if (threadIdx.x == 0) { cnt[0] = 0; cnt[1] = 0; }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
-        const double v[14] = {uni, l1, l2, loo, patch, p1, p2, poo, z, z1, z2, zoo, (double)np, (double)n0};
-        for (int k = 0; k < 14; ++k) out[k] = v[k];
+        red[0][warp] = loo; red[1][warp] = poo; red[2][warp] = zoo;
+        atomicAdd(&cnt[0], np);
+        atomicAdd(&cnt[1], n0);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            loo = fmax(loo, red[0][w]); poo = fmax(poo, red[1][w]); zoo = fmax(zoo, red[2][w]);
+        }
+        loo = fmax(loo, red[0][0]); poo = fmax(poo, red[1][0]); zoo = fmax(zoo, red[2][0]);
+        out[3] = loo; out[7] = poo; out[11] = zoo;
+        out[12] = (double)cnt[0];
+        out[13] = (double)cnt[1];
     }
 }
 
@@ -115,7 +110,7 @@ extern "C" int fdm_output_error(fdm_handle *h, double *norms, int64_t *counts) {
     double4 *terms = d.as<double4>();
     double *sums = reinterpret_cast<double *>(terms + h->NI);
     k_error_terms<<<nblk_d(h->NI, 256), 256, 0, h->s>>>(h->tables(), h->lt, h->B[0].as<double4>(), h->G.gama, terms);
-    k_error_sums<<<1, 32, 0, h->s>>>(h->NI, terms, sums);
+    k_error_sums<<<10, OSUM_NT, 0, h->s>>>(h->NI, terms, sums);
     double s[14];
     FDM_CK(h, cudaMemcpyAsync(s, sums, sizeof s, cudaMemcpyDeviceToHost, h->s));
     FDM_CK(h, cudaStreamSynchronize(h->s));

@@ -84,11 +84,12 @@ __device__ __forceinline__ unsigned long long osum_block_min(unsigned long long 
     return r;
 }
 
-// (...((0 + x[0]) + x[1]) + ...) + x[n-1], x[i] at x[i * stride], by one
-// block of NT threads, EPT consecutive elements per thread and run; every
-// thread returns the sum.
-template <int NT, int EPT>
-__device__ double ordered_sum_block(const double *__restrict__ x, int64_t stride, int64_t n, OSumShared &sh) {
+// (...((0 + x(0)) + x(1)) + ...) + x(n-1), x(i) = get(i), by one block of NT
+// threads, EPT consecutive elements per thread and run; every thread returns
+// the sum.  A subsequence is summed in order by giving +0 for the elements
+// left out (s + 0 = s for every s the sum can hold).
+template <int NT, int EPT, class Get>
+__device__ double ordered_sum_block(const Get &get, int64_t n, OSumShared &sh) {
     const long long TOP = 1ll << 53;
     const int t = threadIdx.x;
     double s = 0.0;
@@ -98,7 +99,7 @@ __device__ double ordered_sum_block(const double *__restrict__ x, int64_t stride
         const int64_t e0 = start + (int64_t)t * EPT;
         double xv[EPT];
 #pragma unroll
-        for (int j = 0; j < EPT; ++j) xv[j] = e0 + j < end ? x[(e0 + j) * stride] : 0.0;
+        for (int j = 0; j < EPT; ++j) xv[j] = e0 + j < end ? get(e0 + j) : 0.0;
         const unsigned hi = (unsigned)__double2hiint(s);
         const int fld = (int)((hi >> 20) & 0x7ffu);
         if (s == 0.0) {
@@ -111,13 +112,13 @@ __device__ double ordered_sum_block(const double *__restrict__ x, int64_t stride
             if (f == ~0ull) {
                 start = end;
             } else {
-                s = s + x[(int64_t)f * stride];
+                s = s + get((int64_t)f);
                 start = (int64_t)f + 1;
             }
             continue;
         }
         if (fld < 53 || fld == 0x7ff || (hi >> 31)) {   // tiny, not finite or negative: one at a time
-            s = s + x[start * stride];
+            s = s + get(start);
             ++start;
             continue;
         }
@@ -168,7 +169,7 @@ __device__ double ordered_sum_block(const double *__restrict__ x, int64_t stride
         s = (double)(M + R) * u;   // exact: an integer below 2^53 times a power of two
         start = A;
         if (A < end) {
-            s = s + x[A * stride];
+            s = s + get(A);
             start = A + 1;
         }
     }
