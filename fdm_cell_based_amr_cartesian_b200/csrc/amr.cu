@@ -323,7 +323,8 @@ static void swap_sets(fdm_handle *h, AmrCtx &X) {
 static int grow_nodes(fdm_handle *h, AmrCtx &X, int64_t n) {
     if (n <= X.cap) return FDM_OK;
     FDM_CK(h, cudaStreamSynchronize(h->s));
-    const int64_t c = n + n / 2 + 1024;
+    int64_t c = n + n / 2 + 1024;
+    if (c < 2 * X.cap) c = 2 * X.cap;   // geometric growth while a run refines from its background mesh
     for (int s = 0; s < 2; ++s) {
         FDM_CK(h, h->amr[3 * s + 0].ensure(c * 8));
         FDM_CK(h, h->amr[3 * s + 1].ensure(c));

@@ -40,16 +40,20 @@ struct DevBuf {
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
-    // At least nbytes; a buffer that has to grow takes 25 % + 1 MiB more, so
-    // that a mesh growing by a few cells per regrid does not reallocate (a
-    // cudaFree synchronises the device) at every regrid.
+    // At least nbytes; a buffer that has to grow takes 25 % + 1 MiB more, and
+    // at least twice what it had, so that a mesh growing by a few cells per
+    // regrid does not reallocate (a cudaFree synchronises the device) at
+    // every regrid, and one growing several-fold (the first regrids of a run
+    // from its background mesh) reallocates a few times, not a dozen.
     cudaError_t ensure(size_t nbytes) {
         if (nbytes <= bytes && p) return cudaSuccess;
+        const size_t had = p ? bytes : 0;
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
         size_t nb = nbytes ? nbytes : 16;
         if (nbytes > 0) nb += nbytes / 4 + (1u << 20);
+        if (nb < 2 * had) nb = 2 * had;
         if (alloc_refused()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, nb);
         if (e != cudaSuccess && nb > nbytes) {   // no room for headroom
