@@ -1829,8 +1829,7 @@ static int run_amr_impl(fdm_handle *h, fdm_handle *lead) {
     k_split_emit<<<nblk(n, TB), TB, 0, h->s>>>(X.A, ol, oi, lk.as<uint64_t>(), lv.as<double4>(),
                                                h->ikey.as<uint64_t>(), h->ival.as<double4>());
     FDM_CK(h, cudaEventRecord(h->amr_ev[4], h->s));
-    FDM_CK(h, cudaStreamSynchronize(h->s));
-    h->NInt = nint;
+    h->NInt = nint;   // the rebuild is ordered after the split on the stream
     const int rc = build_tables(h, nleaf, lk.as<uint64_t>(), lv.as<double>(), 0);   // split keeps key order
     if (rc) return rc;
     FDM_CK(h, cudaEventRecord(h->amr_ev[5], h->s));

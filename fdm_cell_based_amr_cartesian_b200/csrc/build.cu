@@ -667,8 +667,11 @@ __global__ void k_lmax(int64_t NI, const uint8_t *ilvl, int32_t *out) {
 
 // Every index a stage kernel will dereference is checked once here, so that
 // no stage kernel can read or write outside its buffers.
-__global__ void k_validate(Tables T, int32_t *err) {
+// face_counts: the unshared left faces (nux, nuy) as the device counted them
+__global__ void k_validate(Tables T, const int64_t *__restrict__ face_counts, int32_t *err) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    T.nux = face_counts[0];
+    T.nuy = face_counts[1];
     const int64_t NLEAF = T.NI + T.NG + T.NC;
     bool bad = false;
     if (t < T.NI * 8) {
@@ -921,21 +924,15 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     }
     FDM_RC(scan_i32(h, ux, sx, NI));
     FDM_RC(scan_i32(h, uy, sy, NI));
-    int64_t nux, nuy;
-    {
-        k_scan_total<<<1, 32, 0, s>>>(ux, sx, NI, dtot);
-        k_scan_total<<<1, 32, 0, s>>>(uy, sy, NI, dtot + 1);
-        int32_t he[8];
-        int64_t tot[2];
-        FDM_RC(read_back(h, he, tot, 2));
-        nux = tot[0];
-        nuy = tot[1];
-    }
-    h->nux = nux; h->nuy = nuy;
+    // the face counts come back with the final checks; until then the
+    // buffers take their bound (at most one unshared left face per leaf)
+    k_scan_total<<<1, 32, 0, s>>>(ux, sx, NI, dtot + 4);
+    k_scan_total<<<1, 32, 0, s>>>(uy, sy, NI, dtot + 5);
+    const int64_t nux_max = NI, nuy_max = NI;
     FDM_CK(h, h->ifxl.ensure(NI * 4));
     FDM_CK(h, h->ifyl.ensure(NI * 4));
-    FDM_CK(h, h->uxl.ensure((nux > 0 ? nux : 1) * 4));
-    FDM_CK(h, h->uyl.ensure((nuy > 0 ? nuy : 1) * 4));
+    FDM_CK(h, h->uxl.ensure(nux_max * 4));
+    FDM_CK(h, h->uyl.ensure(nuy_max * 4));
     {
         Tables T = h->tables();
         k_face_assign<<<nblk(NI, TB), TB, 0, s>>>(T, ux, uy, sx, sy, h->ifxl.as<int32_t>(), h->ifyl.as<int32_t>(),
@@ -944,8 +941,8 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     // 8. state buffers (corner values copied into all three)
     const int64_t NS = h->NS;
     for (int b = 0; b < 3; ++b) FDM_CK(h, h->B[b].ensure(NS * 32));
-    FDM_CK(h, h->Fx.ensure((NI + nux) * 32));
-    FDM_CK(h, h->Fy.ensure((NI + nuy) * 32));
+    FDM_CK(h, h->Fx.ensure((NI + nux_max) * 32));
+    FDM_CK(h, h->Fy.ensure((NI + nuy_max) * 32));
     FDM_CK(h, h->Ut.ensure(NI * 32));
     k_scatter<<<nblk(n, TB), TB, 0, s>>>(n, perm, h->lslot.as<int32_t>(), prim_in, h->B[0].as<double4>());
     if (NC > 0)
@@ -956,9 +953,9 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     {
         Tables T = h->tables();
         int64_t nv = NI * 8;
-        const int64_t others[5] = {nux, nuy, NR, NG, NI};
+        const int64_t others[5] = {nux_max, nuy_max, NR, NG, NI};
         for (int q = 0; q < 5; ++q) nv = nv > others[q] ? nv : others[q];
-        k_validate<<<nblk(nv, TB), TB, 0, s>>>(T, err);
+        k_validate<<<nblk(nv, TB), TB, 0, s>>>(T, dtot + 4, err);
     }
     // 10. l_max
     int32_t *dl = err + 7;
@@ -969,8 +966,12 @@ int build_tables(fdm_handle *h, int64_t n, const uint64_t *keys_in, const double
     unsigned long long hc[7];
     FDM_CK(h, cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, s));
     FDM_CK(h, cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    int64_t fc[2] = {0, 0};
+    FDM_CK(h, cudaMemcpyAsync(fc, dtot + 4, sizeof(fc), cudaMemcpyDeviceToHost, s));
     FDM_CK(h, cudaStreamSynchronize(s));
     FDM_CK(h, cudaGetLastError());
+    h->nux = fc[0];
+    h->nuy = fc[1];
     if (hc[2] != hc[6]) return arg_fail(h, "internal table check failed: restrict list");
     if (he[BE_OVERFLOW]) return arg_fail(h, "hanging-node stencil larger than supported");
     if (he[BE_INDEX]) return arg_fail(h, "internal table check failed: an index is out of range");
