@@ -1321,6 +1321,10 @@ __global__ void __launch_bounds__(GM4_THREADS) k_gm4_block(Pool P, Geometry G, c
     bool take = false;     // warp 0: this lane's merged entry is an item ...
     int pos = 0;           // ... at this place
     for (;; ++step) {
+        // warp 0 reaches here from lane-level branches of the refinement;
+        // reconverge it before the lane-parallel merge, or its lanes can run
+        // the merge in separate groups
+        __syncwarp();
         if (warp == 0) {
             int c = 0;
             if (step >= max_steps) {
