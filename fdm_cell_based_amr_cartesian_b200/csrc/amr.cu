@@ -584,8 +584,13 @@ __device__ __forceinline__ bool gm1_has_son(const Links &L, const int8_t *d, int
 }
 // gridmodify1 decision of one node (src/mesh.F90:305-353) given the current
 // estimate of all decisions; a decision only reads decisions of nodes that
-// are visited earlier, so iterating to a fixpoint gives the sequential result
-__global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, int32_t *changed, int32_t *any) {
+// are visited earlier, so iterating to a fixpoint gives the sequential result.
+// The estimate is updated in place: a decision may read others already
+// updated in the same sweep (never older than the last sweep's), which only
+// shortens the chains; a sweep that changes nothing wrote nothing, so every
+// decision in it read final values and the fixpoint (unique: the
+// dependencies follow the visit order) is reached.
+__global__ void k_gm1_decide(int64_t n, Links L, int8_t *d, int32_t *changed, int32_t *any) {
     const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (x >= n) return;
     int8_t r = D_NONE;
@@ -607,8 +612,10 @@ __global__ void k_gm1_decide(int64_t n, Links L, const int8_t *d, int8_t *dn, in
             if (all_leaf && ((!left && !right) || (!up && !down))) r = D_COARSEN;
         }
     }
-    dn[x] = r;
-    if (r != d[x]) atomicExch(changed, 1);
+    if (r != d[x]) {
+        d[x] = r;
+        atomicExch(changed, 1);
+    }
     if (any && r != D_NONE) atomicExch(any, 1);
 }
 // values of coarsened nodes, deepest level first (interpA of the sons as they
@@ -1539,14 +1546,14 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
     Links L;
     L.parent = cv.at<int32_t>(b, 0); L.child = cv.at<int32_t>(b, 1); L.nb = cv.at<int32_t>(b, 2);
     L.rank = cv.at<uint64_t>(b, 3); L.leaf0 = cv.at<uint8_t>(b, 4); L.cross = cv.at<int8_t>(b, 5);
-    int8_t *d0 = cv.at<int8_t>(b, 6), *d1 = cv.at<int8_t>(b, 7);
+    int8_t *d0 = cv.at<int8_t>(b, 6);   // the decisions (slot 7 unused)
     int32_t *changed = cv.at<int32_t>(b, 8);
     int32_t *cnt = cv.at<int32_t>(b, 9), *off = cv.at<int32_t>(b, 10);
     AMR_RC(index_set(h, X.A));
     FDM_CK(h, cudaMemsetAsync(changed, 0, 16, h->s));
     k_gm1_links<<<nblk(n, TB), TB, 0, h->s>>>(X.A, h->G, L, changed + 2);
     FDM_CK(h, cudaMemsetAsync(d0, 0, n, h->s));
-    int8_t *cur = d0, *nxt = d1;
+    int8_t *cur = d0;
     // Sweeps are enqueued GM1_SWEEPS at a time and the change flag of the
     // last one is read: once the decisions are settled a sweep changes
     // nothing, so the extra sweeps leave the fixpoint as it is.
@@ -1559,8 +1566,7 @@ static int gridmodify1_pass(fdm_handle *h, AmrCtx &X, bool *did) {
         for (int k = 0; k < GM1_SWEEPS; ++k) {
             const bool last = k == GM1_SWEEPS - 1;
             if (last) FDM_CK(h, cudaMemsetAsync(changed, 0, 8, h->s));   // the level stays
-            k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, nxt, changed, last ? changed + 1 : nullptr);
-            std::swap(cur, nxt);
+            k_gm1_decide<<<nblk(n, TB), TB, 0, h->s>>>(n, L, cur, changed, last ? changed + 1 : nullptr);
         }
         it += GM1_SWEEPS;
         FDM_CK(h, cudaMemcpyAsync(hc, changed, 12, cudaMemcpyDeviceToHost, h->s));
