@@ -157,7 +157,8 @@ struct fdm_handle {
     // CUDA graph of one RK3 step (captured lazily, dropped at regrid)
     cudaGraphExec_t step_graph = nullptr;     // one solute iteration
     cudaGraphExec_t step_graph_g = nullptr;   // the same followed by the j = 1 ghost refresh
-    int64_t graph_version = -1;
+    int64_t graph_version = -1;               // table_version the slots were last checked against
+    bool graph_stale[2] = {true, true};       // step_graph / step_graph_g need a re-capture
     int64_t table_version = 0;
 
     fdm::Tables tables() const {

@@ -195,11 +195,17 @@ static void drop_graph(fdm_handle *h) {
 // CUDA graph of one solute iteration (ghosts: followed by the j = 1 ghost
 // refresh that solute does after an iteration without regrid); both are
 // re-captured after every rebuild of the tables (upload / regrid), replayed
-// otherwise.
+// otherwise.  A re-captured graph of the same shape (the usual case after a
+// regrid: the same kernels with new sizes and table pointers) updates the
+// executable graph in place, which costs far less than instantiating it.
 static int step_graph(fdm_handle *h, cudaGraphExec_t *out, bool ghosts = false) {
-    if (h->graph_version != h->table_version) drop_graph(h);
+    if (h->graph_version != h->table_version) {
+        h->graph_stale[0] = h->graph_stale[1] = true;
+        h->graph_version = h->table_version;
+    }
     cudaGraphExec_t &slot = ghosts ? h->step_graph_g : h->step_graph;
-    if (slot) {
+    bool &stale = h->graph_stale[ghosts ? 1 : 0];
+    if (slot && !stale) {
         *out = slot;
         return FDM_OK;
     }
@@ -209,13 +215,25 @@ static int step_graph(fdm_handle *h, cudaGraphExec_t *out, bool ghosts = false) 
     if (ghosts) launch_ghosts(h, h->B[0].as<double4>(), 1);
     cudaError_t e = cudaStreamEndCapture(h->s, &g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    if (slot) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(slot, g, &info) == cudaSuccess) {
+            cudaGraphDestroy(g);
+            stale = false;
+            *out = slot;
+            return FDM_OK;
+        }
+        cudaGetLastError();   // another shape: instantiate it
+        cudaGraphExecDestroy(slot);
+        slot = nullptr;
+    }
     e = cudaGraphInstantiate(&slot, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         slot = nullptr;
         return cuda_fail(h, e, "cudaGraphInstantiate");
     }
-    h->graph_version = h->table_version;
+    stale = false;
     *out = slot;
     return FDM_OK;
 }
