@@ -526,6 +526,7 @@ struct fdm_batch {
     size_t smem = 0;
     bool any_gate = false;
     cudaGraphExec_t graph = nullptr;
+    bool graph_stale = false;   // the members changed: re-capture, update the graph in place
     bool use_graph = true;           // off when cooperative launches cannot be captured here
     std::vector<int64_t> versions;   // member table versions the descriptors were built for
     std::vector<bool> gates;
@@ -610,7 +611,7 @@ static int batch_refresh(fdm_batch *b) {
         b->thr[m] = b->mem[m]->gate_logit_thr;
         b->jthr[m] = b->mem[m]->gate_jump_thr;
     }
-    drop_batch_graph(b);
+    b->graph_stale = true;
     return FDM_OK;
 }
 
@@ -720,27 +721,37 @@ static int enqueue_batch_stage(fdm_batch *b, int krk) {
 }
 
 // CUDA graph of one step of every member (three cooperative launches);
-// captured again whenever a member's tables or gate change.  Where the
-// capture of a cooperative launch is refused, the three launches are issued
-// directly instead.
+// captured again whenever a member's tables or gate change, and then
+// updated in place when it keeps its shape (instantiated otherwise).  Where
+// the capture of a cooperative launch is refused, the three launches are
+// issued directly instead.
 static int batch_graph(fdm_batch *b) {
     if (batch_stale(b)) {
         int rc = batch_refresh(b);
         if (rc) return rc;
     }
-    if (b->graph || !b->use_graph) return FDM_OK;
+    if (!b->use_graph || (b->graph && !b->graph_stale)) return FDM_OK;
     cudaGraph_t g = nullptr;
     BCK(b, cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
     int rc = FDM_OK;
     for (int krk = 1; krk <= 3 && !rc; ++krk) rc = enqueue_batch_stage(b, krk);
     cudaError_t e = cudaStreamEndCapture(b->s, &g);
-    if (!rc && e == cudaSuccess) {
+    if (!rc && e == cudaSuccess && b->graph) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(b->graph, g, &info) != cudaSuccess) {
+            cudaGetLastError();   // another shape: instantiate it
+            drop_batch_graph(b);
+        }
+    }
+    if (!rc && e == cudaSuccess && !b->graph) {
         e = cudaGraphInstantiate(&b->graph, g, 0);
         if (e != cudaSuccess) b->graph = nullptr;
     }
     if (g) cudaGraphDestroy(g);
+    b->graph_stale = false;
     if (rc || e != cudaSuccess || !b->graph) {
         cudaGetLastError();
+        drop_batch_graph(b);
         b->use_graph = false;
         b->err.clear();
     }
